@@ -1,0 +1,361 @@
+"""Throughput of the TorChannel IMEX time step on B200.
+
+Workload (one "step" = one IMEX time step of the channel):
+  192 x 192 x 128 staggered grid, Lx = 4 pi, Ly = 4 pi / 3, Lz = 2, tanh
+  stretching gamma = 2.6, Re_bulk = 2870, U_bulk = 1; seeded laminar profile
+  + 0.1 uniform noise, rescaled and projected divergence-free, then 10 IMEX
+  warm-up steps to give a developed AB2 history; dt from the CFL rule
+  (CFL 0.25, clamp [3e-4, 1.1e-2]) held fixed during the timed region.
+Metric: grid-point-steps/s = nx*ny*nz*steps / seconds (whole job, all ranks).
+
+Arms:
+  default           this repo's CUDA path (precision: --precision, default mixed)
+  --impl reference  the CPU oracle (numpy FP64 restatement of the reference
+                    step, oracle/) on the host cores, bounded sample
+
+Multi-GPU: one process per GPU, each advancing its own independent channel
+(ensemble replicas, no collective on the hot path); value = sum over ranks of
+grid-point-steps / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 192, 192, 128
+LX, LY, LZ = 4 * np.pi, 4 * np.pi / 3, 2.0
+RE, GAMMA = 2870.0, 2.6
+CFL, DT_MIN, DT_MAX = 0.25, 3e-4, 0.011
+METRIC = "grid-point-steps/s at 192x192x128 IMEX step"
+WORKLOAD = "IMEX channel step 192x192x128 (Re_bulk 2870, gamma 2.6, seeded laminar+0.1 noise)"
+# algorithmic traffic of one IMEX step: 24 stored words per grid point
+# (pass 1: 13, Poisson: 4, projection: 7)
+WORDS_PER_POINT = 24
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def initial_state(seed=0):
+    """Seeded laminar + noise field (initflow.py:4-104 semantics) on the host."""
+    from torchannel_b200.grid import generate_grid
+    from torchannel_b200.init import initialize_flow
+    z_f, z_c, dz_f, dz_c = generate_grid(GAMMA, NZ, LZ)
+    u, v, w, p = initialize_flow(NX, NY, NZ, z_c, LY, LZ, U_bulk=1.0, init_type="parabolic",
+                                 perturbation_intensity=0.1, seed=seed)
+    return (z_f, z_c, dz_f, dz_c), (u, v, w)
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = float(f[2])
+            except ValueError:
+                continue
+            for n, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_profile_traffic(precision):
+    """DRAM bytes per step from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", f"step_traffic_192x192x128_{precision}.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CUDA arm
+# ---------------------------------------------------------------------------
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    from torchannel_b200.core import Channel
+    from torchannel_b200 import _lib as L
+    grid, (u0, v0, w0) = initial_state(seed=rank)
+    z_f, z_c, dz_f, dz_c = grid
+    ch = Channel(NX, NY, NZ, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision=a.precision)
+    ch.set_state(u0, v0, w0)
+    ub = ch.bulk_velocity()
+    ch.set_state(u0 * (1.0 / ub), v0, w0)
+    ch.project_initial()
+    dt = min(max(CFL * (1.0 / ch.cfl_inverse()), DT_MIN), DT_MAX)
+    ch.step("IMEX", dt, 10)
+    for _ in range(a.warmup):
+        ch.step("IMEX", dt)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ch.step("IMEX", dt, a.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    # per-phase timing (separate, instrumented pass of the same steps)
+    ch.timing(True)
+    ch.step("IMEX", dt, min(a.steps, L_RING))
+    phases, nst = ch.timing_read()
+    ch.timing(False)
+    diag = ch.diagnostics()
+    # end-to-end through the public API with host buffers
+    e2e = None if a.no_e2e else run_e2e(a, grid, (u0, v0, w0), dt)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    npts = NX * NY * NZ
+    sec = ms / 1e3
+    value = npts * a.steps * world / sec
+    s = 8 if a.precision == "fp64" else 4
+    peak, peak_kind = measured_peaks()
+    step_bytes = WORDS_PER_POINT * s * npts
+    step_ms = ms / a.steps
+    kern = kernel_table(phases, nst, s, npts)
+    dom = max(kern, key=lambda k: k["ms"])
+    prof = load_profile_traffic(a.precision)
+    traffic_dom = None
+    if prof and dom["name"] in prof.get("per_kernel_bytes", {}):
+        traffic_dom = prof["per_kernel_bytes"][dom["name"]]
+    roof = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+            "frac": dom["gbs"] / peak, "traffic": traffic_dom, "kernel": dom["name"],
+            "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": dom["bytes"], "avg_launch_ms": dom["ms"]}
+    step_roof = {"bound": "hbm", "achieved": step_bytes / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                 "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak, "words_per_point": WORDS_PER_POINT,
+                 "bytes_per_step": step_bytes, "traffic": prof.get("bytes_per_step") if prof else None}
+    cpu = None if a.no_cpu_baseline else cpu_baseline(a.cpu_seconds)
+    line = {
+        "metric": METRIC, "value": value, "unit": "grid-point-steps/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded laminar profile + 0.1 uniform noise, projected)",
+        "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "scheme": "IMEX",
+                   "precision": a.precision, "dt": dt, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (state + history > 126 MB)"},
+        "roofline": roof, "step_roofline": step_roof, "kernels": kern,
+        "cpu_baseline": cpu, "e2e": e2e,
+        "clocks": clk.summary(),
+        "gpu_launches": LAUNCHES_PER_STEP * a.steps,
+        "max_div_after": diag["max_div"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+L_RING = 64
+# kernels per IMEX step: rhs, cn, fftx, ffty, tri, iffty, ifftx, project, finalize
+LAUNCHES_PER_STEP = 9
+
+
+def kernel_table(phases, nst, s, npts):
+    """Per-kernel average launch time and algorithmic bytes per launch.
+    Algorithmic words per grid point (stored precision s bytes; spectral words
+    counted as nx/2+1 complex per nx reals ~ 1 word):
+      rhs  : read u, v, w, r_prev; write u*, r           = 12
+      cn   : read u*, write u**                           = 6
+      fftx : read u**, v**, w** (div); write spectrum     = 4
+      ffty, tri, iffty : read + write spectrum            = 2 each (tri: + 2 FP64 scratch in mixed)
+      ifftx: read spectrum, write p                       = 2
+      proj : read u**, p; write u                         = 7
+    """
+    spec = (NX / 2 + 1) / (NX / 2)  # half spectrum overhead
+    words = {"rhs": 12, "cn": 6, "fftx": 3 + spec, "ffty": 2 * spec, "tri": 2 * spec,
+             "iffty": 2 * spec, "ifftx": spec + 1, "proj": 7, "fin": 0}
+    out = []
+    for k, w in words.items():
+        ms = phases.get(k, 0.0) / max(nst, 1)
+        b = w * s * npts
+        out.append({"name": k, "ms": ms, "bytes": b, "gbs": (b / (ms / 1e3) / 1e9) if ms > 0 else 0.0})
+    return out
+
+
+def run_e2e(a, grid, fields, dt):
+    """Same metric through the public ChannelFlow-compatible API with host
+    buffers: the initial state goes host->device from pinned memory, each
+    step's (u_bulk, forcing) comes back to the host, and the final u, v, w
+    come back at the end; all inside the timed region."""
+    import torch
+    from torchannel_b200.core import Channel
+    z_f, z_c, dz_f, dz_c = grid
+    u0, v0, w0 = fields
+    ch = Channel(NX, NY, NZ, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision=a.precision)
+    hu = torch.from_numpy(u0).pin_memory(); hv = torch.from_numpy(v0).pin_memory()
+    hw = torch.from_numpy(w0).pin_memory()
+    out = torch.empty(2, dtype=torch.float64).pin_memory()
+    du = torch.empty_like(hu, device="cuda"); dv = torch.empty_like(hv, device="cuda")
+    dw = torch.empty_like(hw, device="cuda")
+    # warm-up of the same path
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        du.copy_(hu, non_blocking=True); dv.copy_(hv, non_blocking=True); dw.copy_(hw, non_blocking=True)
+        ch.set_state(du, dv, dw)
+        n = a.steps if rep else 2
+        for _ in range(n):
+            ch.step("IMEX", dt)
+            out.copy_(ch.scalars[:2].flip(0), non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+        u, v, w, _ = ch.get_state()
+        hu2 = u.cpu(); hv2 = v.cpu(); hw2 = w.cpu()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+    sec = t1 - t0
+    bi = (hu.numel() + hv.numel() + hw.numel()) * 8
+    bo = (hu.numel() + hv.numel() + hw.numel()) * 8
+    return {"value": NX * NY * NZ * a.steps / sec, "unit": "grid-point-steps/s",
+            "h2d_bytes_per_step": bi / a.steps, "d2h_bytes_per_step": bo / a.steps + 16,
+            "note": "set_state from pinned host + K x step_imex with per-step (u_bulk, forcing) read-back + get_state to host"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm: the numpy oracle step
+# ---------------------------------------------------------------------------
+def cpu_step_setup(seed=0):
+    from oracle.step import OracleChannel
+    oc = OracleChannel(NX, NY, NZ, LX, LY, LZ, RE, gamma=GAMMA)
+    oc.init_fresh(seed=seed)
+    return oc
+
+
+def cpu_baseline(budget_s, steps=None):
+    oc = cpu_step_setup()
+    oc.step_imex(0.002)           # warm-up (Euler first step)
+    t_all, n = 0.0, 0
+    while (steps is None and (t_all < budget_s or n == 0)) or (steps is not None and n < steps):
+        t0 = time.perf_counter()
+        oc.step_imex(0.002)
+        t_all += time.perf_counter() - t0
+        n += 1
+    return {"value": NX * NY * NZ * n / t_all, "unit": "grid-point-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{n} full IMEX steps at {NX}x{NY}x{NZ} of the numpy FP64 oracle (single thread), "
+                      f"{t_all:.1f} s"}
+
+
+def run_reference(a):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    # bounded: a full 192^3 oracle step takes several seconds on one core
+    per_step_budget = 150.0
+    oc = cpu_step_setup()
+    for _ in range(min(a.warmup, 1)):
+        oc.step_imex(0.002)
+    t_all, n = 0.0, 0
+    while n < a.steps:
+        t0 = time.perf_counter()
+        oc.step_imex(0.002)
+        t_all += time.perf_counter() - t0
+        n += 1
+        if t_all > per_step_budget:
+            break
+    value = NX * NY * NZ * n / t_all
+    cpu = {"value": value, "unit": "grid-point-steps/s", "cores": 1, "kind": "port",
+           "sample": f"{n} of {a.steps} requested IMEX steps at {NX}x{NY}x{NZ} (numpy FP64 oracle, one thread), "
+                     f"{t_all:.1f} s"}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "grid-point-steps/s",
+            "n_gpus": world, "steps": n, "warmup": min(a.warmup, 1), "ms_per_step": 1e3 * t_all / n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded laminar profile + 0.1 uniform noise, projected)",
+            "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "scheme": "IMEX"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": "grid-point-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+/*
+ * torchannel_b200 -- C ABI of the B200-native TorChannel time step.
+ *
+ * The reference (gmcavallazzi/torChannel) is pure Python/PyTorch and has no
+ * FFI of its own; each entry point below replaces the Python function named
+ * beside it, and the Python package torchannel_b200 binds them with ctypes
+ * (torchannel_b200/_lib.py) behind a ChannelFlow-compatible class.
+ *
+ * Conventions
+ *  - Every entry returns an int status (TC_OK = 0); no C++ exception crosses
+ *    the ABI.  tc_last_error() gives a message for the last failure.
+ *  - Array arguments are DEVICE pointers to FP64 arrays in the reference
+ *    layout (C order (x, y, z), z fastest, ghosts included):
+ *      u (nx+1, ny+2, nz+2), v (nx+2, ny+1, nz+2), w (nx+2, ny+2, nz+1),
+ *      p (nx+2, ny+2, nz+2), cell fields such as div (nx, ny, nz).
+ *    Host pointers are marked "host".
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *    stream).  Entries are asynchronous unless they return a host value.
+ *  - The library never allocates device memory: the caller allocates one
+ *    workspace of tc_workspace_bytes() bytes and hands it to tc_create().
+ */
+#ifndef TORCHANNEL_B200_H
+#define TORCHANNEL_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TC_OK = 0,
+  TC_ERR_ARG = 1,         /* bad argument / null pointer */
+  TC_ERR_SIZE = 2,        /* unsupported grid size (FFT lengths need factors 2, 3 only) */
+  TC_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  TC_ERR_WORKSPACE = 4,   /* workspace too small or misaligned */
+  TC_ERR_STATE = 5,       /* call needs a state set with tc_set_state first */
+  TC_ERR_NONFINITE = 6    /* non-finite value found in the state */
+};
+
+enum { TC_FP64 = 0, TC_MIXED = 1 };             /* storage precision of the fields */
+enum { TC_TOP_NOSLIP = 0, TC_TOP_FREESLIP = 1 }; /* boundary_conditions.top_wall.type dirichlet / neumann */
+enum { TC_RHS_SEPARATE = 0, TC_RHS_FUSED = 1 };  /* which reference code path the explicit RHS follows */
+enum { TC_IMEX = 0, TC_AB2 = 1, TC_FE = 2 };     /* time.scheme */
+
+typedef struct tc_grid_desc {
+  int nx, ny, nz;          /* grid.nx, grid.ny, grid.nz */
+  double Lx, Ly, Lz;       /* domain.Lx, Ly, Lz */
+  double nu;               /* 1 / flow.Re */
+  double U_bulk;           /* flow.U_bulk (PI forcing target) */
+  int top_wall;            /* TC_TOP_* */
+  int precision;           /* TC_FP64 or TC_MIXED */
+  int rhs_path;            /* TC_RHS_* */
+  const double* dz_f;      /* host, nz      (utils.py:42) */
+  const double* dz_c;      /* host, nz + 1  (utils.py:43) */
+} tc_grid_desc;
+
+typedef struct tc_ctx tc_ctx;
+
+/* Library version string (host). */
+const char* tc_version(void);
+
+/* Message of the last failed call in this thread (host). */
+const char* tc_last_error(void);
+
+/* Bytes of device workspace needed for this grid (includes 256 B alignment
+ * slack).  Replaces the tensor allocations of ChannelFlow.__init__
+ * (solver.py:215-292, initflow.py:6-9, projection_fft.py:56-86). */
+int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes);
+
+/* Create a context on the current device over a caller-owned workspace.
+ * Synchronous (uploads grid tables).  Replaces initialize_fft_solver
+ * (projection_fft.py:3-99) and the grid set-up of solver.py:215-234. */
+int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, tc_ctx** out);
+
+int tc_destroy(tc_ctx* ctx);
+
+/* Load u, v, w (reference layout, device, FP64) and the bulk forcing; the
+ * AB2 history is cleared (next IMEX/AB2 step is an Euler step, as after
+ * ChannelFlow.__init__ / a restart, solver.py:377-383).  Ghost values are
+ * ignored: periodic and wall ghosts are implied by the DOFs. */
+int tc_set_state(tc_ctx* ctx, const double* u, const double* v, const double* w, double forcing, void* stream);
+
+/* Write u, v, w, p in the reference layout with ghosts filled as
+ * apply_bc_all (solver.py:23-79) and the pressure ghost fill
+ * (projection_fft.py:148-163) leave them.  Any pointer may be NULL. */
+int tc_get_state(tc_ctx* ctx, double* u, double* v, double* w, double* p, void* stream);
+
+/* AB2 history r_prev (the rhs_*_prev buffers of solver.py:377-383,649-651),
+ * DOFs in the u/v/w reference layouts (ghost entries written as 0).
+ * tc_get_history returns TC_ERR_STATE when there is no history yet. */
+int tc_get_history(tc_ctx* ctx, double* ru, double* rv, double* rw, void* stream);
+int tc_set_history(tc_ctx* ctx, const double* ru, const double* rv, const double* rw, void* stream);
+
+/* Advance n_steps steps of `scheme` with time step dt.
+ *   TC_IMEX: ChannelFlow.step_imex (solver.py:580-710)
+ *   TC_AB2 : step_imex with the full-diffusion RHS of
+ *            compute_momentum_rhs_explicit (solver.py:498-534) and no
+ *            implicit solve (docs/NUMERICAL_METHODS.md:260-284)
+ *   TC_FE  : step_forward_euler (solver.py:537-576; forcing fixed at 1.0)
+ * Asynchronous; u_bulk and forcing stay on the device (tc_scalars). */
+int tc_step(tc_ctx* ctx, int scheme, double dt, int n_steps, void* stream);
+
+/* Initial projection of a fresh field: div -> Poisson -> u -= grad p
+ * (dt = 1) (solver.py:345-370). */
+int tc_project_initial(tc_ctx* ctx, void* stream);
+
+/* Device pointer to the FP64 scalar block: [0] forcing, [1] u_bulk of the
+ * last step, [2] CFL 1/dt scale, [3] max|div|, [4] u-plane mean at the
+ * bottom, [5] at the top, [6] non-finite flag. */
+int tc_scalars(tc_ctx* ctx, double** dev_ptr);
+
+/* Set the bulk forcing scalar (solver.py:249,252). */
+int tc_set_forcing(tc_ctx* ctx, double forcing, void* stream);
+
+/* Bulk velocity of the current state (utils.py:207-223) -> host. Syncs. */
+int tc_bulk_velocity(tc_ctx* ctx, double* out_host, void* stream);
+
+/* max over cells of the CFL sums (compute_cfl_fused, operators.py:1232-1333)
+ * -> host.  Syncs. */
+int tc_cfl(tc_ctx* ctx, double* dti_host, void* stream);
+
+/* Diagnostics -> host (syncs): out[0] max|div| (utils.py:226-240),
+ * out[1] u_tau (utils.py:176-204), out[2] u_bulk, out[3] forcing,
+ * out[4] 1 if u, v, w or p holds a NaN/Inf (solver.py:865-868). */
+int tc_diagnostics(tc_ctx* ctx, double* out_host, void* stream);
+
+/* Divergence of the current state, (nx, ny, nz) reference layout
+ * (compute_divergence, utils.py:226-240). */
+int tc_divergence(tc_ctx* ctx, double* div, void* stream);
+
+/* Operator hooks on the current state (used by the parity tests):
+ * explicit RHS without forcing (compute_momentum_rhs_fused_imex /
+ * separate ops, or the full-diffusion variants when full != 0), written to
+ * u/v/w-shaped reference arrays with zero ghosts. */
+int tc_explicit_rhs(tc_ctx* ctx, int full, double* ru, double* rv, double* rw, void* stream);
+
+/* CN implicit z-diffusion of the current state in place
+ * (solve_implicit_diffusion_u/v/w, operators.py:563-811). */
+int tc_implicit_diffusion(tc_ctx* ctx, double dt, void* stream);
+
+/* Standalone FFT Poisson solve: rhs (nx, ny, nz) reference layout, device
+ * FP64 -> p (nx+2, ny+2, nz+2) with ghosts (solve_poisson_fft,
+ * projection_fft.py:101-165; the (0,0) mode is gauged, so p is defined up to
+ * a constant).  Uses the context's workspace; the state is not touched. */
+int tc_poisson_solve(tc_ctx* ctx, const double* rhs, double* p, void* stream);
+
+/* Velocity correction with a given p (reference layout, device)
+ * (project_velocity, projection.py:143-165). */
+int tc_project(tc_ctx* ctx, const double* p, double dt, void* stream);
+
+/* Turbulence statistics (turbstats.py:20-228).  tc_stats_init picks the
+ * z+ planes (turbstats.py:52-69) from z_c (host, nz+2) and clears the FP64
+ * running sums; tc_stats_accumulate adds one sample of the current state;
+ * tc_stats_read copies the sums to host arrays: prof (5*nz: U, uu, vv, ww, uw)
+ * and spec (4*(nx/2)*(ny/2): E_uu, E_vv, E_ww, E_uw, each (nx/2, ny/2)
+ * C order) and the sample count; tc_stats_write loads sums back (restart,
+ * turbstats.py:364-402). */
+int tc_stats_init(tc_ctx* ctx, const double* z_c, double Re_tau_target, double z_plus_target,
+                  int* k_bot, int* k_top);
+int tc_stats_accumulate(tc_ctx* ctx, void* stream);
+int tc_stats_read(tc_ctx* ctx, double* prof_host, double* spec_host, int* n_samples);
+int tc_stats_write(tc_ctx* ctx, const double* prof_host, const double* spec_host, int n_samples);
+
+/* Per-phase timing of tc_step with CUDA events recorded between the
+ * kernels on the launching stream (off by default).  Phases:
+ * TC_PH_RHS (kernel a), TC_PH_CN (b), TC_PH_FFTX, TC_PH_FFTY, TC_PH_TRI,
+ * TC_PH_IFFTY, TC_PH_IFFTX (c), TC_PH_PROJ, TC_PH_FIN (d).
+ * tc_timing_read syncs and returns the summed milliseconds per phase over
+ * the recorded steps (the last TC_TIMING_RING steps at most) and the number
+ * of steps summed; it clears the record.  Has no reference counterpart (the
+ * reference prints wall time only, solver.py:800-805). */
+enum { TC_PH_RHS = 0, TC_PH_CN, TC_PH_FFTX, TC_PH_FFTY, TC_PH_TRI, TC_PH_IFFTY, TC_PH_IFFTX, TC_PH_PROJ,
+       TC_PH_FIN, TC_NPHASE };
+#define TC_TIMING_RING 64
+int tc_timing_enable(tc_ctx* ctx, int on);
+int tc_timing_read(tc_ctx* ctx, double* ms_host, int* n_steps);
+
+/* Read and clear the device error word (syncs). */
+int tc_error(tc_ctx* ctx, int* code_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TORCHANNEL_B200_H */

@@ -1,0 +1,857 @@
+// C ABI of the B200 TorChannel step (include/torchannel_b200.h): context,
+// workspace carving, launch configuration and the extern "C" entry points.
+// The library never allocates device memory; every buffer is carved from the
+// caller's workspace.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/torchannel_b200.h"
+#include "tc_common.cuh"
+#include "tc_fft.cuh"
+#include "tc_poisson.cuh"
+#include "tc_stats.cuh"
+#include "tc_step.cuh"
+
+using namespace tc;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define TC_CUDA(call)                                                                     \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return fail(TC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TC_LAUNCHED()                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess) return fail(TC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Workspace layout
+// ---------------------------------------------------------------------------
+struct Carver {
+  size_t off = 0;
+  char* base = nullptr;
+  template <class P> P* take(size_t nbytes) {
+    off = (off + 255) & ~(size_t)255;
+    P* p = base ? reinterpret_cast<P*>(base + off) : nullptr;
+    off += nbytes;
+    return p;
+  }
+};
+
+struct tc_ctx {
+  int nx, ny, nz, nxh;
+  int precision, top_neumann, rhs_fused;
+  double Lx, Ly, Lz, nu, U_bulk, dx, dy;
+  std::vector<double> dzf, dzc;
+  int dev;
+  size_t tsz;  // sizeof storage type
+  // device buffers (storage type T unless noted)
+  void* st[2][3];
+  void* rh[3];
+  void* p;
+  void* X;
+  cpx<double>* dps;      // FP64 scratch for the Poisson forward sweep
+  void* idzf_t; void* idzc_t;
+  void* twx_t; void* twy_t;
+  double* dzf_d; double* dzc_d;
+  double* k2x; double* k2y; double* cl; double* cr;
+  cpx<double>* twx_d; cpx<double>* twy_d;
+  CnTab tab;
+  double* partials; double* partials2; int npart;
+  double* scal;
+  int* err;
+  // statistics
+  double* st_prof; double* st_spec; double* st_means; cpx<double>* st_S;
+  int k_bot, k_top, stats_ready, n_samples;
+  FftPlan planx, plany;
+  int JT, RB, tri_bt, stats_RB, stats_CB;
+  int cur, have_hist, state_set;
+  double tab_dt;
+  // per-phase timing ring (tc_timing_enable)
+  int timing;
+  int t_head, t_count;
+  cudaEvent_t tev[TC_TIMING_RING][TC_NPHASE + 1];
+  int tev_made;
+};
+
+// Record the boundary event `ph` of the current timed step.
+static void mark(tc_ctx* c, int ph, cudaStream_t s) {
+  if (c->timing) cudaEventRecord(c->tev[c->t_head][ph], s);
+}
+
+template <class T> static Grid<T> make_grid(const tc_ctx* c, int which_unused = 0) {
+  (void)which_unused;
+  Grid<T> g;
+  g.nx = c->nx; g.ny = c->ny; g.nz = c->nz;
+  g.idx = (T)(1.0 / c->dx); g.idy = (T)(1.0 / c->dy);
+  g.nu_idx2 = (T)(c->nu * (1.0 / (c->dx * c->dx)));
+  g.nu_idy2 = (T)(c->nu * (1.0 / (c->dy * c->dy)));
+  g.nu = (T)c->nu;
+  g.idzf = (const T*)c->idzf_t; g.idzc = (const T*)c->idzc_t;
+  g.top_neumann = c->top_neumann; g.rhs_fused = c->rhs_fused;
+  return g;
+}
+
+static size_t carve(tc_ctx* c, char* base) {
+  Carver cv; cv.base = base;
+  const size_t n = (size_t)c->nx * c->ny;
+  const size_t ncell = n * c->nz, nface = n * (c->nz + 1);
+  const size_t T_ = c->tsz;
+  for (int s = 0; s < 2; ++s) {
+    c->st[s][0] = cv.take<char>(ncell * T_);
+    c->st[s][1] = cv.take<char>(ncell * T_);
+    c->st[s][2] = cv.take<char>(nface * T_);
+  }
+  c->rh[0] = cv.take<char>(ncell * T_);
+  c->rh[1] = cv.take<char>(ncell * T_);
+  c->rh[2] = cv.take<char>(nface * T_);
+  c->p = cv.take<char>(ncell * T_);
+  const size_t nspec = (size_t)c->nxh * c->nz * c->ny;
+  c->X = cv.take<char>(nspec * 2 * T_);
+  c->dps = (c->precision == TC_FP64) ? (cpx<double>*)c->X : cv.take<cpx<double>>(nspec * sizeof(cpx<double>));
+  c->idzf_t = cv.take<char>(c->nz * T_);
+  c->idzc_t = cv.take<char>((c->nz + 1) * T_);
+  c->twx_t = cv.take<char>(c->nx * 2 * T_);
+  c->twy_t = cv.take<char>(c->ny * 2 * T_);
+  c->dzf_d = cv.take<double>(c->nz * 8);
+  c->dzc_d = cv.take<double>((c->nz + 1) * 8);
+  c->k2x = cv.take<double>(c->nxh * 8);
+  c->k2y = cv.take<double>(c->ny * 8);
+  c->cl = cv.take<double>(c->nz * 8);
+  c->cr = cv.take<double>(c->nz * 8);
+  c->twx_d = cv.take<cpx<double>>(c->nx * 16);
+  c->twy_d = cv.take<cpx<double>>(c->ny * 16);
+  c->tab.uv = cv.take<double>(6 * c->nz * 8);
+  c->tab.w = cv.take<double>(6 * c->nz * 8);
+  c->tab.beta = cv.take<double>(8);
+  const int gx = (c->nx + 31) / 32, gy = (c->ny + 7) / 8;
+  c->npart = gx * gy * (c->nz + 1);
+  c->partials = cv.take<double>((size_t)c->npart * 8);
+  c->partials2 = cv.take<double>((size_t)c->npart * 8);
+  c->scal = cv.take<double>(SC_COUNT * 8);
+  c->err = cv.take<int>(64);
+  c->st_prof = cv.take<double>(5 * c->nz * 8);
+  c->st_spec = cv.take<double>((size_t)4 * (c->nx / 2) * (c->ny / 2) * 8);
+  c->st_means = cv.take<double>(3 * c->nz * 8);
+  c->st_S = cv.take<cpx<double>>(3 * n * 16);
+  return cv.off + 256;
+}
+
+static int validate(const tc_grid_desc* g) {
+  if (!g) return fail(TC_ERR_ARG, "null grid descriptor");
+  if (g->nx < 4 || g->ny < 4 || g->nz < 4) return fail(TC_ERR_SIZE, "nx, ny, nz must be >= 4");
+  if ((g->nx & 1) || (g->ny & 1)) return fail(TC_ERR_SIZE, "nx and ny must be even");
+  if (g->nz > 800) return fail(TC_ERR_SIZE, "nz must be <= 800");
+  FftPlan a, b;
+  if (!fft_make_plan(g->nx, &a) || !fft_make_plan(g->ny, &b))
+    return fail(TC_ERR_SIZE, "nx and ny must factor into 2 and 3 only");
+  if (g->nx > 4096 || g->ny > 4096) return fail(TC_ERR_SIZE, "nx, ny must be <= 4096");
+  if (g->precision != TC_FP64 && g->precision != TC_MIXED) return fail(TC_ERR_ARG, "bad precision");
+  if (!g->dz_f || !g->dz_c) return fail(TC_ERR_ARG, "null dz_f / dz_c");
+  if (!(g->Lx > 0 && g->Ly > 0 && g->Lz > 0 && g->nu > 0)) return fail(TC_ERR_ARG, "non-positive domain or viscosity");
+  return TC_OK;
+}
+
+static void fill_basic(tc_ctx* c, const tc_grid_desc* g) {
+  c->nx = g->nx; c->ny = g->ny; c->nz = g->nz; c->nxh = g->nx / 2 + 1;
+  c->precision = g->precision; c->top_neumann = g->top_wall == TC_TOP_FREESLIP;
+  c->rhs_fused = g->rhs_path == TC_RHS_FUSED;
+  c->Lx = g->Lx; c->Ly = g->Ly; c->Lz = g->Lz; c->nu = g->nu; c->U_bulk = g->U_bulk;
+  c->dx = g->Lx / g->nx; c->dy = g->Ly / g->ny;
+  c->tsz = g->precision == TC_FP64 ? 8 : 4;
+  fft_make_plan(g->nx, &c->planx);
+  fft_make_plan(g->ny, &c->plany);
+  // launch shapes: x transform rows per block (even divisor of ny, smem <= 100 KB)
+  const size_t cb = 2 * c->tsz;
+  int JT = 16;
+  while (JT > 2 && (c->ny % JT != 0 || (size_t)2 * (JT / 2) * (c->nx + 2) * cb > 100 * 1024)) JT -= 2;
+  c->JT = JT;
+  int RB = 8;
+  while (RB > 1 && (size_t)2 * RB * c->ny * cb > 100 * 1024) RB /= 2;
+  c->RB = RB;
+  c->tri_bt = (64 * (size_t)c->nz * 8 <= 200 * 1024) ? 64 : 32;
+  int sRB = 8;
+  while (sRB > 1 && (size_t)2 * sRB * c->nx * 16 > 100 * 1024) sRB /= 2;
+  c->stats_RB = sRB;
+  int sCB = 8;
+  while (sCB > 1 && (size_t)2 * sCB * c->ny * 16 > 100 * 1024) sCB /= 2;
+  c->stats_CB = sCB;
+}
+
+extern "C" const char* tc_version(void) { return "torchannel_b200 0.1 (sm_100a)"; }
+extern "C" const char* tc_last_error(void) { return g_err.c_str(); }
+
+extern "C" int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes) {
+  int rc = validate(g);
+  if (rc) return rc;
+  if (!bytes) return fail(TC_ERR_ARG, "null bytes");
+  tc_ctx c{};
+  fill_basic(&c, g);
+  *bytes = carve(&c, nullptr);
+  return TC_OK;
+}
+
+template <class T> static int set_smem_attrs(const tc_ctx* c) {
+  const int big = 200 * 1024;
+  TC_CUDA(cudaFuncSetAttribute(k_div_fftx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_ifftx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_ffty<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_ffty<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+  TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  (void)c;
+  return TC_OK;
+}
+
+template <class T> static void to_t(const std::vector<double>& src, std::vector<unsigned char>& dst) {
+  dst.resize(src.size() * sizeof(T));
+  T* d = reinterpret_cast<T*>(dst.data());
+  for (size_t e = 0; e < src.size(); ++e) d[e] = (T)src[e];
+}
+
+static int upload(void* dptr, const std::vector<double>& v, size_t tsz) {
+  if (tsz == 8) {
+    TC_CUDA(cudaMemcpy(dptr, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<unsigned char> b;
+    to_t<float>(v, b);
+    TC_CUDA(cudaMemcpy(dptr, b.data(), b.size(), cudaMemcpyHostToDevice));
+  }
+  return TC_OK;
+}
+
+static std::vector<double> twiddles(int n) {
+  std::vector<double> t(2 * (size_t)n);
+  const double pi = 3.14159265358979323846264338327950288;
+  for (int m = 0; m < n; ++m) {
+    // exp(-2 pi i m / n); use symmetric reduction for accuracy
+    double ang = -2.0 * pi * (double)m / (double)n;
+    t[2 * m] = std::cos(ang);
+    t[2 * m + 1] = std::sin(ang);
+  }
+  return t;
+}
+
+extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, tc_ctx** out) {
+  int rc = validate(g);
+  if (rc) return rc;
+  if (!out || !workspace) return fail(TC_ERR_ARG, "null workspace / out");
+  if (((uintptr_t)workspace) & 255) return fail(TC_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  tc_ctx* c = new tc_ctx();
+  fill_basic(c, g);
+  size_t need = carve(c, (char*)workspace);
+  if (bytes < need) { delete c; return fail(TC_ERR_WORKSPACE, "workspace too small"); }
+  cudaGetDevice(&c->dev);
+  c->dzf.assign(g->dz_f, g->dz_f + g->nz);
+  c->dzc.assign(g->dz_c, g->dz_c + g->nz + 1);
+  auto bail = [&](int r) { delete c; return r; };
+  if (cudaMemset(workspace, 0, need) != cudaSuccess) return bail(fail(TC_ERR_CUDA, "memset workspace"));
+  std::vector<double> idzf(c->nz), idzc(c->nz + 1), cl(c->nz), cr(c->nz);
+  for (int k = 0; k < c->nz; ++k) idzf[k] = 1.0 / c->dzf[k];
+  for (int k = 0; k <= c->nz; ++k) idzc[k] = 1.0 / c->dzc[k];
+  for (int k = 0; k < c->nz; ++k) {
+    cl[k] = 1.0 / (c->dzc[k] * c->dzf[k]);
+    cr[k] = 1.0 / (c->dzc[k + 1] * c->dzf[k]);
+  }
+  // modified wavenumbers (projection_fft.py:26-39): kx = 2 pi m / (nx dx), k~ = (2/dx) sin(kx dx / 2)
+  const double pi = 3.14159265358979323846264338327950288;
+  std::vector<double> k2x(c->nxh), k2y(c->ny);
+  for (int m = 0; m < c->nxh; ++m) {
+    double f = (m < (c->nx + 1) / 2 ? (double)m : (double)(m - c->nx)) / ((double)c->nx * (c->dx / (2 * pi)));
+    double km = (2.0 / c->dx) * std::sin(f * c->dx / 2.0);
+    k2x[m] = km * km;
+  }
+  for (int m = 0; m < c->ny; ++m) {
+    double f = (m < (c->ny + 1) / 2 ? (double)m : (double)(m - c->ny)) / ((double)c->ny * (c->dy / (2 * pi)));
+    double km = (2.0 / c->dy) * std::sin(f * c->dy / 2.0);
+    k2y[m] = km * km;
+  }
+  std::vector<double> twx = twiddles(c->nx), twy = twiddles(c->ny);
+  int r2 = TC_OK;
+  if ((r2 = upload(c->idzf_t, idzf, c->tsz)) || (r2 = upload(c->idzc_t, idzc, c->tsz)) ||
+      (r2 = upload(c->twx_t, twx, c->tsz)) || (r2 = upload(c->twy_t, twy, c->tsz)) ||
+      (r2 = upload(c->dzf_d, c->dzf, 8)) || (r2 = upload(c->dzc_d, c->dzc, 8)) ||
+      (r2 = upload(c->k2x, k2x, 8)) || (r2 = upload(c->k2y, k2y, 8)) || (r2 = upload(c->cl, cl, 8)) ||
+      (r2 = upload(c->cr, cr, 8)) || (r2 = upload(c->twx_d, twx, 8)) || (r2 = upload(c->twy_d, twy, 8)))
+    return bail(r2);
+  r2 = (c->tsz == 8) ? set_smem_attrs<double>(c) : set_smem_attrs<float>(c);
+  if (r2) return bail(r2);
+  if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "create sync"));
+  c->tab_dt = -1.0;
+  *out = c;
+  return TC_OK;
+}
+
+extern "C" int tc_destroy(tc_ctx* ctx) {
+  if (ctx && ctx->tev_made)
+    for (int r = 0; r < TC_TIMING_RING; ++r)
+      for (int p = 0; p <= TC_NPHASE; ++p) cudaEventDestroy(ctx->tev[r][p]);
+  delete ctx;
+  return TC_OK;
+}
+
+#define ST(c) ((cudaStream_t)(c))
+
+// ---------------------------------------------------------------------------
+// Typed implementations
+// ---------------------------------------------------------------------------
+template <class T> static int set_state_impl(tc_ctx* c, const double* u, const double* v, const double* w, cudaStream_t s) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  dim3 blk(32, 8);
+  dim3 gc((nx + 31) / 32, ny, (nz + 31) / 32), gf((nx + 31) / 32, ny, (nz + 1 + 31) / 32);
+  T** S = (T**)c->st[c->cur];
+  k_from_ref<T><<<gc, blk, 0, s>>>(u, S[0], FLD_U, nx, ny, nz, 1.0);
+  k_from_ref<T><<<gc, blk, 0, s>>>(v, S[1], FLD_V, nx, ny, nz, 1.0);
+  k_from_ref<T><<<gf, blk, 0, s>>>(w, S[2], FLD_W, nx, ny, nz, 1.0);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int to_ref(const tc_ctx* c, const T* in, double* out, int kind, cudaStream_t s) {
+  int Xr, Zr;
+  switch (kind) {
+    case FLD_U: Xr = c->nx + 1; Zr = c->nz + 2; break;
+    case FLD_V: Xr = c->nx + 2; Zr = c->nz + 2; break;
+    case FLD_W: Xr = c->nx + 2; Zr = c->nz + 1; break;
+    case FLD_P: Xr = c->nx + 2; Zr = c->nz + 2; break;
+    default: Xr = c->nx; Zr = c->nz; break;
+  }
+  int Yr = (kind == FLD_U || kind == FLD_W || kind == FLD_P) ? c->ny + 2 : (kind == FLD_V ? c->ny + 1 : c->ny);
+  dim3 grid((Xr + 31) / 32, Yr, (Zr + 31) / 32);
+  k_to_ref<T><<<grid, dim3(32, 8), 0, s>>>(in, out, kind, c->nx, c->ny, c->nz, c->top_neumann);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, const T* w, const T* field, T* p,
+                                           double scale, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  const int nx = c->nx, ny = c->ny, nz = c->nz, nxh = c->nxh;
+  cpx<T>* X = (cpx<T>*)c->X;
+  const size_t smx = (size_t)2 * (c->JT / 2) * (nx + 2) * sizeof(cpx<T>);
+  mark(c, TC_PH_FFTX, s);
+  k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, (const cpx<T>*)c->twx_t,
+                                                        (T)scale, c->JT);
+  const int nrows = nxh * nz;
+  const size_t smy = (size_t)2 * c->RB * ny * sizeof(cpx<T>);
+  mark(c, TC_PH_FFTY, s);
+  k_ffty<T, false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, (const cpx<T>*)c->twy_t, c->RB);
+  PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
+  const int nmodes = nxh * ny;
+  mark(c, TC_PH_TRI, s);
+  k_tri<T><<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, c->dps, tb, nxh, ny, nz);
+  mark(c, TC_PH_IFFTY, s);
+  k_ffty<T, true><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, (const cpx<T>*)c->twy_t, c->RB);
+  mark(c, TC_PH_IFFTX, s);
+  k_ifftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, (const cpx<T>*)c->twx_t, c->JT);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, planes); }
+
+template <class T> static int bulk_finalize(tc_ctx* c, double dt, int update, cudaStream_t s) {
+  const double scale = c->dx * c->dy / (c->Lx * c->Ly * c->Lz);
+  k_bulk_finalize<<<1, 256, 0, s>>>(c->partials, c->npart, c->scal, scale, c->U_bulk, dt, update);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  k_project_bulk<T><<<grid3(c, c->nz + 1), dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], (const T*)c->p, (T)dt, c->dzf_d,
+                                                                c->partials);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  const int nxt = c->cur ^ 1;
+  T** A = (T**)c->st[c->cur];
+  T** B = (T**)c->st[nxt];
+  T** R = (T**)c->rh;
+  dim3 blk(32, 8);
+  dim3 grd = grid3(c, c->nz + 1);
+  if (scheme == TC_IMEX && c->tab_dt != dt) {
+    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
+    c->tab_dt = dt;
+  }
+  mark(c, TC_PH_RHS, s);
+  if (scheme == TC_IMEX)
+    k_rhs_update<T, false, UPD_AB2><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
+                                                         c->scal + SC_FORCING, (T)dt, c->have_hist);
+  else if (scheme == TC_AB2)
+    k_rhs_update<T, true, UPD_AB2><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
+                                                        c->scal + SC_FORCING, (T)dt, c->have_hist);
+  else
+    k_rhs_update<T, true, UPD_FE><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
+                                                       c->scal + SC_FORCING, (T)dt, 0);
+  TC_LAUNCHED();
+  mark(c, TC_PH_CN, s);
+  if (scheme == TC_IMEX) {
+    const int ncol = c->nx * c->ny;
+    k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 6 * c->nz * 8, s>>>(B[0], B[1], B[2], c->tab, c->nx, c->ny, c->nz);
+    TC_LAUNCHED();
+  }
+  int rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, (T*)c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
+  if (rc) return rc;
+  mark(c, TC_PH_PROJ, s);
+  if ((rc = project_impl<T>(c, B, dt, s))) return rc;
+  mark(c, TC_PH_FIN, s);
+  if ((rc = bulk_finalize<T>(c, dt, scheme != TC_FE, s))) return rc;
+  mark(c, TC_NPHASE, s);
+  if (c->timing) {
+    c->t_head = (c->t_head + 1) % TC_TIMING_RING;
+    if (c->t_count < TC_TIMING_RING) c->t_count++;
+  }
+  c->cur = nxt;
+  if (scheme != TC_FE) c->have_hist = 1;
+  return TC_OK;
+}
+
+template <class T> static int project_initial_impl(tc_ctx* c, cudaStream_t s) {
+  T** A = (T**)c->st[c->cur];
+  int rc = poisson_impl<T>(c, A[0], A[1], A[2], nullptr, (T*)c->p, 1.0 / ((double)c->nx * (double)c->ny), s);
+  if (rc) return rc;
+  if ((rc = project_impl<T>(c, A, 1.0, s))) return rc;
+  return bulk_finalize<T>(c, 1.0, 0, s);
+}
+
+template <class T> static int bulk_impl(tc_ctx* c, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  T** A = (T**)c->st[c->cur];
+  cudaMemsetAsync(c->partials, 0, (size_t)c->npart * 8, s);
+  k_bulk_partials<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(g, A[0], c->dzf_d, c->partials);
+  TC_LAUNCHED();
+  return bulk_finalize<T>(c, 1.0, 0, s);
+}
+
+template <class T> static int cfl_impl(tc_ctx* c, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  T** A = (T**)c->st[c->cur];
+  dim3 grd = grid3(c, c->nz);
+  k_cfl_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], c->partials2);
+  k_max_finalize<<<1, 256, 0, s>>>(c->partials2, grd.x * grd.y * grd.z, c->scal + SC_DTI);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int diag_impl(tc_ctx* c, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  T** A = (T**)c->st[c->cur];
+  dim3 grd = grid3(c, c->nz);
+  const int nb = grd.x * grd.y * grd.z;
+  // nb = gx*gy*nz <= npart: one partials buffer each for the max and the flag
+  k_diag_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], (const T*)c->p, c->partials2, c->partials);
+  k_max_finalize<<<1, 256, 0, s>>>(c->partials2, nb, c->scal + SC_MAXDIV);
+  k_max_finalize<<<1, 256, 0, s>>>(c->partials, nb, c->scal + SC_NONFINITE);
+  k_utau_sums<T><<<2, 256, 0, s>>>(g, A[0], c->scal);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int stats_impl(tc_ctx* c, cudaStream_t s) {
+  T** A = (T**)c->st[c->cur];
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  k_stats_prof<T><<<nz, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, c->st_prof, c->st_means);
+  k_stats_fill<T><<<(nx * ny + 255) / 256, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, c->k_bot - 1, c->k_top - 1,
+                                                        c->st_means, c->st_S);
+  const int nrows = 3 * ny;
+  k_fft_rows_d<false><<<(nrows + c->stats_RB - 1) / c->stats_RB, 256, (size_t)2 * c->stats_RB * nx * 16, s>>>(
+      c->st_S, nrows, nx, c->planx, c->twx_d, c->stats_RB);
+  const int bpp = (nx + c->stats_CB - 1) / c->stats_CB;
+  k_fft_cols<false><<<3 * bpp, 256, (size_t)2 * c->stats_CB * ny * 16, s>>>(c->st_S, nx, ny, nx, (size_t)nx * ny,
+                                                                          c->plany, c->twy_d, c->stats_CB);
+  const int nspec = (nx / 2) * (ny / 2);
+  k_stats_spec<<<(nspec + 127) / 128, 128, 0, s>>>(c->st_S, nx, ny, c->st_spec);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+template <class T> static int rhs_hook_impl(tc_ctx* c, int full, double* ru, double* rv, double* rw, cudaStream_t s) {
+  Grid<T> g = make_grid<T>(c);
+  T** A = (T**)c->st[c->cur];
+  T** B = (T**)c->st[c->cur ^ 1];  // scratch: the next buffer is free between steps
+  const size_t ncell = (size_t)c->nx * c->ny * c->nz;
+  cudaMemsetAsync(B[2], 0, ncell / c->nz * (c->nz + 1) * sizeof(T), s);
+  dim3 grd = grid3(c, c->nz + 1);
+  if (full)
+    k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+                                                                   B[0], B[1], B[2], c->scal, (T)0, 0);
+  else
+    k_rhs_update<T, false, UPD_RHS_ONLY><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+                                                                    B[0], B[1], B[2], c->scal, (T)0, 0);
+  TC_LAUNCHED();
+  int rc;
+  if ((rc = to_ref<T>(c, B[0], ru, FLD_U, s)) || (rc = to_ref<T>(c, B[1], rv, FLD_V, s)) ||
+      (rc = to_ref<T>(c, B[2], rw, FLD_W, s)))
+    return rc;
+  return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// extern "C" entry points
+// ---------------------------------------------------------------------------
+#define DISPATCH(c, fn, ...) ((c)->tsz == 8 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+extern "C" int tc_set_state(tc_ctx* c, const double* u, const double* v, const double* w, double forcing, void* stream) {
+  if (!c || !u || !v || !w) return fail(TC_ERR_ARG, "null argument");
+  int rc = DISPATCH(c, set_state_impl, c, u, v, w, ST(stream));
+  if (rc) return rc;
+  TC_CUDA(cudaMemsetAsync(c->scal, 0, SC_COUNT * 8, ST(stream)));
+  rc = tc_set_forcing(c, forcing, stream);
+  if (rc) return rc;
+  TC_CUDA(cudaMemsetAsync(c->p, 0, (size_t)c->nx * c->ny * c->nz * c->tsz, ST(stream)));
+  c->have_hist = 0;
+  c->state_set = 1;
+  return TC_OK;
+}
+
+extern "C" int tc_set_forcing(tc_ctx* c, double forcing, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  // a one-element H2D copy from a host stack value must complete before return
+  TC_CUDA(cudaMemcpyAsync(c->scal + SC_FORCING, &forcing, 8, cudaMemcpyHostToDevice, ST(stream)));
+  TC_CUDA(cudaStreamSynchronize(ST(stream)));
+  return TC_OK;
+}
+
+extern "C" int tc_get_state(tc_ctx* c, double* u, double* v, double* w, double* p, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  int rc = TC_OK;
+  void** A = c->st[c->cur];
+  if (c->tsz == 8) {
+    if (u && (rc = to_ref<double>(c, (double*)A[0], u, FLD_U, ST(stream)))) return rc;
+    if (v && (rc = to_ref<double>(c, (double*)A[1], v, FLD_V, ST(stream)))) return rc;
+    if (w && (rc = to_ref<double>(c, (double*)A[2], w, FLD_W, ST(stream)))) return rc;
+    if (p && (rc = to_ref<double>(c, (double*)c->p, p, FLD_P, ST(stream)))) return rc;
+  } else {
+    if (u && (rc = to_ref<float>(c, (float*)A[0], u, FLD_U, ST(stream)))) return rc;
+    if (v && (rc = to_ref<float>(c, (float*)A[1], v, FLD_V, ST(stream)))) return rc;
+    if (w && (rc = to_ref<float>(c, (float*)A[2], w, FLD_W, ST(stream)))) return rc;
+    if (p && (rc = to_ref<float>(c, (float*)c->p, p, FLD_P, ST(stream)))) return rc;
+  }
+  return TC_OK;
+}
+
+template <class T> static int get_hist_impl(tc_ctx* c, double* ru, double* rv, double* rw, cudaStream_t s) {
+  int rc;
+  T** R = (T**)c->rh;
+  if (ru && (rc = to_ref<T>(c, R[0], ru, FLD_U, s))) return rc;
+  if (rv && (rc = to_ref<T>(c, R[1], rv, FLD_V, s))) return rc;
+  if (rw && (rc = to_ref<T>(c, R[2], rw, FLD_W, s))) return rc;
+  return TC_OK;
+}
+
+template <class T> static int set_hist_impl(tc_ctx* c, const double* ru, const double* rv, const double* rw, cudaStream_t s) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  dim3 blk(32, 8);
+  dim3 gc((nx + 31) / 32, ny, (nz + 31) / 32), gf((nx + 31) / 32, ny, (nz + 1 + 31) / 32);
+  T** R = (T**)c->rh;
+  k_from_ref<T><<<gc, blk, 0, s>>>(ru, R[0], FLD_U, nx, ny, nz, 1.0);
+  k_from_ref<T><<<gc, blk, 0, s>>>(rv, R[1], FLD_V, nx, ny, nz, 1.0);
+  k_from_ref<T><<<gf, blk, 0, s>>>(rw, R[2], FLD_W, nx, ny, nz, 1.0);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+extern "C" int tc_get_history(tc_ctx* c, double* ru, double* rv, double* rw, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->have_hist) return fail(TC_ERR_STATE, "no AB2 history yet");
+  return DISPATCH(c, get_hist_impl, c, ru, rv, rw, ST(stream));
+}
+
+extern "C" int tc_set_history(tc_ctx* c, const double* ru, const double* rv, const double* rw, void* stream) {
+  if (!c || !ru || !rv || !rw) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "set the state first");
+  int rc = DISPATCH(c, set_hist_impl, c, ru, rv, rw, ST(stream));
+  if (rc) return rc;
+  c->have_hist = 1;
+  return TC_OK;
+}
+
+extern "C" int tc_step(tc_ctx* c, int scheme, double dt, int n_steps, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  if (scheme != TC_IMEX && scheme != TC_AB2 && scheme != TC_FE) return fail(TC_ERR_ARG, "bad scheme");
+  if (!(dt > 0) || n_steps < 0) return fail(TC_ERR_ARG, "dt must be > 0 and n_steps >= 0");
+  for (int n = 0; n < n_steps; ++n) {
+    int rc = DISPATCH(c, step_impl, c, scheme, dt, ST(stream));
+    if (rc) return rc;
+  }
+  return TC_OK;
+}
+
+extern "C" int tc_project_initial(tc_ctx* c, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  return DISPATCH(c, project_initial_impl, c, ST(stream));
+}
+
+extern "C" int tc_scalars(tc_ctx* c, double** dev_ptr) {
+  if (!c || !dev_ptr) return fail(TC_ERR_ARG, "null argument");
+  *dev_ptr = c->scal;
+  return TC_OK;
+}
+
+static int read_scal(tc_ctx* c, double* host, cudaStream_t s) {
+  TC_CUDA(cudaMemcpyAsync(host, c->scal, SC_COUNT * 8, cudaMemcpyDeviceToHost, s));
+  TC_CUDA(cudaStreamSynchronize(s));
+  return TC_OK;
+}
+
+extern "C" int tc_bulk_velocity(tc_ctx* c, double* out, void* stream) {
+  if (!c || !out) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  // keep the step's u_bulk slot: compute into it, read, then restore is not
+  // needed because the slot always holds the bulk velocity of the state.
+  int rc = DISPATCH(c, bulk_impl, c, ST(stream));
+  if (rc) return rc;
+  double h[SC_COUNT];
+  if ((rc = read_scal(c, h, ST(stream)))) return rc;
+  *out = h[SC_UBULK];
+  return TC_OK;
+}
+
+extern "C" int tc_cfl(tc_ctx* c, double* dti, void* stream) {
+  if (!c || !dti) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  int rc = DISPATCH(c, cfl_impl, c, ST(stream));
+  if (rc) return rc;
+  double h[SC_COUNT];
+  if ((rc = read_scal(c, h, ST(stream)))) return rc;
+  *dti = h[SC_DTI];
+  return TC_OK;
+}
+
+extern "C" int tc_diagnostics(tc_ctx* c, double* out, void* stream) {
+  if (!c || !out) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  int rc = DISPATCH(c, diag_impl, c, ST(stream));
+  if (rc) return rc;
+  double h[SC_COUNT];
+  if ((rc = read_scal(c, h, ST(stream)))) return rc;
+  // u_tau (utils.py:176-204): first cell centre z_c[1] = dz_f[0]/2
+  const double dist = 0.5 * c->dzf[0];
+  const double tb = c->nu * h[SC_UTAU_BOT] / dist;
+  const double ut_b = std::sqrt(std::fabs(tb));
+  double ut = ut_b;
+  if (!c->top_neumann) {
+    const double tt = c->nu * h[SC_UTAU_TOP] / dist;
+    ut = 0.5 * (ut_b + std::sqrt(std::fabs(tt)));
+  }
+  out[0] = h[SC_MAXDIV];
+  out[1] = ut;
+  out[2] = h[SC_UBULK];
+  out[3] = h[SC_FORCING];
+  out[4] = h[SC_NONFINITE];
+  return TC_OK;
+}
+
+template <class T>
+__global__ void k_div_field(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w,
+                            T* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int nx = g.nx, ny = g.ny;
+  const size_t o = pidx(k, j, i, ny, nx);
+  out[o] = (u[o] - u[pidx(k, j, wrap(i - 1, nx), ny, nx)]) * g.idx + (v[o] - v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * g.idy +
+           (w[pidx(k + 1, j, i, ny, nx)] - w[o]) * g.idzf[k];
+}
+
+template <class T> static int divergence_impl(tc_ctx* c, double* div, cudaStream_t s) {
+  T** A = (T**)c->st[c->cur];
+  T** B = (T**)c->st[c->cur ^ 1];
+  Grid<T> g = make_grid<T>(c);
+  k_div_field<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], B[0]);
+  TC_LAUNCHED();
+  return to_ref<T>(c, B[0], div, FLD_CELL, s);
+}
+
+extern "C" int tc_divergence(tc_ctx* c, double* div, void* stream) {
+  if (!c || !div) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  return DISPATCH(c, divergence_impl, c, div, ST(stream));
+}
+
+extern "C" int tc_explicit_rhs(tc_ctx* c, int full, double* ru, double* rv, double* rw, void* stream) {
+  if (!c || !ru || !rv || !rw) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  return DISPATCH(c, rhs_hook_impl, c, full, ru, rv, rw, ST(stream));
+}
+
+template <class T> static int cn_hook_impl(tc_ctx* c, double dt, cudaStream_t s) {
+  T** A = (T**)c->st[c->cur];
+  if (c->tab_dt != dt) {
+    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
+    c->tab_dt = dt;
+  }
+  const int ncol = c->nx * c->ny;
+  k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 6 * c->nz * 8, s>>>(A[0], A[1], A[2], c->tab, c->nx, c->ny, c->nz);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+extern "C" int tc_implicit_diffusion(tc_ctx* c, double dt, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  if (!(dt > 0)) return fail(TC_ERR_ARG, "dt must be > 0");
+  return DISPATCH(c, cn_hook_impl, c, dt, ST(stream));
+}
+
+template <class T> static int poisson_hook_impl(tc_ctx* c, const double* rhs, double* p, cudaStream_t s) {
+  // rhs -> internal cell layout in the pressure buffer of the scratch state,
+  // solve into p, write out with ghosts.
+  T** B = (T**)c->st[c->cur ^ 1];
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  k_from_ref<T><<<dim3((nx + 31) / 32, ny, (nz + 31) / 32), dim3(32, 8), 0, s>>>(rhs, B[0], FLD_CELL, nx, ny, nz, 1.0);
+  TC_LAUNCHED();
+  int rc = poisson_impl<T>(c, nullptr, nullptr, nullptr, B[0], B[1], 1.0 / ((double)nx * (double)ny), s);
+  if (rc) return rc;
+  return to_ref<T>(c, B[1], p, FLD_P, s);
+}
+
+extern "C" int tc_poisson_solve(tc_ctx* c, const double* rhs, double* p, void* stream) {
+  if (!c || !rhs || !p) return fail(TC_ERR_ARG, "null argument");
+  return DISPATCH(c, poisson_hook_impl, c, rhs, p, ST(stream));
+}
+
+template <class T>
+__global__ void k_p_from_ref(const double* __restrict__ ref, T* __restrict__ out, int nx, int ny, int nz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  if (i >= nx || j >= ny || k >= nz) return;
+  out[pidx(k, j, i, ny, nx)] = (T)ref[((size_t)(i + 1) * (ny + 2) + (j + 1)) * (nz + 2) + (k + 1)];
+}
+
+template <class T> static int project_hook_impl(tc_ctx* c, const double* p, double dt, cudaStream_t s) {
+  k_p_from_ref<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(p, (T*)c->p, c->nx, c->ny, c->nz);
+  TC_LAUNCHED();
+  int rc = project_impl<T>(c, (T* const*)c->st[c->cur], dt, s);
+  if (rc) return rc;
+  return bulk_finalize<T>(c, dt, 0, s);
+}
+
+extern "C" int tc_project(tc_ctx* c, const double* p, double dt, void* stream) {
+  if (!c || !p) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  return DISPATCH(c, project_hook_impl, c, p, dt, ST(stream));
+}
+
+extern "C" int tc_stats_init(tc_ctx* c, const double* z_c, double Re_tau_target, double z_plus_target, int* k_bot,
+                             int* k_top) {
+  if (!c || !z_c) return fail(TC_ERR_ARG, "null argument");
+  // turbstats.py:52-69
+  const double u_tau_target = Re_tau_target * c->nu / (c->Lz / 2.0);
+  const double zt = z_plus_target * c->nu / u_tau_target;
+  int kb = 0, kt = 0;
+  double bb = INFINITY, bt = INFINITY;
+  for (int k = 0; k < c->nz; ++k) {
+    double z = z_c[k + 1];
+    double db = std::fabs(z - zt), dt_ = std::fabs(z - (c->Lz - zt));
+    if (db < bb) { bb = db; kb = k; }
+    if (dt_ < bt) { bt = dt_; kt = k; }
+  }
+  c->k_bot = kb + 1;
+  c->k_top = kt + 1;
+  if (k_bot) *k_bot = c->k_bot;
+  if (k_top) *k_top = c->k_top;
+  TC_CUDA(cudaMemset(c->st_prof, 0, 5 * c->nz * 8));
+  TC_CUDA(cudaMemset(c->st_spec, 0, (size_t)4 * (c->nx / 2) * (c->ny / 2) * 8));
+  TC_CUDA(cudaDeviceSynchronize());
+  c->n_samples = 0;
+  c->stats_ready = 1;
+  return TC_OK;
+}
+
+extern "C" int tc_stats_accumulate(tc_ctx* c, void* stream) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->stats_ready) return fail(TC_ERR_STATE, "call tc_stats_init first");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  int rc = DISPATCH(c, stats_impl, c, ST(stream));
+  if (rc) return rc;
+  c->n_samples++;
+  return TC_OK;
+}
+
+extern "C" int tc_stats_read(tc_ctx* c, double* prof, double* spec, int* n_samples) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (!c->stats_ready) return fail(TC_ERR_STATE, "call tc_stats_init first");
+  TC_CUDA(cudaDeviceSynchronize());
+  if (prof) TC_CUDA(cudaMemcpy(prof, c->st_prof, 5 * c->nz * 8, cudaMemcpyDeviceToHost));
+  if (spec) TC_CUDA(cudaMemcpy(spec, c->st_spec, (size_t)4 * (c->nx / 2) * (c->ny / 2) * 8, cudaMemcpyDeviceToHost));
+  if (n_samples) *n_samples = c->n_samples;
+  return TC_OK;
+}
+
+extern "C" int tc_stats_write(tc_ctx* c, const double* prof, const double* spec, int n_samples) {
+  if (!c || !prof || !spec || n_samples < 0) return fail(TC_ERR_ARG, "bad argument");
+  if (!c->stats_ready) return fail(TC_ERR_STATE, "call tc_stats_init first");
+  TC_CUDA(cudaDeviceSynchronize());
+  TC_CUDA(cudaMemcpy(c->st_prof, prof, 5 * c->nz * 8, cudaMemcpyHostToDevice));
+  TC_CUDA(cudaMemcpy(c->st_spec, spec, (size_t)4 * (c->nx / 2) * (c->ny / 2) * 8, cudaMemcpyHostToDevice));
+  c->n_samples = n_samples;
+  return TC_OK;
+}
+
+extern "C" int tc_timing_enable(tc_ctx* c, int on) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (on && !c->tev_made) {
+    for (int r = 0; r < TC_TIMING_RING; ++r)
+      for (int p = 0; p <= TC_NPHASE; ++p) TC_CUDA(cudaEventCreate(&c->tev[r][p]));
+    c->tev_made = 1;
+  }
+  c->timing = on ? 1 : 0;
+  c->t_head = 0;
+  c->t_count = 0;
+  return TC_OK;
+}
+
+extern "C" int tc_timing_read(tc_ctx* c, double* ms, int* n_steps) {
+  if (!c || !ms) return fail(TC_ERR_ARG, "null argument");
+  for (int p = 0; p < TC_NPHASE; ++p) ms[p] = 0.0;
+  if (n_steps) *n_steps = 0;
+  if (!c->tev_made) return TC_OK;
+  TC_CUDA(cudaDeviceSynchronize());
+  for (int q = 0; q < c->t_count; ++q) {
+    int r = (c->t_head - 1 - q + 2 * TC_TIMING_RING) % TC_TIMING_RING;
+    int prev = -1;
+    // phases that did not run in a step (CN outside IMEX) have no event: walk
+    // the recorded boundaries in order and charge each interval to its start
+    for (int p = 0; p <= TC_NPHASE; ++p) {
+      if (cudaEventQuery(c->tev[r][p]) != cudaSuccess) continue;
+      if (prev >= 0) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, c->tev[r][prev], c->tev[r][p]) == cudaSuccess) ms[prev] += t;
+      }
+      prev = p;
+    }
+  }
+  cudaGetLastError();
+  if (n_steps) *n_steps = c->t_count;
+  c->t_count = 0;
+  c->t_head = 0;
+  return TC_OK;
+}
+
+extern "C" int tc_error(tc_ctx* c, int* code) {
+  if (!c || !code) return fail(TC_ERR_ARG, "null argument");
+  TC_CUDA(cudaDeviceSynchronize());
+  TC_CUDA(cudaMemcpy(code, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+  TC_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+  return TC_OK;
+}

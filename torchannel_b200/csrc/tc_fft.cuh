@@ -1,0 +1,122 @@
+// Hand-written mixed-radix (4, 2, 3) complex FFTs on batches of rows held in
+// shared memory.  Stockham autosort formulation (Govindaraju et al., "High
+// performance discrete Fourier transforms on graphics processors", SC'08):
+// every stage reads one buffer and writes the other in natural order, so no
+// bit reversal pass is needed.  Twiddles come from a table
+// tw[m] = exp(-2*pi*i*m/N), m < N, computed on the host in FP64.
+//
+// These transforms replace torch.fft.rfft2 / irfft2 of the reference
+// (projection_fft.py:118,139; turbstats.py:165-173).
+#pragma once
+#include "tc_common.cuh"
+
+namespace tc {
+
+#define TC_FFT_MAX_STAGES 12
+
+struct FftPlan {
+  int n;
+  int nstages;
+  int radix[TC_FFT_MAX_STAGES];
+};
+
+// Host-side: factor n into stages of 4, 2 and 3.  Returns 0 when n has any
+// other prime factor.
+inline int fft_make_plan(int n, FftPlan* p) {
+  p->n = n;
+  p->nstages = 0;
+  if (n < 1) return 0;
+  int m = n;
+  while (m % 4 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 4; m /= 4; }
+  while (m % 2 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 2; m /= 2; }
+  while (m % 3 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 3; m /= 3; }
+  return m == 1;
+}
+
+// Multiply by -i (forward) or +i (inverse).
+template <class T, bool INV> __device__ __forceinline__ cpx<T> mul_mi(cpx<T> a) {
+  return INV ? cmake<T>(-a.y, a.x) : cmake<T>(a.y, -a.x);
+}
+
+template <class T, bool INV> __device__ __forceinline__ void dft2(cpx<T>* v) {
+  cpx<T> a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+template <class T, bool INV> __device__ __forceinline__ void dft4(cpx<T>* v) {
+  cpx<T> s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+  cpx<T> s13 = cadd(v[1], v[3]), d13 = mul_mi<T, INV>(csub(v[1], v[3]));
+  v[0] = cadd(s02, s13);
+  v[2] = csub(s02, s13);
+  v[1] = cadd(d02, d13);
+  v[3] = csub(d02, d13);
+}
+
+// y1 = x0 - (x1+x2)/2 -/+ i s (x1-x2), y2 = x0 - (x1+x2)/2 +/- i s (x1-x2), s = sqrt(3)/2
+template <class T, bool INV> __device__ __forceinline__ void dft3(cpx<T>* v) {
+  const T s = (T)0.86602540378443864676372317075294;
+  cpx<T> x0 = v[0], sum = cadd(v[1], v[2]), dif = csub(v[1], v[2]);
+  cpx<T> t = cmake<T>(x0.x - (T)0.5 * sum.x, x0.y - (T)0.5 * sum.y);
+  cpx<T> r = mul_mi<T, INV>(cscale(dif, s));
+  v[0] = cadd(x0, sum);
+  v[1] = cadd(t, r);
+  v[2] = csub(t, r);
+}
+
+// One Stockham stage over `batch` rows of length n (row stride `rs` elements).
+template <class T, bool INV, int R>
+__device__ __forceinline__ void fft_stage(const cpx<T>* __restrict__ x, cpx<T>* __restrict__ y, int batch,
+                                          int rs, int n, int Ns, const cpx<T>* __restrict__ tw, int tid,
+                                          int nthr) {
+  const int nr = n / R;
+  const int fac = n / (Ns * R);
+  const int total = batch * nr;
+  for (int idx = tid; idx < total; idx += nthr) {
+    int b = idx / nr;
+    int j = idx - b * nr;
+    const cpx<T>* xb = x + (size_t)b * rs;
+    cpx<T>* yb = y + (size_t)b * rs;
+    int k = j % Ns;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = xb[j + r * nr];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        cpx<T> w = tw[r * k * fac];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    if (R == 2) dft2<T, INV>(v);
+    else if (R == 4) dft4<T, INV>(v);
+    else dft3<T, INV>(v);
+    int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) yb[o + r * Ns] = v[r];
+  }
+}
+
+// Batched in-smem FFT.  Data starts in buf[0]; returns the index (0/1) of the
+// buffer that holds the result.  Unnormalised in both directions.  All
+// threads of the block (tid < nthr) must call it; it synchronises.
+template <class T, bool INV>
+__device__ int fft_rows(cpx<T>* buf0, cpx<T>* buf1, int batch, int rs, const FftPlan& pl,
+                        const cpx<T>* __restrict__ tw, int tid, int nthr) {
+  cpx<T>* bufs[2] = {buf0, buf1};
+  int cur = 0;
+  int Ns = 1;
+  for (int s = 0; s < pl.nstages; ++s) {
+    int R = pl.radix[s];
+    if (R == 4) fft_stage<T, INV, 4>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    else if (R == 2) fft_stage<T, INV, 2>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    else fft_stage<T, INV, 3>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    Ns *= R;
+    cur ^= 1;
+    __syncthreads();
+  }
+  return cur;
+}
+
+}  // namespace tc

@@ -1,0 +1,559 @@
+// Time-step kernels: explicit RHS + AB2 update (kernel a), Crank-Nicolson
+// z-diffusion (kernel b), projection + bulk sum + PI forcing (kernel d), CFL
+// and diagnostics reductions, and reference-layout conversions.
+#pragma once
+#include "tc_common.cuh"
+
+namespace tc {
+
+// ---------------------------------------------------------------------------
+// Field accessors (see the layout note in tc_common.cuh)
+// ---------------------------------------------------------------------------
+template <class T> struct Acc {
+  const T* __restrict__ q;
+  int nx, ny, nz;
+  T top;  // sign of the top-wall ghost of u/v: -1 no-slip, +1 free-slip
+  // cell-centred u/v plane k in [-1, nz]
+  __device__ __forceinline__ T c(int k, int j, int i) const {
+    if (k < 0) return -ldg(q + pidx(0, j, i, ny, nx));
+    if (k >= nz) return top * ldg(q + pidx(nz - 1, j, i, ny, nx));
+    return ldg(q + pidx(k, j, i, ny, nx));
+  }
+  // w face f in [0, nz] (walls stored as zeros)
+  __device__ __forceinline__ T f(int k, int j, int i) const { return ldg(q + pidx(k, j, i, ny, nx)); }
+};
+
+template <class T> __device__ __forceinline__ T sq(T a) { return a * a; }
+
+// Scheme of the explicit update.
+enum : int {
+  UPD_AB2 = 0,     // r = rhs + forcing; q* = q + dt(1.5 r - 0.5 r_prev) (Euler without history)
+  UPD_FE = 1,      // q* = q + dt rhs; u gets + dt * 1.0 (solver.py:552-554)
+  UPD_RHS_ONLY = 2 // write rhs (no forcing) to r and stop (operator-level hook)
+};
+
+// ---------------------------------------------------------------------------
+// Kernel (a): fused staggered advection + explicit diffusion + forcing + AB2.
+//
+// Reference: advection_u/v/w (operators.py:126-247), diffusion_xy_u/v/w
+// (:474-548), diffusion_u/v/w (:18-124), compute_momentum_rhs_fused_imex
+// (:1037-1225) and _v2 (:818-1034), AB2 combine solver.py:626-651.
+// FULL=false: IMEX (x/y diffusion only); FULL=true: full Laplacian (AB2/FE).
+// One thread per (i, j, plane k), k in [0, nz]: u/v at cell k < nz and w at
+// face k in [1, nz-1].  Edge planes: internal i = nx-1 is reference u[nx] and
+// j = ny-1 is v[:, ny]; both paths omit advection there, the separate-op path
+// keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
+// ---------------------------------------------------------------------------
+template <class T, bool FULL, int UPD>
+__global__ void __launch_bounds__(256) k_rhs_update(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+                                                    const T* __restrict__ w, T* __restrict__ us,
+                                                    T* __restrict__ vs, T* __restrict__ ws, T* __restrict__ ru,
+                                                    T* __restrict__ rv, T* __restrict__ rw,
+                                                    const double* __restrict__ forcing_dev, T dt, int have_hist) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= nx || j >= ny) return;
+  const T top = g.top_neumann ? T(1) : T(-1);
+  Acc<T> U{u, nx, ny, nz, top}, V{v, nx, ny, nz, top}, W{w, nx, ny, nz, top};
+  const int im = wrap(i - 1, nx), ip = wrap(i + 1, nx);
+  const int jm = wrap(j - 1, ny), jp = wrap(j + 1, ny);
+  const T h = T(0.5);
+  const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
+
+  if (k < nz) {
+    const T idzf = g.idzf[k];
+    // ---------------- u at cell k ----------------
+    {
+      const T U0 = U.c(k, j, i), Uxm = U.c(k, j, im), Uxp = U.c(k, j, ip);
+      const T Uym = U.c(k, jm, i), Uyp = U.c(k, jp, i);
+      const T Uzm = U.c(k - 1, j, i), Uzp = U.c(k + 1, j, i);
+      const bool edge = (i == nx - 1);
+      T r = T(0);
+      if (!(edge && g.rhs_fused)) {
+        r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
+        if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
+      }
+      if (!edge) {
+        const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
+        const T vu_t = h * (V.c(k, j, i) + V.c(k, j, i + 1)) * (h * (U0 + Uyp));
+        const T vu_b = h * (V.c(k, jm, i) + V.c(k, jm, i + 1)) * (h * (Uym + U0));
+        const T wu_t = h * (W.f(k + 1, j, i) + W.f(k + 1, j, i + 1)) * (h * (U0 + Uzp));
+        const T wu_b = h * (W.f(k, j, i) + W.f(k, j, i + 1)) * (h * (Uzm + U0));
+        r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
+      }
+      const size_t o = pidx(k, j, i, ny, nx);
+      if (UPD == UPD_RHS_ONLY) {
+        ru[o] = r;
+      } else if (UPD == UPD_FE) {
+        T q = U0 + dt * r;
+        us[o] = q + dt * T(1);
+      } else {
+        r += forcing;
+        us[o] = have_hist ? U0 + dt * (T(1.5) * r - T(0.5) * ru[o]) : U0 + dt * r;
+        ru[o] = r;
+      }
+    }
+    // ---------------- v at cell k ----------------
+    {
+      const T V0 = V.c(k, j, i), Vxm = V.c(k, j, im), Vxp = V.c(k, j, ip);
+      const T Vym = V.c(k, jm, i), Vyp = V.c(k, jp, i);
+      const T Vzm = V.c(k - 1, j, i), Vzp = V.c(k + 1, j, i);
+      const bool edge = (j == ny - 1);
+      T r = T(0);
+      if (!(edge && g.rhs_fused)) {
+        r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
+        if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
+      }
+      if (!edge) {
+        const T uv_r = h * (U.c(k, j, i) + U.c(k, j + 1, i)) * (h * (V0 + Vxp));
+        const T uv_l = h * (U.c(k, j, im) + U.c(k, j + 1, im)) * (h * (Vxm + V0));
+        const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
+        const T wv_t = h * (W.f(k + 1, j, i) + W.f(k + 1, j + 1, i)) * (h * (V0 + Vzp));
+        const T wv_b = h * (W.f(k, j, i) + W.f(k, j + 1, i)) * (h * (Vzm + V0));
+        r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
+      }
+      const size_t o = pidx(k, j, i, ny, nx);
+      if (UPD == UPD_RHS_ONLY) {
+        rv[o] = r;
+      } else if (UPD == UPD_FE) {
+        vs[o] = V0 + dt * r;
+      } else {
+        vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
+        rv[o] = r;
+      }
+    }
+  }
+  // ---------------- w at face k ----------------
+  if (k >= 1 && k <= nz - 1) {
+    const int f = k;
+    const T W0 = W.f(f, j, i), Wxm = W.f(f, j, im), Wxp = W.f(f, j, ip);
+    const T Wym = W.f(f, jm, i), Wyp = W.f(f, jp, i);
+    const T Wzm = W.f(f - 1, j, i), Wzp = W.f(f + 1, j, i);
+    T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
+    // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+    if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[f] - (W0 - Wzm) * g.idzf[f - 1]) * g.idzc[f - 1];
+    const T uw_r = h * (U.c(f - 1, j, i) + U.c(f, j, i)) * (h * (W0 + Wxp));
+    const T uw_l = h * (U.c(f - 1, j, im) + U.c(f, j, im)) * (h * (Wxm + W0));
+    const T vw_t = h * (V.c(f - 1, j, i) + V.c(f, j, i)) * (h * (W0 + Wyp));
+    const T vw_b = h * (V.c(f - 1, jm, i) + V.c(f, jm, i)) * (h * (Wym + W0));
+    const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[f];
+    r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
+    const size_t o = pidx(f, j, i, ny, nx);
+    if (UPD == UPD_RHS_ONLY) {
+      rw[o] = r;
+    } else if (UPD == UPD_FE) {
+      ws[o] = W0 + dt * r;
+    } else {
+      ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
+      rw[o] = r;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Crank-Nicolson tables.  Row m of a system:
+//   a_m x_{m-1} + b_m x_m + c_m x_{m+1} = q_m + beta (cA_m s_{-1} + cB_m s_0 + cC_m s_{+1})
+// u/v (operators.py:581-644): n = nz rows, row m <-> plane m, explicit
+//   stencil on planes m-1, m, m+1 with the wall closures of :635-644.
+// w (operators.py:753-803): n = nz-1 rows, row m <-> face m+1, explicit
+//   stencil on faces m-1, m, m+1 (the reference's index convention).
+// Thomas factors: inv_den_m = 1/(b_m - a_m cp_{m-1}), cp_m = c_m inv_den_m.
+// Table layout per system: 6 arrays of length nz: a, inv_den, cp, cA, cB, cC.
+// ---------------------------------------------------------------------------
+struct CnTab {
+  double* uv;  // 6*nz
+  double* w;   // 6*nz (first nz-1 rows used)
+  double* beta;
+};
+
+__global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const double* __restrict__ dzc, int nz,
+                            double nu, double dt, int top_neumann) {
+  const double theta = 0.5;
+  const double alpha = theta * dt * nu;
+  const int sys = threadIdx.x;
+  if (sys == 0) {
+    double* a = t.uv; double* iv = a + nz; double* cp = iv + nz;
+    double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
+    double cprev = 0.0;
+    for (int m = 0; m < nz; ++m) {
+      double dl = dzc[m], dr = dzc[m + 1], dc = dzf[m];
+      double lo = -alpha / (dl * dc);
+      double ce = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dc;
+      double up = -alpha / (dr * dc);
+      double am = lo, bm = ce, cm = up;
+      if (m == 0) { am = 0.0; bm = ce - lo; }
+      if (m == nz - 1) { bm = top_neumann ? ce + up : ce - up; cm = 0.0; }
+      double den = bm - am * cprev;
+      double rden = 1.0 / den;
+      a[m] = am; iv[m] = rden; cp[m] = cm * rden; cprev = cp[m];
+      // explicit half (operators.py:635-644)
+      double ea = 1.0 / (dl * dc), eb = -(1.0 / dr + 1.0 / dl) / dc, ec = 1.0 / (dr * dc);
+      if (m == 0) { ea = 0.0; eb = (-1.0 / dr - 2.0 / dl) / dc; }
+      if (m == nz - 1) {
+        if (top_neumann) { eb = -1.0 / (dl * dc); }
+        else { eb = (-2.0 / dr - 1.0 / dl) / dc; }
+        ec = 0.0;
+      }
+      cA[m] = ea; cB[m] = eb; cC[m] = ec;
+    }
+    *t.beta = (1.0 - theta) * dt * nu;
+  } else if (sys == 1) {
+    const int n = nz - 1;
+    double* a = t.w; double* iv = a + nz; double* cp = iv + nz;
+    double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
+    double cprev = 0.0;
+    for (int m = 0; m < n; ++m) {
+      double dl = dzf[m], dr = dzf[m + 1], dcv = dzc[m + 1];
+      double lo = -alpha / (dl * dcv);
+      double ce = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dcv;
+      double up = -alpha / (dr * dcv);
+      double am = (m == 0) ? 0.0 : lo, bm = ce, cm = (m == n - 1) ? 0.0 : up;
+      double den = bm - am * cprev;
+      double rden = 1.0 / den;
+      a[m] = am; iv[m] = rden; cp[m] = cm * rden; cprev = cp[m];
+      double ea = 1.0 / (dl * dcv), eb = -(1.0 / dr + 1.0 / dl) / dcv, ec = 1.0 / (dr * dcv);
+      if (m == 0) ea = 0.0;
+      if (m == n - 1) ec = 0.0;
+      cA[m] = ea; cB[m] = eb; cC[m] = ec;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel (b): batched Thomas solve of the CN systems, one thread per column
+// and component (blockIdx.z = 0 u, 1 v, 2 w).  In place: the forward sweep
+// overwrites each plane with d'_m, the backward sweep with x_m.  Arithmetic in
+// FP64 whatever the storage type.  Replaces solve_implicit_diffusion_u/v/w
+// (operators.py:563-811) whose PCR (tridiag.py:33-58) solves the same systems.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, CnTab t,
+                                                  int nx, int ny, int nz) {
+  extern __shared__ double sh[];
+  const int comp = blockIdx.z;
+  const double* src = comp == 2 ? t.w : t.uv;
+  for (int e = threadIdx.x; e < 6 * nz; e += blockDim.x) sh[e] = src[e];
+  __syncthreads();
+  const double* a = sh; const double* iv = a + nz; const double* cp = iv + nz;
+  const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
+  const double beta = *t.beta;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= nx * ny) return;
+  const size_t plane = (size_t)nx * ny;
+  T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + col;
+  if (comp < 2) {
+    const int n = nz;
+    double qm = 0.0, q0 = (double)q[0];
+    double dprev = 0.0;
+    for (int m = 0; m < n; ++m) {
+      double qn = (m + 1 < n) ? (double)q[(size_t)(m + 1) * plane] : 0.0;
+      double d = q0 + beta * (cA[m] * qm + cB[m] * q0 + cC[m] * qn);
+      double dp = (d - a[m] * dprev) * iv[m];
+      q[(size_t)m * plane] = (T)dp;
+      dprev = dp;
+      qm = q0; q0 = qn;
+    }
+    double x = dprev;
+    q[(size_t)(n - 1) * plane] = (T)x;
+    for (int m = n - 2; m >= 0; --m) {
+      double dp = (double)q[(size_t)m * plane];
+      x = dp - cp[m] * x;
+      q[(size_t)m * plane] = (T)x;
+    }
+  } else {
+    // unknowns at faces 1..nz-1; row m <-> face m+1; explicit stencil on faces m-1, m, m+1
+    const int n = nz - 1;
+    double pm = 0.0, p0 = (double)q[0], p1 = (double)q[plane];
+    double dprev = 0.0;
+    for (int m = 0; m < n; ++m) {
+      double p2 = (m + 2 <= nz - 1) ? (double)q[(size_t)(m + 2) * plane] : 0.0;
+      double d = p1 + beta * (cA[m] * pm + cB[m] * p0 + cC[m] * p1);
+      double dp = (d - a[m] * dprev) * iv[m];
+      q[(size_t)(m + 1) * plane] = (T)dp;
+      dprev = dp;
+      pm = p0; p0 = p1; p1 = p2;
+    }
+    double x = dprev;
+    for (int m = n - 2; m >= 0; --m) {
+      double dp = (double)q[(size_t)(m + 1) * plane];
+      x = dp - cp[m] * x;
+      q[(size_t)(m + 1) * plane] = (T)x;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel (d): projection u -= dt grad p (projection.py:143-165), in place,
+// fused with the per-block partial sums of the bulk velocity
+// (utils.py:207-223, sum of u * dz_f over all DOFs; dx*dy/V applied later).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
+                                                      T* __restrict__ w, const T* __restrict__ p, T dt,
+                                                      const double* __restrict__ dzf,
+                                                      double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double acc = 0.0;
+  if (i < nx && j < ny) {
+    const int ip = wrap(i + 1, nx), jp = wrap(j + 1, ny);
+    if (k < nz) {
+      const T P0 = ldg(p + pidx(k, j, i, ny, nx));
+      const size_t o = pidx(k, j, i, ny, nx);
+      T un = u[o] - dt * ((ldg(p + pidx(k, j, ip, ny, nx)) - P0) * g.idx);
+      u[o] = un;
+      v[o] = v[o] - dt * ((ldg(p + pidx(k, jp, i, ny, nx)) - P0) * g.idy);
+      acc = (double)un * dzf[k];
+    }
+    if (k >= 1 && k <= nz - 1) {
+      const size_t o = pidx(k, j, i, ny, nx);
+      w[o] = w[o] - dt * ((ldg(p + pidx(k, j, i, ny, nx)) - ldg(p + pidx(k - 1, j, i, ny, nx))) * g.idzc[k]);
+    }
+  }
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+}
+
+// Bulk sum over all DOFs without projection (used at set-up and for
+// diagnostics).
+template <class T>
+__global__ void __launch_bounds__(256) k_bulk_partials(Grid<T> g, const T* __restrict__ u,
+                                                       const double* __restrict__ dzf,
+                                                       double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double acc = 0.0;
+  if (i < g.nx && j < g.ny && k < g.nz) acc = (double)u[pidx(k, j, i, g.ny, g.nx)] * dzf[k];
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+}
+
+// Scalars slot layout (FP64, device).
+enum : int {
+  SC_FORCING = 0,
+  SC_UBULK = 1,
+  SC_DTI = 2,
+  SC_MAXDIV = 3,
+  SC_UTAU_BOT = 4,
+  SC_UTAU_TOP = 5,
+  SC_NONFINITE = 6,
+  SC_COUNT = 8
+};
+
+// Deterministic final reduction of the bulk partials and the PI forcing update
+// forcing += (U_b - u_b)/dt * 0.1 (solver.py:701-708).
+__global__ void k_bulk_finalize(const double* __restrict__ partials, int n, double* __restrict__ scal,
+                                double scale, double U_target, double dt, int update_forcing) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) acc += partials[e];
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) {
+    double ub = s * scale;
+    scal[SC_UBULK] = ub;
+    if (update_forcing) scal[SC_FORCING] += (U_target - ub) / dt * 0.1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CFL inverse time scale (operators.py:1232-1333): per-block maxima.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_cfl_partials(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+                                                      const T* __restrict__ w, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double m = 0.0;
+  if (i < nx && j < ny && k < nz) {
+    const double top = g.top_neumann ? 1.0 : -1.0;
+    Acc<T> U{u, nx, ny, nz, (T)top}, V{v, nx, ny, nz, (T)top}, W{w, nx, ny, nz, (T)top};
+    const int im = wrap(i - 1, nx), ip = wrap(i + 1, nx), jm = wrap(j - 1, ny), jp = wrap(j + 1, ny);
+    const double idx = (double)g.idx, idy = (double)g.idy, idzf = (double)g.idzf[k];
+    double ux = fabs((double)U.c(k, j, i));
+    double vx = 0.25 * fabs((double)V.c(k, j, i) + (double)V.c(k, jm, i) + (double)V.c(k, j, ip) + (double)V.c(k, jm, ip));
+    double wx = 0.25 * fabs((double)W.f(k + 1, j, i) + (double)W.f(k, j, i) + (double)W.f(k + 1, j, ip) + (double)W.f(k, j, ip));
+    m = ux * idx + vx * idy + wx * idzf;
+    double uy = 0.25 * fabs((double)U.c(k, j, i) + (double)U.c(k, jp, i) + (double)U.c(k, jp, im) + (double)U.c(k, j, im));
+    double vy = fabs((double)V.c(k, j, i));
+    double wy = 0.25 * fabs((double)W.f(k + 1, j, i) + (double)W.f(k + 1, jp, i) + (double)W.f(k, jp, i) + (double)W.f(k, j, i));
+    m = fmax(m, uy * idx + vy * idy + wy * idzf);
+    if (k < nz - 1) {
+      double uz = 0.25 * fabs((double)U.c(k, j, i) + (double)U.c(k, j, im) + (double)U.c(k + 1, j, im) + (double)U.c(k + 1, j, i));
+      double vz = 0.25 * fabs((double)V.c(k, j, i) + (double)V.c(k, jm, i) + (double)V.c(k + 1, jm, i) + (double)V.c(k + 1, j, i));
+      double wz = fabs((double)W.f(k + 1, j, i));
+      m = fmax(m, uz * idx + vz * idy + wz * (double)g.idzc[k + 1]);
+    }
+  }
+  double r = block_max(m, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = r;
+}
+
+__global__ void k_max_finalize(const double* __restrict__ partials, int n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double m = 0.0;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) m = fmax(m, partials[e]);
+  double r = block_max(m, sh);
+  if (threadIdx.x == 0) *out = r;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics: max |div| (utils.py:226-240), non-finite scan of u, v, w, p
+// (solver.py:865-868) -> per-block partials (max, flag).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_diag_partials(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+                                                       const T* __restrict__ w, const T* __restrict__ p,
+                                                       double* __restrict__ pmax, double* __restrict__ pflag) {
+  __shared__ double sh[32];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double m = 0.0, bad = 0.0;
+  if (i < nx && j < ny && k < nz) {
+    const size_t o = pidx(k, j, i, ny, nx);
+    double du = ((double)u[o] - (double)u[pidx(k, j, wrap(i - 1, nx), ny, nx)]) * (double)g.idx;
+    double dv = ((double)v[o] - (double)v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * (double)g.idy;
+    double dw = ((double)w[pidx(k + 1, j, i, ny, nx)] - (double)w[o]) * (double)g.idzf[k];
+    m = fabs(du + dv + dw);
+    double s = (double)u[o] + (double)v[o] + (double)w[pidx(k + 1, j, i, ny, nx)] + (double)p[o];
+    if (!isfinite(s)) bad = 1.0;
+    if (!isfinite(m)) m = INFINITY;
+  }
+  double r = block_max(m, sh);
+  double b = block_max(bad, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    size_t bi = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    pmax[bi] = r;
+    pflag[bi] = b;
+  }
+}
+
+// Ghost-inclusive plane sum of u (utils.py:187,201 take torch.mean over the
+// whole (nx+1, ny+2) plane, periodic copies included): weights count how many
+// reference entries alias each DOF.  One block per plane (bot, top).
+template <class T>
+__global__ void k_utau_sums(Grid<T> g, const T* __restrict__ u, double* __restrict__ scal) {
+  __shared__ double sh[32];
+  const int nx = g.nx, ny = g.ny;
+  const int k = blockIdx.x == 0 ? 0 : g.nz - 1;
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+    int j = e / nx, i = e - j * nx;
+    double wgt = (i == nx - 1 ? 2.0 : 1.0) * (1.0 + (j == 0 ? 1.0 : 0.0) + (j == ny - 1 ? 1.0 : 0.0));
+    acc += wgt * (double)u[pidx(k, j, i, ny, nx)];
+  }
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) scal[SC_UTAU_BOT + blockIdx.x] = s / ((double)(nx + 1) * (double)(ny + 2));
+}
+
+// ---------------------------------------------------------------------------
+// Reference layout <-> internal layout.
+// Reference arrays are C order (X, Y, Z) with Z fastest.  A 32x32 tile over
+// (x, z) for a fixed y row is staged through shared memory so both sides
+// coalesce.
+// ---------------------------------------------------------------------------
+enum : int { FLD_U = 0, FLD_V = 1, FLD_W = 2, FLD_P = 3, FLD_CELL = 4 };
+
+// Gather the DOFs of a reference array into the internal layout.
+// FLD_U/V: ref (Xr, Yr, nz+2) -> internal [nz][ny][nx] = ref[i+1, j+1, k+1]
+// FLD_W:   ref (nx+2, ny+2, nz+1) -> internal [nz+1][ny][nx] = ref[i+1, j+1, k]
+//          (wall planes written as 0)
+// FLD_CELL: ref (nx, ny, nz) -> internal [nz][ny][nx] = ref[i, j, k] * scale
+template <class T>
+__global__ void k_from_ref(const double* __restrict__ ref, T* __restrict__ out, int kind, int nx, int ny, int nz,
+                           double scale) {
+  __shared__ double tile[32][33];
+  const int j = blockIdx.y;
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.z * 32;
+  int Yr, Zr, ox, oy, oz, NK;
+  switch (kind) {
+    case FLD_U: Yr = ny + 2; Zr = nz + 2; ox = 1; oy = 1; oz = 1; NK = nz; break;
+    case FLD_V: Yr = ny + 1; Zr = nz + 2; ox = 1; oy = 1; oz = 1; NK = nz; break;
+    case FLD_W: Yr = ny + 2; Zr = nz + 1; ox = 1; oy = 1; oz = 0; NK = nz + 1; break;
+    default: Yr = ny; Zr = nz; ox = 0; oy = 0; oz = 0; NK = nz; break;
+  }
+  // read: threadIdx.x along z (contiguous in ref)
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int i = i0 + r, k = k0 + threadIdx.x;
+    double val = 0.0;
+    if (i < nx && k < NK) val = ref[((size_t)(i + ox) * Yr + (j + oy)) * Zr + (k + oz)] * scale;
+    tile[r][threadIdx.x] = val;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int k = k0 + r, i = i0 + threadIdx.x;
+    if (i < nx && k < NK) {
+      double val = tile[threadIdx.x][r];
+      if (kind == FLD_W && (k == 0 || k == nz)) val = 0.0;
+      out[pidx(k, j, i, ny, nx)] = (T)val;
+    }
+  }
+}
+
+// Materialise a full reference array (ghosts included) from the internal
+// layout, with the ghost rules of apply_bc_all (solver.py:23-79) and of the
+// pressure ghost fill (projection_fft.py:148-163).
+template <class T>
+__global__ void k_to_ref(const T* __restrict__ in, double* __restrict__ ref, int kind, int nx, int ny, int nz,
+                         int top_neumann) {
+  __shared__ double tile[32][33];
+  int Xr, Yr, Zr;
+  switch (kind) {
+    case FLD_U: Xr = nx + 1; Yr = ny + 2; Zr = nz + 2; break;
+    case FLD_V: Xr = nx + 2; Yr = ny + 1; Zr = nz + 2; break;
+    case FLD_W: Xr = nx + 2; Yr = ny + 2; Zr = nz + 1; break;
+    case FLD_P: Xr = nx + 2; Yr = ny + 2; Zr = nz + 2; break;
+    default: Xr = nx; Yr = ny; Zr = nz; break;
+  }
+  const int J = blockIdx.y;
+  const int I0 = blockIdx.x * 32, K0 = blockIdx.z * 32;
+  // internal row index for J
+  int j;
+  if (kind == FLD_CELL) j = J;
+  else if (kind == FLD_V) j = (J == 0) ? ny - 1 : J - 1;
+  else j = (J == 0) ? ny - 1 : (J == ny + 1 ? 0 : J - 1);
+  const double top = top_neumann ? 1.0 : -1.0;
+  // read internal: threadIdx.x along x
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int K = K0 + r, I = I0 + threadIdx.x;
+    double val = 0.0;
+    if (I < Xr && K < Zr) {
+      int i;
+      if (kind == FLD_CELL) i = I;
+      else if (kind == FLD_U) i = (I == 0) ? nx - 1 : I - 1;
+      else i = (I == 0) ? nx - 1 : (I == nx + 1 ? 0 : I - 1);
+      if (kind == FLD_W || kind == FLD_CELL) {
+        val = (double)in[pidx(K, j, i, ny, nx)];
+      } else if (kind == FLD_P) {
+        int k = K == 0 ? 0 : (K == nz + 1 ? nz - 1 : K - 1);
+        val = (double)in[pidx(k, j, i, ny, nx)];
+      } else {
+        if (K == 0) val = -(double)in[pidx(0, j, i, ny, nx)];
+        else if (K == nz + 1) val = top * (double)in[pidx(nz - 1, j, i, ny, nx)];
+        else val = (double)in[pidx(K - 1, j, i, ny, nx)];
+      }
+    }
+    tile[r][threadIdx.x] = val;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int I = I0 + r, K = K0 + threadIdx.x;
+    if (I < Xr && K < Zr) ref[((size_t)I * Yr + J) * Zr + K] = tile[threadIdx.x][r];
+  }
+}
+
+}  // namespace tc
