@@ -145,6 +145,21 @@ int tc_implicit_diffusion(tc_ctx* ctx, double dt, void* stream);
  * a constant).  Uses the context's workspace; the state is not touched. */
 int tc_poisson_solve(tc_ctx* ctx, const double* rhs, double* p, void* stream);
 
+/* Same solve as tc_poisson_solve for callers that cannot allocate device
+ * memory (their device memory belongs to a host application's own pool, or
+ * they must not risk the device-wide synchronisation of cudaMalloc/cudaFree):
+ * no context, no workspace, and no allocation of any kind.  No counterpart in
+ * the reference.  dz_f (nz) and dz_c (nz+1) are DEVICE arrays; rhs and p as in
+ * tc_poisson_solve; FP64.  The scratch is one static 64 MiB array in device
+ * memory per GPU that loads the library, held until the process exits; grids
+ * needing more (about nx*ny*nz*16 bytes, e.g. above 128x128x128) get
+ * TC_ERR_SIZE.  The first call on each device looks the array up and sets
+ * kernel attributes there: make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU (other streams,
+ * other host threads) race; serialise them. */
+int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, double Ly, const double* dz_f,
+                             const double* dz_c, const double* rhs, double* p, void* stream);
+
 /* Velocity correction with a given p (reference layout, device)
  * (project_velocity, projection.py:143-165). */
 int tc_project(tc_ctx* ctx, const double* p, double dt, void* stream);

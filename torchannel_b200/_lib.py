@@ -52,6 +52,7 @@ SIGNATURES = [
     ("tc_explicit_rhs", _I, [_V, _I, _V, _V, _V, _V]),
     ("tc_implicit_diffusion", _I, [_V, _D, _V]),
     ("tc_poisson_solve", _I, [_V, _V, _V, _V]),
+    ("tc_poisson_solve_noalloc", _I, [_I, _I, _I, _D, _D, _V, _V, _V, _V, _V]),
     ("tc_project", _I, [_V, _V, _D, _V]),
     ("tc_stats_init", _I, [_V, _dp, _D, _D, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     ("tc_stats_accumulate", _I, [_V, _V]),

@@ -855,3 +855,137 @@ extern "C" int tc_error(tc_ctx* c, int* code) {
   TC_CUDA(cudaMemset(c->err, 0, sizeof(int)));
   return TC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Poisson solve that allocates nothing (tc_poisson_solve_noalloc).
+//
+// Some callers cannot hand this library a workspace: a host application whose
+// device memory is owned by its own pool manager and forbids direct
+// cudaMalloc / cudaFree, or a latency-critical loop that must not pay the
+// device-wide synchronisation a cudaMalloc / cudaFree can cause.  For them the
+// spectral intermediate and the small tables live in one fixed-size array in
+// device global memory that the library owns for the life of the process.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define TC_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define TC_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char tc_noalloc_scratch[TC_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[TC_NOALLOC_MAX_DEVICES];
+
+// The host-side name tc_noalloc_scratch is not a device address: look the
+// address up once per device (with that device current) and pass it on.
+static int noalloc_setup(int dev, unsigned char** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, tc_noalloc_scratch);
+    if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    int r = set_smem_attrs<double>(nullptr);
+    if (r) return r;
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *out = (unsigned char*)g_noalloc_ptr[dev];
+  return TC_OK;
+}
+
+// Poisson tables from the grid (same definitions as tc_create's host tables:
+// projection_fft.py:26-82), computed on the device so that nothing is copied
+// from host memory.
+__global__ void k_noalloc_tables(int nx, int ny, int nz, double dx, double dy, const double* __restrict__ dzf,
+                                 const double* __restrict__ dzc, double* k2x, double* k2y, double* cl, double* cr,
+                                 cpx<double>* twx, cpx<double>* twy) {
+  const int nxh = nx / 2 + 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nxh + ny + nz + nx + ny; e += gridDim.x * blockDim.x) {
+    int m = e;
+    if (m < nxh) {
+      double s = sinpi((double)m / (double)nx) * (2.0 / dx);
+      k2x[m] = s * s;
+      continue;
+    }
+    m -= nxh;
+    if (m < ny) {
+      double s = sinpi((double)m / (double)ny) * (2.0 / dy);
+      k2y[m] = s * s;
+      continue;
+    }
+    m -= ny;
+    if (m < nz) {
+      cl[m] = 1.0 / (dzc[m] * dzf[m]);
+      cr[m] = 1.0 / (dzc[m + 1] * dzf[m]);
+      continue;
+    }
+    m -= nz;
+    if (m < nx) {
+      double s, c;
+      sincospi(-2.0 * (double)m / (double)nx, &s, &c);
+      twx[m] = cpx<double>{c, s};
+      continue;
+    }
+    m -= nx;
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)ny, &s, &c);
+    twy[m] = cpx<double>{c, s};
+  }
+}
+
+static size_t noalloc_bytes(int nx, int ny, int nz, size_t off[8]) {
+  const size_t nxh = nx / 2 + 1;
+  // field (rhs in, p out), spectrum, k2x, k2y, cl, cr, x and y twiddles
+  const size_t sz[8] = {(size_t)nx * ny * nz * 8, nxh * nz * ny * 16, nxh * 8, (size_t)ny * 8,
+                        (size_t)nz * 8, (size_t)nz * 8, (size_t)nx * 16, (size_t)ny * 16};
+  size_t o = 0;
+  for (int e = 0; e < 8; ++e) {
+    o = (o + 255) & ~(size_t)255;
+    off[e] = o;
+    o += sz[e];
+  }
+  return o;
+}
+
+extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, double Ly, const double* dz_f,
+                                        const double* dz_c, const double* rhs, double* p, void* stream) {
+  if (!dz_f || !dz_c || !rhs || !p) return fail(TC_ERR_ARG, "null argument");
+  if (nx < 4 || ny < 4 || nz < 4 || (nx & 1) || (ny & 1) || nz > 800 || !(Lx > 0) || !(Ly > 0))
+    return fail(TC_ERR_SIZE, "nx, ny even >= 4, 4 <= nz <= 800, Lx, Ly > 0 required");
+  FftPlan a, b;
+  if (!fft_make_plan(nx, &a) || !fft_make_plan(ny, &b) || nx > 4096 || ny > 4096)
+    return fail(TC_ERR_SIZE, "nx and ny must factor into 2 and 3 only (<= 4096)");
+  size_t off[8];
+  const size_t need = noalloc_bytes(nx, ny, nz, off);
+  if (need > TC_NOALLOC_SCRATCH_BYTES)
+    return fail(TC_ERR_SIZE, "grid needs " + std::to_string(need) + " bytes of scratch; the static maximum is " +
+                                 std::to_string((size_t)TC_NOALLOC_SCRATCH_BYTES) + " bytes");
+  int dev = 0;
+  TC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= TC_NOALLOC_MAX_DEVICES) return fail(TC_ERR_ARG, "device index out of range");
+  unsigned char* base = nullptr;
+  int rc = noalloc_setup(dev, &base);
+  if (rc) return rc;
+  cudaStream_t s = ST(stream);
+  // a context view over the static scratch (launch shapes as tc_create picks them)
+  tc_grid_desc g{};
+  g.nx = nx; g.ny = ny; g.nz = nz; g.Lx = Lx; g.Ly = Ly; g.Lz = 1.0; g.nu = 1.0; g.precision = TC_FP64;
+  tc_ctx c{};
+  fill_basic(&c, &g);
+  double* field = (double*)(base + off[0]);
+  c.X = base + off[1];
+  c.dps = (cpx<double>*)c.X;
+  c.k2x = (double*)(base + off[2]); c.k2y = (double*)(base + off[3]);
+  c.cl = (double*)(base + off[4]); c.cr = (double*)(base + off[5]);
+  c.twx_t = base + off[6]; c.twy_t = base + off[7];
+  const int ntab = c.nxh + ny + nz + nx + ny;
+  k_noalloc_tables<<<(ntab + 255) / 256, 256, 0, s>>>(nx, ny, nz, c.dx, c.dy, dz_f, dz_c, c.k2x, c.k2y, c.cl, c.cr,
+                                                     (cpx<double>*)c.twx_t, (cpx<double>*)c.twy_t);
+  k_from_ref<double><<<dim3((nx + 31) / 32, ny, (nz + 31) / 32), dim3(32, 8), 0, s>>>(rhs, field, FLD_CELL, nx, ny,
+                                                                                        nz, 1.0);
+  TC_LAUNCHED();
+  // every pass overwrites what it reads next, so no buffer needs clearing;
+  // the solve writes p over the consumed right-hand side
+  rc = poisson_impl<double>(&c, nullptr, nullptr, nullptr, field, field, 1.0 / ((double)nx * (double)ny), s);
+  if (rc) return rc;
+  return to_ref<double>(&c, field, p, FLD_P, s);
+}
