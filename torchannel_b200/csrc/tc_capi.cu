@@ -60,11 +60,11 @@ struct tc_ctx {
   // device buffers (storage type T unless noted)
   void* st[2][3];
   void* rh[3];
-  void* p;
-  void* X;
-  cpx<double>* dps;      // FP64 scratch for the Poisson forward sweep
+  double* p;             // pressure, FP64 in both precisions
+  cpx<double>* X;        // spectral intermediate, FP64 in both precisions
   void* idzf_t; void* idzc_t;
-  void* twx_t; void* twy_t;
+  double* ubase_d; void* ubase_t;  // base profile of u (mixed precision)
+  unsigned int* ticket;  // last-block counter of k_project_bulk
   double* dzf_d; double* dzc_d;
   double* k2x; double* k2y; double* cl; double* cr;
   cpx<double>* twx_d; cpx<double>* twy_d;
@@ -101,6 +101,9 @@ template <class T> static Grid<T> make_grid(const tc_ctx* c, int which_unused = 
   g.nu = (T)c->nu;
   g.idzf = (const T*)c->idzf_t; g.idzc = (const T*)c->idzc_t;
   g.top_neumann = c->top_neumann; g.rhs_fused = c->rhs_fused;
+  const bool mixed = c->precision == TC_MIXED;
+  g.ubase_t = mixed ? (const T*)c->ubase_t : nullptr;
+  g.ubase_d = mixed ? c->ubase_d : nullptr;
   return g;
 }
 
@@ -117,14 +120,14 @@ static size_t carve(tc_ctx* c, char* base) {
   c->rh[0] = cv.take<char>(ncell * T_);
   c->rh[1] = cv.take<char>(ncell * T_);
   c->rh[2] = cv.take<char>(nface * T_);
-  c->p = cv.take<char>(ncell * T_);
+  c->p = cv.take<double>(ncell * 8);
   const size_t nspec = (size_t)c->nxh * c->nz * c->ny;
-  c->X = cv.take<char>(nspec * 2 * T_);
-  c->dps = (c->precision == TC_FP64) ? (cpx<double>*)c->X : cv.take<cpx<double>>(nspec * sizeof(cpx<double>));
+  c->X = cv.take<cpx<double>>(nspec * 16);
   c->idzf_t = cv.take<char>(c->nz * T_);
   c->idzc_t = cv.take<char>((c->nz + 1) * T_);
-  c->twx_t = cv.take<char>(c->nx * 2 * T_);
-  c->twy_t = cv.take<char>(c->ny * 2 * T_);
+  c->ubase_d = cv.take<double>(c->nz * 8);
+  c->ubase_t = cv.take<char>(c->nz * T_);
+  c->ticket = cv.take<unsigned int>(256);
   c->dzf_d = cv.take<double>(c->nz * 8);
   c->dzc_d = cv.take<double>((c->nz + 1) * 8);
   c->k2x = cv.take<double>(c->nxh * 8);
@@ -206,10 +209,10 @@ extern "C" int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes) {
 template <class T> static int set_smem_attrs(const tc_ctx* c) {
   const int big = 200 * 1024;
   TC_CUDA(cudaFuncSetAttribute(k_div_fftx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_ifftx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_ffty<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_ffty<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_ifftx, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_ffty<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_ffty<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -283,7 +286,6 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
   std::vector<double> twx = twiddles(c->nx), twy = twiddles(c->ny);
   int r2 = TC_OK;
   if ((r2 = upload(c->idzf_t, idzf, c->tsz)) || (r2 = upload(c->idzc_t, idzc, c->tsz)) ||
-      (r2 = upload(c->twx_t, twx, c->tsz)) || (r2 = upload(c->twy_t, twy, c->tsz)) ||
       (r2 = upload(c->dzf_d, c->dzf, 8)) || (r2 = upload(c->dzc_d, c->dzc, 8)) ||
       (r2 = upload(c->k2x, k2x, 8)) || (r2 = upload(c->k2y, k2y, 8)) || (r2 = upload(c->cl, cl, 8)) ||
       (r2 = upload(c->cr, cr, 8)) || (r2 = upload(c->twx_d, twx, 8)) || (r2 = upload(c->twy_d, twy, 8)))
@@ -307,21 +309,34 @@ extern "C" int tc_destroy(tc_ctx* ctx) {
 #define ST(c) ((cudaStream_t)(c))
 
 // ---------------------------------------------------------------------------
-// Typed implementations
+// Typed implementations (T = storage type of the velocity fields)
 // ---------------------------------------------------------------------------
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, int n) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) b[e] = (float)a[e];
+}
+
 template <class T> static int set_state_impl(tc_ctx* c, const double* u, const double* v, const double* w, cudaStream_t s) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
   dim3 blk(32, 8);
   dim3 gc((nx + 31) / 32, ny, (nz + 31) / 32), gf((nx + 31) / 32, ny, (nz + 1 + 31) / 32);
   T** S = (T**)c->st[c->cur];
-  k_from_ref<T><<<gc, blk, 0, s>>>(u, S[0], FLD_U, nx, ny, nz, 1.0);
-  k_from_ref<T><<<gc, blk, 0, s>>>(v, S[1], FLD_V, nx, ny, nz, 1.0);
-  k_from_ref<T><<<gf, blk, 0, s>>>(w, S[2], FLD_W, nx, ny, nz, 1.0);
+  const double* base = nullptr;
+  if (c->precision == TC_MIXED) {
+    // base profile = per-plane mean of the incoming u; u is stored as u - U0[k]
+    k_plane_mean_ref_u<<<nz, 256, 0, s>>>(u, nx, ny, nz, c->ubase_d);
+    k_d2f<<<(nz + 255) / 256, 256, 0, s>>>(c->ubase_d, (float*)c->ubase_t, nz);
+    base = c->ubase_d;
+  }
+  k_from_ref<T><<<gc, blk, 0, s>>>(u, S[0], FLD_U, nx, ny, nz, 1.0, base);
+  k_from_ref<T><<<gc, blk, 0, s>>>(v, S[1], FLD_V, nx, ny, nz, 1.0, nullptr);
+  k_from_ref<T><<<gf, blk, 0, s>>>(w, S[2], FLD_W, nx, ny, nz, 1.0, nullptr);
   TC_LAUNCHED();
   return TC_OK;
 }
 
-template <class T> static int to_ref(const tc_ctx* c, const T* in, double* out, int kind, cudaStream_t s) {
+template <class T> static int to_ref(const tc_ctx* c, const T* in, double* out, int kind, cudaStream_t s,
+                                     const double* base = nullptr) {
   int Xr, Zr;
   switch (kind) {
     case FLD_U: Xr = c->nx + 1; Zr = c->nz + 2; break;
@@ -332,49 +347,47 @@ template <class T> static int to_ref(const tc_ctx* c, const T* in, double* out, 
   }
   int Yr = (kind == FLD_U || kind == FLD_W || kind == FLD_P) ? c->ny + 2 : (kind == FLD_V ? c->ny + 1 : c->ny);
   dim3 grid((Xr + 31) / 32, Yr, (Zr + 31) / 32);
-  k_to_ref<T><<<grid, dim3(32, 8), 0, s>>>(in, out, kind, c->nx, c->ny, c->nz, c->top_neumann);
+  k_to_ref<T><<<grid, dim3(32, 8), 0, s>>>(in, out, kind, c->nx, c->ny, c->nz, c->top_neumann, base);
   TC_LAUNCHED();
   return TC_OK;
 }
 
-template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, const T* w, const T* field, T* p,
-                                           double scale, cudaStream_t s) {
+static const double* ubase_of(const tc_ctx* c) { return c->precision == TC_MIXED ? c->ubase_d : nullptr; }
+
+// Poisson solve of L p = scale * (div(u, v, w) or field): spectrum and p FP64.
+// `field` and `p` may alias (the field is consumed by the first pass).
+template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, const T* w, const double* field,
+                                           double* p, double scale, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
   const int nx = c->nx, ny = c->ny, nz = c->nz, nxh = c->nxh;
-  cpx<T>* X = (cpx<T>*)c->X;
-  const size_t smx = (size_t)2 * (c->JT / 2) * (nx + 2) * sizeof(cpx<T>);
+  cpx<double>* X = c->X;
+  const size_t smx = (size_t)2 * (c->JT / 2) * (nx + 2) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTX, s);
-  k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, (const cpx<T>*)c->twx_t,
-                                                        (T)scale, c->JT);
+  k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, c->twx_d, scale, c->JT);
   const int nrows = nxh * nz;
-  const size_t smy = (size_t)2 * c->RB * ny * sizeof(cpx<T>);
+  const size_t smy = (size_t)2 * c->RB * ny * sizeof(cpx<double>);
   mark(c, TC_PH_FFTY, s);
-  k_ffty<T, false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, (const cpx<T>*)c->twy_t, c->RB);
+  k_ffty<false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
   const int nmodes = nxh * ny;
   mark(c, TC_PH_TRI, s);
-  k_tri<T><<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, c->dps, tb, nxh, ny, nz);
+  k_tri<<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, tb, nxh, ny, nz);
   mark(c, TC_PH_IFFTY, s);
-  k_ffty<T, true><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, (const cpx<T>*)c->twy_t, c->RB);
+  k_ffty<true><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   mark(c, TC_PH_IFFTX, s);
-  k_ifftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, (const cpx<T>*)c->twx_t, c->JT);
+  k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
   TC_LAUNCHED();
   return TC_OK;
 }
 
 static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, planes); }
 
-template <class T> static int bulk_finalize(tc_ctx* c, double dt, int update, cudaStream_t s) {
-  const double scale = c->dx * c->dy / (c->Lx * c->Ly * c->Lz);
-  k_bulk_finalize<<<1, 256, 0, s>>>(c->partials, c->npart, c->scal, scale, c->U_bulk, dt, update);
-  TC_LAUNCHED();
-  return TC_OK;
-}
+static double bulk_scale(const tc_ctx* c) { return c->dx * c->dy / (c->Lx * c->Ly * c->Lz); }
 
-template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, cudaStream_t s) {
+template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, int update_forcing, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
-  k_project_bulk<T><<<grid3(c, c->nz + 1), dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], (const T*)c->p, (T)dt, c->dzf_d,
-                                                                c->partials);
+  BulkArgs ba{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, update_forcing};
+  k_project_bulk<T><<<grid3(c, c->nz + 1), dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt, c->dzf_d, ba);
   TC_LAUNCHED();
   return TC_OK;
 }
@@ -405,15 +418,15 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   mark(c, TC_PH_CN, s);
   if (scheme == TC_IMEX) {
     const int ncol = c->nx * c->ny;
-    k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 6 * c->nz * 8, s>>>(B[0], B[1], B[2], c->tab, c->nx, c->ny, c->nz);
+    k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 7 * c->nz * 8, s>>>(B[0], B[1], B[2], c->tab, ubase_of(c),
+                                                                             c->nx, c->ny, c->nz);
     TC_LAUNCHED();
   }
-  int rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, (T*)c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
+  int rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
   if (rc) return rc;
   mark(c, TC_PH_PROJ, s);
-  if ((rc = project_impl<T>(c, B, dt, s))) return rc;
+  if ((rc = project_impl<T>(c, B, dt, scheme != TC_FE, s))) return rc;
   mark(c, TC_PH_FIN, s);
-  if ((rc = bulk_finalize<T>(c, dt, scheme != TC_FE, s))) return rc;
   mark(c, TC_NPHASE, s);
   if (c->timing) {
     c->t_head = (c->t_head + 1) % TC_TIMING_RING;
@@ -426,19 +439,19 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
 
 template <class T> static int project_initial_impl(tc_ctx* c, cudaStream_t s) {
   T** A = (T**)c->st[c->cur];
-  int rc = poisson_impl<T>(c, A[0], A[1], A[2], nullptr, (T*)c->p, 1.0 / ((double)c->nx * (double)c->ny), s);
+  int rc = poisson_impl<T>(c, A[0], A[1], A[2], nullptr, c->p, 1.0 / ((double)c->nx * (double)c->ny), s);
   if (rc) return rc;
-  if ((rc = project_impl<T>(c, A, 1.0, s))) return rc;
-  return bulk_finalize<T>(c, 1.0, 0, s);
+  return project_impl<T>(c, A, 1.0, 0, s);
 }
 
 template <class T> static int bulk_impl(tc_ctx* c, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
   T** A = (T**)c->st[c->cur];
-  cudaMemsetAsync(c->partials, 0, (size_t)c->npart * 8, s);
-  k_bulk_partials<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(g, A[0], c->dzf_d, c->partials);
+  dim3 grd = grid3(c, c->nz);
+  k_bulk_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], c->dzf_d, c->partials);
+  k_bulk_finalize<<<1, 256, 0, s>>>(c->partials, grd.x * grd.y * grd.z, c->scal, bulk_scale(c), c->U_bulk, 1.0, 0);
   TC_LAUNCHED();
-  return bulk_finalize<T>(c, 1.0, 0, s);
+  return TC_OK;
 }
 
 template <class T> static int cfl_impl(tc_ctx* c, cudaStream_t s) {
@@ -457,7 +470,7 @@ template <class T> static int diag_impl(tc_ctx* c, cudaStream_t s) {
   dim3 grd = grid3(c, c->nz);
   const int nb = grd.x * grd.y * grd.z;
   // nb = gx*gy*nz <= npart: one partials buffer each for the max and the flag
-  k_diag_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], (const T*)c->p, c->partials2, c->partials);
+  k_diag_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], c->p, c->partials2, c->partials);
   k_max_finalize<<<1, 256, 0, s>>>(c->partials2, nb, c->scal + SC_MAXDIV);
   k_max_finalize<<<1, 256, 0, s>>>(c->partials, nb, c->scal + SC_NONFINITE);
   k_utau_sums<T><<<2, 256, 0, s>>>(g, A[0], c->scal);
@@ -468,9 +481,9 @@ template <class T> static int diag_impl(tc_ctx* c, cudaStream_t s) {
 template <class T> static int stats_impl(tc_ctx* c, cudaStream_t s) {
   T** A = (T**)c->st[c->cur];
   const int nx = c->nx, ny = c->ny, nz = c->nz;
-  k_stats_prof<T><<<nz, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, c->st_prof, c->st_means);
+  k_stats_prof<T><<<nz, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, ubase_of(c), c->st_prof, c->st_means);
   k_stats_fill<T><<<(nx * ny + 255) / 256, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, c->k_bot - 1, c->k_top - 1,
-                                                        c->st_means, c->st_S);
+                                                        ubase_of(c), c->st_means, c->st_S);
   const int nrows = 3 * ny;
   k_fft_rows_d<false><<<(nrows + c->stats_RB - 1) / c->stats_RB, 256, (size_t)2 * c->stats_RB * nx * 16, s>>>(
       c->st_S, nrows, nx, c->planx, c->twx_d, c->stats_RB);
@@ -516,7 +529,7 @@ extern "C" int tc_set_state(tc_ctx* c, const double* u, const double* v, const d
   TC_CUDA(cudaMemsetAsync(c->scal, 0, SC_COUNT * 8, ST(stream)));
   rc = tc_set_forcing(c, forcing, stream);
   if (rc) return rc;
-  TC_CUDA(cudaMemsetAsync(c->p, 0, (size_t)c->nx * c->ny * c->nz * c->tsz, ST(stream)));
+  TC_CUDA(cudaMemsetAsync(c->p, 0, (size_t)c->nx * c->ny * c->nz * 8, ST(stream)));
   c->have_hist = 0;
   c->state_set = 1;
   return TC_OK;
@@ -530,23 +543,20 @@ extern "C" int tc_set_forcing(tc_ctx* c, double forcing, void* stream) {
   return TC_OK;
 }
 
+template <class T> static int get_state_impl(tc_ctx* c, double* u, double* v, double* w, double* p, cudaStream_t s) {
+  int rc = TC_OK;
+  T** A = (T**)c->st[c->cur];
+  if (u && (rc = to_ref<T>(c, A[0], u, FLD_U, s, ubase_of(c)))) return rc;
+  if (v && (rc = to_ref<T>(c, A[1], v, FLD_V, s))) return rc;
+  if (w && (rc = to_ref<T>(c, A[2], w, FLD_W, s))) return rc;
+  if (p && (rc = to_ref<double>(c, c->p, p, FLD_P, s))) return rc;
+  return TC_OK;
+}
+
 extern "C" int tc_get_state(tc_ctx* c, double* u, double* v, double* w, double* p, void* stream) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
   if (!c->state_set) return fail(TC_ERR_STATE, "no state");
-  int rc = TC_OK;
-  void** A = c->st[c->cur];
-  if (c->tsz == 8) {
-    if (u && (rc = to_ref<double>(c, (double*)A[0], u, FLD_U, ST(stream)))) return rc;
-    if (v && (rc = to_ref<double>(c, (double*)A[1], v, FLD_V, ST(stream)))) return rc;
-    if (w && (rc = to_ref<double>(c, (double*)A[2], w, FLD_W, ST(stream)))) return rc;
-    if (p && (rc = to_ref<double>(c, (double*)c->p, p, FLD_P, ST(stream)))) return rc;
-  } else {
-    if (u && (rc = to_ref<float>(c, (float*)A[0], u, FLD_U, ST(stream)))) return rc;
-    if (v && (rc = to_ref<float>(c, (float*)A[1], v, FLD_V, ST(stream)))) return rc;
-    if (w && (rc = to_ref<float>(c, (float*)A[2], w, FLD_W, ST(stream)))) return rc;
-    if (p && (rc = to_ref<float>(c, (float*)c->p, p, FLD_P, ST(stream)))) return rc;
-  }
-  return TC_OK;
+  return DISPATCH(c, get_state_impl, c, u, v, w, p, ST(stream));
 }
 
 template <class T> static int get_hist_impl(tc_ctx* c, double* ru, double* rv, double* rw, cudaStream_t s) {
@@ -563,9 +573,9 @@ template <class T> static int set_hist_impl(tc_ctx* c, const double* ru, const d
   dim3 blk(32, 8);
   dim3 gc((nx + 31) / 32, ny, (nz + 31) / 32), gf((nx + 31) / 32, ny, (nz + 1 + 31) / 32);
   T** R = (T**)c->rh;
-  k_from_ref<T><<<gc, blk, 0, s>>>(ru, R[0], FLD_U, nx, ny, nz, 1.0);
-  k_from_ref<T><<<gc, blk, 0, s>>>(rv, R[1], FLD_V, nx, ny, nz, 1.0);
-  k_from_ref<T><<<gf, blk, 0, s>>>(rw, R[2], FLD_W, nx, ny, nz, 1.0);
+  k_from_ref<T><<<gc, blk, 0, s>>>(ru, R[0], FLD_U, nx, ny, nz, 1.0, nullptr);
+  k_from_ref<T><<<gc, blk, 0, s>>>(rv, R[1], FLD_V, nx, ny, nz, 1.0, nullptr);
+  k_from_ref<T><<<gf, blk, 0, s>>>(rw, R[2], FLD_W, nx, ny, nz, 1.0, nullptr);
   TC_LAUNCHED();
   return TC_OK;
 }
@@ -618,8 +628,6 @@ static int read_scal(tc_ctx* c, double* host, cudaStream_t s) {
 extern "C" int tc_bulk_velocity(tc_ctx* c, double* out, void* stream) {
   if (!c || !out) return fail(TC_ERR_ARG, "null argument");
   if (!c->state_set) return fail(TC_ERR_STATE, "no state");
-  // keep the step's u_bulk slot: compute into it, read, then restore is not
-  // needed because the slot always holds the bulk velocity of the state.
   int rc = DISPATCH(c, bulk_impl, c, ST(stream));
   if (rc) return rc;
   double h[SC_COUNT];
@@ -665,22 +673,27 @@ extern "C" int tc_diagnostics(tc_ctx* c, double* out, void* stream) {
 
 template <class T>
 __global__ void k_div_field(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w,
-                            T* __restrict__ out) {
+                            double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   const int nx = g.nx, ny = g.ny;
   const size_t o = pidx(k, j, i, ny, nx);
-  out[o] = (u[o] - u[pidx(k, j, wrap(i - 1, nx), ny, nx)]) * g.idx + (v[o] - v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * g.idy +
-           (w[pidx(k + 1, j, i, ny, nx)] - w[o]) * g.idzf[k];
+  out[o] = ((double)u[o] - (double)u[pidx(k, j, wrap(i - 1, nx), ny, nx)]) * (double)g.idx +
+           ((double)v[o] - (double)v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * (double)g.idy +
+           ((double)w[pidx(k + 1, j, i, ny, nx)] - (double)w[o]) * (double)g.idzf[k];
 }
+
+// The next state buffer is free between steps; its u, v, w regions are
+// carved back to back, so its start holds nx*ny*nz doubles in either precision.
+static double* scratch_field(tc_ctx* c) { return (double*)c->st[c->cur ^ 1][0]; }
 
 template <class T> static int divergence_impl(tc_ctx* c, double* div, cudaStream_t s) {
   T** A = (T**)c->st[c->cur];
-  T** B = (T**)c->st[c->cur ^ 1];
   Grid<T> g = make_grid<T>(c);
-  k_div_field<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], B[0]);
+  double* f = scratch_field(c);
+  k_div_field<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], f);
   TC_LAUNCHED();
-  return to_ref<T>(c, B[0], div, FLD_CELL, s);
+  return to_ref<double>(c, f, div, FLD_CELL, s);
 }
 
 extern "C" int tc_divergence(tc_ctx* c, double* div, void* stream) {
@@ -702,7 +715,8 @@ template <class T> static int cn_hook_impl(tc_ctx* c, double dt, cudaStream_t s)
     c->tab_dt = dt;
   }
   const int ncol = c->nx * c->ny;
-  k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 6 * c->nz * 8, s>>>(A[0], A[1], A[2], c->tab, c->nx, c->ny, c->nz);
+  k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 7 * c->nz * 8, s>>>(A[0], A[1], A[2], c->tab, ubase_of(c),
+                                                                           c->nx, c->ny, c->nz);
   TC_LAUNCHED();
   return TC_OK;
 }
@@ -715,15 +729,16 @@ extern "C" int tc_implicit_diffusion(tc_ctx* c, double dt, void* stream) {
 }
 
 template <class T> static int poisson_hook_impl(tc_ctx* c, const double* rhs, double* p, cudaStream_t s) {
-  // rhs -> internal cell layout in the pressure buffer of the scratch state,
-  // solve into p, write out with ghosts.
-  T** B = (T**)c->st[c->cur ^ 1];
+  // rhs -> internal cell layout in the free state buffer, solve in place
+  // (the solve consumes the field before it writes p), write out with ghosts.
   const int nx = c->nx, ny = c->ny, nz = c->nz;
-  k_from_ref<T><<<dim3((nx + 31) / 32, ny, (nz + 31) / 32), dim3(32, 8), 0, s>>>(rhs, B[0], FLD_CELL, nx, ny, nz, 1.0);
+  double* f = scratch_field(c);
+  k_from_ref<double><<<dim3((nx + 31) / 32, ny, (nz + 31) / 32), dim3(32, 8), 0, s>>>(rhs, f, FLD_CELL, nx, ny, nz,
+                                                                                       1.0, nullptr);
   TC_LAUNCHED();
-  int rc = poisson_impl<T>(c, nullptr, nullptr, nullptr, B[0], B[1], 1.0 / ((double)nx * (double)ny), s);
+  int rc = poisson_impl<T>(c, nullptr, nullptr, nullptr, f, f, 1.0 / ((double)nx * (double)ny), s);
   if (rc) return rc;
-  return to_ref<T>(c, B[1], p, FLD_P, s);
+  return to_ref<double>(c, f, p, FLD_P, s);
 }
 
 extern "C" int tc_poisson_solve(tc_ctx* c, const double* rhs, double* p, void* stream) {
@@ -731,19 +746,16 @@ extern "C" int tc_poisson_solve(tc_ctx* c, const double* rhs, double* p, void* s
   return DISPATCH(c, poisson_hook_impl, c, rhs, p, ST(stream));
 }
 
-template <class T>
-__global__ void k_p_from_ref(const double* __restrict__ ref, T* __restrict__ out, int nx, int ny, int nz) {
+__global__ void k_p_from_ref(const double* __restrict__ ref, double* __restrict__ out, int nx, int ny, int nz) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
   if (i >= nx || j >= ny || k >= nz) return;
-  out[pidx(k, j, i, ny, nx)] = (T)ref[((size_t)(i + 1) * (ny + 2) + (j + 1)) * (nz + 2) + (k + 1)];
+  out[pidx(k, j, i, ny, nx)] = ref[((size_t)(i + 1) * (ny + 2) + (j + 1)) * (nz + 2) + (k + 1)];
 }
 
 template <class T> static int project_hook_impl(tc_ctx* c, const double* p, double dt, cudaStream_t s) {
-  k_p_from_ref<T><<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(p, (T*)c->p, c->nx, c->ny, c->nz);
+  k_p_from_ref<<<grid3(c, c->nz), dim3(32, 8), 0, s>>>(p, c->p, c->nx, c->ny, c->nz);
   TC_LAUNCHED();
-  int rc = project_impl<T>(c, (T* const*)c->st[c->cur], dt, s);
-  if (rc) return rc;
-  return bulk_finalize<T>(c, dt, 0, s);
+  return project_impl<T>(c, (T* const*)c->st[c->cur], dt, 0, s);
 }
 
 extern "C" int tc_project(tc_ctx* c, const double* p, double dt, void* stream) {
@@ -972,16 +984,15 @@ extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, doubl
   tc_ctx c{};
   fill_basic(&c, &g);
   double* field = (double*)(base + off[0]);
-  c.X = base + off[1];
-  c.dps = (cpx<double>*)c.X;
+  c.X = (cpx<double>*)(base + off[1]);
   c.k2x = (double*)(base + off[2]); c.k2y = (double*)(base + off[3]);
   c.cl = (double*)(base + off[4]); c.cr = (double*)(base + off[5]);
-  c.twx_t = base + off[6]; c.twy_t = base + off[7];
+  c.twx_d = (cpx<double>*)(base + off[6]); c.twy_d = (cpx<double>*)(base + off[7]);
   const int ntab = c.nxh + ny + nz + nx + ny;
   k_noalloc_tables<<<(ntab + 255) / 256, 256, 0, s>>>(nx, ny, nz, c.dx, c.dy, dz_f, dz_c, c.k2x, c.k2y, c.cl, c.cr,
-                                                     (cpx<double>*)c.twx_t, (cpx<double>*)c.twy_t);
+                                                     c.twx_d, c.twy_d);
   k_from_ref<double><<<dim3((nx + 31) / 32, ny, (nz + 31) / 32), dim3(32, 8), 0, s>>>(rhs, field, FLD_CELL, nx, ny,
-                                                                                        nz, 1.0);
+                                                                                        nz, 1.0, nullptr);
   TC_LAUNCHED();
   // every pass overwrites what it reads next, so no buffer needs clearing;
   // the solve writes p over the consumed right-hand side

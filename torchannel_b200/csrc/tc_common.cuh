@@ -38,6 +38,10 @@ template <class T> struct Grid {
   const T* idzc;         // 1/dz_c[k], k <= nz
   int top_neumann;       // 1: free-slip top wall
   int rhs_fused;         // 1: explicit RHS with the reference CUDA-path edge planes
+  // Base profile of u (mixed precision): u is stored as u - U0[k] so that the
+  // FP32 values stay small; nullptr in the FP64 form.
+  const T* ubase_t;      // U0[k] in the storage type
+  const double* ubase_d; // U0[k] in FP64
 };
 
 __host__ __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }

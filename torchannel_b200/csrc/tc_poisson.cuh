@@ -21,67 +21,71 @@ struct PoissonTabs {
 };
 
 // Divergence (utils.py:226-240) of (u, v, w) scaled by `scale`, or a given
-// cell field times `scale` when u == nullptr; then forward real FFT along x of
-// JT rows of plane k.  Writes X[m][k][j] for m < nx/2+1.
+// FP64 cell field times `scale` when u == nullptr; then forward real FFT along
+// x of JT rows of plane k.  Writes X[m][k][j] for m < nx/2+1.  The spectrum
+// and the transforms are FP64 whatever the velocity storage type: pressure
+// errors reach the post-projection divergence amplified by dt/(dz_c dz_f),
+// which is ~1e4 next to the walls of a stretched grid.
 template <class T>
 __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
-                                                  const T* __restrict__ w, const T* __restrict__ field,
-                                                  cpx<T>* __restrict__ X, FftPlan plx,
-                                                  const cpx<T>* __restrict__ twx, T scale, int JT) {
+                                                  const T* __restrict__ w, const double* __restrict__ field,
+                                                  cpx<double>* __restrict__ X, FftPlan plx,
+                                                  const cpx<double>* __restrict__ twx, double scale, int JT) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxh = nx / 2 + 1;
   const int rs = nx + 2;
-  cpx<T>* b0 = reinterpret_cast<cpx<T>*>(smraw);
-  cpx<T>* b1 = b0 + (JT / 2) * rs;
+  cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
+  cpx<double>* b1 = b0 + (JT / 2) * rs;
   const int k = blockIdx.y, j0 = blockIdx.x * JT;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  const double idx = (double)g.idx, idy = (double)g.idy, idzf = (double)g.idzf[k];
   for (int e = tid; e < JT * nx; e += nthr) {
     int r = e / nx, i = e - r * nx, j = j0 + r;
-    T val;
+    double val;
     if (u != nullptr) {
       const size_t o = pidx(k, j, i, ny, nx);
-      val = (u[o] - u[pidx(k, j, wrap(i - 1, nx), ny, nx)]) * g.idx +
-            (v[o] - v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * g.idy +
-            (w[pidx(k + 1, j, i, ny, nx)] - w[o]) * g.idzf[k];
+      val = ((double)u[o] - (double)u[pidx(k, j, wrap(i - 1, nx), ny, nx)]) * idx +
+            ((double)v[o] - (double)v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * idy +
+            ((double)w[pidx(k + 1, j, i, ny, nx)] - (double)w[o]) * idzf;
     } else {
       val = field[pidx(k, j, i, ny, nx)];
     }
     val *= scale;
-    T* dst = reinterpret_cast<T*>(&b0[(r >> 1) * rs + i]);
+    double* dst = reinterpret_cast<double*>(&b0[(r >> 1) * rs + i]);
     dst[r & 1] = val;
   }
   __syncthreads();
-  int which = fft_rows<T, false>(b0, b1, JT / 2, rs, plx, twx, tid, nthr);
-  const cpx<T>* Z = which ? b1 : b0;
+  int which = fft_rows<double, false>(b0, b1, JT / 2, rs, plx, twx, tid, nthr);
+  const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nxh * JT; e += nthr) {
     int m = e / JT, r = e - m * JT, pr = r >> 1;
-    cpx<T> Zm = Z[pr * rs + m];
-    cpx<T> Zn = cconj(Z[pr * rs + (m == 0 ? 0 : nx - m)]);
-    cpx<T> out;
-    if ((r & 1) == 0) out = cscale(cadd(Zm, Zn), T(0.5));
+    cpx<double> Zm = Z[pr * rs + m];
+    cpx<double> Zn = cconj(Z[pr * rs + (m == 0 ? 0 : nx - m)]);
+    cpx<double> out;
+    if ((r & 1) == 0) out = cscale(cadd(Zm, Zn), 0.5);
     else {
-      cpx<T> d = csub(Zm, Zn);  // (Z - conj Z(-m)) / (2i) = -i/2 * d
-      out = cmake<T>(T(0.5) * d.y, T(-0.5) * d.x);
+      cpx<double> d = csub(Zm, Zn);  // (Z - conj Z(-m)) / (2i) = -i/2 * d
+      out = cmake<double>(0.5 * d.y, -0.5 * d.x);
     }
     X[((size_t)m * nz + k) * ny + j0 + r] = out;
   }
 }
 
 // In-place complex FFT along y of the rows X[kx][k][:] (RB rows per block).
-template <class T, bool INV>
-__global__ void __launch_bounds__(256) k_ffty(cpx<T>* __restrict__ X, int nrows, int ny, FftPlan ply,
-                                              const cpx<T>* __restrict__ twy, int RB) {
+template <bool INV>
+__global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int nrows, int ny, FftPlan ply,
+                                              const cpx<double>* __restrict__ twy, int RB) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  cpx<T>* b0 = reinterpret_cast<cpx<T>*>(smraw);
-  cpx<T>* b1 = b0 + RB * ny;
+  cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
+  cpx<double>* b1 = b0 + RB * ny;
   const int r0 = blockIdx.x * RB;
   const int nb = min(RB, nrows - r0);
   const int tid = threadIdx.x, nthr = blockDim.x;
-  cpx<T>* base = X + (size_t)r0 * ny;
+  cpx<double>* base = X + (size_t)r0 * ny;
   for (int e = tid; e < nb * ny; e += nthr) b0[e] = base[e];
   __syncthreads();
-  int which = fft_rows<T, INV>(b0, b1, nb, ny, ply, twy, tid, nthr);
-  const cpx<T>* Z = which ? b1 : b0;
+  int which = fft_rows<double, INV>(b0, b1, nb, ny, ply, twy, tid, nthr);
+  const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nb * ny; e += nthr) base[e] = Z[e];
 }
 
@@ -89,83 +93,98 @@ __global__ void __launch_bounds__(256) k_ffty(cpx<T>* __restrict__ X, int nrows,
 // (projection_fft.py:167-215), with the tridiagonal rows of
 // projection_fft.py:44-82 built on the fly.  The (0,0) mode is singular: its
 // last unknown is pinned to 0 (explicit gauge) instead of dividing by the
-// roundoff-level pivot.  FP64 arithmetic; d' goes to `dps` (FP64, may alias X
-// when T is double), c' to shared memory.
-template <class T>
-__global__ void __launch_bounds__(64) k_tri(cpx<T>* __restrict__ X, cpx<double>* __restrict__ dps,
-                                            PoissonTabs tb, int nxh, int ny, int nz) {
+// roundoff-level pivot.  FP64; d' in place in X, c' in shared memory.  Loads
+// are issued TRI_B levels ahead of the dependent recurrence.
+#define TRI_B 8
+__global__ void __launch_bounds__(64) k_tri(cpx<double>* __restrict__ X, PoissonTabs tb, int nxh, int ny, int nz) {
   extern __shared__ double cps[];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nxh * ny) return;
   const int kx = t / ny, ky = t - kx * ny;
   const double K2 = tb.k2x[kx] + tb.k2y[ky];
   const size_t stride = ny;
-  const size_t base = (size_t)kx * nz * ny + ky;
+  cpx<double>* col = X + (size_t)kx * nz * ny + ky;
   const int bt = blockDim.x;
   double* cpl = cps + threadIdx.x;
+  cpx<double> buf[TRI_B];
   // forward
   double dpr = 0.0, dpi = 0.0, cprev = 0.0;
-  for (int k = 0; k < nz; ++k) {
-    const double cl = tb.cl[k], cr = tb.cr[k];
-    double a = (k == 0) ? 0.0 : cl;
-    double b = -(cl + cr + K2);
-    if (k == 0) b += cl;
-    if (k == nz - 1) b += cr;
-    double c = (k == nz - 1) ? 0.0 : cr;
-    cpx<T> dv = X[base + (size_t)k * stride];
-    double den = b - a * cprev;
-    double rden = 1.0 / den;
-    double cpk = c * rden;
-    dpr = ((double)dv.x - a * dpr) * rden;
-    dpi = ((double)dv.y - a * dpi) * rden;
-    cpl[(size_t)k * bt] = cpk;
-    cprev = cpk;
-    dps[base + (size_t)k * stride] = cpx<double>{dpr, dpi};
+  for (int k0 = 0; k0 < nz; k0 += TRI_B) {
+#pragma unroll
+    for (int b = 0; b < TRI_B; ++b)
+      if (k0 + b < nz) buf[b] = col[(size_t)(k0 + b) * stride];
+#pragma unroll
+    for (int b = 0; b < TRI_B; ++b) {
+      const int k = k0 + b;
+      if (k < nz) {
+        const double cl = tb.cl[k], cr = tb.cr[k];
+        const double a = (k == 0) ? 0.0 : cl;
+        double bb = -(cl + cr + K2);
+        if (k == 0) bb += cl;
+        if (k == nz - 1) bb += cr;
+        const double c = (k == nz - 1) ? 0.0 : cr;
+        const double rden = 1.0 / (bb - a * cprev);
+        const double cpk = c * rden;
+        dpr = (buf[b].x - a * dpr) * rden;
+        dpi = (buf[b].y - a * dpi) * rden;
+        cpl[(size_t)k * bt] = cpk;
+        cprev = cpk;
+        col[(size_t)k * stride] = cpx<double>{dpr, dpi};
+      }
+    }
   }
   // backward
   double xr = dpr, xi = dpi;
   if (kx == 0 && ky == 0) { xr = 0.0; xi = 0.0; }
-  X[base + (size_t)(nz - 1) * stride] = cpx<T>{(T)xr, (T)xi};
-  for (int k = nz - 2; k >= 0; --k) {
-    cpx<double> d = dps[base + (size_t)k * stride];
-    const double cpk = cpl[(size_t)k * bt];
-    xr = d.x - cpk * xr;
-    xi = d.y - cpk * xi;
-    X[base + (size_t)k * stride] = cpx<T>{(T)xr, (T)xi};
+  col[(size_t)(nz - 1) * stride] = cpx<double>{xr, xi};
+  for (int k1 = nz - 2; k1 >= 0; k1 -= TRI_B) {
+#pragma unroll
+    for (int b = 0; b < TRI_B; ++b)
+      if (k1 - b >= 0) buf[b] = col[(size_t)(k1 - b) * stride];
+#pragma unroll
+    for (int b = 0; b < TRI_B; ++b) {
+      const int k = k1 - b;
+      if (k >= 0) {
+        const double cpk = cpl[(size_t)k * bt];
+        xr = buf[b].x - cpk * xr;
+        xi = buf[b].y - cpk * xi;
+        col[(size_t)k * stride] = cpx<double>{xr, xi};
+      }
+    }
   }
 }
 
-// Inverse real FFT along x of JT rows of plane k; writes p[k][j][i].
-template <class T>
-__global__ void __launch_bounds__(256) k_ifftx(const cpx<T>* __restrict__ X, T* __restrict__ p, int nx, int ny,
-                                               int nz, FftPlan plx, const cpx<T>* __restrict__ twx, int JT) {
+// Inverse real FFT along x of JT rows of plane k; writes p[k][j][i] (FP64).
+__global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X, double* __restrict__ p, int nx,
+                                               int ny, int nz, FftPlan plx, const cpx<double>* __restrict__ twx,
+                                               int JT) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nxh = nx / 2 + 1, rs = nx + 2;
-  cpx<T>* b0 = reinterpret_cast<cpx<T>*>(smraw);
-  cpx<T>* b1 = b0 + (JT / 2) * rs;
+  cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
+  cpx<double>* b1 = b0 + (JT / 2) * rs;
   const int k = blockIdx.y, j0 = blockIdx.x * JT;
   const int tid = threadIdx.x, nthr = blockDim.x;
   // stage the half spectra: S[r][m] in b1 (JT * nxh <= JT/2 * rs entries)
   for (int e = tid; e < nxh * JT; e += nthr) {
     int m = e / JT, r = e - m * JT;
-    cpx<T> val = X[((size_t)m * nz + k) * ny + j0 + r];
-    if (m == 0 || 2 * m == nx) val.y = T(0);  // DC / Nyquist are real (irfft ignores the imaginary part)
+    cpx<double> val = X[((size_t)m * nz + k) * ny + j0 + r];
+    if (m == 0 || 2 * m == nx) val.y = 0.0;  // DC / Nyquist are real (irfft ignores the imaginary part)
     b1[r * nxh + m] = val;
   }
   __syncthreads();
   for (int e = tid; e < (JT / 2) * nx; e += nthr) {
     int pr = e / nx, m = e - pr * nx;
-    cpx<T> A, B;
+    cpx<double> A, B;
     if (m < nxh) { A = b1[(2 * pr) * nxh + m]; B = b1[(2 * pr + 1) * nxh + m]; }
     else { A = cconj(b1[(2 * pr) * nxh + nx - m]); B = cconj(b1[(2 * pr + 1) * nxh + nx - m]); }
-    b0[pr * rs + m] = cmake<T>(A.x - B.y, A.y + B.x);  // A + i B
+    b0[pr * rs + m] = cmake<double>(A.x - B.y, A.y + B.x);  // A + i B
   }
   __syncthreads();
-  int which = fft_rows<T, true>(b0, b1, JT / 2, rs, plx, twx, tid, nthr);
-  const cpx<T>* Z = which ? b1 : b0;
+  int which = fft_rows<double, true>(b0, b1, JT / 2, rs, plx, twx, tid, nthr);
+  const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < JT * nx; e += nthr) {
     int r = e / nx, i = e - r * nx;
-    cpx<T> z = Z[(r >> 1) * rs + i];
+    cpx<double> z = Z[(r >> 1) * rs + i];
     p[pidx(k, j0 + r, i, ny, nx)] = (r & 1) ? z.y : z.x;
   }
 }

@@ -15,8 +15,10 @@ namespace tc {
 // Cell-centred values of plane k at (j, i) (turbstats.py:114-135).
 template <class T> struct CellCentre {
   const T* u; const T* v; const T* w; int nx, ny;
+  const double* ubase;  // base profile of the stored u, or nullptr
   __device__ __forceinline__ double uc(int k, int j, int i) const {
-    return 0.5 * ((double)u[pidx(k, j, wrap(i - 1, nx), ny, nx)] + (double)u[pidx(k, j, i, ny, nx)]);
+    return 0.5 * ((double)u[pidx(k, j, wrap(i - 1, nx), ny, nx)] + (double)u[pidx(k, j, i, ny, nx)]) +
+           (ubase ? ubase[k] : 0.0);
   }
   __device__ __forceinline__ double vc(int k, int j, int i) const {
     return 0.5 * ((double)v[pidx(k, wrap(j - 1, ny), i, ny, nx)] + (double)v[pidx(k, j, i, ny, nx)]);
@@ -31,10 +33,11 @@ template <class T> struct CellCentre {
 template <class T>
 __global__ void __launch_bounds__(256) k_stats_prof(const T* __restrict__ u, const T* __restrict__ v,
                                                     const T* __restrict__ w, int nx, int ny, int nz,
+                                                    const double* __restrict__ ubase,
                                                     double* __restrict__ prof, double* __restrict__ means) {
   __shared__ double sh[32];
   const int k = blockIdx.x;
-  CellCentre<T> C{u, v, w, nx, ny};
+  CellCentre<T> C{u, v, w, nx, ny, ubase};
   const int n = nx * ny;
   double su = 0, sv = 0, sw = 0;
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
@@ -66,9 +69,9 @@ __global__ void __launch_bounds__(256) k_stats_prof(const T* __restrict__ u, con
 // S2 = v_b + i v_t; S is [3][ny][nx] complex double.
 template <class T>
 __global__ void k_stats_fill(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, int nx,
-                             int ny, int nz, int kb, int kt, const double* __restrict__ means,
-                             cpx<double>* __restrict__ S) {
-  CellCentre<T> C{u, v, w, nx, ny};
+                             int ny, int nz, int kb, int kt, const double* __restrict__ ubase,
+                             const double* __restrict__ means, cpx<double>* __restrict__ S) {
+  CellCentre<T> C{u, v, w, nx, ny, ubase};
   const int n = nx * ny;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     int j = e / nx, i = e - j * nx;

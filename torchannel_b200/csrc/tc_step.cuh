@@ -13,11 +13,13 @@ template <class T> struct Acc {
   const T* __restrict__ q;
   int nx, ny, nz;
   T top;  // sign of the top-wall ghost of u/v: -1 no-slip, +1 free-slip
-  // cell-centred u/v plane k in [-1, nz]
+  const T* __restrict__ base;  // per-plane base profile added to the stored values, or nullptr
+  __device__ __forceinline__ T b(int k) const { return base ? ldg(base + k) : T(0); }
+  // cell-centred u/v plane k in [-1, nz] (total value: stored + base)
   __device__ __forceinline__ T c(int k, int j, int i) const {
-    if (k < 0) return -ldg(q + pidx(0, j, i, ny, nx));
-    if (k >= nz) return top * ldg(q + pidx(nz - 1, j, i, ny, nx));
-    return ldg(q + pidx(k, j, i, ny, nx));
+    if (k < 0) return -(ldg(q + pidx(0, j, i, ny, nx)) + b(0));
+    if (k >= nz) return top * (ldg(q + pidx(nz - 1, j, i, ny, nx)) + b(nz - 1));
+    return ldg(q + pidx(k, j, i, ny, nx)) + b(k);
   }
   // w face f in [0, nz] (walls stored as zeros)
   __device__ __forceinline__ T f(int k, int j, int i) const { return ldg(q + pidx(k, j, i, ny, nx)); }
@@ -56,7 +58,7 @@ __global__ void __launch_bounds__(256) k_rhs_update(Grid<T> g, const T* __restri
   const int k = blockIdx.z;
   if (i >= nx || j >= ny) return;
   const T top = g.top_neumann ? T(1) : T(-1);
-  Acc<T> U{u, nx, ny, nz, top}, V{v, nx, ny, nz, top}, W{w, nx, ny, nz, top};
+  Acc<T> U{u, nx, ny, nz, top, g.ubase_t}, V{v, nx, ny, nz, top, nullptr}, W{w, nx, ny, nz, top, nullptr};
   const int im = wrap(i - 1, nx), ip = wrap(i + 1, nx);
   const int jm = wrap(j - 1, ny), jp = wrap(j + 1, ny);
   const T h = T(0.5);
@@ -66,7 +68,9 @@ __global__ void __launch_bounds__(256) k_rhs_update(Grid<T> g, const T* __restri
     const T idzf = g.idzf[k];
     // ---------------- u at cell k ----------------
     {
-      const T U0 = U.c(k, j, i), Uxm = U.c(k, j, im), Uxp = U.c(k, j, ip);
+      const size_t o = pidx(k, j, i, ny, nx);
+      const T Uraw = ldg(u + o);  // stored value (u - U0[k] in mixed precision)
+      const T U0 = Uraw + U.b(k), Uxm = U.c(k, j, im), Uxp = U.c(k, j, ip);
       const T Uym = U.c(k, jm, i), Uyp = U.c(k, jp, i);
       const T Uzm = U.c(k - 1, j, i), Uzp = U.c(k + 1, j, i);
       const bool edge = (i == nx - 1);
@@ -83,15 +87,14 @@ __global__ void __launch_bounds__(256) k_rhs_update(Grid<T> g, const T* __restri
         const T wu_b = h * (W.f(k, j, i) + W.f(k, j, i + 1)) * (h * (Uzm + U0));
         r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
       }
-      const size_t o = pidx(k, j, i, ny, nx);
       if (UPD == UPD_RHS_ONLY) {
         ru[o] = r;
       } else if (UPD == UPD_FE) {
-        T q = U0 + dt * r;
+        T q = Uraw + dt * r;
         us[o] = q + dt * T(1);
       } else {
         r += forcing;
-        us[o] = have_hist ? U0 + dt * (T(1.5) * r - T(0.5) * ru[o]) : U0 + dt * r;
+        us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
         ru[o] = r;
       }
     }
@@ -225,16 +228,22 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
 // Kernel (b): batched Thomas solve of the CN systems, one thread per column
 // and component (blockIdx.z = 0 u, 1 v, 2 w).  In place: the forward sweep
 // overwrites each plane with d'_m, the backward sweep with x_m.  Arithmetic in
-// FP64 whatever the storage type.  Replaces solve_implicit_diffusion_u/v/w
-// (operators.py:563-811) whose PCR (tridiag.py:33-58) solves the same systems.
+// FP64 whatever the storage type; u is solved for its total value (stored +
+// base profile).  Loads are issued in batches of CN_B planes ahead of the
+// dependent recurrence so that each thread keeps CN_B requests in flight.
+// Replaces solve_implicit_diffusion_u/v/w (operators.py:563-811) whose PCR
+// (tridiag.py:33-58) solves the same systems.
 // ---------------------------------------------------------------------------
+#define CN_B 8
 template <class T>
 __global__ void __launch_bounds__(128) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, CnTab t,
-                                                  int nx, int ny, int nz) {
+                                                  const double* __restrict__ ubase, int nx, int ny, int nz) {
   extern __shared__ double sh[];
   const int comp = blockIdx.z;
   const double* src = comp == 2 ? t.w : t.uv;
+  double* shb = sh + 6 * nz;  // base profile (u only)
   for (int e = threadIdx.x; e < 6 * nz; e += blockDim.x) sh[e] = src[e];
+  for (int e = threadIdx.x; e < nz; e += blockDim.x) shb[e] = (comp == 0 && ubase) ? ubase[e] : 0.0;
   __syncthreads();
   const double* a = sh; const double* iv = a + nz; const double* cp = iv + nz;
   const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
@@ -243,98 +252,89 @@ __global__ void __launch_bounds__(128) k_cn_solve(T* __restrict__ u, T* __restri
   if (col >= nx * ny) return;
   const size_t plane = (size_t)nx * ny;
   T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + col;
+  double buf[CN_B];
   if (comp < 2) {
+    // rows m = 0..nz-1 on planes m; explicit stencil on planes m-1, m, m+1
     const int n = nz;
-    double qm = 0.0, q0 = (double)q[0];
+    double qm = 0.0, q0 = (double)q[0] + shb[0];
     double dprev = 0.0;
-    for (int m = 0; m < n; ++m) {
-      double qn = (m + 1 < n) ? (double)q[(size_t)(m + 1) * plane] : 0.0;
-      double d = q0 + beta * (cA[m] * qm + cB[m] * q0 + cC[m] * qn);
-      double dp = (d - a[m] * dprev) * iv[m];
-      q[(size_t)m * plane] = (T)dp;
-      dprev = dp;
-      qm = q0; q0 = qn;
+    for (int m0 = 0; m0 < n; m0 += CN_B) {
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m0 + b + 1;
+        buf[b] = (m < n) ? (double)q[(size_t)m * plane] + shb[m] : 0.0;
+      }
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m0 + b;
+        if (m < n) {
+          const double qn = buf[b];
+          const double d = q0 + beta * (cA[m] * qm + cB[m] * q0 + cC[m] * qn);
+          const double dp = (d - a[m] * dprev) * iv[m];
+          q[(size_t)m * plane] = (T)(dp - shb[m]);  // kept as (d' - base) so it round-trips exactly in FP64
+          dprev = dp;
+          qm = q0; q0 = qn;
+        }
+      }
     }
+    // backward sweep: x_{n-1} = d'_{n-1}
     double x = dprev;
-    q[(size_t)(n - 1) * plane] = (T)x;
-    for (int m = n - 2; m >= 0; --m) {
-      double dp = (double)q[(size_t)m * plane];
-      x = dp - cp[m] * x;
-      q[(size_t)m * plane] = (T)x;
+    q[(size_t)(n - 1) * plane] = (T)(x - shb[n - 1]);
+    for (int m1 = n - 2; m1 >= 0; m1 -= CN_B) {
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m1 - b;
+        buf[b] = (m >= 0) ? (double)q[(size_t)m * plane] + shb[m] : 0.0;
+      }
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m1 - b;
+        if (m >= 0) {
+          x = buf[b] - cp[m] * x;
+          q[(size_t)m * plane] = (T)(x - shb[m]);
+        }
+      }
     }
   } else {
     // unknowns at faces 1..nz-1; row m <-> face m+1; explicit stencil on faces m-1, m, m+1
     const int n = nz - 1;
     double pm = 0.0, p0 = (double)q[0], p1 = (double)q[plane];
     double dprev = 0.0;
-    for (int m = 0; m < n; ++m) {
-      double p2 = (m + 2 <= nz - 1) ? (double)q[(size_t)(m + 2) * plane] : 0.0;
-      double d = p1 + beta * (cA[m] * pm + cB[m] * p0 + cC[m] * p1);
-      double dp = (d - a[m] * dprev) * iv[m];
-      q[(size_t)(m + 1) * plane] = (T)dp;
-      dprev = dp;
-      pm = p0; p0 = p1; p1 = p2;
+    for (int m0 = 0; m0 < n; m0 += CN_B) {
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int f = m0 + b + 2;
+        buf[b] = (f <= nz - 1) ? (double)q[(size_t)f * plane] : 0.0;
+      }
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m0 + b;
+        if (m < n) {
+          const double d = p1 + beta * (cA[m] * pm + cB[m] * p0 + cC[m] * p1);
+          const double dp = (d - a[m] * dprev) * iv[m];
+          q[(size_t)(m + 1) * plane] = (T)dp;
+          dprev = dp;
+          pm = p0; p0 = p1; p1 = buf[b];
+        }
+      }
     }
     double x = dprev;
-    for (int m = n - 2; m >= 0; --m) {
-      double dp = (double)q[(size_t)(m + 1) * plane];
-      x = dp - cp[m] * x;
-      q[(size_t)(m + 1) * plane] = (T)x;
+    for (int m1 = n - 2; m1 >= 0; m1 -= CN_B) {
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m1 - b;
+        buf[b] = (m >= 0) ? (double)q[(size_t)(m + 1) * plane] : 0.0;
+      }
+#pragma unroll
+      for (int b = 0; b < CN_B; ++b) {
+        const int m = m1 - b;
+        if (m >= 0) {
+          x = buf[b] - cp[m] * x;
+          q[(size_t)(m + 1) * plane] = (T)x;
+        }
+      }
     }
   }
-}
-
-// ---------------------------------------------------------------------------
-// Kernel (d): projection u -= dt grad p (projection.py:143-165), in place,
-// fused with the per-block partial sums of the bulk velocity
-// (utils.py:207-223, sum of u * dz_f over all DOFs; dx*dy/V applied later).
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
-                                                      T* __restrict__ w, const T* __restrict__ p, T dt,
-                                                      const double* __restrict__ dzf,
-                                                      double* __restrict__ partials) {
-  __shared__ double sh[32];
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  double acc = 0.0;
-  if (i < nx && j < ny) {
-    const int ip = wrap(i + 1, nx), jp = wrap(j + 1, ny);
-    if (k < nz) {
-      const T P0 = ldg(p + pidx(k, j, i, ny, nx));
-      const size_t o = pidx(k, j, i, ny, nx);
-      T un = u[o] - dt * ((ldg(p + pidx(k, j, ip, ny, nx)) - P0) * g.idx);
-      u[o] = un;
-      v[o] = v[o] - dt * ((ldg(p + pidx(k, jp, i, ny, nx)) - P0) * g.idy);
-      acc = (double)un * dzf[k];
-    }
-    if (k >= 1 && k <= nz - 1) {
-      const size_t o = pidx(k, j, i, ny, nx);
-      w[o] = w[o] - dt * ((ldg(p + pidx(k, j, i, ny, nx)) - ldg(p + pidx(k - 1, j, i, ny, nx))) * g.idzc[k]);
-    }
-  }
-  double s = block_sum(acc, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0)
-    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
-}
-
-// Bulk sum over all DOFs without projection (used at set-up and for
-// diagnostics).
-template <class T>
-__global__ void __launch_bounds__(256) k_bulk_partials(Grid<T> g, const T* __restrict__ u,
-                                                       const double* __restrict__ dzf,
-                                                       double* __restrict__ partials) {
-  __shared__ double sh[32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  double acc = 0.0;
-  if (i < g.nx && j < g.ny && k < g.nz) acc = (double)u[pidx(k, j, i, g.ny, g.nx)] * dzf[k];
-  double s = block_sum(acc, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0)
-    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
 }
 
 // Scalars slot layout (FP64, device).
@@ -349,19 +349,97 @@ enum : int {
   SC_COUNT = 8
 };
 
-// Deterministic final reduction of the bulk partials and the PI forcing update
-// forcing += (U_b - u_b)/dt * 0.1 (solver.py:701-708).
-__global__ void k_bulk_finalize(const double* __restrict__ partials, int n, double* __restrict__ scal,
-                                double scale, double U_target, double dt, int update_forcing) {
-  __shared__ double sh[32];
+// Deterministic final reduction of `n` bulk partials and the PI forcing update
+// forcing += (U_b - u_b)/dt * 0.1 (solver.py:701-708), done by one block.
+__device__ __forceinline__ void bulk_reduce_block(const double* partials, int n, double* scal, double scale,
+                                                  double U_target, double dt, int update_forcing, double* sh) {
   double acc = 0.0;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) acc += partials[e];
+  for (int e = threadIdx.x + blockDim.x * threadIdx.y; e < n; e += blockDim.x * blockDim.y) acc += __ldcg(partials + e);
   double s = block_sum(acc, sh);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
     double ub = s * scale;
     scal[SC_UBULK] = ub;
     if (update_forcing) scal[SC_FORCING] += (U_target - ub) / dt * 0.1;
   }
+}
+
+struct BulkArgs {
+  double* partials;
+  unsigned int* ticket;  // zero between launches; the last block resets it
+  double* scal;
+  double scale, U_target, dt;
+  int update_forcing;
+};
+
+// ---------------------------------------------------------------------------
+// Kernel (d): projection u -= dt grad p (projection.py:143-165), in place,
+// fused with the bulk velocity (utils.py:207-223: sum of u dz_f dx dy / V over
+// all DOFs) and the PI forcing update: every block writes its partial sum, the
+// last block to finish reduces them in a fixed order.  p is FP64.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
+                                                      T* __restrict__ w, const double* __restrict__ p, double dt,
+                                                      const double* __restrict__ dzf, BulkArgs ba) {
+  __shared__ double sh[32];
+  __shared__ int last;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double acc = 0.0;
+  if (i < nx && j < ny) {
+    const int ip = wrap(i + 1, nx), jp = wrap(j + 1, ny);
+    if (k < nz) {
+      const double P0 = ldg(p + pidx(k, j, i, ny, nx));
+      const size_t o = pidx(k, j, i, ny, nx);
+      T un = (T)((double)u[o] - dt * ((ldg(p + pidx(k, j, ip, ny, nx)) - P0) * (double)g.idx));
+      u[o] = un;
+      v[o] = (T)((double)v[o] - dt * ((ldg(p + pidx(k, jp, i, ny, nx)) - P0) * (double)g.idy));
+      acc = ((double)un + (g.ubase_d ? g.ubase_d[k] : 0.0)) * dzf[k];
+    }
+    if (k >= 1 && k <= nz - 1) {
+      const size_t o = pidx(k, j, i, ny, nx);
+      w[o] = (T)((double)w[o] - dt * ((ldg(p + o) - ldg(p + pidx(k - 1, j, i, ny, nx))) * (double)g.idzc[k]));
+    }
+  }
+  double s = block_sum(acc, sh);
+  const int nb = gridDim.x * gridDim.y * gridDim.z;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    ba.partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+    __threadfence();
+    unsigned int t = atomicAdd(ba.ticket, 1u);
+    last = (t == (unsigned)nb - 1u);
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    bulk_reduce_block(ba.partials, nb, ba.scal, ba.scale, ba.U_target, ba.dt, ba.update_forcing, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) *ba.ticket = 0u;
+  }
+}
+
+// Bulk sum over all DOFs without projection (set-up and diagnostics).
+template <class T>
+__global__ void __launch_bounds__(256) k_bulk_partials(Grid<T> g, const T* __restrict__ u,
+                                                       const double* __restrict__ dzf,
+                                                       double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double acc = 0.0;
+  if (i < g.nx && j < g.ny && k < g.nz)
+    acc = ((double)u[pidx(k, j, i, g.ny, g.nx)] + (g.ubase_d ? g.ubase_d[k] : 0.0)) * dzf[k];
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+}
+
+__global__ void k_bulk_finalize(const double* __restrict__ partials, int n, double* __restrict__ scal,
+                                double scale, double U_target, double dt, int update_forcing) {
+  __shared__ double sh[32];
+  bulk_reduce_block(partials, n, scal, scale, U_target, dt, update_forcing, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -378,7 +456,7 @@ __global__ void __launch_bounds__(256) k_cfl_partials(Grid<T> g, const T* __rest
   double m = 0.0;
   if (i < nx && j < ny && k < nz) {
     const double top = g.top_neumann ? 1.0 : -1.0;
-    Acc<T> U{u, nx, ny, nz, (T)top}, V{v, nx, ny, nz, (T)top}, W{w, nx, ny, nz, (T)top};
+    Acc<T> U{u, nx, ny, nz, (T)top, g.ubase_t}, V{v, nx, ny, nz, (T)top, nullptr}, W{w, nx, ny, nz, (T)top, nullptr};
     const int im = wrap(i - 1, nx), ip = wrap(i + 1, nx), jm = wrap(j - 1, ny), jp = wrap(j + 1, ny);
     const double idx = (double)g.idx, idy = (double)g.idy, idzf = (double)g.idzf[k];
     double ux = fabs((double)U.c(k, j, i));
@@ -411,11 +489,12 @@ __global__ void k_max_finalize(const double* __restrict__ partials, int n, doubl
 
 // ---------------------------------------------------------------------------
 // Diagnostics: max |div| (utils.py:226-240), non-finite scan of u, v, w, p
-// (solver.py:865-868) -> per-block partials (max, flag).
+// (solver.py:865-868) -> per-block partials (max, flag).  The base profile of
+// u cancels in the x difference.
 // ---------------------------------------------------------------------------
 template <class T>
 __global__ void __launch_bounds__(256) k_diag_partials(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
-                                                       const T* __restrict__ w, const T* __restrict__ p,
+                                                       const T* __restrict__ w, const double* __restrict__ p,
                                                        double* __restrict__ pmax, double* __restrict__ pflag) {
   __shared__ double sh[32];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -429,7 +508,7 @@ __global__ void __launch_bounds__(256) k_diag_partials(Grid<T> g, const T* __res
     double dv = ((double)v[o] - (double)v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * (double)g.idy;
     double dw = ((double)w[pidx(k + 1, j, i, ny, nx)] - (double)w[o]) * (double)g.idzf[k];
     m = fabs(du + dv + dw);
-    double s = (double)u[o] + (double)v[o] + (double)w[pidx(k + 1, j, i, ny, nx)] + (double)p[o];
+    double s = (double)u[o] + (double)v[o] + (double)w[pidx(k + 1, j, i, ny, nx)] + p[o];
     if (!isfinite(s)) bad = 1.0;
     if (!isfinite(m)) m = INFINITY;
   }
@@ -450,11 +529,12 @@ __global__ void k_utau_sums(Grid<T> g, const T* __restrict__ u, double* __restri
   __shared__ double sh[32];
   const int nx = g.nx, ny = g.ny;
   const int k = blockIdx.x == 0 ? 0 : g.nz - 1;
+  const double bk = g.ubase_d ? g.ubase_d[k] : 0.0;
   double acc = 0.0;
   for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
     int j = e / nx, i = e - j * nx;
     double wgt = (i == nx - 1 ? 2.0 : 1.0) * (1.0 + (j == 0 ? 1.0 : 0.0) + (j == ny - 1 ? 1.0 : 0.0));
-    acc += wgt * (double)u[pidx(k, j, i, ny, nx)];
+    acc += wgt * ((double)u[pidx(k, j, i, ny, nx)] + bk);
   }
   double s = block_sum(acc, sh);
   if (threadIdx.x == 0) scal[SC_UTAU_BOT + blockIdx.x] = s / ((double)(nx + 1) * (double)(ny + 2));
@@ -469,13 +549,13 @@ __global__ void k_utau_sums(Grid<T> g, const T* __restrict__ u, double* __restri
 enum : int { FLD_U = 0, FLD_V = 1, FLD_W = 2, FLD_P = 3, FLD_CELL = 4 };
 
 // Gather the DOFs of a reference array into the internal layout.
-// FLD_U/V: ref (Xr, Yr, nz+2) -> internal [nz][ny][nx] = ref[i+1, j+1, k+1]
+// FLD_U/V: ref (Xr, Yr, nz+2) -> internal [nz][ny][nx] = ref[i+1, j+1, k+1] - base[k]
 // FLD_W:   ref (nx+2, ny+2, nz+1) -> internal [nz+1][ny][nx] = ref[i+1, j+1, k]
 //          (wall planes written as 0)
 // FLD_CELL: ref (nx, ny, nz) -> internal [nz][ny][nx] = ref[i, j, k] * scale
 template <class T>
 __global__ void k_from_ref(const double* __restrict__ ref, T* __restrict__ out, int kind, int nx, int ny, int nz,
-                           double scale) {
+                           double scale, const double* __restrict__ base) {
   __shared__ double tile[32][33];
   const int j = blockIdx.y;
   const int i0 = blockIdx.x * 32, k0 = blockIdx.z * 32;
@@ -499,17 +579,33 @@ __global__ void k_from_ref(const double* __restrict__ ref, T* __restrict__ out, 
     if (i < nx && k < NK) {
       double val = tile[threadIdx.x][r];
       if (kind == FLD_W && (k == 0 || k == nz)) val = 0.0;
+      if (base) val -= base[k];
       out[pidx(k, j, i, ny, nx)] = (T)val;
     }
   }
 }
 
+// Per-plane mean of the DOFs of a reference u array: the base profile of the
+// mixed-precision storage.  One block per plane.
+__global__ void k_plane_mean_ref_u(const double* __restrict__ ref, int nx, int ny, int nz, double* __restrict__ out) {
+  __shared__ double sh[32];
+  const int k = blockIdx.x;
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+    int i = e / ny, j = e - i * ny;
+    acc += ref[((size_t)(i + 1) * (ny + 2) + (j + 1)) * (nz + 2) + (k + 1)];
+  }
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) out[k] = s / ((double)nx * (double)ny);
+}
+
 // Materialise a full reference array (ghosts included) from the internal
 // layout, with the ghost rules of apply_bc_all (solver.py:23-79) and of the
-// pressure ghost fill (projection_fft.py:148-163).
+// pressure ghost fill (projection_fft.py:148-163).  `base` (u only) is added
+// back to the stored values.
 template <class T>
 __global__ void k_to_ref(const T* __restrict__ in, double* __restrict__ ref, int kind, int nx, int ny, int nz,
-                         int top_neumann) {
+                         int top_neumann, const double* __restrict__ base) {
   __shared__ double tile[32][33];
   int Xr, Yr, Zr;
   switch (kind) {
@@ -542,9 +638,10 @@ __global__ void k_to_ref(const T* __restrict__ in, double* __restrict__ ref, int
         int k = K == 0 ? 0 : (K == nz + 1 ? nz - 1 : K - 1);
         val = (double)in[pidx(k, j, i, ny, nx)];
       } else {
-        if (K == 0) val = -(double)in[pidx(0, j, i, ny, nx)];
-        else if (K == nz + 1) val = top * (double)in[pidx(nz - 1, j, i, ny, nx)];
-        else val = (double)in[pidx(K - 1, j, i, ny, nx)];
+        auto tot = [&](int k) { return (double)in[pidx(k, j, i, ny, nx)] + (base ? base[k] : 0.0); };
+        if (K == 0) val = -tot(0);
+        else if (K == nz + 1) val = top * tot(nz - 1);
+        else val = tot(K - 1);
       }
     }
     tile[r][threadIdx.x] = val;
