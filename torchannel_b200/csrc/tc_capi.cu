@@ -387,7 +387,8 @@ static double bulk_scale(const tc_ctx* c) { return c->dx * c->dy / (c->Lx * c->L
 template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, int update_forcing, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
   BulkArgs ba{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, update_forcing};
-  k_project_bulk<T><<<grid3(c, c->nz + 1), dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt, c->dzf_d, ba);
+  k_project_bulk<T><<<grid3(c, (c->nz + PROJ_KC - 1) / PROJ_KC), dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt,
+                                                                                      c->dzf_d, ba);
   TC_LAUNCHED();
   return TC_OK;
 }
@@ -398,8 +399,8 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   T** A = (T**)c->st[c->cur];
   T** B = (T**)c->st[nxt];
   T** R = (T**)c->rh;
-  dim3 blk(32, 8);
-  dim3 grd = grid3(c, c->nz + 1);
+  dim3 blk(RHS_TX, RHS_TY);
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + RHS_KC - 1) / RHS_KC);
   if (scheme == TC_IMEX && c->tab_dt != dt) {
     k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
     c->tab_dt = dt;
@@ -502,12 +503,12 @@ template <class T> static int rhs_hook_impl(tc_ctx* c, int full, double* ru, dou
   T** B = (T**)c->st[c->cur ^ 1];  // scratch: the next buffer is free between steps
   const size_t ncell = (size_t)c->nx * c->ny * c->nz;
   cudaMemsetAsync(B[2], 0, ncell / c->nz * (c->nz + 1) * sizeof(T), s);
-  dim3 grd = grid3(c, c->nz + 1);
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + RHS_KC - 1) / RHS_KC);
   if (full)
-    k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+    k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, RHS_TY), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                    B[0], B[1], B[2], c->scal, (T)0, 0);
   else
-    k_rhs_update<T, false, UPD_RHS_ONLY><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+    k_rhs_update<T, false, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, RHS_TY), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                     B[0], B[1], B[2], c->scal, (T)0, 0);
   TC_LAUNCHED();
   int rc;

@@ -38,7 +38,10 @@ __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict
   cpx<double>* b1 = b0 + (JT / 2) * rs;
   const int k = blockIdx.y, j0 = blockIdx.x * JT;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const double idx = (double)g.idx, idy = (double)g.idy, idzf = (double)g.idzf[k];
+  // grid reciprocals are read only on the divergence path (a field-only
+  // caller may pass a grid without z tables)
+  const double idx = (double)g.idx, idy = (double)g.idy;
+  const double idzf = (u != nullptr) ? (double)g.idzf[k] : 0.0;
   for (int e = tid; e < JT * nx; e += nthr) {
     int r = e / nx, i = e - r * nx, j = j0 + r;
     double val;

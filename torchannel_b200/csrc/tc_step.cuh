@@ -41,117 +41,184 @@ enum : int {
 // (:474-548), diffusion_u/v/w (:18-124), compute_momentum_rhs_fused_imex
 // (:1037-1225) and _v2 (:818-1034), AB2 combine solver.py:626-651.
 // FULL=false: IMEX (x/y diffusion only); FULL=true: full Laplacian (AB2/FE).
-// One thread per (i, j, plane k), k in [0, nz]: u/v at cell k < nz and w at
-// face k in [1, nz-1].  Edge planes: internal i = nx-1 is reference u[nx] and
-// j = ny-1 is v[:, ny]; both paths omit advection there, the separate-op path
+//
+// 2.5-D z march: a block owns a RHS_TX x RHS_TY column tile and walks
+// RHS_KC planes; iteration k computes u, v at cell k and w at face k.  The
+// u, v, w planes k-1, k, k+1 (periodic x/y halo of one cell, z ghosts already
+// applied, u with its base profile added) sit in a 3-slot shared-memory ring;
+// plane k+2 is fetched into registers while plane k is computed.
+// Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
+// v[:, ny]; both reference paths omit advection there, the separate-op path
 // keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
 // ---------------------------------------------------------------------------
+#define RHS_TX 32
+#define RHS_TY 8
+#define RHS_KC 16
+#define RHS_HX (RHS_TX + 2)
+#define RHS_HY (RHS_TY + 2)
+#define RHS_NH (RHS_HX * RHS_HY)
+
 template <class T, bool FULL, int UPD>
-__global__ void __launch_bounds__(256) k_rhs_update(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
-                                                    const T* __restrict__ w, T* __restrict__ us,
-                                                    T* __restrict__ vs, T* __restrict__ ws, T* __restrict__ ru,
-                                                    T* __restrict__ rv, T* __restrict__ rw,
-                                                    const double* __restrict__ forcing_dev, T dt, int have_hist) {
+__global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const T* __restrict__ u,
+                                                                const T* __restrict__ v, const T* __restrict__ w,
+                                                                T* __restrict__ us, T* __restrict__ vs,
+                                                                T* __restrict__ ws, T* __restrict__ ru,
+                                                                T* __restrict__ rv, T* __restrict__ rw,
+                                                                const double* __restrict__ forcing_dev, T dt,
+                                                                int have_hist) {
+  __shared__ T su[3][RHS_HY][RHS_HX];
+  __shared__ T sv[3][RHS_HY][RHS_HX];
+  __shared__ T sw[3][RHS_HY][RHS_HX];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i >= nx || j >= ny) return;
+  const size_t plane = (size_t)nx * ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx;
+  const int i0 = blockIdx.x * RHS_TX, j0 = blockIdx.y * RHS_TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = (i < nx) && (j < ny);
+  const int kb = blockIdx.z * RHS_KC;
+  const int ke = min(kb + RHS_KC, nz + 1);
   const T top = g.top_neumann ? T(1) : T(-1);
-  Acc<T> U{u, nx, ny, nz, top, g.ubase_t}, V{v, nx, ny, nz, top, nullptr}, W{w, nx, ny, nz, top, nullptr};
-  const int im = wrap(i - 1, nx), ip = wrap(i + 1, nx);
-  const int jm = wrap(j - 1, ny), jp = wrap(j + 1, ny);
   const T h = T(0.5);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
+  const T* __restrict__ base = g.ubase_t;
 
-  if (k < nz) {
-    const T idzf = g.idzf[k];
-    // ---------------- u at cell k ----------------
-    {
-      const size_t o = pidx(k, j, i, ny, nx);
-      const T Uraw = ldg(u + o);  // stored value (u - U0[k] in mixed precision)
-      const T U0 = Uraw + U.b(k), Uxm = U.c(k, j, im), Uxp = U.c(k, j, ip);
-      const T Uym = U.c(k, jm, i), Uyp = U.c(k, jp, i);
-      const T Uzm = U.c(k - 1, j, i), Uzp = U.c(k + 1, j, i);
-      const bool edge = (i == nx - 1);
-      T r = T(0);
-      if (!(edge && g.rhs_fused)) {
-        r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
-        if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
+  // halo elements owned by this thread for plane loads: e0 = tid, e1 = tid + 256
+  const int e1 = tid + RHS_TX * RHS_TY;
+  const bool has1 = e1 < RHS_NH;
+  const int hy0 = tid / RHS_HX, hx0 = tid - hy0 * RHS_HX;
+  const int hy1 = e1 / RHS_HX, hx1 = e1 - hy1 * RHS_HX;
+  auto modp = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
+  const size_t off0 = (size_t)modp(j0 - 1 + hy0, ny) * nx + modp(i0 - 1 + hx0, nx);
+  const size_t off1 = has1 ? (size_t)modp(j0 - 1 + hy1, ny) * nx + modp(i0 - 1 + hx1, nx) : 0;
+
+  auto bk = [&](int p) { return base ? ldg(base + p) : T(0); };
+  auto ucell = [&](const T* q, bool isu, int p, size_t off) -> T {
+    if (p < -1 || p > nz) return T(0);
+    if (p == -1) return -(ldg(q + off) + (isu ? bk(0) : T(0)));
+    if (p == nz) return top * (ldg(q + (size_t)(nz - 1) * plane + off) + (isu ? bk(nz - 1) : T(0)));
+    return ldg(q + (size_t)p * plane + off) + (isu ? bk(p) : T(0));
+  };
+  auto wface = [&](int p, size_t off) -> T {
+    if (p < 0 || p > nz) return T(0);
+    return ldg(w + (size_t)p * plane + off);
+  };
+  T reg[6];
+  auto fetch = [&](int p) {
+    reg[0] = ucell(u, true, p, off0);
+    reg[1] = ucell(v, false, p, off0);
+    reg[2] = wface(p, off0);
+    if (has1) {
+      reg[3] = ucell(u, true, p, off1);
+      reg[4] = ucell(v, false, p, off1);
+      reg[5] = wface(p, off1);
+    }
+  };
+  auto put = [&](int slot) {
+    su[slot][hy0][hx0] = reg[0]; sv[slot][hy0][hx0] = reg[1]; sw[slot][hy0][hx0] = reg[2];
+    if (has1) { su[slot][hy1][hx1] = reg[3]; sv[slot][hy1][hx1] = reg[4]; sw[slot][hy1][hx1] = reg[5]; }
+  };
+  auto slot_of = [&](int p) { return (p - kb + 1) % 3; };  // p >= kb - 1
+
+  // prologue: planes kb-1, kb, kb+1
+  for (int p = kb - 1; p <= kb + 1; ++p) { fetch(p); put(slot_of(p)); }
+  __syncthreads();
+
+  const int cx = tx + 1, cy = ty + 1;
+  for (int k = kb; k < ke; ++k) {
+    fetch(k + 2);  // in flight while plane k is computed
+    const int sm = slot_of(k - 1), s0 = slot_of(k), sp = slot_of(k + 1);
+    if (active && k < nz) {
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const T idzf = g.idzf[k];
+      // ---------------- u at cell k ----------------
+      {
+        const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
+        const T Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
+        const T Uzm = su[sm][cy][cx], Uzp = su[sp][cy][cx];
+        const bool edge = (i == nx - 1);
+        T r = T(0);
+        if (!(edge && g.rhs_fused)) {
+          r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
+          if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
+        }
+        if (!edge) {
+          const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
+          const T vu_t = h * (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (h * (U0 + Uyp));
+          const T vu_b = h * (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (h * (Uym + U0));
+          const T wu_t = h * (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (h * (U0 + Uzp));
+          const T wu_b = h * (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (h * (Uzm + U0));
+          r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
+        }
+        if (UPD == UPD_RHS_ONLY) {
+          ru[o] = r;
+        } else {
+          const T Uraw = base ? ldg(u + o) : U0;  // stored value (u - U0[k] in mixed precision)
+          if (UPD == UPD_FE) {
+            T q = Uraw + dt * r;
+            us[o] = q + dt * T(1);
+          } else {
+            r += forcing;
+            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
+            ru[o] = r;
+          }
+        }
       }
-      if (!edge) {
-        const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
-        const T vu_t = h * (V.c(k, j, i) + V.c(k, j, i + 1)) * (h * (U0 + Uyp));
-        const T vu_b = h * (V.c(k, jm, i) + V.c(k, jm, i + 1)) * (h * (Uym + U0));
-        const T wu_t = h * (W.f(k + 1, j, i) + W.f(k + 1, j, i + 1)) * (h * (U0 + Uzp));
-        const T wu_b = h * (W.f(k, j, i) + W.f(k, j, i + 1)) * (h * (Uzm + U0));
-        r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
+      // ---------------- v at cell k ----------------
+      {
+        const T V0 = sv[s0][cy][cx], Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1];
+        const T Vym = sv[s0][cy - 1][cx], Vyp = sv[s0][cy + 1][cx];
+        const T Vzm = sv[sm][cy][cx], Vzp = sv[sp][cy][cx];
+        const bool edge = (j == ny - 1);
+        T r = T(0);
+        if (!(edge && g.rhs_fused)) {
+          r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
+          if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
+        }
+        if (!edge) {
+          const T uv_r = h * (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (h * (V0 + Vxp));
+          const T uv_l = h * (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (h * (Vxm + V0));
+          const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
+          const T wv_t = h * (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (h * (V0 + Vzp));
+          const T wv_b = h * (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (h * (Vzm + V0));
+          r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
+        }
+        if (UPD == UPD_RHS_ONLY) {
+          rv[o] = r;
+        } else if (UPD == UPD_FE) {
+          vs[o] = V0 + dt * r;
+        } else {
+          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
+          rv[o] = r;
+        }
       }
+    }
+    // ---------------- w at face k ----------------
+    if (active && k >= 1 && k <= nz - 1) {
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const T W0 = sw[s0][cy][cx], Wxm = sw[s0][cy][cx - 1], Wxp = sw[s0][cy][cx + 1];
+      const T Wym = sw[s0][cy - 1][cx], Wyp = sw[s0][cy + 1][cx];
+      const T Wzm = sw[sm][cy][cx], Wzp = sw[sp][cy][cx];
+      T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
+      // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+      if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
+      const T uw_r = h * (su[sm][cy][cx] + su[s0][cy][cx]) * (h * (W0 + Wxp));
+      const T uw_l = h * (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (h * (Wxm + W0));
+      const T vw_t = h * (sv[sm][cy][cx] + sv[s0][cy][cx]) * (h * (W0 + Wyp));
+      const T vw_b = h * (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (h * (Wym + W0));
+      const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[k];
+      r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
       if (UPD == UPD_RHS_ONLY) {
-        ru[o] = r;
+        rw[o] = r;
       } else if (UPD == UPD_FE) {
-        T q = Uraw + dt * r;
-        us[o] = q + dt * T(1);
+        ws[o] = W0 + dt * r;
       } else {
-        r += forcing;
-        us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
-        ru[o] = r;
+        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
+        rw[o] = r;
       }
     }
-    // ---------------- v at cell k ----------------
-    {
-      const T V0 = V.c(k, j, i), Vxm = V.c(k, j, im), Vxp = V.c(k, j, ip);
-      const T Vym = V.c(k, jm, i), Vyp = V.c(k, jp, i);
-      const T Vzm = V.c(k - 1, j, i), Vzp = V.c(k + 1, j, i);
-      const bool edge = (j == ny - 1);
-      T r = T(0);
-      if (!(edge && g.rhs_fused)) {
-        r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
-        if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
-      }
-      if (!edge) {
-        const T uv_r = h * (U.c(k, j, i) + U.c(k, j + 1, i)) * (h * (V0 + Vxp));
-        const T uv_l = h * (U.c(k, j, im) + U.c(k, j + 1, im)) * (h * (Vxm + V0));
-        const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
-        const T wv_t = h * (W.f(k + 1, j, i) + W.f(k + 1, j + 1, i)) * (h * (V0 + Vzp));
-        const T wv_b = h * (W.f(k, j, i) + W.f(k, j + 1, i)) * (h * (Vzm + V0));
-        r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
-      }
-      const size_t o = pidx(k, j, i, ny, nx);
-      if (UPD == UPD_RHS_ONLY) {
-        rv[o] = r;
-      } else if (UPD == UPD_FE) {
-        vs[o] = V0 + dt * r;
-      } else {
-        vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
-        rv[o] = r;
-      }
-    }
-  }
-  // ---------------- w at face k ----------------
-  if (k >= 1 && k <= nz - 1) {
-    const int f = k;
-    const T W0 = W.f(f, j, i), Wxm = W.f(f, j, im), Wxp = W.f(f, j, ip);
-    const T Wym = W.f(f, jm, i), Wyp = W.f(f, jp, i);
-    const T Wzm = W.f(f - 1, j, i), Wzp = W.f(f + 1, j, i);
-    T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
-    // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
-    if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[f] - (W0 - Wzm) * g.idzf[f - 1]) * g.idzc[f - 1];
-    const T uw_r = h * (U.c(f - 1, j, i) + U.c(f, j, i)) * (h * (W0 + Wxp));
-    const T uw_l = h * (U.c(f - 1, j, im) + U.c(f, j, im)) * (h * (Wxm + W0));
-    const T vw_t = h * (V.c(f - 1, j, i) + V.c(f, j, i)) * (h * (W0 + Wyp));
-    const T vw_b = h * (V.c(f - 1, jm, i) + V.c(f, jm, i)) * (h * (Wym + W0));
-    const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[f];
-    r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
-    const size_t o = pidx(f, j, i, ny, nx);
-    if (UPD == UPD_RHS_ONLY) {
-      rw[o] = r;
-    } else if (UPD == UPD_FE) {
-      ws[o] = W0 + dt * r;
-    } else {
-      ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
-      rw[o] = r;
-    }
+    __syncthreads();          // everyone is done with the slot of plane k-1
+    put(slot_of(k + 2));      // == slot of plane k-1
+    __syncthreads();
   }
 }
 
@@ -374,9 +441,12 @@ struct BulkArgs {
 // ---------------------------------------------------------------------------
 // Kernel (d): projection u -= dt grad p (projection.py:143-165), in place,
 // fused with the bulk velocity (utils.py:207-223: sum of u dz_f dx dy / V over
-// all DOFs) and the PI forcing update: every block writes its partial sum, the
-// last block to finish reduces them in a fixed order.  p is FP64.
+// all DOFs) and the PI forcing update.  Each thread walks PROJ_KC planes of
+// one (i, j) column (p of the plane below is carried in a register); every
+// block writes one partial sum and the last block to finish reduces them in a
+// fixed order.  p is FP64.
 // ---------------------------------------------------------------------------
+#define PROJ_KC 16
 template <class T>
 __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
                                                       T* __restrict__ w, const double* __restrict__ p, double dt,
@@ -386,21 +456,25 @@ __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * PROJ_KC;
+  const int k1 = min(k0 + PROJ_KC, nz);
   double acc = 0.0;
   if (i < nx && j < ny) {
     const int ip = wrap(i + 1, nx), jp = wrap(j + 1, ny);
-    if (k < nz) {
-      const double P0 = ldg(p + pidx(k, j, i, ny, nx));
+    const double idx = (double)g.idx, idy = (double)g.idy;
+    double pbelow = (k0 > 0) ? ldg(p + pidx(k0 - 1, j, i, ny, nx)) : 0.0;
+#pragma unroll 4
+    for (int k = k0; k < k1; ++k) {
       const size_t o = pidx(k, j, i, ny, nx);
-      T un = (T)((double)u[o] - dt * ((ldg(p + pidx(k, j, ip, ny, nx)) - P0) * (double)g.idx));
+      const double P0 = ldg(p + o);
+      const double Pxp = ldg(p + pidx(k, j, ip, ny, nx));
+      const double Pyp = ldg(p + pidx(k, jp, i, ny, nx));
+      T un = (T)((double)u[o] - dt * ((Pxp - P0) * idx));
       u[o] = un;
-      v[o] = (T)((double)v[o] - dt * ((ldg(p + pidx(k, jp, i, ny, nx)) - P0) * (double)g.idy));
-      acc = ((double)un + (g.ubase_d ? g.ubase_d[k] : 0.0)) * dzf[k];
-    }
-    if (k >= 1 && k <= nz - 1) {
-      const size_t o = pidx(k, j, i, ny, nx);
-      w[o] = (T)((double)w[o] - dt * ((ldg(p + o) - ldg(p + pidx(k - 1, j, i, ny, nx))) * (double)g.idzc[k]));
+      v[o] = (T)((double)v[o] - dt * ((Pyp - P0) * idy));
+      acc += ((double)un + (g.ubase_d ? g.ubase_d[k] : 0.0)) * dzf[k];
+      if (k >= 1) w[o] = (T)((double)w[o] - dt * ((P0 - pbelow) * (double)g.idzc[k]));
+      pbelow = P0;
     }
   }
   double s = block_sum(acc, sh);
