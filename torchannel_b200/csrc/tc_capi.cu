@@ -177,19 +177,18 @@ static void fill_basic(tc_ctx* c, const tc_grid_desc* g) {
   fft_make_plan(g->nx, &c->planx);
   fft_make_plan(g->ny, &c->plany);
   // launch shapes: x transform rows per block (even divisor of ny, smem <= 100 KB)
-  const size_t cb = 2 * c->tsz;
   int JT = 16;
-  while (JT > 2 && (c->ny % JT != 0 || (size_t)2 * (JT / 2) * (c->nx + 2) * cb > 100 * 1024)) JT -= 2;
+  while (JT > 2 && (c->ny % JT != 0 || ((size_t)2 * (JT / 2) * (c->nx + 2) + c->nx) * 16 > 100 * 1024)) JT -= 2;
   c->JT = JT;
   int RB = 8;
-  while (RB > 1 && (size_t)2 * RB * c->ny * cb > 100 * 1024) RB /= 2;
+  while (RB > 1 && ((size_t)2 * RB + 1) * c->ny * 16 > 100 * 1024) RB /= 2;
   c->RB = RB;
   c->tri_bt = (64 * (size_t)c->nz * 8 <= 200 * 1024) ? 64 : 32;
   int sRB = 8;
-  while (sRB > 1 && (size_t)2 * sRB * c->nx * 16 > 100 * 1024) sRB /= 2;
+  while (sRB > 1 && ((size_t)2 * sRB + 1) * c->nx * 16 > 100 * 1024) sRB /= 2;
   c->stats_RB = sRB;
   int sCB = 8;
-  while (sCB > 1 && (size_t)2 * sCB * c->ny * 16 > 100 * 1024) sCB /= 2;
+  while (sCB > 1 && ((size_t)2 * sCB + 1) * c->ny * 16 > 100 * 1024) sCB /= 2;
   c->stats_CB = sCB;
 }
 
@@ -361,11 +360,11 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   Grid<T> g = make_grid<T>(c);
   const int nx = c->nx, ny = c->ny, nz = c->nz, nxh = c->nxh;
   cpx<double>* X = c->X;
-  const size_t smx = (size_t)2 * (c->JT / 2) * (nx + 2) * sizeof(cpx<double>);
+  const size_t smx = ((size_t)2 * (c->JT / 2) * (nx + 2) + nx) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTX, s);
   k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, c->twx_d, scale, c->JT);
   const int nrows = nxh * nz;
-  const size_t smy = (size_t)2 * c->RB * ny * sizeof(cpx<double>);
+  const size_t smy = ((size_t)2 * c->RB * ny + ny) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTY, s);
   k_ffty<false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
@@ -387,8 +386,8 @@ static double bulk_scale(const tc_ctx* c) { return c->dx * c->dy / (c->Lx * c->L
 template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, int update_forcing, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
   BulkArgs ba{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, update_forcing};
-  k_project_bulk<T><<<grid3(c, (c->nz + PROJ_KC - 1) / PROJ_KC), dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt,
-                                                                                      c->dzf_d, ba);
+  dim3 grd((c->nx / 2 + 31) / 32, (c->ny + 7) / 8, c->nz);
+  k_project_bulk<T><<<grd, dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt, c->dzf_d, ba);
   TC_LAUNCHED();
   return TC_OK;
 }
@@ -400,7 +399,7 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   T** B = (T**)c->st[nxt];
   T** R = (T**)c->rh;
   dim3 blk(RHS_TX, RHS_TY);
-  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + RHS_KC - 1) / RHS_KC);
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, c->nz + 1);
   if (scheme == TC_IMEX && c->tab_dt != dt) {
     k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
     c->tab_dt = dt;
@@ -486,10 +485,10 @@ template <class T> static int stats_impl(tc_ctx* c, cudaStream_t s) {
   k_stats_fill<T><<<(nx * ny + 255) / 256, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, c->k_bot - 1, c->k_top - 1,
                                                         ubase_of(c), c->st_means, c->st_S);
   const int nrows = 3 * ny;
-  k_fft_rows_d<false><<<(nrows + c->stats_RB - 1) / c->stats_RB, 256, (size_t)2 * c->stats_RB * nx * 16, s>>>(
+  k_fft_rows_d<false><<<(nrows + c->stats_RB - 1) / c->stats_RB, 256, ((size_t)2 * c->stats_RB + 1) * nx * 16, s>>>(
       c->st_S, nrows, nx, c->planx, c->twx_d, c->stats_RB);
   const int bpp = (nx + c->stats_CB - 1) / c->stats_CB;
-  k_fft_cols<false><<<3 * bpp, 256, (size_t)2 * c->stats_CB * ny * 16, s>>>(c->st_S, nx, ny, nx, (size_t)nx * ny,
+  k_fft_cols<false><<<3 * bpp, 256, ((size_t)2 * c->stats_CB + 1) * ny * 16, s>>>(c->st_S, nx, ny, nx, (size_t)nx * ny,
                                                                           c->plany, c->twy_d, c->stats_CB);
   const int nspec = (nx / 2) * (ny / 2);
   k_stats_spec<<<(nspec + 127) / 128, 128, 0, s>>>(c->st_S, nx, ny, c->st_spec);
@@ -503,7 +502,7 @@ template <class T> static int rhs_hook_impl(tc_ctx* c, int full, double* ru, dou
   T** B = (T**)c->st[c->cur ^ 1];  // scratch: the next buffer is free between steps
   const size_t ncell = (size_t)c->nx * c->ny * c->nz;
   cudaMemsetAsync(B[2], 0, ncell / c->nz * (c->nz + 1) * sizeof(T), s);
-  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + RHS_KC - 1) / RHS_KC);
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, c->nz + 1);
   if (full)
     k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, RHS_TY), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                    B[0], B[1], B[2], c->scal, (T)0, 0);

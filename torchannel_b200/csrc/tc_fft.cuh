@@ -1,9 +1,10 @@
-// Hand-written mixed-radix (4, 2, 3) complex FFTs on batches of rows held in
+// Hand-written mixed-radix (8, 4, 2, 3) complex FFTs on batches of rows held in
 // shared memory.  Stockham autosort formulation (Govindaraju et al., "High
 // performance discrete Fourier transforms on graphics processors", SC'08):
 // every stage reads one buffer and writes the other in natural order, so no
 // bit reversal pass is needed.  Twiddles come from a table
-// tw[m] = exp(-2*pi*i*m/N), m < N, computed on the host in FP64.
+// tw[m] = exp(-2*pi*i*m/N), m < N, computed on the host in FP64 and staged in
+// shared memory by the calling kernel.
 //
 // These transforms replace torch.fft.rfft2 / irfft2 of the reference
 // (projection_fft.py:118,139; turbstats.py:165-173).
@@ -20,13 +21,14 @@ struct FftPlan {
   int radix[TC_FFT_MAX_STAGES];
 };
 
-// Host-side: factor n into stages of 4, 2 and 3.  Returns 0 when n has any
+// Host-side: factor n into stages of 8, 4, 2 and 3.  Returns 0 when n has any
 // other prime factor.
 inline int fft_make_plan(int n, FftPlan* p) {
   p->n = n;
   p->nstages = 0;
   if (n < 1) return 0;
   int m = n;
+  while (m % 8 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 8; m /= 8; }
   while (m % 4 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 4; m /= 4; }
   while (m % 2 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 2; m /= 2; }
   while (m % 3 == 0) { if (p->nstages >= TC_FFT_MAX_STAGES) return 0; p->radix[p->nstages++] = 3; m /= 3; }
@@ -51,6 +53,29 @@ template <class T, bool INV> __device__ __forceinline__ void dft4(cpx<T>* v) {
   v[2] = csub(s02, s13);
   v[1] = cadd(d02, d13);
   v[3] = csub(d02, d13);
+}
+
+// radix 8 from two radix-4 halves: y_k = E_k + W8^k O_k, y_{k+4} = E_k - W8^k O_k
+template <class T, bool INV> __device__ __forceinline__ void dft8(cpx<T>* v) {
+  const T r = (T)0.70710678118654752440084436210485;  // 1/sqrt(2)
+  cpx<T> e[4] = {v[0], v[2], v[4], v[6]};
+  cpx<T> o[4] = {v[1], v[3], v[5], v[7]};
+  dft4<T, INV>(e);
+  dft4<T, INV>(o);
+  {  // W8^1 = (1 -/+ i)/sqrt(2)
+    T a = o[1].x, b = o[1].y;
+    o[1] = INV ? cmake<T>((a - b) * r, (a + b) * r) : cmake<T>((a + b) * r, (b - a) * r);
+  }
+  o[2] = mul_mi<T, INV>(o[2]);  // W8^2 = -/+ i
+  {  // W8^3 = (-1 -/+ i)/sqrt(2)
+    T a = o[3].x, b = o[3].y;
+    o[3] = INV ? cmake<T>((-a - b) * r, (a - b) * r) : cmake<T>((b - a) * r, -(a + b) * r);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    v[q] = cadd(e[q], o[q]);
+    v[q + 4] = csub(e[q], o[q]);
+  }
 }
 
 // y1 = x0 - (x1+x2)/2 -/+ i s (x1-x2), y2 = x0 - (x1+x2)/2 +/- i s (x1-x2), s = sqrt(3)/2
@@ -91,11 +116,20 @@ __device__ __forceinline__ void fft_stage(const cpx<T>* __restrict__ x, cpx<T>* 
     }
     if (R == 2) dft2<T, INV>(v);
     else if (R == 4) dft4<T, INV>(v);
+    else if (R == 8) dft8<T, INV>(v);
     else dft3<T, INV>(v);
     int o = (j / Ns) * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) yb[o + r * Ns] = v[r];
   }
+}
+
+// Stage a twiddle table of n entries into shared memory (callers then pass
+// the shared copy to fft_rows).  No trailing barrier: fft_rows callers
+// synchronise after loading their data.
+template <class T>
+__device__ __forceinline__ void stage_twiddles(cpx<T>* dst, const cpx<T>* __restrict__ src, int n, int tid, int nthr) {
+  for (int e = tid; e < n; e += nthr) dst[e] = src[e];
 }
 
 // Batched in-smem FFT.  Data starts in buf[0]; returns the index (0/1) of the
@@ -109,7 +143,8 @@ __device__ int fft_rows(cpx<T>* buf0, cpx<T>* buf1, int batch, int rs, const Fft
   int Ns = 1;
   for (int s = 0; s < pl.nstages; ++s) {
     int R = pl.radix[s];
-    if (R == 4) fft_stage<T, INV, 4>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    if (R == 8) fft_stage<T, INV, 8>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    else if (R == 4) fft_stage<T, INV, 4>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
     else if (R == 2) fft_stage<T, INV, 2>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
     else fft_stage<T, INV, 3>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
     Ns *= R;

@@ -36,8 +36,10 @@ __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict
   const int rs = nx + 2;
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + (JT / 2) * rs;
+  cpx<double>* stw = b1 + (JT / 2) * rs;  // twiddles (nx)
   const int k = blockIdx.y, j0 = blockIdx.x * JT;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  stage_twiddles(stw, twx, nx, tid, nthr);
   // grid reciprocals are read only on the divergence path (a field-only
   // caller may pass a grid without z tables)
   const double idx = (double)g.idx, idy = (double)g.idy;
@@ -58,7 +60,7 @@ __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict
     dst[r & 1] = val;
   }
   __syncthreads();
-  int which = fft_rows<double, false>(b0, b1, JT / 2, rs, plx, twx, tid, nthr);
+  int which = fft_rows<double, false>(b0, b1, JT / 2, rs, plx, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nxh * JT; e += nthr) {
     int m = e / JT, r = e - m * JT, pr = r >> 1;
@@ -81,13 +83,15 @@ __global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int n
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + RB * ny;
+  cpx<double>* stw = b1 + RB * ny;  // twiddles (ny)
   const int r0 = blockIdx.x * RB;
   const int nb = min(RB, nrows - r0);
   const int tid = threadIdx.x, nthr = blockDim.x;
   cpx<double>* base = X + (size_t)r0 * ny;
+  stage_twiddles(stw, twy, ny, tid, nthr);
   for (int e = tid; e < nb * ny; e += nthr) b0[e] = base[e];
   __syncthreads();
-  int which = fft_rows<double, INV>(b0, b1, nb, ny, ply, twy, tid, nthr);
+  int which = fft_rows<double, INV>(b0, b1, nb, ny, ply, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nb * ny; e += nthr) base[e] = Z[e];
 }
@@ -98,7 +102,7 @@ __global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int n
 // last unknown is pinned to 0 (explicit gauge) instead of dividing by the
 // roundoff-level pivot.  FP64; d' in place in X, c' in shared memory.  Loads
 // are issued TRI_B levels ahead of the dependent recurrence.
-#define TRI_B 8
+#define TRI_B 32
 __global__ void __launch_bounds__(64) k_tri(cpx<double>* __restrict__ X, PoissonTabs tb, int nxh, int ny, int nz) {
   extern __shared__ double cps[];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -165,8 +169,10 @@ __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X
   const int nxh = nx / 2 + 1, rs = nx + 2;
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + (JT / 2) * rs;
+  cpx<double>* stw = b1 + (JT / 2) * rs;  // twiddles (nx)
   const int k = blockIdx.y, j0 = blockIdx.x * JT;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  stage_twiddles(stw, twx, nx, tid, nthr);
   // stage the half spectra: S[r][m] in b1 (JT * nxh <= JT/2 * rs entries)
   for (int e = tid; e < nxh * JT; e += nthr) {
     int m = e / JT, r = e - m * JT;
@@ -183,7 +189,7 @@ __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X
     b0[pr * rs + m] = cmake<double>(A.x - B.y, A.y + B.x);  // A + i B
   }
   __syncthreads();
-  int which = fft_rows<double, true>(b0, b1, JT / 2, rs, plx, twx, tid, nthr);
+  int which = fft_rows<double, true>(b0, b1, JT / 2, rs, plx, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < JT * nx; e += nthr) {
     int r = e / nx, i = e - r * nx;

@@ -94,6 +94,8 @@ __global__ void __launch_bounds__(256) k_fft_cols(cpx<double>* __restrict__ S, i
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + CB * nlen;
+  cpx<double>* stw = b1 + CB * nlen;
+  stage_twiddles(stw, tw, nlen, threadIdx.x, blockDim.x);
   const int blocks_per_plane = (ncols_per_plane + CB - 1) / CB;
   const int plane = blockIdx.x / blocks_per_plane;
   const int c0 = (blockIdx.x - plane * blocks_per_plane) * CB;
@@ -105,7 +107,7 @@ __global__ void __launch_bounds__(256) k_fft_cols(cpx<double>* __restrict__ S, i
     b0[c * nlen + r] = base[(size_t)r * cs + c];
   }
   __syncthreads();
-  int which = fft_rows<double, INV>(b0, b1, nc, nlen, pl, tw, tid, nthr);
+  int which = fft_rows<double, INV>(b0, b1, nc, nlen, pl, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nc * nlen; e += nthr) {
     int r = e / nc, c = e - r * nc;
@@ -120,12 +122,14 @@ __global__ void __launch_bounds__(256) k_fft_rows_d(cpx<double>* __restrict__ S,
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + RB * nlen;
+  cpx<double>* stw = b1 + RB * nlen;
+  stage_twiddles(stw, tw, nlen, threadIdx.x, blockDim.x);
   const int r0 = blockIdx.x * RB;
   const int nb = min(RB, nrows - r0);
   cpx<double>* base = S + (size_t)r0 * nlen;
   for (int e = threadIdx.x; e < nb * nlen; e += blockDim.x) b0[e] = base[e];
   __syncthreads();
-  int which = fft_rows<double, INV>(b0, b1, nb, nlen, pl, tw, threadIdx.x, blockDim.x);
+  int which = fft_rows<double, INV>(b0, b1, nb, nlen, pl, stw, threadIdx.x, blockDim.x);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = threadIdx.x; e < nb * nlen; e += blockDim.x) base[e] = Z[e];
 }

@@ -42,18 +42,17 @@ enum : int {
 // (:1037-1225) and _v2 (:818-1034), AB2 combine solver.py:626-651.
 // FULL=false: IMEX (x/y diffusion only); FULL=true: full Laplacian (AB2/FE).
 //
-// 2.5-D z march: a block owns a RHS_TX x RHS_TY column tile and walks
-// RHS_KC planes; iteration k computes u, v at cell k and w at face k.  The
-// u, v, w planes k-1, k, k+1 (periodic x/y halo of one cell, z ghosts already
-// applied, u with its base profile added) sit in a 3-slot shared-memory ring;
-// plane k+2 is fetched into registers while plane k is computed.
+// A block owns a RHS_TX x RHS_TY tile of one plane k and computes u, v at
+// cell k and w at face k.  It first stages the u, v, w planes k-1, k, k+1 of
+// the tile with a one-cell periodic halo (z ghosts applied, u with its base
+// profile added) in shared memory -- every load of the block is independent
+// and issued up front -- then evaluates the stencils from shared memory.
 // Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
 // v[:, ny]; both reference paths omit advection there, the separate-op path
 // keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
 // ---------------------------------------------------------------------------
 #define RHS_TX 32
 #define RHS_TY 8
-#define RHS_KC 16
 #define RHS_HX (RHS_TX + 2)
 #define RHS_HY (RHS_TY + 2)
 #define RHS_NH (RHS_HX * RHS_HY)
@@ -75,150 +74,125 @@ __global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const
   const int i0 = blockIdx.x * RHS_TX, j0 = blockIdx.y * RHS_TY;
   const int i = i0 + tx, j = j0 + ty;
   const bool active = (i < nx) && (j < ny);
-  const int kb = blockIdx.z * RHS_KC;
-  const int ke = min(kb + RHS_KC, nz + 1);
+  const int k = blockIdx.z;  // cell k for u, v (k < nz); face k for w (1 <= k <= nz-1)
   const T top = g.top_neumann ? T(1) : T(-1);
   const T h = T(0.5);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
   const T* __restrict__ base = g.ubase_t;
-
-  // halo elements owned by this thread for plane loads: e0 = tid, e1 = tid + 256
-  const int e1 = tid + RHS_TX * RHS_TY;
-  const bool has1 = e1 < RHS_NH;
-  const int hy0 = tid / RHS_HX, hx0 = tid - hy0 * RHS_HX;
-  const int hy1 = e1 / RHS_HX, hx1 = e1 - hy1 * RHS_HX;
-  auto modp = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
-  const size_t off0 = (size_t)modp(j0 - 1 + hy0, ny) * nx + modp(i0 - 1 + hx0, nx);
-  const size_t off1 = has1 ? (size_t)modp(j0 - 1 + hy1, ny) * nx + modp(i0 - 1 + hx1, nx) : 0;
-
   auto bk = [&](int p) { return base ? ldg(base + p) : T(0); };
-  auto ucell = [&](const T* q, bool isu, int p, size_t off) -> T {
-    if (p < -1 || p > nz) return T(0);
-    if (p == -1) return -(ldg(q + off) + (isu ? bk(0) : T(0)));
-    if (p == nz) return top * (ldg(q + (size_t)(nz - 1) * plane + off) + (isu ? bk(nz - 1) : T(0)));
-    return ldg(q + (size_t)p * plane + off) + (isu ? bk(p) : T(0));
-  };
-  auto wface = [&](int p, size_t off) -> T {
-    if (p < 0 || p > nz) return T(0);
-    return ldg(w + (size_t)p * plane + off);
-  };
-  T reg[6];
-  auto fetch = [&](int p) {
-    reg[0] = ucell(u, true, p, off0);
-    reg[1] = ucell(v, false, p, off0);
-    reg[2] = wface(p, off0);
-    if (has1) {
-      reg[3] = ucell(u, true, p, off1);
-      reg[4] = ucell(v, false, p, off1);
-      reg[5] = wface(p, off1);
+  // stage planes k-1, k, k+1 (slot 0, 1, 2)
+  for (int e = tid; e < 3 * RHS_NH; e += RHS_TX * RHS_TY) {
+    const int sl = e / RHS_NH, r = e - sl * RHS_NH;
+    const int hy = r / RHS_HX, hx = r - hy * RHS_HX;
+    int jj = (j0 - 1 + hy) % ny; if (jj < 0) jj += ny;
+    int ii = (i0 - 1 + hx) % nx; if (ii < 0) ii += nx;
+    const size_t off = (size_t)jj * nx + ii;
+    const int p = k - 1 + sl;
+    T uu, vv, ww;
+    if (p < 0) {
+      uu = -(ldg(u + off) + bk(0));
+      vv = -ldg(v + off);
+    } else if (p >= nz) {
+      uu = top * (ldg(u + (size_t)(nz - 1) * plane + off) + bk(nz - 1));
+      vv = top * ldg(v + (size_t)(nz - 1) * plane + off);
+    } else {
+      uu = ldg(u + (size_t)p * plane + off) + bk(p);
+      vv = ldg(v + (size_t)p * plane + off);
     }
-  };
-  auto put = [&](int slot) {
-    su[slot][hy0][hx0] = reg[0]; sv[slot][hy0][hx0] = reg[1]; sw[slot][hy0][hx0] = reg[2];
-    if (has1) { su[slot][hy1][hx1] = reg[3]; sv[slot][hy1][hx1] = reg[4]; sw[slot][hy1][hx1] = reg[5]; }
-  };
-  auto slot_of = [&](int p) { return (p - kb + 1) % 3; };  // p >= kb - 1
-
-  // prologue: planes kb-1, kb, kb+1
-  for (int p = kb - 1; p <= kb + 1; ++p) { fetch(p); put(slot_of(p)); }
+    ww = (p >= 0 && p <= nz) ? ldg(w + (size_t)p * plane + off) : T(0);
+    su[sl][hy][hx] = uu; sv[sl][hy][hx] = vv; sw[sl][hy][hx] = ww;
+  }
   __syncthreads();
-
   const int cx = tx + 1, cy = ty + 1;
-  for (int k = kb; k < ke; ++k) {
-    fetch(k + 2);  // in flight while plane k is computed
-    const int sm = slot_of(k - 1), s0 = slot_of(k), sp = slot_of(k + 1);
-    if (active && k < nz) {
-      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-      const T idzf = g.idzf[k];
-      // ---------------- u at cell k ----------------
-      {
-        const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
-        const T Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
-        const T Uzm = su[sm][cy][cx], Uzp = su[sp][cy][cx];
-        const bool edge = (i == nx - 1);
-        T r = T(0);
-        if (!(edge && g.rhs_fused)) {
-          r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
-          if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
-        }
-        if (!edge) {
-          const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
-          const T vu_t = h * (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (h * (U0 + Uyp));
-          const T vu_b = h * (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (h * (Uym + U0));
-          const T wu_t = h * (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (h * (U0 + Uzp));
-          const T wu_b = h * (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (h * (Uzm + U0));
-          r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
-        }
-        if (UPD == UPD_RHS_ONLY) {
-          ru[o] = r;
-        } else {
-          const T Uraw = base ? ldg(u + o) : U0;  // stored value (u - U0[k] in mixed precision)
-          if (UPD == UPD_FE) {
-            T q = Uraw + dt * r;
-            us[o] = q + dt * T(1);
-          } else {
-            r += forcing;
-            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
-            ru[o] = r;
-          }
-        }
+  const int sm = 0, s0 = 1, sp = 2;
+  if (active && k < nz) {
+    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+    const T idzf = g.idzf[k];
+    // ---------------- u at cell k ----------------
+    {
+      const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
+      const T Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
+      const T Uzm = su[sm][cy][cx], Uzp = su[sp][cy][cx];
+      const bool edge = (i == nx - 1);
+      T r = T(0);
+      if (!(edge && g.rhs_fused)) {
+        r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
+        if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
       }
-      // ---------------- v at cell k ----------------
-      {
-        const T V0 = sv[s0][cy][cx], Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1];
-        const T Vym = sv[s0][cy - 1][cx], Vyp = sv[s0][cy + 1][cx];
-        const T Vzm = sv[sm][cy][cx], Vzp = sv[sp][cy][cx];
-        const bool edge = (j == ny - 1);
-        T r = T(0);
-        if (!(edge && g.rhs_fused)) {
-          r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
-          if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
-        }
-        if (!edge) {
-          const T uv_r = h * (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (h * (V0 + Vxp));
-          const T uv_l = h * (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (h * (Vxm + V0));
-          const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
-          const T wv_t = h * (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (h * (V0 + Vzp));
-          const T wv_b = h * (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (h * (Vzm + V0));
-          r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
-        }
-        if (UPD == UPD_RHS_ONLY) {
-          rv[o] = r;
-        } else if (UPD == UPD_FE) {
-          vs[o] = V0 + dt * r;
-        } else {
-          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
-          rv[o] = r;
-        }
+      if (!edge) {
+        const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
+        const T vu_t = h * (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (h * (U0 + Uyp));
+        const T vu_b = h * (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (h * (Uym + U0));
+        const T wu_t = h * (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (h * (U0 + Uzp));
+        const T wu_b = h * (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (h * (Uzm + U0));
+        r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
       }
-    }
-    // ---------------- w at face k ----------------
-    if (active && k >= 1 && k <= nz - 1) {
-      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-      const T W0 = sw[s0][cy][cx], Wxm = sw[s0][cy][cx - 1], Wxp = sw[s0][cy][cx + 1];
-      const T Wym = sw[s0][cy - 1][cx], Wyp = sw[s0][cy + 1][cx];
-      const T Wzm = sw[sm][cy][cx], Wzp = sw[sp][cy][cx];
-      T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
-      // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
-      if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
-      const T uw_r = h * (su[sm][cy][cx] + su[s0][cy][cx]) * (h * (W0 + Wxp));
-      const T uw_l = h * (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (h * (Wxm + W0));
-      const T vw_t = h * (sv[sm][cy][cx] + sv[s0][cy][cx]) * (h * (W0 + Wyp));
-      const T vw_b = h * (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (h * (Wym + W0));
-      const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[k];
-      r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
       if (UPD == UPD_RHS_ONLY) {
-        rw[o] = r;
-      } else if (UPD == UPD_FE) {
-        ws[o] = W0 + dt * r;
+        ru[o] = r;
       } else {
-        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
-        rw[o] = r;
+        const T Uraw = base ? ldg(u + o) : U0;  // stored value (u - U0[k] in mixed precision)
+        if (UPD == UPD_FE) {
+          T q = Uraw + dt * r;
+          us[o] = q + dt * T(1);
+        } else {
+          r += forcing;
+          us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
+          ru[o] = r;
+        }
       }
     }
-    __syncthreads();          // everyone is done with the slot of plane k-1
-    put(slot_of(k + 2));      // == slot of plane k-1
-    __syncthreads();
+    // ---------------- v at cell k ----------------
+    {
+      const T V0 = sv[s0][cy][cx], Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1];
+      const T Vym = sv[s0][cy - 1][cx], Vyp = sv[s0][cy + 1][cx];
+      const T Vzm = sv[sm][cy][cx], Vzp = sv[sp][cy][cx];
+      const bool edge = (j == ny - 1);
+      T r = T(0);
+      if (!(edge && g.rhs_fused)) {
+        r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
+        if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
+      }
+      if (!edge) {
+        const T uv_r = h * (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (h * (V0 + Vxp));
+        const T uv_l = h * (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (h * (Vxm + V0));
+        const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
+        const T wv_t = h * (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (h * (V0 + Vzp));
+        const T wv_b = h * (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (h * (Vzm + V0));
+        r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
+      }
+      if (UPD == UPD_RHS_ONLY) {
+        rv[o] = r;
+      } else if (UPD == UPD_FE) {
+        vs[o] = V0 + dt * r;
+      } else {
+        vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
+        rv[o] = r;
+      }
+    }
+  }
+  // ---------------- w at face k ----------------
+  if (active && k >= 1 && k <= nz - 1) {
+    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+    const T W0 = sw[s0][cy][cx], Wxm = sw[s0][cy][cx - 1], Wxp = sw[s0][cy][cx + 1];
+    const T Wym = sw[s0][cy - 1][cx], Wyp = sw[s0][cy + 1][cx];
+    const T Wzm = sw[sm][cy][cx], Wzp = sw[sp][cy][cx];
+    T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
+    // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+    if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
+    const T uw_r = h * (su[sm][cy][cx] + su[s0][cy][cx]) * (h * (W0 + Wxp));
+    const T uw_l = h * (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (h * (Wxm + W0));
+    const T vw_t = h * (sv[sm][cy][cx] + sv[s0][cy][cx]) * (h * (W0 + Wyp));
+    const T vw_b = h * (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (h * (Wym + W0));
+    const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[k];
+    r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
+    if (UPD == UPD_RHS_ONLY) {
+      rw[o] = r;
+    } else if (UPD == UPD_FE) {
+      ws[o] = W0 + dt * r;
+    } else {
+      ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
+      rw[o] = r;
+    }
   }
 }
 
@@ -420,8 +394,15 @@ enum : int {
 // forcing += (U_b - u_b)/dt * 0.1 (solver.py:701-708), done by one block.
 __device__ __forceinline__ void bulk_reduce_block(const double* partials, int n, double* scal, double scale,
                                                   double U_target, double dt, int update_forcing, double* sh) {
-  double acc = 0.0;
-  for (int e = threadIdx.x + blockDim.x * threadIdx.y; e < n; e += blockDim.x * blockDim.y) acc += __ldcg(partials + e);
+  const int t = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  double a8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int e = t;
+  for (; e + 7 * nt < n; e += 8 * nt) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a8[q] += __ldcg(partials + e + q * nt);
+  }
+  for (; e < n; e += nt) a8[0] += __ldcg(partials + e);
+  double acc = ((a8[0] + a8[1]) + (a8[2] + a8[3])) + ((a8[4] + a8[5]) + (a8[6] + a8[7]));
   double s = block_sum(acc, sh);
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     double ub = s * scale;
@@ -441,40 +422,50 @@ struct BulkArgs {
 // ---------------------------------------------------------------------------
 // Kernel (d): projection u -= dt grad p (projection.py:143-165), in place,
 // fused with the bulk velocity (utils.py:207-223: sum of u dz_f dx dy / V over
-// all DOFs) and the PI forcing update.  Each thread walks PROJ_KC planes of
-// one (i, j) column (p of the plane below is carried in a register); every
-// block writes one partial sum and the last block to finish reduces them in a
-// fixed order.  p is FP64.
+// all DOFs) and the PI forcing update.  Each thread owns two x-adjacent points
+// of one plane and moves them with 2-wide vector loads/stores; every block
+// writes one partial sum and the last block to finish reduces them in a fixed
+// order.  p is FP64.  nx is even, so the pairs never straddle a row.
 // ---------------------------------------------------------------------------
-#define PROJ_KC 16
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using t = double2; };
+template <> struct Vec2<float> { using t = float2; };
+
 template <class T>
 __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
                                                       T* __restrict__ w, const double* __restrict__ p, double dt,
                                                       const double* __restrict__ dzf, BulkArgs ba) {
+  using V2 = typename Vec2<T>::t;
   __shared__ double sh[32];
   __shared__ int last;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k0 = blockIdx.z * PROJ_KC;
-  const int k1 = min(k0 + PROJ_KC, nz);
+  const int k = blockIdx.z;
   double acc = 0.0;
   if (i < nx && j < ny) {
-    const int ip = wrap(i + 1, nx), jp = wrap(j + 1, ny);
-    const double idx = (double)g.idx, idy = (double)g.idy;
-    double pbelow = (k0 > 0) ? ldg(p + pidx(k0 - 1, j, i, ny, nx)) : 0.0;
-#pragma unroll 4
-    for (int k = k0; k < k1; ++k) {
-      const size_t o = pidx(k, j, i, ny, nx);
-      const double P0 = ldg(p + o);
-      const double Pxp = ldg(p + pidx(k, j, ip, ny, nx));
-      const double Pyp = ldg(p + pidx(k, jp, i, ny, nx));
-      T un = (T)((double)u[o] - dt * ((Pxp - P0) * idx));
-      u[o] = un;
-      v[o] = (T)((double)v[o] - dt * ((Pyp - P0) * idy));
-      acc += ((double)un + (g.ubase_d ? g.ubase_d[k] : 0.0)) * dzf[k];
-      if (k >= 1) w[o] = (T)((double)w[o] - dt * ((P0 - pbelow) * (double)g.idzc[k]));
-      pbelow = P0;
+    const int jp = wrap(j + 1, ny), ipp = wrap(i + 2, nx);
+    const size_t o = pidx(k, j, i, ny, nx);
+    const double2 P = *reinterpret_cast<const double2*>(p + o);
+    const double P2 = ldg(p + pidx(k, j, ipp, ny, nx));
+    const double2 Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
+    V2 uu = *reinterpret_cast<V2*>(u + o);
+    V2 vv = *reinterpret_cast<V2*>(v + o);
+    const double cx = dt * (double)g.idx, cy = dt * (double)g.idy;
+    uu.x = (T)((double)uu.x - cx * (P.y - P.x));
+    uu.y = (T)((double)uu.y - cx * (P2 - P.y));
+    vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
+    vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
+    *reinterpret_cast<V2*>(u + o) = uu;
+    *reinterpret_cast<V2*>(v + o) = vv;
+    acc = ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
+    if (k >= 1) {
+      const double2 Pm = *reinterpret_cast<const double2*>(p + pidx(k - 1, j, i, ny, nx));
+      const double cz = dt * (double)g.idzc[k];
+      V2 ww = *reinterpret_cast<V2*>(w + o);
+      ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
+      ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
+      *reinterpret_cast<V2*>(w + o) = ww;
     }
   }
   double s = block_sum(acc, sh);
