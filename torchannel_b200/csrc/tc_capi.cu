@@ -154,7 +154,7 @@ static size_t carve(tc_ctx* c, char* base) {
 
 static int validate(const tc_grid_desc* g) {
   if (!g) return fail(TC_ERR_ARG, "null grid descriptor");
-  if (g->nx < 4 || g->ny < 4 || g->nz < 4) return fail(TC_ERR_SIZE, "nx, ny, nz must be >= 4");
+  if (g->nx < 8 || g->ny < 8 || g->nz < 4) return fail(TC_ERR_SIZE, "nx, ny must be >= 8 and nz >= 4");
   if ((g->nx & 1) || (g->ny & 1)) return fail(TC_ERR_SIZE, "nx and ny must be even");
   if (g->nz > 800) return fail(TC_ERR_SIZE, "nz must be <= 800");
   FftPlan a, b;
@@ -178,17 +178,18 @@ static void fill_basic(tc_ctx* c, const tc_grid_desc* g) {
   fft_make_plan(g->ny, &c->plany);
   // launch shapes: x transform rows per block (even divisor of ny, smem <= 100 KB)
   int JT = 16;
-  while (JT > 2 && (c->ny % JT != 0 || ((size_t)2 * (JT / 2) * (c->nx + 2) + c->nx) * 16 > 100 * 1024)) JT -= 2;
+  while (JT > 2 && (c->ny % JT != 0 || ((size_t)2 * (JT / 2) * padded_len<double>(c->nx) + c->nx) * 16 > 100 * 1024))
+    JT -= 2;
   c->JT = JT;
   int RB = 8;
-  while (RB > 1 && ((size_t)2 * RB + 1) * c->ny * 16 > 100 * 1024) RB /= 2;
+  while (RB > 1 && ((size_t)2 * RB * padded_len<double>(c->ny) + c->ny) * 16 > 100 * 1024) RB /= 2;
   c->RB = RB;
   c->tri_bt = (64 * (size_t)c->nz * 8 <= 200 * 1024) ? 64 : 32;
   int sRB = 8;
-  while (sRB > 1 && ((size_t)2 * sRB + 1) * c->nx * 16 > 100 * 1024) sRB /= 2;
+  while (sRB > 1 && ((size_t)2 * sRB * padded_len<double>(c->nx) + c->nx) * 16 > 100 * 1024) sRB /= 2;
   c->stats_RB = sRB;
   int sCB = 8;
-  while (sCB > 1 && ((size_t)2 * sCB + 1) * c->ny * 16 > 100 * 1024) sCB /= 2;
+  while (sCB > 1 && ((size_t)2 * sCB * padded_len<double>(c->ny) + c->ny) * 16 > 100 * 1024) sCB /= 2;
   c->stats_CB = sCB;
 }
 
@@ -360,11 +361,11 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   Grid<T> g = make_grid<T>(c);
   const int nx = c->nx, ny = c->ny, nz = c->nz, nxh = c->nxh;
   cpx<double>* X = c->X;
-  const size_t smx = ((size_t)2 * (c->JT / 2) * (nx + 2) + nx) * sizeof(cpx<double>);
+  const size_t smx = ((size_t)2 * (c->JT / 2) * padded_len<double>(nx) + nx) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTX, s);
   k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, c->twx_d, scale, c->JT);
   const int nrows = nxh * nz;
-  const size_t smy = ((size_t)2 * c->RB * ny + ny) * sizeof(cpx<double>);
+  const size_t smy = ((size_t)2 * c->RB * padded_len<double>(ny) + ny) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTY, s);
   k_ffty<false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
@@ -485,10 +486,11 @@ template <class T> static int stats_impl(tc_ctx* c, cudaStream_t s) {
   k_stats_fill<T><<<(nx * ny + 255) / 256, 256, 0, s>>>(A[0], A[1], A[2], nx, ny, nz, c->k_bot - 1, c->k_top - 1,
                                                         ubase_of(c), c->st_means, c->st_S);
   const int nrows = 3 * ny;
-  k_fft_rows_d<false><<<(nrows + c->stats_RB - 1) / c->stats_RB, 256, ((size_t)2 * c->stats_RB + 1) * nx * 16, s>>>(
+  k_fft_rows_d<false><<<(nrows + c->stats_RB - 1) / c->stats_RB, 256,
+                        ((size_t)2 * c->stats_RB * padded_len<double>(nx) + nx) * 16, s>>>(
       c->st_S, nrows, nx, c->planx, c->twx_d, c->stats_RB);
   const int bpp = (nx + c->stats_CB - 1) / c->stats_CB;
-  k_fft_cols<false><<<3 * bpp, 256, ((size_t)2 * c->stats_CB + 1) * ny * 16, s>>>(c->st_S, nx, ny, nx, (size_t)nx * ny,
+  k_fft_cols<false><<<3 * bpp, 256, ((size_t)2 * c->stats_CB * padded_len<double>(ny) + ny) * 16, s>>>(c->st_S, nx, ny, nx, (size_t)nx * ny,
                                                                           c->plany, c->twy_d, c->stats_CB);
   const int nspec = (nx / 2) * (ny / 2);
   k_stats_spec<<<(nspec + 127) / 128, 128, 0, s>>>(c->st_S, nx, ny, c->st_spec);
@@ -961,8 +963,8 @@ static size_t noalloc_bytes(int nx, int ny, int nz, size_t off[8]) {
 extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, double Ly, const double* dz_f,
                                         const double* dz_c, const double* rhs, double* p, void* stream) {
   if (!dz_f || !dz_c || !rhs || !p) return fail(TC_ERR_ARG, "null argument");
-  if (nx < 4 || ny < 4 || nz < 4 || (nx & 1) || (ny & 1) || nz > 800 || !(Lx > 0) || !(Ly > 0))
-    return fail(TC_ERR_SIZE, "nx, ny even >= 4, 4 <= nz <= 800, Lx, Ly > 0 required");
+  if (nx < 8 || ny < 8 || nz < 4 || (nx & 1) || (ny & 1) || nz > 800 || !(Lx > 0) || !(Ly > 0))
+    return fail(TC_ERR_SIZE, "nx, ny even >= 8, 4 <= nz <= 800, Lx, Ly > 0 required");
   FftPlan a, b;
   if (!fft_make_plan(nx, &a) || !fft_make_plan(ny, &b) || nx > 4096 || ny > 4096)
     return fail(TC_ERR_SIZE, "nx and ny must factor into 2 and 3 only (<= 4096)");

@@ -89,23 +89,40 @@ template <class T, bool INV> __device__ __forceinline__ void dft3(cpx<T>* v) {
   v[2] = csub(t, r);
 }
 
-// One Stockham stage over `batch` rows of length n (row stride `rs` elements).
-template <class T, bool INV, int R>
+// Shared-memory layout of the transform buffers: element e of a row sits at
+// padi(e) = e + e/8 (FP64 complex) or e + e/16 (FP32 complex).  The early
+// Stockham stages store at a stride of R elements, which without the pad
+// would put a whole warp on one bank group.
+template <class T> __host__ __device__ __forceinline__ constexpr int pad_shift() {
+  return sizeof(cpx<T>) >= 16 ? 3 : 4;
+}
+template <class T> __device__ __forceinline__ int padi(int e) { return e + (e >> pad_shift<T>()); }
+// Row pitch of a padded row of n elements.
+template <class T> __host__ __device__ __forceinline__ int padded_len(int n) {
+  return n + (n >> pad_shift<T>()) + 1;
+}
+
+// One Stockham stage over `batch` rows (row pitch `rs`, padded layout).  NC
+// and NSC are the transform length and current span when known at compile
+// time (0: use the run-time n and Ns).
+template <class T, bool INV, int R, int NC, int NSC>
 __device__ __forceinline__ void fft_stage(const cpx<T>* __restrict__ x, cpx<T>* __restrict__ y, int batch,
-                                          int rs, int n, int Ns, const cpx<T>* __restrict__ tw, int tid,
+                                          int rs, int n_rt, int Ns_rt, const cpx<T>* __restrict__ tw, int tid,
                                           int nthr) {
+  const int n = NC ? NC : n_rt;
+  const int Ns = NC ? NSC : Ns_rt;
   const int nr = n / R;
   const int fac = n / (Ns * R);
   const int total = batch * nr;
   for (int idx = tid; idx < total; idx += nthr) {
-    int b = idx / nr;
-    int j = idx - b * nr;
+    const int b = idx / nr;
+    const int j = idx - b * nr;
     const cpx<T>* xb = x + (size_t)b * rs;
     cpx<T>* yb = y + (size_t)b * rs;
-    int k = j % Ns;
+    const int k = j % Ns;
     cpx<T> v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = xb[j + r * nr];
+    for (int r = 0; r < R; ++r) v[r] = xb[padi<T>(j + r * nr)];
     if (Ns > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
@@ -118,9 +135,9 @@ __device__ __forceinline__ void fft_stage(const cpx<T>* __restrict__ x, cpx<T>* 
     else if (R == 4) dft4<T, INV>(v);
     else if (R == 8) dft8<T, INV>(v);
     else dft3<T, INV>(v);
-    int o = (j / Ns) * Ns * R + k;
+    const int o = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) yb[o + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) yb[padi<T>(o + r * Ns)] = v[r];
   }
 }
 
@@ -132,21 +149,53 @@ __device__ __forceinline__ void stage_twiddles(cpx<T>* dst, const cpx<T>* __rest
   for (int e = tid; e < n; e += nthr) dst[e] = src[e];
 }
 
-// Batched in-smem FFT.  Data starts in buf[0]; returns the index (0/1) of the
-// buffer that holds the result.  Unnormalised in both directions.  All
-// threads of the block (tid < nthr) must call it; it synchronises.
+// Radix of the stage that starts at span NS of a length-N transform.
+template <int N, int NS> struct NextRadix {
+  static constexpr int rem = N / NS;
+  static constexpr int value = (rem % 8 == 0) ? 8 : (rem % 4 == 0) ? 4 : (rem % 2 == 0) ? 2 : 3;
+};
+
+// Compile-time-length batched FFT: returns the index (0: a, 1: b) of the
+// buffer holding the result.
+template <class T, bool INV, int N, int NS>
+__device__ __forceinline__ int fft_rows_c(cpx<T>* a, cpx<T>* b, int batch, int rs, const cpx<T>* __restrict__ tw,
+                                          int tid, int nthr) {
+  if constexpr (NS >= N) {
+    return 0;
+  } else {
+    constexpr int R = NextRadix<N, NS>::value;
+    fft_stage<T, INV, R, N, NS>(a, b, batch, rs, N, NS, tw, tid, nthr);
+    __syncthreads();
+    return 1 ^ fft_rows_c<T, INV, N, NS * R>(b, a, batch, rs, tw, tid, nthr);
+  }
+}
+
+// Batched in-smem FFT (padded layout).  Data starts in buf0; returns the
+// index (0/1) of the buffer that holds the result.  Unnormalised in both
+// directions.  All threads of the block must call it; it synchronises.
+// Common lengths use compile-time plans; others the run-time plan.
 template <class T, bool INV>
 __device__ int fft_rows(cpx<T>* buf0, cpx<T>* buf1, int batch, int rs, const FftPlan& pl,
                         const cpx<T>* __restrict__ tw, int tid, int nthr) {
+  switch (pl.n) {
+    case 64: return fft_rows_c<T, INV, 64, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    case 96: return fft_rows_c<T, INV, 96, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    case 128: return fft_rows_c<T, INV, 128, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    case 192: return fft_rows_c<T, INV, 192, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    case 256: return fft_rows_c<T, INV, 256, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    case 384: return fft_rows_c<T, INV, 384, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    case 768: return fft_rows_c<T, INV, 768, 1>(buf0, buf1, batch, rs, tw, tid, nthr);
+    default: break;
+  }
   cpx<T>* bufs[2] = {buf0, buf1};
   int cur = 0;
   int Ns = 1;
   for (int s = 0; s < pl.nstages; ++s) {
     int R = pl.radix[s];
-    if (R == 8) fft_stage<T, INV, 8>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
-    else if (R == 4) fft_stage<T, INV, 4>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
-    else if (R == 2) fft_stage<T, INV, 2>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
-    else fft_stage<T, INV, 3>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    if (R == 8) fft_stage<T, INV, 8, 0, 0>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    else if (R == 4) fft_stage<T, INV, 4, 0, 0>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    else if (R == 2) fft_stage<T, INV, 2, 0, 0>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
+    else fft_stage<T, INV, 3, 0, 0>(bufs[cur], bufs[cur ^ 1], batch, rs, pl.n, Ns, tw, tid, nthr);
     Ns *= R;
     cur ^= 1;
     __syncthreads();

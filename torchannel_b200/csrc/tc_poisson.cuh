@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict
                                                   const cpx<double>* __restrict__ twx, double scale, int JT) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxh = nx / 2 + 1;
-  const int rs = nx + 2;
+  const int rs = padded_len<double>(nx);
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + (JT / 2) * rs;
   cpx<double>* stw = b1 + (JT / 2) * rs;  // twiddles (nx)
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict
       val = field[pidx(k, j, i, ny, nx)];
     }
     val *= scale;
-    double* dst = reinterpret_cast<double*>(&b0[(r >> 1) * rs + i]);
+    double* dst = reinterpret_cast<double*>(&b0[(r >> 1) * rs + padi<double>(i)]);
     dst[r & 1] = val;
   }
   __syncthreads();
@@ -64,8 +64,8 @@ __global__ void __launch_bounds__(256) k_div_fftx(Grid<T> g, const T* __restrict
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nxh * JT; e += nthr) {
     int m = e / JT, r = e - m * JT, pr = r >> 1;
-    cpx<double> Zm = Z[pr * rs + m];
-    cpx<double> Zn = cconj(Z[pr * rs + (m == 0 ? 0 : nx - m)]);
+    cpx<double> Zm = Z[pr * rs + padi<double>(m)];
+    cpx<double> Zn = cconj(Z[pr * rs + padi<double>(m == 0 ? 0 : nx - m)]);
     cpx<double> out;
     if ((r & 1) == 0) out = cscale(cadd(Zm, Zn), 0.5);
     else {
@@ -81,19 +81,26 @@ template <bool INV>
 __global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int nrows, int ny, FftPlan ply,
                                               const cpx<double>* __restrict__ twy, int RB) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  const int rs = padded_len<double>(ny);
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
-  cpx<double>* b1 = b0 + RB * ny;
-  cpx<double>* stw = b1 + RB * ny;  // twiddles (ny)
+  cpx<double>* b1 = b0 + RB * rs;
+  cpx<double>* stw = b1 + RB * rs;  // twiddles (ny)
   const int r0 = blockIdx.x * RB;
   const int nb = min(RB, nrows - r0);
   const int tid = threadIdx.x, nthr = blockDim.x;
   cpx<double>* base = X + (size_t)r0 * ny;
   stage_twiddles(stw, twy, ny, tid, nthr);
-  for (int e = tid; e < nb * ny; e += nthr) b0[e] = base[e];
+  for (int e = tid; e < nb * ny; e += nthr) {
+    const int r = e / ny, jj = e - r * ny;
+    b0[r * rs + padi<double>(jj)] = base[e];
+  }
   __syncthreads();
-  int which = fft_rows<double, INV>(b0, b1, nb, ny, ply, stw, tid, nthr);
+  int which = fft_rows<double, INV>(b0, b1, nb, rs, ply, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
-  for (int e = tid; e < nb * ny; e += nthr) base[e] = Z[e];
+  for (int e = tid; e < nb * ny; e += nthr) {
+    const int r = e / ny, jj = e - r * ny;
+    base[e] = Z[r * rs + padi<double>(jj)];
+  }
 }
 
 // Thomas sweep along z for every mode (kx, ky), one thread per mode
@@ -166,14 +173,15 @@ __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X
                                                int ny, int nz, FftPlan plx, const cpx<double>* __restrict__ twx,
                                                int JT) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int nxh = nx / 2 + 1, rs = nx + 2;
+  const int nxh = nx / 2 + 1, rs = padded_len<double>(nx);
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
   cpx<double>* b1 = b0 + (JT / 2) * rs;
   cpx<double>* stw = b1 + (JT / 2) * rs;  // twiddles (nx)
   const int k = blockIdx.y, j0 = blockIdx.x * JT;
   const int tid = threadIdx.x, nthr = blockDim.x;
   stage_twiddles(stw, twx, nx, tid, nthr);
-  // stage the half spectra: S[r][m] in b1 (JT * nxh <= JT/2 * rs entries)
+  // stage the half spectra: S[r][m] in b1 (JT * nxh <= JT/2 * rs entries,
+  // unpadded: this staging is not an FFT buffer)
   for (int e = tid; e < nxh * JT; e += nthr) {
     int m = e / JT, r = e - m * JT;
     cpx<double> val = X[((size_t)m * nz + k) * ny + j0 + r];
@@ -186,14 +194,14 @@ __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X
     cpx<double> A, B;
     if (m < nxh) { A = b1[(2 * pr) * nxh + m]; B = b1[(2 * pr + 1) * nxh + m]; }
     else { A = cconj(b1[(2 * pr) * nxh + nx - m]); B = cconj(b1[(2 * pr + 1) * nxh + nx - m]); }
-    b0[pr * rs + m] = cmake<double>(A.x - B.y, A.y + B.x);  // A + i B
+    b0[pr * rs + padi<double>(m)] = cmake<double>(A.x - B.y, A.y + B.x);  // A + i B
   }
   __syncthreads();
   int which = fft_rows<double, true>(b0, b1, JT / 2, rs, plx, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < JT * nx; e += nthr) {
     int r = e / nx, i = e - r * nx;
-    cpx<double> z = Z[(r >> 1) * rs + i];
+    cpx<double> z = Z[(r >> 1) * rs + padi<double>(i)];
     p[pidx(k, j0 + r, i, ny, nx)] = (r & 1) ? z.y : z.x;
   }
 }

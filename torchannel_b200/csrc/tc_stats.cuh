@@ -92,9 +92,10 @@ __global__ void __launch_bounds__(256) k_fft_cols(cpx<double>* __restrict__ S, i
                                                   int cs, size_t plane_stride, FftPlan pl,
                                                   const cpx<double>* __restrict__ tw, int CB) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  const int rs = padded_len<double>(nlen);
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
-  cpx<double>* b1 = b0 + CB * nlen;
-  cpx<double>* stw = b1 + CB * nlen;
+  cpx<double>* b1 = b0 + CB * rs;
+  cpx<double>* stw = b1 + CB * rs;
   stage_twiddles(stw, tw, nlen, threadIdx.x, blockDim.x);
   const int blocks_per_plane = (ncols_per_plane + CB - 1) / CB;
   const int plane = blockIdx.x / blocks_per_plane;
@@ -104,14 +105,14 @@ __global__ void __launch_bounds__(256) k_fft_cols(cpx<double>* __restrict__ S, i
   const int tid = threadIdx.x, nthr = blockDim.x;
   for (int e = tid; e < nc * nlen; e += nthr) {
     int r = e / nc, c = e - r * nc;
-    b0[c * nlen + r] = base[(size_t)r * cs + c];
+    b0[c * rs + padi<double>(r)] = base[(size_t)r * cs + c];
   }
   __syncthreads();
-  int which = fft_rows<double, INV>(b0, b1, nc, nlen, pl, stw, tid, nthr);
+  int which = fft_rows<double, INV>(b0, b1, nc, rs, pl, stw, tid, nthr);
   const cpx<double>* Z = which ? b1 : b0;
   for (int e = tid; e < nc * nlen; e += nthr) {
     int r = e / nc, c = e - r * nc;
-    base[(size_t)r * cs + c] = Z[c * nlen + r];
+    base[(size_t)r * cs + c] = Z[c * rs + padi<double>(r)];
   }
 }
 
@@ -120,18 +121,25 @@ template <bool INV>
 __global__ void __launch_bounds__(256) k_fft_rows_d(cpx<double>* __restrict__ S, int nrows, int nlen, FftPlan pl,
                                                     const cpx<double>* __restrict__ tw, int RB) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  const int rs = padded_len<double>(nlen);
   cpx<double>* b0 = reinterpret_cast<cpx<double>*>(smraw);
-  cpx<double>* b1 = b0 + RB * nlen;
-  cpx<double>* stw = b1 + RB * nlen;
+  cpx<double>* b1 = b0 + RB * rs;
+  cpx<double>* stw = b1 + RB * rs;
   stage_twiddles(stw, tw, nlen, threadIdx.x, blockDim.x);
   const int r0 = blockIdx.x * RB;
   const int nb = min(RB, nrows - r0);
   cpx<double>* base = S + (size_t)r0 * nlen;
-  for (int e = threadIdx.x; e < nb * nlen; e += blockDim.x) b0[e] = base[e];
+  for (int e = threadIdx.x; e < nb * nlen; e += blockDim.x) {
+    const int r = e / nlen, q = e - r * nlen;
+    b0[r * rs + padi<double>(q)] = base[e];
+  }
   __syncthreads();
-  int which = fft_rows<double, INV>(b0, b1, nb, nlen, pl, stw, threadIdx.x, blockDim.x);
+  int which = fft_rows<double, INV>(b0, b1, nb, rs, pl, stw, threadIdx.x, blockDim.x);
   const cpx<double>* Z = which ? b1 : b0;
-  for (int e = threadIdx.x; e < nb * nlen; e += blockDim.x) base[e] = Z[e];
+  for (int e = threadIdx.x; e < nb * nlen; e += blockDim.x) {
+    const int r = e / nlen, q = e - r * nlen;
+    base[e] = Z[r * rs + padi<double>(q)];
+  }
 }
 
 // Separate the packed spectra and accumulate the folded, wall-averaged
