@@ -9,7 +9,10 @@ Workload (one "step" = one IMEX time step of the channel):
 Metric: grid-point-steps/s = nx*ny*nz*steps / seconds (whole job, all ranks).
 
 Arms:
-  default           this repo's CUDA path (precision: --precision, default mixed)
+  default           this repo's CUDA path, mixed precision (FP32 velocity fields
+                    and history; FP64 Poisson, tridiagonal arithmetic, bulk
+                    forcing); the plain FP64 form is timed in the same run as
+                    "fp64_plain" (--precision fp64 makes it the headline)
   --impl reference  the CPU oracle (numpy FP64 restatement of the reference
                     step, oracle/) on the host cores, bounded sample
 
@@ -47,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -179,6 +183,30 @@ def run_b200(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
+    # the other precision on the same state and dt, for the mixed-vs-FP64 comparison
+    other = None
+    if not a.no_fp64_compare and a.precision == "mixed":
+        ch2 = Channel(NX, NY, NZ, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision="fp64")
+        ch2.set_state(u0, v0, w0)
+        ub2 = ch2.bulk_velocity()
+        ch2.set_state(u0 * (1.0 / ub2), v0, w0)
+        ch2.project_initial()
+        ch2.step("IMEX", dt, 10 + a.warmup)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        ch2.step("IMEX", dt, a.steps)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms2 = f0.elapsed_time(f1)
+        if world > 1:
+            t = torch.tensor([ms2], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms2 = float(t.item())
+        d2 = ch2.diagnostics()
+        other = {"value": NX * NY * NZ * a.steps * world / (ms2 / 1e3), "ms_per_step": ms2 / a.steps,
+                 "max_div_after": d2["max_div"], "u_bulk": d2["u_bulk"], "u_tau": d2["u_tau"]}
+        del ch2
     # per-phase timing (separate, instrumented pass of the same steps)
     ch.timing(True)
     ch.step("IMEX", dt, min(a.steps, L_RING))
@@ -226,32 +254,40 @@ def run_b200(a):
         "gpu_launches": LAUNCHES_PER_STEP * a.steps,
         "max_div_after": diag["max_div"],
     }
+    if other is not None:
+        line["fp64_plain"] = other
+        line["mixed_speedup_over_fp64"] = value / other["value"]
+        line["mixed_vs_fp64_after_steps"] = {"u_bulk_abs_err": abs(diag["u_bulk"] - other["u_bulk"]),
+                                             "u_tau_rel_err": abs(diag["u_tau"] - other["u_tau"]) / other["u_tau"]}
     print(json.dumps(line), flush=True)
 
 
 L_RING = 64
-# kernels per IMEX step: rhs, cn, fftx, ffty, tri, iffty, ifftx, project, finalize
-LAUNCHES_PER_STEP = 9
+# kernels per IMEX step: rhs, cn, div+fftx, ffty, tri, iffty, ifftx, project(+bulk+forcing)
+LAUNCHES_PER_STEP = 8
 
 
 def kernel_table(phases, nst, s, npts):
     """Per-kernel average launch time and algorithmic bytes per launch.
-    Algorithmic words per grid point (stored precision s bytes; spectral words
-    counted as nx/2+1 complex per nx reals ~ 1 word):
-      rhs  : read u, v, w, r_prev; write u*, r           = 12
-      cn   : read u*, write u**                           = 6
-      fftx : read u**, v**, w** (div); write spectrum     = 4
-      ffty, tri, iffty : read + write spectrum            = 2 each (tri: + 2 FP64 scratch in mixed)
-      ifftx: read spectrum, write p                       = 2
-      proj : read u**, p; write u                         = 7
+    Bytes per grid point (s = storage bytes of the velocity fields and AB2
+    history, 8 FP64 / 4 mixed; the Poisson spectrum, p and the LU factor
+    tables are FP64; a half spectrum holds (nx/2+1)/nx complex per point):
+      rhs  : read u, v, w, r_prev; write u*, v*, w*, r      = 12 s
+      cn   : read u*, write u** (3 components)              =  6 s
+      fftx : read u**, v**, w** (divergence); write X       =  3 s + 16 h
+      ffty, iffty : read + write X                          = 32 h
+      tri  : read + write X, read the two factor tables     = 32 h + 16 h
+      ifftx: read X, write p                                = 16 h + 8
+      proj : read u**, v**, w**, p; write u, v, w           =  6 s + 8
+    with h = (nx/2+1)/nx.
     """
-    spec = (NX / 2 + 1) / (NX / 2)  # half spectrum overhead
-    words = {"rhs": 12, "cn": 6, "fftx": 3 + spec, "ffty": 2 * spec, "tri": 2 * spec,
-             "iffty": 2 * spec, "ifftx": spec + 1, "proj": 7, "fin": 0}
+    hh = (NX / 2 + 1) / NX
+    bpp = {"rhs": 12 * s, "cn": 6 * s, "fftx": 3 * s + 16 * hh, "ffty": 32 * hh, "tri": 48 * hh,
+           "iffty": 32 * hh, "ifftx": 16 * hh + 8, "proj": 6 * s + 8, "fin": 0}
     out = []
-    for k, w in words.items():
+    for k, w in bpp.items():
         ms = phases.get(k, 0.0) / max(nst, 1)
-        b = w * s * npts
+        b = w * npts
         out.append({"name": k, "ms": ms, "bytes": b, "gbs": (b / (ms / 1e3) / 1e9) if ms > 0 else 0.0})
     return out
 

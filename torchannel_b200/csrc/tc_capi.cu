@@ -62,6 +62,7 @@ struct tc_ctx {
   void* rh[3];
   double* p;             // pressure, FP64 in both precisions
   cpx<double>* X;        // spectral intermediate, FP64 in both precisions
+  double* tri_rden; double* tri_cp;  // per-mode LU factors of the z systems
   void* idzf_t; void* idzc_t;
   double* ubase_d; void* ubase_t;  // base profile of u (mixed precision)
   unsigned int* ticket;  // last-block counter of k_project_bulk
@@ -123,6 +124,8 @@ static size_t carve(tc_ctx* c, char* base) {
   c->p = cv.take<double>(ncell * 8);
   const size_t nspec = (size_t)c->nxh * c->nz * c->ny;
   c->X = cv.take<cpx<double>>(nspec * 16);
+  c->tri_rden = cv.take<double>(nspec * 8);
+  c->tri_cp = cv.take<double>(nspec * 8);
   c->idzf_t = cv.take<char>(c->nz * T_);
   c->idzc_t = cv.take<char>((c->nz + 1) * T_);
   c->ubase_d = cv.take<double>(c->nz * 8);
@@ -292,6 +295,12 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     return bail(r2);
   r2 = (c->tsz == 8) ? set_smem_attrs<double>(c) : set_smem_attrs<float>(c);
   if (r2) return bail(r2);
+  {
+    PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
+    const int nmodes = c->nxh * c->ny;
+    k_tri_factors<<<(nmodes + 127) / 128, 128>>>(tb, c->tri_rden, c->tri_cp, c->nxh, c->ny, c->nz);
+    if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
+  }
   if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "create sync"));
   c->tab_dt = -1.0;
   *out = c;
@@ -371,7 +380,10 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
   const int nmodes = nxh * ny;
   mark(c, TC_PH_TRI, s);
-  k_tri<<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, tb, nxh, ny, nz);
+  if (c->tri_rden)
+    k_tri_lu<<<(nmodes + 127) / 128, 128, 0, s>>>(X, c->tri_rden, c->tri_cp, tb, nxh, ny, nz);
+  else
+    k_tri<<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, tb, nxh, ny, nz);
   mark(c, TC_PH_IFFTY, s);
   k_ffty<true><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   mark(c, TC_PH_IFFTX, s);
@@ -400,7 +412,7 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   T** B = (T**)c->st[nxt];
   T** R = (T**)c->rh;
   dim3 blk(RHS_TX, RHS_TY);
-  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, c->nz + 1);
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (scheme == TC_IMEX && c->tab_dt != dt) {
     k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
     c->tab_dt = dt;
@@ -504,7 +516,7 @@ template <class T> static int rhs_hook_impl(tc_ctx* c, int full, double* ru, dou
   T** B = (T**)c->st[c->cur ^ 1];  // scratch: the next buffer is free between steps
   const size_t ncell = (size_t)c->nx * c->ny * c->nz;
   cudaMemsetAsync(B[2], 0, ncell / c->nz * (c->nz + 1) * sizeof(T), s);
-  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, c->nz + 1);
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (full)
     k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, RHS_TY), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                    B[0], B[1], B[2], c->scal, (T)0, 0);

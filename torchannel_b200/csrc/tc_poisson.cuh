@@ -168,6 +168,103 @@ __global__ void __launch_bounds__(64) k_tri(cpx<double>* __restrict__ X, Poisson
   }
 }
 
+// LU factors of every mode's z system, computed once per grid: the rows of
+// projection_fft.py:44-82 do not depend on dt or on the data, so
+// rden[k] = 1/(b_k - a_k c'_{k-1}) and c'_k = c_k rden[k] are tabulated in the
+// layout of X ([kx][k][ky]) with the same arithmetic as the sweep of k_tri.
+__global__ void __launch_bounds__(128) k_tri_factors(PoissonTabs tb, double* __restrict__ rden_t,
+                                                     double* __restrict__ cp_t, int nxh, int ny, int nz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxh * ny) return;
+  const int kx = t / ny, ky = t - kx * ny;
+  const double K2 = tb.k2x[kx] + tb.k2y[ky];
+  const size_t base = (size_t)kx * nz * ny + ky;
+  double cprev = 0.0;
+  for (int k = 0; k < nz; ++k) {
+    const double cl = tb.cl[k], cr = tb.cr[k];
+    const double a = (k == 0) ? 0.0 : cl;
+    double bb = -(cl + cr + K2);
+    if (k == 0) bb += cl;
+    if (k == nz - 1) bb += cr;
+    const double c = (k == nz - 1) ? 0.0 : cr;
+    const double rden = 1.0 / (bb - a * cprev);
+    const double cpk = c * rden;
+    rden_t[base + (size_t)k * ny] = rden;
+    cp_t[base + (size_t)k * ny] = cpk;
+    cprev = cpk;
+  }
+}
+
+// Division-free Thomas sweep with the tabulated factors: forward
+// d'_k = (d_k - a_k d'_{k-1}) rden_k, backward x_k = d'_k - c'_k x_{k+1}, the
+// (0,0) mode gauged (x_{nz-1} = 0).  One thread per mode; the next TRIF_B
+// levels are in flight while the current ones are used.
+#define TRIF_B 16
+__global__ void __launch_bounds__(128) k_tri_lu(cpx<double>* __restrict__ X, const double* __restrict__ rden_t,
+                                                const double* __restrict__ cp_t, PoissonTabs tb, int nxh, int ny,
+                                                int nz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxh * ny) return;
+  const int kx = t / ny, ky = t - kx * ny;
+  const size_t base = (size_t)kx * nz * ny + ky;
+  cpx<double>* col = X + base;
+  const double* rd = rden_t + base;
+  const double* cpt = cp_t + base;
+  const size_t st = ny;
+  cpx<double> dc[TRIF_B], dn[TRIF_B];
+  double fc[TRIF_B], fn[TRIF_B];
+#pragma unroll
+  for (int b = 0; b < TRIF_B; ++b) {
+    if (b < nz) { dc[b] = col[(size_t)b * st]; fc[b] = ldg(rd + (size_t)b * st); }
+  }
+  double dpr = 0.0, dpi = 0.0;
+  for (int k0 = 0; k0 < nz; k0 += TRIF_B) {
+#pragma unroll
+    for (int b = 0; b < TRIF_B; ++b) {
+      const int kk = k0 + TRIF_B + b;
+      if (kk < nz) { dn[b] = col[(size_t)kk * st]; fn[b] = ldg(rd + (size_t)kk * st); }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIF_B; ++b) {
+      const int k = k0 + b;
+      if (k < nz) {
+        const double a = (k == 0) ? 0.0 : tb.cl[k];
+        dpr = (dc[b].x - a * dpr) * fc[b];
+        dpi = (dc[b].y - a * dpi) * fc[b];
+        col[(size_t)k * st] = cpx<double>{dpr, dpi};
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIF_B; ++b) { dc[b] = dn[b]; fc[b] = fn[b]; }
+  }
+  double xr = dpr, xi = dpi;
+  if (kx == 0 && ky == 0) { xr = 0.0; xi = 0.0; }
+  col[(size_t)(nz - 1) * st] = cpx<double>{xr, xi};
+#pragma unroll
+  for (int b = 0; b < TRIF_B; ++b) {
+    const int k = nz - 2 - b;
+    if (k >= 0) { dc[b] = col[(size_t)k * st]; fc[b] = ldg(cpt + (size_t)k * st); }
+  }
+  for (int k1 = nz - 2; k1 >= 0; k1 -= TRIF_B) {
+#pragma unroll
+    for (int b = 0; b < TRIF_B; ++b) {
+      const int k = k1 - TRIF_B - b;
+      if (k >= 0) { dn[b] = col[(size_t)k * st]; fn[b] = ldg(cpt + (size_t)k * st); }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIF_B; ++b) {
+      const int k = k1 - b;
+      if (k >= 0) {
+        xr = dc[b].x - fc[b] * xr;
+        xi = dc[b].y - fc[b] * xi;
+        col[(size_t)k * st] = cpx<double>{xr, xi};
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIF_B; ++b) { dc[b] = dn[b]; fc[b] = fn[b]; }
+  }
+}
+
 // Inverse real FFT along x of JT rows of plane k; writes p[k][j][i] (FP64).
 __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X, double* __restrict__ p, int nx,
                                                int ny, int nz, FftPlan plx, const cpx<double>* __restrict__ twx,

@@ -42,17 +42,20 @@ enum : int {
 // (:1037-1225) and _v2 (:818-1034), AB2 combine solver.py:626-651.
 // FULL=false: IMEX (x/y diffusion only); FULL=true: full Laplacian (AB2/FE).
 //
-// A block owns a RHS_TX x RHS_TY tile of one plane k and computes u, v at
-// cell k and w at face k.  It first stages the u, v, w planes k-1, k, k+1 of
-// the tile with a one-cell periodic halo (z ghosts applied, u with its base
-// profile added) in shared memory -- every load of the block is independent
-// and issued up front -- then evaluates the stencils from shared memory.
-// Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
+// A block owns a RHS_TX x RHS_TY tile and RHS_KB (rhs_kb<T>()) consecutive
+// planes k = kb..kb+RHS_KB-1 (u, v at cell k, w at face k).  It first stages the u,
+// v, w planes kb-1 .. kb+RHS_KB with a one-cell periodic halo (z ghosts
+// applied, u with its base profile added) in shared memory -- every load of
+// the block is independent and issued up front; halo offsets are computed
+// once per thread -- then evaluates the stencils of each plane from shared
+// memory.  Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
 // v[:, ny]; both reference paths omit advection there, the separate-op path
 // keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
 // ---------------------------------------------------------------------------
 #define RHS_TX 32
 #define RHS_TY 8
+// planes per block: 4 in FP32, 3 in FP64 (static shared memory <= 48 KB)
+template <class T> __host__ __device__ constexpr int rhs_kb() { return sizeof(T) == 8 ? 3 : 4; }
 #define RHS_HX (RHS_TX + 2)
 #define RHS_HY (RHS_TY + 2)
 #define RHS_NH (RHS_HX * RHS_HY)
@@ -65,134 +68,159 @@ __global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const
                                                                 T* __restrict__ rv, T* __restrict__ rw,
                                                                 const double* __restrict__ forcing_dev, T dt,
                                                                 int have_hist) {
-  __shared__ T su[3][RHS_HY][RHS_HX];
-  __shared__ T sv[3][RHS_HY][RHS_HX];
-  __shared__ T sw[3][RHS_HY][RHS_HX];
+  constexpr int RHS_KB = rhs_kb<T>();
+  constexpr int RHS_NS = RHS_KB + 2;
+  __shared__ T su[RHS_NS][RHS_HY][RHS_HX];
+  __shared__ T sv[RHS_NS][RHS_HY][RHS_HX];
+  __shared__ T sw[RHS_NS][RHS_HY][RHS_HX];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx;
   const int i0 = blockIdx.x * RHS_TX, j0 = blockIdx.y * RHS_TY;
   const int i = i0 + tx, j = j0 + ty;
   const bool active = (i < nx) && (j < ny);
-  const int k = blockIdx.z;  // cell k for u, v (k < nz); face k for w (1 <= k <= nz-1)
+  const int kb = blockIdx.z * RHS_KB;  // planes kb .. kb+RHS_KB-1 (<= nz)
   const T top = g.top_neumann ? T(1) : T(-1);
   const T h = T(0.5);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
   const T* __restrict__ base = g.ubase_t;
-  auto bk = [&](int p) { return base ? ldg(base + p) : T(0); };
-  // stage planes k-1, k, k+1 (slot 0, 1, 2)
-  for (int e = tid; e < 3 * RHS_NH; e += RHS_TX * RHS_TY) {
-    const int sl = e / RHS_NH, r = e - sl * RHS_NH;
-    const int hy = r / RHS_HX, hx = r - hy * RHS_HX;
-    int jj = (j0 - 1 + hy) % ny; if (jj < 0) jj += ny;
-    int ii = (i0 - 1 + hx) % nx; if (ii < 0) ii += nx;
-    const size_t off = (size_t)jj * nx + ii;
-    const int p = k - 1 + sl;
-    T uu, vv, ww;
-    if (p < 0) {
-      uu = -(ldg(u + off) + bk(0));
-      vv = -ldg(v + off);
-    } else if (p >= nz) {
-      uu = top * (ldg(u + (size_t)(nz - 1) * plane + off) + bk(nz - 1));
-      vv = top * ldg(v + (size_t)(nz - 1) * plane + off);
-    } else {
-      uu = ldg(u + (size_t)p * plane + off) + bk(p);
-      vv = ldg(v + (size_t)p * plane + off);
+  // halo elements of this thread: e0 = tid, e1 = tid + 256 (if < RHS_NH)
+  const int e1 = tid + RHS_TX * RHS_TY;
+  const bool has1 = e1 < RHS_NH;
+  size_t off[2];
+  int hyx[2][2];
+  {
+    const int es[2] = {tid, e1};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int hy = es[q] / RHS_HX, hx = es[q] - (es[q] / RHS_HX) * RHS_HX;
+      int jj = j0 - 1 + hy, ii = i0 - 1 + hx;
+      while (jj < 0) jj += ny;
+      while (jj >= ny) jj -= ny;
+      while (ii < 0) ii += nx;
+      while (ii >= nx) ii -= nx;
+      off[q] = (size_t)jj * nx + ii;
+      hyx[q][0] = hy; hyx[q][1] = hx;
     }
-    ww = (p >= 0 && p <= nz) ? ldg(w + (size_t)p * plane + off) : T(0);
-    su[sl][hy][hx] = uu; sv[sl][hy][hx] = vv; sw[sl][hy][hx] = ww;
+  }
+  // stage planes p = kb-1 .. kb+RHS_KB into slots 0 .. RHS_NS-1
+#pragma unroll
+  for (int sl = 0; sl < RHS_NS; ++sl) {
+    const int p = kb - 1 + sl;
+    // cell plane read for u/v with its z-ghost rule: sign * (q[pc] + base[pc])
+    const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
+    const T sgn = p < 0 ? T(-1) : (p >= nz ? top : T(1));
+    const T bb = base ? ldg(base + pc) : T(0);
+    const bool wok = (p >= 0) && (p <= nz);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if (q == 1 && !has1) break;
+      const size_t oc = (size_t)pc * plane + off[q];
+      const T uu = sgn * (ldg(u + oc) + bb);
+      const T vv = sgn * ldg(v + oc);
+      const T ww = wok ? ldg(w + (size_t)p * plane + off[q]) : T(0);
+      su[sl][hyx[q][0]][hyx[q][1]] = uu;
+      sv[sl][hyx[q][0]][hyx[q][1]] = vv;
+      sw[sl][hyx[q][0]][hyx[q][1]] = ww;
+    }
   }
   __syncthreads();
   const int cx = tx + 1, cy = ty + 1;
-  const int sm = 0, s0 = 1, sp = 2;
-  if (active && k < nz) {
-    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-    const T idzf = g.idzf[k];
-    // ---------------- u at cell k ----------------
-    {
-      const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
-      const T Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
-      const T Uzm = su[sm][cy][cx], Uzp = su[sp][cy][cx];
-      const bool edge = (i == nx - 1);
-      T r = T(0);
-      if (!(edge && g.rhs_fused)) {
-        r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
-        if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
-      }
-      if (!edge) {
-        const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
-        const T vu_t = h * (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (h * (U0 + Uyp));
-        const T vu_b = h * (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (h * (Uym + U0));
-        const T wu_t = h * (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (h * (U0 + Uzp));
-        const T wu_b = h * (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (h * (Uzm + U0));
-        r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
-      }
-      if (UPD == UPD_RHS_ONLY) {
-        ru[o] = r;
-      } else {
-        const T Uraw = base ? ldg(u + o) : U0;  // stored value (u - U0[k] in mixed precision)
-        if (UPD == UPD_FE) {
-          T q = Uraw + dt * r;
-          us[o] = q + dt * T(1);
-        } else {
-          r += forcing;
-          us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
+#pragma unroll 1
+  for (int kk = 0; kk < RHS_KB; ++kk) {
+    const int k = kb + kk;
+    if (k > nz) break;
+    const int sm = kk, s0 = kk + 1, sp = kk + 2;
+    if (active && k < nz) {
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const T idzf = g.idzf[k];
+      // ---------------- u at cell k ----------------
+      {
+        const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
+        const T Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
+        const T Uzm = su[sm][cy][cx], Uzp = su[sp][cy][cx];
+        const bool edge = (i == nx - 1);
+        T r = T(0);
+        if (!(edge && g.rhs_fused)) {
+          r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
+          if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
+        }
+        if (!edge) {
+          const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
+          const T vu_t = h * (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (h * (U0 + Uyp));
+          const T vu_b = h * (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (h * (Uym + U0));
+          const T wu_t = h * (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (h * (U0 + Uzp));
+          const T wu_b = h * (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (h * (Uzm + U0));
+          r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
+        }
+        if (UPD == UPD_RHS_ONLY) {
           ru[o] = r;
+        } else {
+          const T Uraw = base ? ldg(u + o) : U0;  // stored value (u - U0[k] in mixed precision)
+          if (UPD == UPD_FE) {
+            T q = Uraw + dt * r;
+            us[o] = q + dt * T(1);
+          } else {
+            r += forcing;
+            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
+            ru[o] = r;
+          }
+        }
+      }
+      // ---------------- v at cell k ----------------
+      {
+        const T V0 = sv[s0][cy][cx], Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1];
+        const T Vym = sv[s0][cy - 1][cx], Vyp = sv[s0][cy + 1][cx];
+        const T Vzm = sv[sm][cy][cx], Vzp = sv[sp][cy][cx];
+        const bool edge = (j == ny - 1);
+        T r = T(0);
+        if (!(edge && g.rhs_fused)) {
+          r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
+          if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
+        }
+        if (!edge) {
+          const T uv_r = h * (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (h * (V0 + Vxp));
+          const T uv_l = h * (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (h * (Vxm + V0));
+          const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
+          const T wv_t = h * (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (h * (V0 + Vzp));
+          const T wv_b = h * (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (h * (Vzm + V0));
+          r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
+        }
+        if (UPD == UPD_RHS_ONLY) {
+          rv[o] = r;
+        } else if (UPD == UPD_FE) {
+          vs[o] = V0 + dt * r;
+        } else {
+          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
+          rv[o] = r;
         }
       }
     }
-    // ---------------- v at cell k ----------------
-    {
-      const T V0 = sv[s0][cy][cx], Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1];
-      const T Vym = sv[s0][cy - 1][cx], Vyp = sv[s0][cy + 1][cx];
-      const T Vzm = sv[sm][cy][cx], Vzp = sv[sp][cy][cx];
-      const bool edge = (j == ny - 1);
-      T r = T(0);
-      if (!(edge && g.rhs_fused)) {
-        r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
-        if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
-      }
-      if (!edge) {
-        const T uv_r = h * (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (h * (V0 + Vxp));
-        const T uv_l = h * (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (h * (Vxm + V0));
-        const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
-        const T wv_t = h * (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (h * (V0 + Vzp));
-        const T wv_b = h * (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (h * (Vzm + V0));
-        r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
-      }
+    // ---------------- w at face k ----------------
+    if (active && k >= 1 && k <= nz - 1) {
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const T W0 = sw[s0][cy][cx], Wxm = sw[s0][cy][cx - 1], Wxp = sw[s0][cy][cx + 1];
+      const T Wym = sw[s0][cy - 1][cx], Wyp = sw[s0][cy + 1][cx];
+      const T Wzm = sw[sm][cy][cx], Wzp = sw[sp][cy][cx];
+      T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
+      // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+      if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
+      const T uw_r = h * (su[sm][cy][cx] + su[s0][cy][cx]) * (h * (W0 + Wxp));
+      const T uw_l = h * (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (h * (Wxm + W0));
+      const T vw_t = h * (sv[sm][cy][cx] + sv[s0][cy][cx]) * (h * (W0 + Wyp));
+      const T vw_b = h * (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (h * (Wym + W0));
+      const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[k];
+      r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
       if (UPD == UPD_RHS_ONLY) {
-        rv[o] = r;
+        rw[o] = r;
       } else if (UPD == UPD_FE) {
-        vs[o] = V0 + dt * r;
+        ws[o] = W0 + dt * r;
       } else {
-        vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
-        rv[o] = r;
+        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
+        rw[o] = r;
       }
     }
-  }
-  // ---------------- w at face k ----------------
-  if (active && k >= 1 && k <= nz - 1) {
-    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-    const T W0 = sw[s0][cy][cx], Wxm = sw[s0][cy][cx - 1], Wxp = sw[s0][cy][cx + 1];
-    const T Wym = sw[s0][cy - 1][cx], Wyp = sw[s0][cy + 1][cx];
-    const T Wzm = sw[sm][cy][cx], Wzp = sw[sp][cy][cx];
-    T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
-    // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
-    if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
-    const T uw_r = h * (su[sm][cy][cx] + su[s0][cy][cx]) * (h * (W0 + Wxp));
-    const T uw_l = h * (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (h * (Wxm + W0));
-    const T vw_t = h * (sv[sm][cy][cx] + sv[s0][cy][cx]) * (h * (W0 + Wyp));
-    const T vw_b = h * (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (h * (Wym + W0));
-    const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[k];
-    r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
-    if (UPD == UPD_RHS_ONLY) {
-      rw[o] = r;
-    } else if (UPD == UPD_FE) {
-      ws[o] = W0 + dt * r;
-    } else {
-      ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
-      rw[o] = r;
-    }
+
   }
 }
 
@@ -275,7 +303,7 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
 // Replaces solve_implicit_diffusion_u/v/w (operators.py:563-811) whose PCR
 // (tridiag.py:33-58) solves the same systems.
 // ---------------------------------------------------------------------------
-#define CN_B 8
+#define CN_B 16
 template <class T>
 __global__ void __launch_bounds__(128) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, CnTab t,
                                                   const double* __restrict__ ubase, int nx, int ny, int nz) {
@@ -293,88 +321,68 @@ __global__ void __launch_bounds__(128) k_cn_solve(T* __restrict__ u, T* __restri
   if (col >= nx * ny) return;
   const size_t plane = (size_t)nx * ny;
   T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + col;
-  double buf[CN_B];
-  if (comp < 2) {
-    // rows m = 0..nz-1 on planes m; explicit stencil on planes m-1, m, m+1
-    const int n = nz;
-    double qm = 0.0, q0 = (double)q[0] + shb[0];
-    double dprev = 0.0;
-    for (int m0 = 0; m0 < n; m0 += CN_B) {
+  // The forward sweep of u/v runs over rows m = 0..nz-1 on planes m; w over
+  // rows m = 0..nz-2 whose unknown sits on face m+1.  `lo` maps row m to its
+  // plane; the explicit CN stencil of row m uses the original values of the
+  // rows m-1, m, m+1 (u/v) or of faces m-1, m, m+1 (w).
+  const int n = comp < 2 ? nz : nz - 1;
+  const int lo = comp < 2 ? 0 : 1;
+  T cur[CN_B], nxt[CN_B];
+  // element r of the look-ahead stream: u/v plane r+1 (row r+1), w face r+2
+  auto ld = [&](int r) -> T {
+    const int pl = comp < 2 ? r + 1 : r + 2;
+    return (pl <= (comp < 2 ? nz - 1 : nz - 1)) ? q[(size_t)pl * plane] : T(0);
+  };
 #pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m0 + b + 1;
-        buf[b] = (m < n) ? (double)q[(size_t)m * plane] + shb[m] : 0.0;
-      }
+  for (int b = 0; b < CN_B; ++b) cur[b] = ld(b);
+  double sm1 = 0.0;                                   // value at row m-1 (u/v) / face m-1 (w)
+  double s0 = comp < 2 ? (double)q[0] + shb[0] : (double)q[0];  // row m (u/v) / face m (w)
+  double s1 = comp < 2 ? 0.0 : (double)q[plane];      // w: face m+1 (the unknown of row m)
+  double dprev = 0.0;
+  for (int m0 = 0; m0 < n; m0 += CN_B) {
 #pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m0 + b;
-        if (m < n) {
-          const double qn = buf[b];
-          const double d = q0 + beta * (cA[m] * qm + cB[m] * q0 + cC[m] * qn);
-          const double dp = (d - a[m] * dprev) * iv[m];
-          q[(size_t)m * plane] = (T)(dp - shb[m]);  // kept as (d' - base) so it round-trips exactly in FP64
-          dprev = dp;
-          qm = q0; q0 = qn;
-        }
-      }
-    }
-    // backward sweep: x_{n-1} = d'_{n-1}
-    double x = dprev;
-    q[(size_t)(n - 1) * plane] = (T)(x - shb[n - 1]);
-    for (int m1 = n - 2; m1 >= 0; m1 -= CN_B) {
+    for (int b = 0; b < CN_B; ++b) nxt[b] = ld(m0 + CN_B + b);  // next batch in flight
 #pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m1 - b;
-        buf[b] = (m >= 0) ? (double)q[(size_t)m * plane] + shb[m] : 0.0;
-      }
-#pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m1 - b;
-        if (m >= 0) {
-          x = buf[b] - cp[m] * x;
-          q[(size_t)m * plane] = (T)(x - shb[m]);
-        }
-      }
-    }
-  } else {
-    // unknowns at faces 1..nz-1; row m <-> face m+1; explicit stencil on faces m-1, m, m+1
-    const int n = nz - 1;
-    double pm = 0.0, p0 = (double)q[0], p1 = (double)q[plane];
-    double dprev = 0.0;
-    for (int m0 = 0; m0 < n; m0 += CN_B) {
-#pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int f = m0 + b + 2;
-        buf[b] = (f <= nz - 1) ? (double)q[(size_t)f * plane] : 0.0;
-      }
-#pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m0 + b;
-        if (m < n) {
-          const double d = p1 + beta * (cA[m] * pm + cB[m] * p0 + cC[m] * p1);
-          const double dp = (d - a[m] * dprev) * iv[m];
+    for (int b = 0; b < CN_B; ++b) {
+      const int m = m0 + b;
+      if (m < n) {
+        double d, dp;
+        if (comp < 2) {
+          const double qn = (m + 1 < n) ? (double)cur[b] + shb[m + 1] : 0.0;
+          d = s0 + beta * (cA[m] * sm1 + cB[m] * s0 + cC[m] * qn);
+          dp = (d - a[m] * dprev) * iv[m];
+          q[(size_t)m * plane] = (T)(dp - shb[m]);
+          sm1 = s0; s0 = qn;
+        } else {
+          d = s1 + beta * (cA[m] * sm1 + cB[m] * s0 + cC[m] * s1);
+          dp = (d - a[m] * dprev) * iv[m];
           q[(size_t)(m + 1) * plane] = (T)dp;
-          dprev = dp;
-          pm = p0; p0 = p1; p1 = buf[b];
+          sm1 = s0; s0 = s1; s1 = (double)cur[b];
         }
+        dprev = dp;
       }
     }
-    double x = dprev;
-    for (int m1 = n - 2; m1 >= 0; m1 -= CN_B) {
 #pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m1 - b;
-        buf[b] = (m >= 0) ? (double)q[(size_t)(m + 1) * plane] : 0.0;
-      }
+    for (int b = 0; b < CN_B; ++b) cur[b] = nxt[b];
+  }
+  // backward sweep over rows n-2 .. 0 (x_{n-1} = d'_{n-1} already stored)
+  double x = dprev;
+  auto ldb = [&](int m) -> T { return m >= 0 ? q[(size_t)(m + lo) * plane] : T(0); };
 #pragma unroll
-      for (int b = 0; b < CN_B; ++b) {
-        const int m = m1 - b;
-        if (m >= 0) {
-          x = buf[b] - cp[m] * x;
-          q[(size_t)(m + 1) * plane] = (T)x;
-        }
+  for (int b = 0; b < CN_B; ++b) cur[b] = ldb(n - 2 - b);
+  for (int m1 = n - 2; m1 >= 0; m1 -= CN_B) {
+#pragma unroll
+    for (int b = 0; b < CN_B; ++b) nxt[b] = ldb(m1 - CN_B - b);
+#pragma unroll
+    for (int b = 0; b < CN_B; ++b) {
+      const int m = m1 - b;
+      if (m >= 0) {
+        x = ((double)cur[b] + (comp < 2 ? shb[m] : 0.0)) - cp[m] * x;
+        q[(size_t)(m + lo) * plane] = (T)(x - (comp < 2 ? shb[m] : 0.0));
       }
     }
+#pragma unroll
+    for (int b = 0; b < CN_B; ++b) cur[b] = nxt[b];
   }
 }
 
