@@ -101,6 +101,13 @@ int tc_set_history(tc_ctx* ctx, const double* ru, const double* rv, const double
  * Asynchronous; u_bulk and forcing stay on the device (tc_scalars). */
 int tc_step(tc_ctx* ctx, int scheme, double dt, int n_steps, void* stream);
 
+/* Replay of captured steps: with n_steps >= 4, once the AB2 history exists
+ * and the CN tables match dt, tc_step captures two consecutive steps into a
+ * CUDA graph (once per scheme / dt / buffer parity) and replays it; this
+ * switch turns that off (on by default).  No reference counterpart (the
+ * reference captures only its Poisson solve, solver.py:389-414). */
+int tc_use_graphs(tc_ctx* ctx, int on);
+
 /* Initial projection of a fresh field: div -> Poisson -> u -= grad p
  * (dt = 1) (solver.py:345-370). */
 int tc_project_initial(tc_ctx* ctx, void* stream);

@@ -251,3 +251,19 @@ def test_history_roundtrip(torch_cuda):
     b.step("IMEX", 0.002, 2)
     for x, y in zip(a.get_state()[:3], b.get_state()[:3]):
         assert np.array_equal(np_(x), np_(y))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_is_bitwise_identical(torch_cuda, precision):
+    nx, ny, nz = 32, 24, 16
+    oc = make_oracle(nx, ny, nz, seed=13)
+    a, b = make_gpu(oc, precision), make_gpu(oc, precision)
+    a.use_graphs(False)
+    for ch in (a, b):
+        ch.set_state(oc.u, oc.v, oc.w)
+        ch.step("IMEX", 0.003, 9)      # 1 plain + graph pairs + remainder
+        ch.step("IMEX", 0.002, 6)      # dt change: new tables, new graph
+        ch.step("AB2", 0.0005, 5)
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(np_(x), np_(y))
+    assert np.array_equal(np_(a.scalars), np_(b.scalars))

@@ -139,6 +139,9 @@ class Channel:
         L.check(self.lib.tc_step(self.ctx, SCHEMES[scheme] if isinstance(scheme, str) else int(scheme),
                                  float(dt), int(n_steps), _stream()))
 
+    def use_graphs(self, on=True):
+        L.check(self.lib.tc_use_graphs(self.ctx, int(bool(on))))
+
     def project_initial(self):
         L.check(self.lib.tc_project_initial(self.ctx, _stream()))
 

@@ -80,6 +80,12 @@ struct tc_ctx {
   int JT, RB, tri_bt, stats_RB, stats_CB;
   int cur, have_hist, state_set;
   double tab_dt;
+  // CUDA graph of two consecutive steps (tc_step replays it for n_steps >= 4)
+  cudaStream_t cap_stream;
+  cudaGraphExec_t gexec;
+  int g_valid, g_scheme, g_cur;
+  double g_dt;
+  int graphs_on;
   // per-phase timing ring (tc_timing_enable)
   int timing;
   int t_head, t_count;
@@ -303,11 +309,14 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
   }
   if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "create sync"));
   c->tab_dt = -1.0;
+  c->graphs_on = 1;
   *out = c;
   return TC_OK;
 }
 
 extern "C" int tc_destroy(tc_ctx* ctx) {
+  if (ctx && ctx->g_valid) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx && ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx && ctx->tev_made)
     for (int r = 0; r < TC_TIMING_RING; ++r)
       for (int p = 0; p <= TC_NPHASE; ++p) cudaEventDestroy(ctx->tev[r][p]);
@@ -609,15 +618,61 @@ extern "C" int tc_set_history(tc_ctx* c, const double* ru, const double* rv, con
   return TC_OK;
 }
 
+// Capture two consecutive steps (the state buffers swap once per step, so a
+// pair returns to the same buffers) into an executable graph.
+static int build_graph(tc_ctx* c, int scheme, double dt) {
+  if (c->g_valid) {
+    cudaGraphExecDestroy(c->gexec);
+    c->g_valid = 0;
+  }
+  if (!c->cap_stream) TC_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  const int cur0 = c->cur, hist0 = c->have_hist;
+  TC_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int rc = TC_OK;
+  for (int q = 0; q < 2 && rc == TC_OK; ++q) rc = DISPATCH(c, step_impl, c, scheme, dt, c->cap_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->cap_stream, &graph);
+  c->cur = cur0;  // capture launched nothing: restore the host-side state
+  c->have_hist = hist0;
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  c->g_valid = 1; c->g_scheme = scheme; c->g_dt = dt; c->g_cur = cur0;
+  return TC_OK;
+}
+
 extern "C" int tc_step(tc_ctx* c, int scheme, double dt, int n_steps, void* stream) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
   if (!c->state_set) return fail(TC_ERR_STATE, "no state");
   if (scheme != TC_IMEX && scheme != TC_AB2 && scheme != TC_FE) return fail(TC_ERR_ARG, "bad scheme");
   if (!(dt > 0) || n_steps < 0) return fail(TC_ERR_ARG, "dt must be > 0 and n_steps >= 0");
-  for (int n = 0; n < n_steps; ++n) {
+  int n = 0;
+  // plain launches until the history exists and the CN tables match dt
+  while (n < n_steps && (!c->have_hist || (scheme == TC_IMEX && c->tab_dt != dt) || c->timing || !c->graphs_on ||
+                         n_steps - n < 4)) {
+    int rc = DISPATCH(c, step_impl, c, scheme, dt, ST(stream));
+    if (rc) return rc;
+    ++n;
+  }
+  if (n_steps - n >= 2) {
+    if (!c->g_valid || c->g_scheme != scheme || c->g_dt != dt || c->g_cur != c->cur) {
+      int rc = build_graph(c, scheme, dt);
+      if (rc) return rc;
+    }
+    for (; n + 2 <= n_steps; n += 2) TC_CUDA(cudaGraphLaunch(c->gexec, ST(stream)));
+  }
+  for (; n < n_steps; ++n) {
     int rc = DISPATCH(c, step_impl, c, scheme, dt, ST(stream));
     if (rc) return rc;
   }
+  return TC_OK;
+}
+
+extern "C" int tc_use_graphs(tc_ctx* c, int on) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  c->graphs_on = on ? 1 : 0;
   return TC_OK;
 }
 
