@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="step", choices=["step", "ensemble", "poisson"],
+                    help="step: the headline IMEX step; ensemble: 16 uneven channels (config 4); "
+                         "poisson: the FFT Poisson solve alone at 192x192x128 and 384x384x256 (config 2)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -385,10 +388,116 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(a):
+    """16 independent channels of uneven size (nx, ny in {64, 96, 128}, nz in
+    {48, 64, 96}, Re_bulk U[2000, 5600], gamma U[2.2, 2.8], per-member seeds),
+    mixed precision, each on its own stream; ranks own disjoint members."""
+    import torch
+    import torch.distributed as dist
+    from torchannel_b200.ensemble import Ensemble, aggregate, make_members, partition
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    members = make_members(16, seed=0)
+    mine = [members[m] for m in partition(len(members), world, rank)]
+    ens = Ensemble(mine, precision=a.precision)
+    ens.step(a.warmup)
+    ens.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ens.step(a.steps, concurrent=True)
+    ens.synchronize()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    value, pts, max_ms = aggregate(ens.points() * a.steps, ms)
+    t0 = time.perf_counter()
+    ens.step(a.steps, concurrent=False)
+    torch.cuda.synchronize()
+    ms_seq = (time.perf_counter() - t0) * 1e3
+    value_seq, _, _ = aggregate(ens.points() * a.steps, ms_seq)
+    diag = ens.diagnostics()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"metric": "grid-point-steps/s, 16-member uneven ensemble (IMEX)", "value": value,
+                          "unit": "grid-point-steps/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                          "ms_per_step": max_ms / a.steps, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+                          "data": "synthetic (seeded laminar + 0.1 noise per member)",
+                          "config": {"workload": "ensemble of 16 channels", "members": members,
+                                     "parallelism": f"members over {world} rank(s), streams per member"},
+                          "one_at_a_time": {"value": value_seq},
+                          "max_div_after": max(d["max_div"] for d in diag)}), flush=True)
+
+
+def _poisson_residual(p, rhs, dx, dy, dz_c, dz_f):
+    """L p - rhs on the interior: 3-point periodic x/y, the stretched z rows
+    with Neumann closures (the operator the solve inverts)."""
+    pi = p[1:-1, 1:-1, 1:-1]
+    lap = (np.roll(pi, -1, 0) - 2 * pi + np.roll(pi, 1, 0)) / dx ** 2
+    lap += (np.roll(pi, -1, 1) - 2 * pi + np.roll(pi, 1, 1)) / dy ** 2
+    cl, cr = 1.0 / (dz_c[:-1] * dz_f), 1.0 / (dz_c[1:] * dz_f)
+    up = np.concatenate([pi[:, :, 1:], pi[:, :, -1:]], axis=2)
+    dn = np.concatenate([pi[:, :, :1], pi[:, :, :-1]], axis=2)
+    return lap + cr * (up - pi) - cl * (pi - dn) - rhs
+
+
+def run_poisson(a):
+    """Poisson solve alone on a seeded uniform random right-hand side with
+    zero dz_f-weighted mean (FP64 spectrum), through tc_poisson_solve on
+    device buffers (reference layout in and out)."""
+    import torch
+    from torchannel_b200.core import Channel
+    from torchannel_b200.grid import generate_grid
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    peak, _ = measured_peaks()
+    res = []
+    for (nx, ny, nz) in ((192, 192, 128), (384, 384, 256)):
+        z_f, z_c, dz_f, dz_c = generate_grid(GAMMA, nz, LZ)
+        rng = np.random.default_rng(1)
+        rhs = rng.random((nx, ny, nz)) - 0.5
+        rhs -= np.sum(rhs * dz_f) / (nx * ny * LZ)
+        ch = Channel(nx, ny, nz, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision=a.precision)
+        rd = torch.as_tensor(rhs, device="cuda")
+        for _ in range(a.warmup):
+            p = ch.poisson_solve(rd)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            p = ch.poisson_solve(rd)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        pn = p.cpu().numpy()
+        r = _poisson_residual(pn, rhs, LX / nx, LY / ny, dz_c, dz_f)
+        algo = 4 * 8 * nx * ny * nz  # read rhs, write/read the spectrum, write p (FP64 words)
+        res.append({"grid": [nx, ny, nz], "ms_per_solve": ms, "points_per_s": nx * ny * nz / (ms / 1e3),
+                    "algorithmic_gbs": algo / (ms / 1e3) / 1e9, "frac_of_peak": algo / (ms / 1e3) / 1e9 / peak,
+                    "max_residual": float(np.max(np.abs(r))), "max_rhs": float(np.max(np.abs(rhs))),
+                    "includes": "reference-layout conversion in and out"})
+        del ch
+    print(json.dumps({"metric": "Poisson solves/s (FFT + per-mode tridiagonal + inverse FFT)",
+                      "value": 1e3 / res[0]["ms_per_solve"], "unit": "solves/s at 192x192x128", "n_gpus": 1,
+                      "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "dtype": "f64",
+                      "data": "synthetic (seeded uniform random, zero dz_f-weighted mean)",
+                      "config": {"workload": "Poisson microbench"}, "results": res}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "ensemble":
+        run_ensemble(a)
+    elif a.workload == "poisson":
+        run_poisson(a)
     else:
         run_b200(a)
 

@@ -267,3 +267,22 @@ def test_graph_replay_is_bitwise_identical(torch_cuda, precision):
     for x, y in zip(a.get_state(), b.get_state()):
         assert np.array_equal(np_(x), np_(y))
     assert np.array_equal(np_(a.scalars), np_(b.scalars))
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(192, 192, 128), (384, 384, 256)])
+def test_poisson_full_size_residual(torch_cuda, nx, ny, nz):
+    """Full-size Poisson microbench grids: the discrete residual of the
+    returned p (size-independent property; FP64 roundoff scale)."""
+    from oracle.grid import generate_grid
+    from torchannel_b200.core import Channel
+    Lx, Ly, Lz = 4 * np.pi, 4 * np.pi / 3, 2.0
+    z_f, z_c, dz_f, dz_c = generate_grid(2.6, nz, Lz)
+    rng = np.random.default_rng(1)
+    rhs = rng.random((nx, ny, nz)) - 0.5
+    rhs -= np.sum(rhs * dz_f) / (nx * ny * Lz)
+    ch = Channel(nx, ny, nz, Lx, Ly, Lz, 1 / 2870.0, dz_f, dz_c)
+    p = np_(ch.poisson_solve(rhs))
+    r = poisson.poisson_residual(p, rhs, nx, ny, nz, Lx / nx, Ly / ny, dz_c, dz_f)
+    # the operator's largest coefficients are ~1/dz_min^2; roundoff relative to them
+    scale = np.max(np.abs(p)) * np.max(1.0 / (dz_c[:-1] * dz_f))
+    assert np.max(np.abs(r)) < 1e-12 * scale + 1e-9
