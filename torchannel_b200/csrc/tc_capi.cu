@@ -145,8 +145,8 @@ static size_t carve(tc_ctx* c, char* base) {
   c->cr = cv.take<double>(c->nz * 8);
   c->twx_d = cv.take<cpx<double>>(c->nx * 16);
   c->twy_d = cv.take<cpx<double>>(c->ny * 16);
-  c->tab.uv = cv.take<double>(6 * c->nz * 8);
-  c->tab.w = cv.take<double>(6 * c->nz * 8);
+  c->tab.uv = cv.take<double>(8 * c->nz * 8);
+  c->tab.w = cv.take<double>(8 * c->nz * 8);
   c->tab.beta = cv.take<double>(8);
   const int gx = (c->nx + 31) / 32, gy = (c->ny + 7) / 8;
   c->npart = gx * gy * (c->nz + 1);
@@ -165,7 +165,7 @@ static int validate(const tc_grid_desc* g) {
   if (!g) return fail(TC_ERR_ARG, "null grid descriptor");
   if (g->nx < 8 || g->ny < 8 || g->nz < 4) return fail(TC_ERR_SIZE, "nx, ny must be >= 8 and nz >= 4");
   if ((g->nx & 1) || (g->ny & 1)) return fail(TC_ERR_SIZE, "nx and ny must be even");
-  if (g->nz > 800) return fail(TC_ERR_SIZE, "nz must be <= 800");
+  if (g->nz > 512) return fail(TC_ERR_SIZE, "nz must be <= 512");
   FftPlan a, b;
   if (!fft_make_plan(g->nx, &a) || !fft_make_plan(g->ny, &b))
     return fail(TC_ERR_SIZE, "nx and ny must factor into 2 and 3 only");
@@ -222,7 +222,7 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   TC_CUDA(cudaFuncSetAttribute(k_ffty<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_ffty<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   (void)c;
@@ -401,6 +401,11 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   return TC_OK;
 }
 
+static int cn_chunks(const tc_ctx* c) { return (c->nz + CN_L - 1) / CN_L; }
+template <class T> static size_t cn_smem(const tc_ctx* c) {
+  return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32) * 8 + (size_t)(c->nz + 2) * 32 * sizeof(T);
+}
+
 static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, planes); }
 
 static double bulk_scale(const tc_ctx* c) { return c->dx * c->dy / (c->Lx * c->Ly * c->Lz); }
@@ -440,8 +445,8 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   mark(c, TC_PH_CN, s);
   if (scheme == TC_IMEX) {
     const int ncol = c->nx * c->ny;
-    k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 7 * c->nz * 8, s>>>(B[0], B[1], B[2], c->tab, ubase_of(c),
-                                                                             c->nx, c->ny, c->nz);
+    k_cn_solve<T><<<dim3((ncol + 31) / 32, 1, 3), dim3(32, cn_chunks(c)), cn_smem<T>(c), s>>>(
+        B[0], B[1], B[2], c->tab, ubase_of(c), c->nx, c->ny, c->nz);
     TC_LAUNCHED();
   }
   int rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
@@ -784,8 +789,8 @@ template <class T> static int cn_hook_impl(tc_ctx* c, double dt, cudaStream_t s)
     c->tab_dt = dt;
   }
   const int ncol = c->nx * c->ny;
-  k_cn_solve<T><<<dim3((ncol + 127) / 128, 1, 3), 128, 7 * c->nz * 8, s>>>(A[0], A[1], A[2], c->tab, ubase_of(c),
-                                                                           c->nx, c->ny, c->nz);
+  k_cn_solve<T><<<dim3((ncol + 31) / 32, 1, 3), dim3(32, cn_chunks(c)), cn_smem<T>(c), s>>>(
+      A[0], A[1], A[2], c->tab, ubase_of(c), c->nx, c->ny, c->nz);
   TC_LAUNCHED();
   return TC_OK;
 }

@@ -232,13 +232,29 @@ __global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const
 // w (operators.py:753-803): n = nz-1 rows, row m <-> face m+1, explicit
 //   stencil on faces m-1, m, m+1 (the reference's index convention).
 // Thomas factors: inv_den_m = 1/(b_m - a_m cp_{m-1}), cp_m = c_m inv_den_m.
-// Table layout per system: 6 arrays of length nz: a, inv_den, cp, cA, cB, cC.
+// Chunked sweep (rows split in chunks of CN_L): with f_m = -a_m inv_den_m,
+// G_m = prod_{j = chunk start .. m} f_j and H_m = prod_{j = m .. chunk end}
+// (-cp_j), a chunk swept from zero boundary values is corrected by
+// d'_m += G_m d'_(start-1) and x_m += H_m x_(end+1).
+// Table layout per system: 8 arrays of length nz: a, inv_den, cp, cA, cB, cC, G, H.
 // ---------------------------------------------------------------------------
+#define CN_L 32
 struct CnTab {
-  double* uv;  // 6*nz
-  double* w;   // 6*nz (first nz-1 rows used)
+  double* uv;  // 8*nz
+  double* w;   // 8*nz (first nz-1 rows used)
   double* beta;
 };
+
+__device__ __forceinline__ void cn_chunk_products(double* a, double* iv, double* cp, double* G, double* H, int n) {
+  for (int m = 0; m < n; ++m) {
+    const double f = -a[m] * iv[m];
+    G[m] = (m % CN_L == 0) ? f : G[m - 1] * f;
+  }
+  for (int m = n - 1; m >= 0; --m) {
+    const int e = min((m / CN_L + 1) * CN_L, n) - 1;
+    H[m] = (m == e) ? -cp[m] : H[m + 1] * (-cp[m]);
+  }
+}
 
 __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const double* __restrict__ dzc, int nz,
                             double nu, double dt, int top_neumann) {
@@ -270,6 +286,7 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
       }
       cA[m] = ea; cB[m] = eb; cC[m] = ec;
     }
+    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz);
     *t.beta = (1.0 - theta) * dt * nu;
   } else if (sys == 1) {
     const int n = nz - 1;
@@ -290,99 +307,126 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
       if (m == n - 1) ec = 0.0;
       cA[m] = ea; cB[m] = eb; cC[m] = ec;
     }
+    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Kernel (b): batched Thomas solve of the CN systems, one thread per column
-// and component (blockIdx.z = 0 u, 1 v, 2 w).  In place: the forward sweep
-// overwrites each plane with d'_m, the backward sweep with x_m.  Arithmetic in
-// FP64 whatever the storage type; u is solved for its total value (stored +
-// base profile).  Loads are issued in batches of CN_B planes ahead of the
-// dependent recurrence so that each thread keeps CN_B requests in flight.
-// Replaces solve_implicit_diffusion_u/v/w (operators.py:563-811) whose PCR
-// (tridiag.py:33-58) solves the same systems.
+// Kernel (b): batched tridiagonal solve of the CN systems
+// (solve_implicit_diffusion_u/v/w, operators.py:563-811; the reference's PCR,
+// tridiag.py:33-58, solves the same systems).  A block owns 32 consecutive
+// columns of one component (blockIdx.z = 0 u, 1 v, 2 w) and one warp per
+// chunk of CN_L rows.  The columns' planes -1..nz are staged in shared memory
+// (coalesced; u with its base profile added), each thread sweeps its chunk
+// forward and backward from zero boundary values in registers, and the chunk
+// ends are stitched with one value per chunk boundary (G/H tables), so every
+// value is read and written once.  FP64 arithmetic whatever the storage type.
 // ---------------------------------------------------------------------------
-#define CN_B 16
 template <class T>
-__global__ void __launch_bounds__(128) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, CnTab t,
-                                                  const double* __restrict__ ubase, int nx, int ny, int nz) {
-  extern __shared__ double sh[];
+__global__ void __launch_bounds__(1024) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+                                                   CnTab t, const double* __restrict__ ubase, int nx, int ny,
+                                                   int nz) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   const int comp = blockIdx.z;
+  const int lane = threadIdx.x, chunk = threadIdx.y, nchunk = blockDim.y;
+  const int tid = chunk * 32 + lane, nthr = 32 * nchunk;
+  double* tab = reinterpret_cast<double*>(smraw);           // 8*nz
+  double* shb = tab + 8 * nz;                                // nz (base, u only)
+  double* bnd = shb + nz;                                    // 2 * nchunk * 32
+  T* win = reinterpret_cast<T*>(bnd + 2 * nchunk * 32);      // (nz+2) * 32, plane p+1 at row p+1
   const double* src = comp == 2 ? t.w : t.uv;
-  double* shb = sh + 6 * nz;  // base profile (u only)
-  for (int e = threadIdx.x; e < 6 * nz; e += blockDim.x) sh[e] = src[e];
-  for (int e = threadIdx.x; e < nz; e += blockDim.x) shb[e] = (comp == 0 && ubase) ? ubase[e] : 0.0;
-  __syncthreads();
-  const double* a = sh; const double* iv = a + nz; const double* cp = iv + nz;
-  const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
-  const double beta = *t.beta;
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= nx * ny) return;
-  const size_t plane = (size_t)nx * ny;
-  T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + col;
-  // The forward sweep of u/v runs over rows m = 0..nz-1 on planes m; w over
-  // rows m = 0..nz-2 whose unknown sits on face m+1.  `lo` maps row m to its
-  // plane; the explicit CN stencil of row m uses the original values of the
-  // rows m-1, m, m+1 (u/v) or of faces m-1, m, m+1 (w).
-  const int n = comp < 2 ? nz : nz - 1;
-  const int lo = comp < 2 ? 0 : 1;
-  T cur[CN_B], nxt[CN_B];
-  // element r of the look-ahead stream: u/v plane r+1 (row r+1), w face r+2
-  auto ld = [&](int r) -> T {
-    const int pl = comp < 2 ? r + 1 : r + 2;
-    return (pl <= (comp < 2 ? nz - 1 : nz - 1)) ? q[(size_t)pl * plane] : T(0);
-  };
-#pragma unroll
-  for (int b = 0; b < CN_B; ++b) cur[b] = ld(b);
-  double sm1 = 0.0;                                   // value at row m-1 (u/v) / face m-1 (w)
-  double s0 = comp < 2 ? (double)q[0] + shb[0] : (double)q[0];  // row m (u/v) / face m (w)
-  double s1 = comp < 2 ? 0.0 : (double)q[plane];      // w: face m+1 (the unknown of row m)
-  double dprev = 0.0;
-  for (int m0 = 0; m0 < n; m0 += CN_B) {
-#pragma unroll
-    for (int b = 0; b < CN_B; ++b) nxt[b] = ld(m0 + CN_B + b);  // next batch in flight
-#pragma unroll
-    for (int b = 0; b < CN_B; ++b) {
-      const int m = m0 + b;
-      if (m < n) {
-        double d, dp;
-        if (comp < 2) {
-          const double qn = (m + 1 < n) ? (double)cur[b] + shb[m + 1] : 0.0;
-          d = s0 + beta * (cA[m] * sm1 + cB[m] * s0 + cC[m] * qn);
-          dp = (d - a[m] * dprev) * iv[m];
-          q[(size_t)m * plane] = (T)(dp - shb[m]);
-          sm1 = s0; s0 = qn;
-        } else {
-          d = s1 + beta * (cA[m] * sm1 + cB[m] * s0 + cC[m] * s1);
-          dp = (d - a[m] * dprev) * iv[m];
-          q[(size_t)(m + 1) * plane] = (T)dp;
-          sm1 = s0; s0 = s1; s1 = (double)cur[b];
-        }
-        dprev = dp;
-      }
-    }
-#pragma unroll
-    for (int b = 0; b < CN_B; ++b) cur[b] = nxt[b];
+  for (int e = tid; e < 8 * nz; e += nthr) tab[e] = src[e];
+  for (int e = tid; e < nz; e += nthr) shb[e] = (comp == 0 && ubase) ? ubase[e] : 0.0;
+  const int col0 = blockIdx.x * 32;
+  const int col = col0 + lane;
+  const int ncols = nx * ny;
+  const size_t plane = (size_t)ncols;
+  T* q = comp == 0 ? u : (comp == 1 ? v : w);
+  // stage planes -1..nz of the block's columns (u/v planes, or w faces
+  // including the walls); out-of-range planes are zero
+  const int nstage = nz + 2;
+  for (int e = tid; e < nstage * 32; e += nthr) {
+    const int r = e >> 5, l = e & 31, pl = r - 1, cc = col0 + l;
+    T val = T(0);
+    const int plmax = comp < 2 ? nz - 1 : nz;
+    if (cc < ncols && pl >= 0 && pl <= plmax) val = q[(size_t)pl * plane + cc];
+    win[r * 32 + l] = val;
   }
-  // backward sweep over rows n-2 .. 0 (x_{n-1} = d'_{n-1} already stored)
-  double x = dprev;
-  auto ldb = [&](int m) -> T { return m >= 0 ? q[(size_t)(m + lo) * plane] : T(0); };
+  __syncthreads();
+  const double* a = tab; const double* iv = a + nz; const double* cp = iv + nz;
+  const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
+  const double* G = cC + nz; const double* H = G + nz;
+  const double beta = *t.beta;
+  const int n = comp < 2 ? nz : nz - 1;
+  const int s0 = chunk * CN_L, e0 = min(s0 + CN_L, n);      // rows [s0, e0)
+  const bool act = s0 < n;
+  // stencil source of row m: u/v planes m-1, m, m+1 (own: plane m); w faces
+  // m-1, m, m+1 (own: face m+1).  win row index = plane + 1.
+  auto src_val = [&](int pl) -> double {
+    return (double)win[(pl + 1) * 32 + lane] + ((comp < 2 && pl >= 0 && pl < nz) ? shb[pl] : 0.0);
+  };
+  double y[CN_L];
+  double yend = 0.0;
+  if (act) {
+    double yp = 0.0;
 #pragma unroll
-  for (int b = 0; b < CN_B; ++b) cur[b] = ldb(n - 2 - b);
-  for (int m1 = n - 2; m1 >= 0; m1 -= CN_B) {
-#pragma unroll
-    for (int b = 0; b < CN_B; ++b) nxt[b] = ldb(m1 - CN_B - b);
-#pragma unroll
-    for (int b = 0; b < CN_B; ++b) {
-      const int m = m1 - b;
-      if (m >= 0) {
-        x = ((double)cur[b] + (comp < 2 ? shb[m] : 0.0)) - cp[m] * x;
-        q[(size_t)(m + lo) * plane] = (T)(x - (comp < 2 ? shb[m] : 0.0));
+    for (int tt = 0; tt < CN_L; ++tt) {
+      const int m = s0 + tt;
+      if (m < e0) {
+        const double sm = src_val(m - 1), sc = src_val(m), sp = src_val(m + 1);
+        const double own = comp < 2 ? sc : sp;
+        const double d = own + beta * (cA[m] * sm + cB[m] * sc + cC[m] * sp);
+        yp = (d - a[m] * yp) * iv[m];
+        y[tt] = yp;
       }
     }
+    yend = yp;
+  }
+  bnd[chunk * 32 + lane] = yend;
+  __syncthreads();
+  // true d' entering this chunk: scan the chunk ends below it
+  double Din = 0.0;
+  for (int c = 0; c < chunk; ++c) {
+    const int ce = min(c * CN_L + CN_L, n) - 1;
+    Din = bnd[c * 32 + lane] + G[ce] * Din;
+  }
+  double zstart = 0.0;
+  if (act) {
 #pragma unroll
-    for (int b = 0; b < CN_B; ++b) cur[b] = nxt[b];
+    for (int tt = 0; tt < CN_L; ++tt) {
+      const int m = s0 + tt;
+      if (m < e0) y[tt] += G[m] * Din;
+    }
+    // backward from a zero value beyond the chunk end
+    double zn = 0.0;
+#pragma unroll
+    for (int tt = CN_L - 1; tt >= 0; --tt) {
+      const int m = s0 + tt;
+      if (m < e0) {
+        zn = y[tt] - cp[m] * zn;
+        y[tt] = zn;
+      }
+    }
+    zstart = zn;
+  }
+  bnd[(nchunk + chunk) * 32 + lane] = zstart;
+  __syncthreads();
+  // true x just beyond this chunk: scan the chunk starts above it
+  double Xin = 0.0;
+  for (int c = nchunk - 1; c > chunk; --c) {
+    const int cs = c * CN_L;
+    if (cs < n) Xin = bnd[(nchunk + c) * 32 + lane] + H[cs] * Xin;
+  }
+  if (act && col < ncols) {
+#pragma unroll
+    for (int tt = 0; tt < CN_L; ++tt) {
+      const int m = s0 + tt;
+      if (m < e0) {
+        const double x = y[tt] + H[m] * Xin;
+        const int pl = comp < 2 ? m : m + 1;
+        q[(size_t)pl * plane + col] = (T)(x - ((comp < 2) ? shb[m] : 0.0));
+      }
+    }
   }
 }
 
