@@ -49,7 +49,12 @@ def test_explicit_rhs(torch_cuda, nx, ny, nz, path, full, top):
         assert rel(dof(name, np_(g), nx, ny, nz), dof(name, r, nx, ny, nz)) < TOL, name
 
 
-@pytest.mark.parametrize("nx,ny,nz", SIZES)
+# nz past one 32-row chunk of the CN solve: ragged last chunks (70, 33 -> w has
+# 32 rows), 8 chunks (256) and the deep-channel form (300, 512 rows)
+CN_SIZES = SIZES + [(16, 12, 70), (8, 16, 33), (8, 8, 256), (8, 8, 300), (8, 8, 512)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", CN_SIZES)
 @pytest.mark.parametrize("top", ["dirichlet", "neumann"])
 def test_implicit_diffusion(torch_cuda, nx, ny, nz, top):
     oc = make_oracle(nx, ny, nz, top=top)
@@ -66,14 +71,32 @@ def test_implicit_diffusion(torch_cuda, nx, ny, nz, top):
         assert rel(dof(name, np_(g), nx, ny, nz), dof(name, r, nx, ny, nz)) < TOL, name
 
 
-@pytest.mark.parametrize("nx,ny,nz", SIZES + [(64, 64, 48), (96, 48, 32)])
-def test_poisson(torch_cuda, nx, ny, nz):
+def _fused(ch, fused, nz):
+    """Select the Poisson path; the fused cluster kernel must be available for
+    portable cluster sizes (nz <= 128: at most 8 CTAs of 16 planes)."""
+    try:
+        ch.use_fused_poisson(fused)
+    except Exception:
+        if nz <= 128:
+            raise
+        pytest.skip("16-CTA cluster not schedulable on this device")
+
+
+# (32,24,128): 8 CTAs of 16 planes; (16,12,100): 8 CTAs, ragged last chunk;
+# (16,12,200): 16-CTA cluster
+POISSON_SIZES = SIZES + [(64, 64, 48), (96, 48, 32), (32, 24, 128), (16, 12, 100), (16, 12, 200)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", POISSON_SIZES)
+@pytest.mark.parametrize("fused", [True, False])
+def test_poisson(torch_cuda, nx, ny, nz, fused):
     oc = make_oracle(nx, ny, nz)
     rng = np.random.default_rng(1)
     rhs = rng.random((nx, ny, nz)) - 0.5
     rhs -= np.sum(rhs * oc.dz_f) / (nx * ny * oc.Lz)     # dz_f-weighted zero mean
     ref = poisson.solve_poisson_fft(rhs, oc.fd)
     ch = make_gpu(oc)
+    _fused(ch, fused, nz)
     p = np_(ch.poisson_solve(rhs))
     assert rel(dof("p", p, nx, ny, nz), dof("p", ref, nx, ny, nz)) < 1e-11
     res = poisson.poisson_residual(p, rhs, nx, ny, nz, oc.dx, oc.dy, oc.dz_c, oc.dz_f)
@@ -270,7 +293,8 @@ def test_graph_replay_is_bitwise_identical(torch_cuda, precision):
 
 
 @pytest.mark.parametrize("nx,ny,nz", [(192, 192, 128), (384, 384, 256)])
-def test_poisson_full_size_residual(torch_cuda, nx, ny, nz):
+@pytest.mark.parametrize("fused", [True, False])
+def test_poisson_full_size_residual(torch_cuda, nx, ny, nz, fused):
     """Full-size Poisson microbench grids: the discrete residual of the
     returned p (size-independent property; FP64 roundoff scale)."""
     from oracle.grid import generate_grid
@@ -281,8 +305,25 @@ def test_poisson_full_size_residual(torch_cuda, nx, ny, nz):
     rhs = rng.random((nx, ny, nz)) - 0.5
     rhs -= np.sum(rhs * dz_f) / (nx * ny * Lz)
     ch = Channel(nx, ny, nz, Lx, Ly, Lz, 1 / 2870.0, dz_f, dz_c)
+    _fused(ch, fused, nz)
     p = np_(ch.poisson_solve(rhs))
     r = poisson.poisson_residual(p, rhs, nx, ny, nz, Lx / nx, Ly / ny, dz_c, dz_f)
     # the operator's largest coefficients are ~1/dz_min^2; roundoff relative to them
     scale = np.max(np.abs(p)) * np.max(1.0 / (dz_c[:-1] * dz_f))
     assert np.max(np.abs(r)) < 1e-12 * scale + 1e-9
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_poisson_steps_match_three_kernel_path(torch_cuda, precision):
+    """IMEX steps with the fused y/z Poisson kernel and with the three-kernel
+    path: same state up to the rounding of the chunked sweep."""
+    nx, ny, nz = 48, 32, 64
+    oc = make_oracle(nx, ny, nz, seed=21)
+    a, b = make_gpu(oc, precision), make_gpu(oc, precision)
+    a.use_fused_poisson(True)
+    b.use_fused_poisson(False)
+    for ch in (a, b):
+        ch.set_state(oc.u, oc.v, oc.w)
+        ch.step("IMEX", 0.003, 8)
+    for x, y in zip(a.get_state()[:3], b.get_state()[:3]):
+        assert rel(np_(x), np_(y)) < (1e-12 if precision == "fp64" else 1e-6)

@@ -142,6 +142,11 @@ class Channel:
     def use_graphs(self, on=True):
         L.check(self.lib.tc_use_graphs(self.ctx, int(bool(on))))
 
+    def use_fused_poisson(self, on=True):
+        """One cluster kernel for the y transforms and the z solve (on) or three
+        kernels (off); raises when the grid's cluster shape does not fit."""
+        L.check(self.lib.tc_use_fused_poisson(self.ctx, int(bool(on))))
+
     def project_initial(self):
         L.check(self.lib.tc_project_initial(self.ctx, _stream()))
 

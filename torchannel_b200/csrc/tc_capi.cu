@@ -63,6 +63,7 @@ struct tc_ctx {
   double* p;             // pressure, FP64 in both precisions
   cpx<double>* X;        // spectral intermediate, FP64 in both precisions
   double* tri_rden; double* tri_cp;  // per-mode LU factors of the z systems
+  double* tri_cpb;                    // c' below each chunk of k_yz_solve ([kx][16][ky])
   void* idzf_t; void* idzc_t;
   double* ubase_d; void* ubase_t;  // base profile of u (mixed precision)
   unsigned int* ticket;  // last-block counter of k_project_bulk
@@ -78,6 +79,10 @@ struct tc_ctx {
   int k_bot, k_top, stats_ready, n_samples;
   FftPlan planx, plany;
   int JT, RB, tri_bt, stats_RB, stats_CB;
+  // fused y/z Poisson middle (k_yz_solve): cluster size, planes per CTA,
+  // FFT batch rows, threads, shared memory; yz_ok = launchable here
+  int yz_CS, yz_P, yz_FB, yz_thr, yz_ok, yz_on;
+  size_t yz_smem;
   int cur, have_hist, state_set;
   double tab_dt;
   // CUDA graph of two consecutive steps (tc_step replays it for n_steps >= 4)
@@ -132,6 +137,7 @@ static size_t carve(tc_ctx* c, char* base) {
   c->X = cv.take<cpx<double>>(nspec * 16);
   c->tri_rden = cv.take<double>(nspec * 8);
   c->tri_cp = cv.take<double>(nspec * 8);
+  c->tri_cpb = cv.take<double>((size_t)c->nxh * 16 * c->ny * 8);
   c->idzf_t = cv.take<char>(c->nz * T_);
   c->idzc_t = cv.take<char>((c->nz + 1) * T_);
   c->ubase_d = cv.take<double>(c->nz * 8);
@@ -200,6 +206,21 @@ static void fill_basic(tc_ctx* c, const tc_grid_desc* g) {
   int sCB = 8;
   while (sCB > 1 && ((size_t)2 * sCB * padded_len<double>(c->ny) + c->ny) * 16 > 100 * 1024) sCB /= 2;
   c->stats_CB = sCB;
+  // fused y/z middle: clusters of CS CTAs (power of two, <= 16) of about 16
+  // planes each, the FFT scratch shrunk until a CTA fits in 200 KB
+  int CS = 1;
+  while (CS < 16 && CS * 16 < c->nz) CS *= 2;
+  const int P = (c->nz + CS - 1) / CS;
+  int FB = P < 8 ? P : 8;
+  auto yz_bytes = [&](int fb) {
+    return (size_t)(P + fb) * padded_len<double>(c->ny) * 16 + (size_t)c->ny * 16 + (size_t)6 * c->ny * 8;
+  };
+  while (FB > 1 && yz_bytes(FB) > 200 * 1024) FB /= 2;
+  c->yz_CS = CS; c->yz_P = P; c->yz_FB = FB;
+  c->yz_thr = ((c->ny + 31) / 32) * 32;  // one thread per column ky
+  if (c->yz_thr < 256) c->yz_thr = 256;
+  c->yz_smem = yz_bytes(FB);
+  c->yz_ok = 0; c->yz_on = 0;
 }
 
 extern "C" const char* tc_version(void) { return "torchannel_b200 0.1 (sm_100a)"; }
@@ -215,6 +236,36 @@ extern "C" int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes) {
   return TC_OK;
 }
 
+static cudaLaunchConfig_t yz_config(const tc_ctx* c, cudaLaunchAttribute* at, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(c->nxh * c->yz_CS, 1, 1);
+  cfg.blockDim = dim3(c->yz_thr, 1, 1);
+  cfg.dynamicSmemBytes = c->yz_smem;
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = c->yz_CS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// Whether the cluster shape of k_yz_solve can be resident on this device.
+static int yz_probe(tc_ctx* c) {
+  if (c->yz_smem > 200 * 1024 || c->yz_thr > 512 || c->yz_P > 32) return 0;
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = yz_config(c, at, 0);
+  int ncl = 0;
+  cudaError_t e = c->yz_P <= 16 ? cudaOccupancyMaxActiveClusters(&ncl, k_yz_solve<16>, &cfg)
+                                : cudaOccupancyMaxActiveClusters(&ncl, k_yz_solve<32>, &cfg);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return ncl > 0;
+}
+
 template <class T> static int set_smem_attrs(const tc_ctx* c) {
   const int big = 200 * 1024;
   TC_CUDA(cudaFuncSetAttribute(k_div_fftx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -222,7 +273,13 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   TC_CUDA(cudaFuncSetAttribute(k_ffty<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_ffty<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_yz_solve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_yz_solve<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  TC_CUDA(cudaFuncSetAttribute(k_yz_solve<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_yz_solve<32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, sizeof(T) == 4 ? 2 : 1, 512>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   (void)c;
@@ -307,6 +364,14 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     k_tri_factors<<<(nmodes + 127) / 128, 128>>>(tb, c->tri_rden, c->tri_cp, c->nxh, c->ny, c->nz);
     if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
   }
+  c->yz_ok = yz_probe(c);
+  c->yz_on = c->yz_ok;
+  if (c->yz_ok) {
+    PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
+    const int nmodes = c->nxh * c->ny;
+    k_tri_chunk_cp<<<(nmodes + 127) / 128, 128>>>(tb, c->tri_cpb, c->nxh, c->ny, c->nz, c->yz_CS, c->yz_P);
+    if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "chunk factors launch"));
+  }
   if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "create sync"));
   c->tab_dt = -1.0;
   c->graphs_on = 1;
@@ -385,6 +450,24 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   const int nrows = nxh * nz;
   const size_t smy = ((size_t)2 * c->RB * padded_len<double>(ny) + ny) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTY, s);
+  if (c->yz_on) {
+    // one fused launch: the tri and inverse-y phases are empty
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = yz_config(c, at, s);
+    PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
+    if (c->yz_P <= 16)
+      TC_CUDA(cudaLaunchKernelEx(&cfg, k_yz_solve<16>, X, (const double*)c->tri_cpb, tb, c->plany,
+                                 (const cpx<double>*)c->twy_d, ny, nz, c->yz_P, c->yz_FB));
+    else
+      TC_CUDA(cudaLaunchKernelEx(&cfg, k_yz_solve<32>, X, (const double*)c->tri_cpb, tb, c->plany,
+                                 (const cpx<double>*)c->twy_d, ny, nz, c->yz_P, c->yz_FB));
+    mark(c, TC_PH_TRI, s);
+    mark(c, TC_PH_IFFTY, s);
+    mark(c, TC_PH_IFFTX, s);
+    k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
+    TC_LAUNCHED();
+    return TC_OK;
+  }
   k_ffty<false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
   const int nmodes = nxh * ny;
@@ -401,9 +484,25 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   return TC_OK;
 }
 
-static int cn_chunks(const tc_ctx* c) { return (c->nz + CN_L - 1) / CN_L; }
+// Chunk length of the CN solve: 16 rows up to nz = 256 (at most 16 warps),
+// 32 rows for deeper channels (nz <= 512).  The G/H tables follow it.
+static int cn_len(const tc_ctx* c) { return c->nz <= 256 ? 16 : 32; }
+static int cn_chunks(const tc_ctx* c) { return (c->nz + cn_len(c) - 1) / cn_len(c); }
 template <class T> static size_t cn_smem(const tc_ctx* c) {
-  return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32) * 8 + (size_t)(c->nz + 2) * 32 * sizeof(T);
+  const int vec = (cn_len(c) == 16 && sizeof(T) == 4) ? 2 : 1;
+  return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32 * vec) * 8;
+}
+template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s) {
+  const int ncol = c->nx * c->ny;
+  const dim3 blk(32, cn_chunks(c));
+  if (cn_len(c) == 16) {
+    constexpr int V = sizeof(T) == 4 ? 2 : 1;
+    const dim3 grid((ncol / V + 31) / 32, 1, 3);
+    k_cn_solve<T, 16, V, 512><<<grid, blk, cn_smem<T>(c), s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz);
+  } else {
+    const dim3 grid((ncol + 31) / 32, 1, 3);
+    k_cn_solve<T, 32, 1, 512><<<grid, blk, cn_smem<T>(c), s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz);
+  }
 }
 
 static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, planes); }
@@ -428,7 +527,7 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   dim3 blk(RHS_TX, RHS_TY);
   dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (scheme == TC_IMEX && c->tab_dt != dt) {
-    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
+    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c));
     c->tab_dt = dt;
   }
   mark(c, TC_PH_RHS, s);
@@ -444,9 +543,7 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   TC_LAUNCHED();
   mark(c, TC_PH_CN, s);
   if (scheme == TC_IMEX) {
-    const int ncol = c->nx * c->ny;
-    k_cn_solve<T><<<dim3((ncol + 31) / 32, 1, 3), dim3(32, cn_chunks(c)), cn_smem<T>(c), s>>>(
-        B[0], B[1], B[2], c->tab, ubase_of(c), c->nx, c->ny, c->nz);
+    launch_cn<T>(c, B[0], B[1], B[2], s);
     TC_LAUNCHED();
   }
   int rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
@@ -681,6 +778,19 @@ extern "C" int tc_use_graphs(tc_ctx* c, int on) {
   return TC_OK;
 }
 
+extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (on && !c->yz_ok) return fail(TC_ERR_SIZE, "fused y/z Poisson kernel not launchable for this grid");
+  if ((on ? 1 : 0) != c->yz_on) {
+    c->yz_on = on ? 1 : 0;
+    if (c->g_valid) {  // the captured steps hold the other path
+      cudaGraphExecDestroy(c->gexec);
+      c->g_valid = 0;
+    }
+  }
+  return TC_OK;
+}
+
 extern "C" int tc_project_initial(tc_ctx* c, void* stream) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
   if (!c->state_set) return fail(TC_ERR_STATE, "no state");
@@ -785,12 +895,10 @@ extern "C" int tc_explicit_rhs(tc_ctx* c, int full, double* ru, double* rv, doub
 template <class T> static int cn_hook_impl(tc_ctx* c, double dt, cudaStream_t s) {
   T** A = (T**)c->st[c->cur];
   if (c->tab_dt != dt) {
-    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
+    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c));
     c->tab_dt = dt;
   }
-  const int ncol = c->nx * c->ny;
-  k_cn_solve<T><<<dim3((ncol + 31) / 32, 1, 3), dim3(32, cn_chunks(c)), cn_smem<T>(c), s>>>(
-      A[0], A[1], A[2], c->tab, ubase_of(c), c->nx, c->ny, c->nz);
+  launch_cn<T>(c, A[0], A[1], A[2], s);
   TC_LAUNCHED();
   return TC_OK;
 }

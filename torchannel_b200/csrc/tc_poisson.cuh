@@ -8,6 +8,8 @@
 // Two real rows travel as one complex row through the x transforms
 // (z = a + i b; A = (Z + conj Z(-m))/2, B = (Z - conj Z(-m))/(2i)).
 #pragma once
+#include <cooperative_groups.h>
+
 #include "tc_common.cuh"
 #include "tc_fft.cuh"
 
@@ -263,6 +265,192 @@ __global__ void __launch_bounds__(128) k_tri_lu(cpx<double>* __restrict__ X, con
 #pragma unroll
     for (int b = 0; b < TRIF_B; ++b) { dc[b] = dn[b]; fc[b] = fn[b]; }
   }
+}
+
+// Batched in-place FFT of `nr` padded rows of R, FB rows at a time through
+// the scratch rows S (the Stockham passes alternate between the two).
+template <bool INV>
+__device__ __forceinline__ void yz_fft_rows(cpx<double>* R, cpx<double>* S, int nr, int FB, int rs, int ny,
+                                            const FftPlan& ply, const cpx<double>* tw, int tid, int nthr) {
+  for (int b0 = 0; b0 < nr; b0 += FB) {
+    const int nb = min(FB, nr - b0);
+    cpx<double>* A = R + (size_t)b0 * rs;
+    if (fft_rows<double, INV>(A, S, nb, rs, ply, tw, tid, nthr)) {
+      for (int e = tid; e < nb * ny; e += nthr) {
+        const int r = e / ny, j = e - r * ny;
+        A[r * rs + padi<double>(j)] = S[r * rs + padi<double>(j)];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// c' of every mode's z system at the last level below each chunk of P
+// levels (k = r P - 1, r = 1 .. CS-1), with the arithmetic of k_tri_factors
+// so that k_yz_solve's on-the-fly factors equal the tabulated ones bit for
+// bit.  Layout cpb[kx][r][ky]; r = 0 holds 0 (no level below the first
+// chunk).
+__global__ void __launch_bounds__(128) k_tri_chunk_cp(PoissonTabs tb, double* __restrict__ cpb, int nxh, int ny,
+                                                      int nz, int CS, int P) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxh * ny) return;
+  const int kx = t / ny, ky = t - kx * ny;
+  const double K2 = tb.k2x[kx] + tb.k2y[ky];
+  double* out = cpb + (size_t)kx * CS * ny + ky;
+  out[0] = 0.0;
+  double cprev = 0.0;
+  for (int k = 0; k < nz; ++k) {
+    const double cl = tb.cl[k], cr = tb.cr[k];
+    const double a = (k == 0) ? 0.0 : cl;
+    double bb = -(cl + cr + K2);
+    if (k == 0) bb += cl;
+    if (k == nz - 1) bb += cr;
+    const double c = (k == nz - 1) ? 0.0 : cr;
+    const double rden = 1.0 / (bb - a * cprev);
+    cprev = c * rden;
+    if ((k + 1) % P == 0 && (k + 1) / P < CS) out[(size_t)((k + 1) / P) * ny] = cprev;
+  }
+  for (int r = (nz + P - 1) / P; r < CS; ++r) out[(size_t)r * ny] = 0.0;  // empty chunks
+}
+
+// Fused middle of the Poisson solve: [FFT along y] -> [Thomas along z] ->
+// [inverse FFT along y] of one kx slab X[kx][:][:] per thread-block cluster
+// of CS CTAs, so the spectrum crosses HBM once each way instead of three
+// times and no factor table is read.  CTA r of the cluster holds planes
+// [r P, r P + P) of the slab in shared memory (padded rows); one thread per
+// column ky sweeps both parts of its chunk.  The LU factors
+// (rden_k = 1/(b_k - a_k c'_{k-1}), c'_k = c_k rden_k, projection_fft.py:44-82
+// rows) are rebuilt on the fly from c' below the chunk (k_tri_chunk_cp) and
+// kept in registers.  The chunk is swept forward from a zero boundary value;
+// the chunk ends, with the chunk products G = prod (-a_k rden_k), are read
+// from the lower CTAs through distributed shared memory and scanned into
+// d'(start-1), and the backward sweep adds G_k d'(start-1) (G_k the product
+// from the chunk start to k) to each forward value; the backward pass is
+// stitched the same way with H = prod (-c'_k) and x(end+1) from the upper
+// CTAs.  The (0,0) mode is gauged as in k_tri_lu (x_{nz-1} = 0); its singular
+// last pivot is never used.  Every CTA takes the same three cluster barriers;
+// the last keeps each CTA's shared memory alive until no peer reads it.
+template <int PM>
+__global__ void __launch_bounds__(512) k_yz_solve(cpx<double>* __restrict__ X, const double* __restrict__ cpb,
+                                                  PoissonTabs tb, FftPlan ply, const cpx<double>* __restrict__ twy,
+                                                  int ny, int nz, int P, int FB) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int CS = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int kx = blockIdx.x / CS;
+  const int rs = padded_len<double>(ny);
+  cpx<double>* R = reinterpret_cast<cpx<double>*>(smraw);    // P rows
+  cpx<double>* S = R + (size_t)P * rs;                         // FB scratch rows
+  cpx<double>* tw = S + (size_t)FB * rs;                       // ny twiddles
+  cpx<double>* eV = tw + ny;                                   // ny: forward chunk-end values
+  cpx<double>* sZ = eV + ny;                                   // ny: backward chunk-start values
+  double* eG = reinterpret_cast<double*>(sZ + ny);             // ny: forward chunk products
+  double* sH = eG + ny;                                        // ny: backward chunk products
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int k0 = rank * P;
+  const int nr = max(0, min(P, nz - k0));
+  cpx<double>* slab = X + ((size_t)kx * nz + k0) * ny;
+  stage_twiddles(tw, twy, ny, tid, nthr);
+#pragma unroll 4
+  for (int e = tid; e < nr * ny; e += nthr) {
+    const int r = e / ny, j = e - r * ny;
+    R[r * rs + padi<double>(j)] = slab[e];
+  }
+  __syncthreads();
+  yz_fft_rows<false>(R, S, nr, FB, rs, ny, ply, tw, tid, nthr);
+
+  // one column per thread (blockDim >= ny); factors in registers
+  const int j = tid;
+  const bool colt = j < ny;
+  const double K2 = colt ? tb.k2x[kx] + tb.k2y[j] : 0.0;
+  double cpv[PM], gv[PM];
+  cpx<double>* col = R + (colt ? padi<double>(j) : 0);
+  if (colt) {
+    double cprev = cpb[((size_t)kx * CS + rank) * ny + j];
+    double yr = 0.0, yi = 0.0, g = 1.0;
+#pragma unroll
+    for (int r = 0; r < PM; ++r) {
+      if (r < nr) {
+        const int k = k0 + r;
+        const double cl = tb.cl[k], cr = tb.cr[k];
+        const double a = (k == 0) ? 0.0 : cl;
+        double bb = -(cl + cr + K2);
+        if (k == 0) bb += cl;
+        if (k == nz - 1) bb += cr;
+        const double c = (k == nz - 1) ? 0.0 : cr;
+        const double rd = 1.0 / (bb - a * cprev);
+        const double cpk = (k == nz - 1) ? 0.0 : c * rd;  // last level: c = 0 (never 0 * inf)
+        const cpx<double> d = col[r * rs];
+        yr = (d.x - a * yr) * rd;
+        yi = (d.y - a * yi) * rd;
+        col[r * rs] = cpx<double>{yr, yi};
+        g *= -a * rd;
+        gv[r] = g;
+        cpv[r] = cpk;
+        cprev = cpk;
+      }
+    }
+    eV[j] = cpx<double>{yr, yi};
+    eG[j] = g;
+  }
+  cluster.sync();
+  if (colt) {
+    // true d'(start-1) from the lower chunks
+    double dr = 0.0, di = 0.0;
+    for (int c = 0; c < rank; ++c) {
+      const cpx<double> v = *cluster.map_shared_rank(eV + j, c);
+      const double gg = *cluster.map_shared_rank(eG + j, c);
+      dr = v.x + gg * dr;
+      di = v.y + gg * di;
+    }
+    const bool gauge = (kx == 0) && (j == 0);
+    double zr = 0.0, zi = 0.0, h = 1.0;
+#pragma unroll
+    for (int r = PM - 1; r >= 0; --r) {
+      if (r < nr) {
+        const int k = k0 + r;
+        const cpx<double> y = col[r * rs];
+        double vr = y.x + gv[r] * dr, vi = y.y + gv[r] * di;
+        if (gauge && k == nz - 1) { vr = 0.0; vi = 0.0; }
+        zr = vr - cpv[r] * zr;
+        zi = vi - cpv[r] * zi;
+        col[r * rs] = cpx<double>{zr, zi};
+        h *= -cpv[r];
+        gv[r] = h;  // H_k from here on
+      }
+    }
+    sZ[j] = cpx<double>{zr, zi};
+    sH[j] = h;
+  }
+  cluster.sync();
+  if (colt) {
+    // true x(end+1) from the upper chunks; x_k = z_k + H_k x(end+1)
+    double xr = 0.0, xi = 0.0;
+    for (int c = CS - 1; c > rank; --c) {
+      const cpx<double> v = *cluster.map_shared_rank(sZ + j, c);
+      const double hh = *cluster.map_shared_rank(sH + j, c);
+      xr = v.x + hh * xr;
+      xi = v.y + hh * xi;
+    }
+#pragma unroll
+    for (int r = 0; r < PM; ++r) {
+      if (r < nr) {
+        const cpx<double> z = col[r * rs];
+        col[r * rs] = cpx<double>{z.x + gv[r] * xr, z.y + gv[r] * xi};
+      }
+    }
+  }
+  cluster.barrier_arrive();  // this CTA reads no peer memory after here
+  __syncthreads();
+  yz_fft_rows<true>(R, S, nr, FB, rs, ny, ply, tw, tid, nthr);
+#pragma unroll 4
+  for (int e = tid; e < nr * ny; e += nthr) {
+    const int r = e / ny, jj = e - r * ny;
+    slab[e] = R[r * rs + padi<double>(jj)];
+  }
+  cluster.barrier_wait();
 }
 
 // Inverse real FFT along x of JT rows of plane k; writes p[k][j][i] (FP64).

@@ -232,32 +232,32 @@ __global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const
 // w (operators.py:753-803): n = nz-1 rows, row m <-> face m+1, explicit
 //   stencil on faces m-1, m, m+1 (the reference's index convention).
 // Thomas factors: inv_den_m = 1/(b_m - a_m cp_{m-1}), cp_m = c_m inv_den_m.
-// Chunked sweep (rows split in chunks of CN_L): with f_m = -a_m inv_den_m,
+// Chunked sweep (rows split in chunks of L, 16 or 32): with f_m = -a_m inv_den_m,
 // G_m = prod_{j = chunk start .. m} f_j and H_m = prod_{j = m .. chunk end}
 // (-cp_j), a chunk swept from zero boundary values is corrected by
 // d'_m += G_m d'_(start-1) and x_m += H_m x_(end+1).
 // Table layout per system: 8 arrays of length nz: a, inv_den, cp, cA, cB, cC, G, H.
 // ---------------------------------------------------------------------------
-#define CN_L 32
 struct CnTab {
   double* uv;  // 8*nz
   double* w;   // 8*nz (first nz-1 rows used)
   double* beta;
 };
 
-__device__ __forceinline__ void cn_chunk_products(double* a, double* iv, double* cp, double* G, double* H, int n) {
+__device__ __forceinline__ void cn_chunk_products(double* a, double* iv, double* cp, double* G, double* H, int n,
+                                                  int L) {
   for (int m = 0; m < n; ++m) {
     const double f = -a[m] * iv[m];
-    G[m] = (m % CN_L == 0) ? f : G[m - 1] * f;
+    G[m] = (m % L == 0) ? f : G[m - 1] * f;
   }
   for (int m = n - 1; m >= 0; --m) {
-    const int e = min((m / CN_L + 1) * CN_L, n) - 1;
+    const int e = min((m / L + 1) * L, n) - 1;
     H[m] = (m == e) ? -cp[m] : H[m + 1] * (-cp[m]);
   }
 }
 
 __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const double* __restrict__ dzc, int nz,
-                            double nu, double dt, int top_neumann) {
+                            double nu, double dt, int top_neumann, int L) {
   const double theta = 0.5;
   const double alpha = theta * dt * nu;
   const int sys = threadIdx.x;
@@ -286,7 +286,7 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
       }
       cA[m] = ea; cB[m] = eb; cC[m] = ec;
     }
-    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz);
+    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz, L);
     *t.beta = (1.0 - theta) * dt * nu;
   } else if (sys == 1) {
     const int n = nz - 1;
@@ -307,23 +307,43 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
       if (m == n - 1) ec = 0.0;
       cA[m] = ea; cB[m] = eb; cC[m] = ec;
     }
-    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n);
+    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n, L);
   }
 }
 
 // ---------------------------------------------------------------------------
 // Kernel (b): batched tridiagonal solve of the CN systems
 // (solve_implicit_diffusion_u/v/w, operators.py:563-811; the reference's PCR,
-// tridiag.py:33-58, solves the same systems).  A block owns 32 consecutive
-// columns of one component (blockIdx.z = 0 u, 1 v, 2 w) and one warp per
-// chunk of CN_L rows.  The columns' planes -1..nz are staged in shared memory
-// (coalesced; u with its base profile added), each thread sweeps its chunk
-// forward and backward from zero boundary values in registers, and the chunk
-// ends are stitched with one value per chunk boundary (G/H tables), so every
-// value is read and written once.  FP64 arithmetic whatever the storage type.
+// tridiag.py:33-58, solves the same systems).  A block owns 32*VEC
+// consecutive columns of one component (blockIdx.z = 0 u, 1 v, 2 w) and one
+// warp per chunk of L rows; a thread owns VEC adjacent columns (VEC = 2 for
+// FP32 storage: 8-byte loads).  Each thread loads the L + 2 planes its
+// chunk's stencil needs straight into registers (coalesced across the warp,
+// all loads in flight together), sweeps the chunk forward and backward from
+// zero boundary values, and the chunk ends are stitched with one value per
+// chunk boundary (G/H tables).  Every value is read and written once; the
+// arithmetic is FP64 (u with its base profile added).
 // ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(1024) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+template <class T, int VEC> struct CnVec;
+template <> struct CnVec<double, 1> {
+  static __device__ __forceinline__ void ld(const double* p, double (&o)[1]) { o[0] = *p; }
+  static __device__ __forceinline__ void st(double* p, const double (&o)[1]) { *p = o[0]; }
+};
+template <> struct CnVec<float, 1> {
+  static __device__ __forceinline__ void ld(const float* p, float (&o)[1]) { o[0] = *p; }
+  static __device__ __forceinline__ void st(float* p, const double (&o)[1]) { *p = (float)o[0]; }
+};
+template <> struct CnVec<float, 2> {
+  static __device__ __forceinline__ void ld(const float* p, float (&o)[2]) {
+    const float2 x = *reinterpret_cast<const float2*>(p);
+    o[0] = x.x; o[1] = x.y;
+  }
+  static __device__ __forceinline__ void st(float* p, const double (&o)[2]) {
+    *reinterpret_cast<float2*>(p) = make_float2((float)o[0], (float)o[1]);
+  }
+};
+template <class T, int L, int VEC, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
                                                    CnTab t, const double* __restrict__ ubase, int nx, int ny,
                                                    int nz) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -332,99 +352,135 @@ __global__ void __launch_bounds__(1024) k_cn_solve(T* __restrict__ u, T* __restr
   const int tid = chunk * 32 + lane, nthr = 32 * nchunk;
   double* tab = reinterpret_cast<double*>(smraw);           // 8*nz
   double* shb = tab + 8 * nz;                                // nz (base, u only)
-  double* bnd = shb + nz;                                    // 2 * nchunk * 32
-  T* win = reinterpret_cast<T*>(bnd + 2 * nchunk * 32);      // (nz+2) * 32, plane p+1 at row p+1
+  double* bnd = shb + nz;                                    // 2 * nchunk * 32 * VEC
   const double* src = comp == 2 ? t.w : t.uv;
   for (int e = tid; e < 8 * nz; e += nthr) tab[e] = src[e];
   for (int e = tid; e < nz; e += nthr) shb[e] = (comp == 0 && ubase) ? ubase[e] : 0.0;
-  const int col0 = blockIdx.x * 32;
-  const int col = col0 + lane;
+  // nx*ny is even, so with VEC = 2 a pair of columns is valid as a whole
+  const int col = (blockIdx.x * 32 + lane) * VEC;
   const int ncols = nx * ny;
+  const bool colok = col < ncols;
   const size_t plane = (size_t)ncols;
-  T* q = comp == 0 ? u : (comp == 1 ? v : w);
-  // stage planes -1..nz of the block's columns (u/v planes, or w faces
-  // including the walls); out-of-range planes are zero
-  const int nstage = nz + 2;
-  for (int e = tid; e < nstage * 32; e += nthr) {
-    const int r = e >> 5, l = e & 31, pl = r - 1, cc = col0 + l;
-    T val = T(0);
-    const int plmax = comp < 2 ? nz - 1 : nz;
-    if (cc < ncols && pl >= 0 && pl <= plmax) val = q[(size_t)pl * plane + cc];
-    win[r * 32 + l] = val;
+  T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + (colok ? col : 0);
+  const int n = comp < 2 ? nz : nz - 1;
+  const int s0 = chunk * L, e0 = min(s0 + L, n);            // rows [s0, e0)
+  const bool act = s0 < n;
+  // window: stencil sources of rows s0..e0-1 = planes (u/v) or faces (w)
+  // s0-1 .. e0; row m uses wv[m-s0], wv[m-s0+1], wv[m-s0+2]; the unknown of
+  // row m is plane m (u/v: wv[m-s0+1]) or face m+1 (w: wv[m-s0+2])
+  T wv[L + 2][VEC];
+  const int plmax = comp < 2 ? nz - 1 : nz;
+#pragma unroll
+  for (int tt = 0; tt < L + 2; ++tt) {
+    const int pl = s0 - 1 + tt;
+    if (act && colok && pl >= 0 && pl <= plmax) {
+      CnVec<T, VEC>::ld(q + (size_t)pl * plane, wv[tt]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) wv[tt][c] = T(0);
+    }
   }
-  __syncthreads();
+  __syncthreads();  // tables staged
   const double* a = tab; const double* iv = a + nz; const double* cp = iv + nz;
   const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
   const double* G = cC + nz; const double* H = G + nz;
   const double beta = *t.beta;
-  const int n = comp < 2 ? nz : nz - 1;
-  const int s0 = chunk * CN_L, e0 = min(s0 + CN_L, n);      // rows [s0, e0)
-  const bool act = s0 < n;
-  // stencil source of row m: u/v planes m-1, m, m+1 (own: plane m); w faces
-  // m-1, m, m+1 (own: face m+1).  win row index = plane + 1.
-  auto src_val = [&](int pl) -> double {
-    return (double)win[(pl + 1) * 32 + lane] + ((comp < 2 && pl >= 0 && pl < nz) ? shb[pl] : 0.0);
+  // base profile of window entry tt (u/v planes in range; zero for w)
+  auto wb = [&](int tt) -> double {
+    const int pl = s0 - 1 + tt;
+    return (comp < 2 && pl >= 0 && pl < nz) ? shb[pl] : 0.0;
   };
-  double y[CN_L];
-  double yend = 0.0;
-  if (act) {
-    double yp = 0.0;
+  double y[L][VEC];
+  double yend[VEC];
 #pragma unroll
-    for (int tt = 0; tt < CN_L; ++tt) {
+  for (int c = 0; c < VEC; ++c) yend[c] = 0.0;
+  if (act) {
+    double yp[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) yp[c] = 0.0;
+    double bm = wb(0), bc = wb(1);
+#pragma unroll
+    for (int tt = 0; tt < L; ++tt) {
       const int m = s0 + tt;
       if (m < e0) {
-        const double sm = src_val(m - 1), sc = src_val(m), sp = src_val(m + 1);
-        const double own = comp < 2 ? sc : sp;
-        const double d = own + beta * (cA[m] * sm + cB[m] * sc + cC[m] * sp);
-        yp = (d - a[m] * yp) * iv[m];
-        y[tt] = yp;
+        const double bp = wb(tt + 2);
+        const double am = a[m], ivm = iv[m], ca = cA[m], cb = cB[m], cc = cC[m];
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) {
+          const double sm = (double)wv[tt][c] + bm, sc = (double)wv[tt + 1][c] + bc, sp = (double)wv[tt + 2][c] + bp;
+          const double own = comp < 2 ? sc : sp;
+          const double d = own + beta * (ca * sm + cb * sc + cc * sp);
+          yp[c] = (d - am * yp[c]) * ivm;
+          y[tt][c] = yp[c];
+        }
+        bm = bc; bc = bp;
       }
     }
-    yend = yp;
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) yend[c] = yp[c];
   }
-  bnd[chunk * 32 + lane] = yend;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) bnd[(chunk * VEC + c) * 32 + lane] = yend[c];
   __syncthreads();
   // true d' entering this chunk: scan the chunk ends below it
-  double Din = 0.0;
-  for (int c = 0; c < chunk; ++c) {
-    const int ce = min(c * CN_L + CN_L, n) - 1;
-    Din = bnd[c * 32 + lane] + G[ce] * Din;
+  double Din[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) Din[c] = 0.0;
+  for (int k = 0; k < chunk; ++k) {
+    const double g = G[min(k * L + L, n) - 1];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) Din[c] = bnd[(k * VEC + c) * 32 + lane] + g * Din[c];
   }
-  double zstart = 0.0;
+  double zstart[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) zstart[c] = 0.0;
   if (act) {
+    // backward from a zero value beyond the chunk end, with the d' shift
+    double zn[VEC];
 #pragma unroll
-    for (int tt = 0; tt < CN_L; ++tt) {
-      const int m = s0 + tt;
-      if (m < e0) y[tt] += G[m] * Din;
-    }
-    // backward from a zero value beyond the chunk end
-    double zn = 0.0;
+    for (int c = 0; c < VEC; ++c) zn[c] = 0.0;
 #pragma unroll
-    for (int tt = CN_L - 1; tt >= 0; --tt) {
+    for (int tt = L - 1; tt >= 0; --tt) {
       const int m = s0 + tt;
       if (m < e0) {
-        zn = y[tt] - cp[m] * zn;
-        y[tt] = zn;
+        const double g = G[m], cpm = cp[m];
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) {
+          zn[c] = (y[tt][c] + g * Din[c]) - cpm * zn[c];
+          y[tt][c] = zn[c];
+        }
       }
     }
-    zstart = zn;
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) zstart[c] = zn[c];
   }
-  bnd[(nchunk + chunk) * 32 + lane] = zstart;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) bnd[((nchunk + chunk) * VEC + c) * 32 + lane] = zstart[c];
   __syncthreads();
   // true x just beyond this chunk: scan the chunk starts above it
-  double Xin = 0.0;
-  for (int c = nchunk - 1; c > chunk; --c) {
-    const int cs = c * CN_L;
-    if (cs < n) Xin = bnd[(nchunk + c) * 32 + lane] + H[cs] * Xin;
-  }
-  if (act && col < ncols) {
+  double Xin[VEC];
 #pragma unroll
-    for (int tt = 0; tt < CN_L; ++tt) {
+  for (int c = 0; c < VEC; ++c) Xin[c] = 0.0;
+  for (int k = nchunk - 1; k > chunk; --k) {
+    const int cs = k * L;
+    if (cs < n) {
+      const double h = H[cs];
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) Xin[c] = bnd[((nchunk + k) * VEC + c) * 32 + lane] + h * Xin[c];
+    }
+  }
+  if (act && colok) {
+#pragma unroll
+    for (int tt = 0; tt < L; ++tt) {
       const int m = s0 + tt;
       if (m < e0) {
-        const double x = y[tt] + H[m] * Xin;
+        const double h = H[m];
+        const double bs = comp < 2 ? shb[m] : 0.0;
+        double o[VEC];
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) o[c] = (y[tt][c] + h * Xin[c]) - bs;
         const int pl = comp < 2 ? m : m + 1;
-        q[(size_t)pl * plane + col] = (T)(x - ((comp < 2) ? shb[m] : 0.0));
+        CnVec<T, VEC>::st(q + (size_t)pl * plane, o);
       }
     }
   }
