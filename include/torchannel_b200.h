@@ -108,12 +108,13 @@ int tc_step(tc_ctx* ctx, int scheme, double dt, int n_steps, void* stream);
  * reference captures only its Poisson solve, solver.py:389-414). */
 int tc_use_graphs(tc_ctx* ctx, int on);
 
-/* Poisson path: on (the default where the device can schedule it), the
- * y transform, the z tridiagonal solve and the inverse y transform of
- * projection_fft.py:117-139 run as one kernel per kx slab on a thread-block
- * cluster; off, as three kernels.  Same arithmetic up to rounding of the
- * chunked sweep.  TC_ERR_SIZE when `on` is asked for a grid whose cluster
- * shape does not fit.  No reference counterpart. */
+/* Poisson path: on, the y transform, the z tridiagonal solve and the
+ * inverse y transform of projection_fft.py:117-139 run as one kernel per kx
+ * slab on a thread-block cluster; off (the default), as three kernels with
+ * register-resident transforms, which measure faster on B200.  Same
+ * arithmetic up to rounding of the chunked sweeps.  TC_ERR_SIZE when `on` is
+ * asked for a grid whose cluster shape does not fit.  No reference
+ * counterpart. */
 int tc_use_fused_poisson(tc_ctx* ctx, int on);
 
 /* Initial projection of a fresh field: div -> Poisson -> u -= grad p

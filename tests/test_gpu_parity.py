@@ -200,8 +200,10 @@ def test_fe_vs_reference_golden(torch_cuda, golden):
 @pytest.mark.parametrize("scheme", ["IMEX", "AB2", "FE"])
 @pytest.mark.parametrize("path", ["separate", "fused"])
 @pytest.mark.parametrize("top", ["dirichlet", "neumann"])
-def test_steps_vs_oracle(torch_cuda, scheme, path, top):
-    nx, ny, nz = 24, 36, 20
+@pytest.mark.parametrize("nx,ny,nz", [(24, 36, 20), (64, 64, 40)])
+def test_steps_vs_oracle(torch_cuda, scheme, path, top, nx, ny, nz):
+    """(64, 64, 40) takes the register-resident x and y transforms and the
+    chunked z solve (3 chunks of 16 levels, the last ragged)."""
     oc = make_oracle(nx, ny, nz, seed=11, top=top, rhs_path=path)
     ch = make_gpu(oc)
     ch.set_state(oc.u, oc.v, oc.w, forcing=0.0)

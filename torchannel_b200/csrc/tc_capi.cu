@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/torchannel_b200.h"
@@ -82,6 +83,7 @@ struct tc_ctx {
   // fused y/z Poisson middle (k_yz_solve): cluster size, planes per CTA,
   // FFT batch rows, threads, shared memory; yz_ok = launchable here
   int yz_CS, yz_P, yz_FB, yz_thr, yz_ok, yz_on;
+  int nsm, yreg_blocks;  // SM count; resident-block cap of the y register FFT
   size_t yz_smem;
   int cur, have_hist, state_set;
   double tab_dt;
@@ -236,6 +238,92 @@ extern "C" int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes) {
   return TC_OK;
 }
 
+// ---- register-FFT launches (lengths N1 * 16, N1 in 4, 6, 8, 12, 16, 24) ----
+template <class F> static void for_each_n1(int n, F&& f) {
+  switch (n / 16) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 12: f(std::integral_constant<int, 12>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: f(std::integral_constant<int, 24>{}); break;
+  }
+}
+template <int N1> static size_t fftx_reg_smem() {
+  return (size_t)8 * ((RowFft<N1>::TILE + 7) / 8 * 8 + 1) * sizeof(cpx<double>);
+}
+template <int N1> static size_t ifftx_reg_smem() {
+  constexpr int NH = RowFft<N1>::N / 2 + 1;
+  return ((size_t)16 * ((NH + 7) / 8 * 8 + 1) + (size_t)8 * RowFft<N1>::TILE) * sizeof(cpx<double>);
+}
+template <int N1> static size_t ffty_reg_smem() {
+  return (size_t)4 * RowFft<N1>::RPW * RowFft<N1>::TILE * sizeof(cpx<double>);
+}
+// x transforms take the register path for supported nx when ny is a multiple
+// of 16 (16 rows a block); y transforms for supported ny.
+static bool xreg_ok(const tc_ctx* c) { return rowfft_supported(c->nx) && c->ny % 16 == 0; }
+static bool yreg_ok(const tc_ctx* c) { return rowfft_supported(c->ny); }
+
+// Shared-memory opt-in and the resident-block count of the y kernel.
+template <class T> static int reg_fft_setup(tc_ctx* c) {
+  int rc = TC_OK;
+  if (xreg_ok(c)) {
+    for_each_n1(c->nx, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      if (cudaFuncSetAttribute(k_div_fftx_reg<T, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fftx_reg_smem<N1>()) != cudaSuccess ||
+          cudaFuncSetAttribute(k_ifftx_reg<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ifftx_reg_smem<N1>()) != cudaSuccess)
+        rc = fail(TC_ERR_CUDA, "register x FFT attributes");
+    });
+  }
+  c->yreg_blocks = c->nsm;
+  if (yreg_ok(c)) {
+    for_each_n1(c->ny, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      int nb = 0;
+      if (cudaFuncSetAttribute(k_ffty_reg<N1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ffty_reg_smem<N1>()) != cudaSuccess ||
+          cudaFuncSetAttribute(k_ffty_reg<N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ffty_reg_smem<N1>()) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ffty_reg<N1, false>, 128, ffty_reg_smem<N1>()) !=
+              cudaSuccess)
+        rc = fail(TC_ERR_CUDA, "register y FFT setup");
+      if (nb > 0) c->yreg_blocks = nb * c->nsm;
+    });
+  }
+  if (c->yreg_blocks < 1) c->yreg_blocks = 1;
+  return rc;
+}
+
+template <bool INV> static void ffty_reg(const tc_ctx* c, cpx<double>* X, int nrows, cudaStream_t s) {
+  for_each_n1(c->ny, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    const int rpb = 4 * RowFft<N1>::RPW;
+    int nblk = (nrows + rpb - 1) / rpb;
+    if (nblk > c->yreg_blocks) nblk = c->yreg_blocks;
+    k_ffty_reg<N1, INV><<<nblk, 128, ffty_reg_smem<N1>(), s>>>(X, nrows, c->twy_d);
+  });
+}
+
+template <class T>
+static void fftx_reg(const tc_ctx* c, Grid<T> g, const T* u, const T* v, const T* w, const double* field,
+                     cpx<double>* X, double scale, cudaStream_t s) {
+  for_each_n1(c->nx, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    k_div_fftx_reg<T, N1><<<dim3(c->ny / 16, c->nz), 32 * 8 / RowFft<N1>::RPW, fftx_reg_smem<N1>(), s>>>(
+        g, u, v, w, field, X, c->twx_d, scale);
+  });
+}
+
+static void ifftx_reg(const tc_ctx* c, const cpx<double>* X, double* p, cudaStream_t s) {
+  for_each_n1(c->nx, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    k_ifftx_reg<N1><<<dim3(c->ny / 16, c->nz), 32 * 8 / RowFft<N1>::RPW, ifftx_reg_smem<N1>(), s>>>(
+        X, p, c->ny, c->nz, c->twx_d);
+  });
+}
+
 static cudaLaunchConfig_t yz_config(const tc_ctx* c, cudaLaunchAttribute* at, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(c->nxh * c->yz_CS, 1, 1);
@@ -358,6 +446,10 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     return bail(r2);
   r2 = (c->tsz == 8) ? set_smem_attrs<double>(c) : set_smem_attrs<float>(c);
   if (r2) return bail(r2);
+  if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
+    return bail(fail(TC_ERR_CUDA, "SM count"));
+  r2 = (c->tsz == 8) ? reg_fft_setup<double>(c) : reg_fft_setup<float>(c);
+  if (r2) return bail(r2);
   {
     PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
     const int nmodes = c->nxh * c->ny;
@@ -365,7 +457,7 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
   }
   c->yz_ok = yz_probe(c);
-  c->yz_on = c->yz_ok;
+  c->yz_on = 0;  // the three-kernel path with register FFTs is faster
   if (c->yz_ok) {
     PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
     const int nmodes = c->nxh * c->ny;
@@ -446,7 +538,11 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   cpx<double>* X = c->X;
   const size_t smx = ((size_t)2 * (c->JT / 2) * padded_len<double>(nx) + nx) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTX, s);
-  k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, c->twx_d, scale, c->JT);
+  const bool xreg = xreg_ok(c);
+  if (xreg)
+    fftx_reg<T>(c, g, u, v, w, field, X, scale, s);
+  else
+    k_div_fftx<T><<<dim3(ny / c->JT, nz), 256, smx, s>>>(g, u, v, w, field, X, c->planx, c->twx_d, scale, c->JT);
   const int nrows = nxh * nz;
   const size_t smy = ((size_t)2 * c->RB * padded_len<double>(ny) + ny) * sizeof(cpx<double>);
   mark(c, TC_PH_FFTY, s);
@@ -464,11 +560,18 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
     mark(c, TC_PH_TRI, s);
     mark(c, TC_PH_IFFTY, s);
     mark(c, TC_PH_IFFTX, s);
-    k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
+    if (xreg)
+      ifftx_reg(c, X, p, s);
+    else
+      k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
     TC_LAUNCHED();
     return TC_OK;
   }
-  k_ffty<false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
+  const bool yreg = yreg_ok(c);
+  if (yreg)
+    ffty_reg<false>(c, X, nrows, s);
+  else
+    k_ffty<false><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
   const int nmodes = nxh * ny;
   mark(c, TC_PH_TRI, s);
@@ -477,9 +580,15 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   else
     k_tri<<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, tb, nxh, ny, nz);
   mark(c, TC_PH_IFFTY, s);
-  k_ffty<true><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
+  if (yreg)
+    ffty_reg<true>(c, X, nrows, s);
+  else
+    k_ffty<true><<<(nrows + c->RB - 1) / c->RB, 256, smy, s>>>(X, nrows, ny, c->plany, c->twy_d, c->RB);
   mark(c, TC_PH_IFFTX, s);
-  k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
+  if (xreg)
+    ifftx_reg(c, X, p, s);
+  else
+    k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
   TC_LAUNCHED();
   return TC_OK;
 }
@@ -1165,6 +1274,10 @@ extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, doubl
   g.nx = nx; g.ny = ny; g.nz = nz; g.Lx = Lx; g.Ly = Ly; g.Lz = 1.0; g.nu = 1.0; g.precision = TC_FP64;
   tc_ctx c{};
   fill_basic(&c, &g);
+  c.dev = dev;
+  TC_CUDA(cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, dev));
+  rc = reg_fft_setup<double>(&c);
+  if (rc) return rc;
   double* field = (double*)(base + off[0]);
   c.X = (cpx<double>*)(base + off[1]);
   c.k2x = (double*)(base + off[2]); c.k2y = (double*)(base + off[3]);

@@ -12,6 +12,7 @@
 
 #include "tc_common.cuh"
 #include "tc_fft.cuh"
+#include "tc_fft_reg.cuh"
 
 namespace tc {
 
@@ -103,6 +104,137 @@ __global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int n
     const int r = e / ny, jj = e - r * ny;
     base[e] = Z[r * rs + padi<double>(jj)];
   }
+}
+
+// In-place complex FFT along y of the rows X[kx][k][:] with the register
+// transform (ny = N1 * 16): RowFft<N1>::RPW rows per warp, each row read and
+// written once, no block barrier; warps stride over the rows.
+template <int N1, bool INV>
+__global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, int nrows,
+                                                 const cpx<double>* __restrict__ twy) {
+  using RF = RowFft<N1>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;   // row of the warp, lane in the row
+  const int wpb = blockDim.x >> 5;
+  cpx<double>* tile = reinterpret_cast<cpx<double>*>(smraw) + (size_t)(warp * RF::RPW + sub) * RF::TILE;
+  const int rstep = gridDim.x * wpb * RF::RPW;
+  for (int row0 = (blockIdx.x * wpb + warp) * RF::RPW; row0 < nrows; row0 += rstep) {
+    const int row = row0 + sub;
+    const bool ok = sub < RF::RPW && row < nrows;
+    cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
+    if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
+    __syncwarp();
+    if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+    __syncwarp();
+  }
+}
+
+// Divergence (as k_div_fftx) of rows j0 .. j0+15 of plane k and forward real
+// FFT along x with the register transform (nx = N1 * 16); two real rows
+// travel as one complex row, RowFft<N1>::RPW such rows per warp (8 / RPW
+// warps a block).  The unpacked half spectra are written transposed,
+// X[m][k][j], as in k_div_fftx.
+template <class T, int N1>
+__global__ void __launch_bounds__(256) k_div_fftx_reg(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+                                                     const T* __restrict__ w, const double* __restrict__ field,
+                                                     cpx<double>* __restrict__ X,
+                                                     const cpx<double>* __restrict__ twx, double scale) {
+  using RF = RowFft<N1>;
+  constexpr int N = RF::N, NH = N / 2 + 1;
+  constexpr int ZP = (RF::TILE + 7) / 8 * 8 + 1;          // row pitch of the spectra (16 B mod 128 B)
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cpx<double>* zs = reinterpret_cast<cpx<double>*>(smraw);  // 8 packed rows x ZP
+  const int ny = g.ny, nz = g.nz;
+  const int k = blockIdx.y, j0 = blockIdx.x * 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
+  const int pr = warp * RF::RPW + sub;                      // packed row: j = j0 + 2 pr, +1
+  const bool ok = sub < RF::RPW && pr < 8;
+  cpx<double>* tile = zs + (size_t)(ok ? pr : 0) * ZP;
+  const double idx = (double)g.idx, idy = (double)g.idy;
+  const double idzf = (u != nullptr) ? (double)g.idzf[k] : 0.0;
+  const int ja = j0 + 2 * pr, jb = ja + 1;
+  auto divv = [&](int j, int i) -> double {
+    double val;
+    if (u != nullptr) {
+      const size_t o = pidx(k, j, i, ny, N);
+      val = ((double)u[o] - (double)u[pidx(k, j, i == 0 ? N - 1 : i - 1, ny, N)]) * idx +
+            ((double)v[o] - (double)v[pidx(k, j == 0 ? ny - 1 : j - 1, i, ny, N)]) * idy +
+            ((double)w[pidx(k + 1, j, i, ny, N)] - (double)w[o]) * idzf;
+    } else {
+      val = field[pidx(k, j, i, ny, N)];
+    }
+    return val * scale;
+  };
+  if (ok && l < RF::N2)
+    rowfft_pass1<N1, false>([&](int i) { return cmake<double>(divv(ja, i), divv(jb, i)); }, l, tile, twx);
+  __syncwarp();
+  cpx<double> b[RF::N2];
+  if (ok && l < N1) {
+#pragma unroll
+    for (int n2 = 0; n2 < RF::N2; ++n2) b[n2] = tile[l * RF::TP + n2];
+  }
+  __syncwarp();
+  if (ok && l < N1) {
+    Dft<RF::N2, false>::run(b);
+#pragma unroll
+    for (int k2 = 0; k2 < RF::N2; ++k2) tile[l + N1 * k2] = b[k2];  // Z[m], natural order
+  }
+  __syncthreads();
+  // unpack: A = (Z[m] + conj Z[N-m]) / 2 (row ja), B = (Z[m] - conj Z[N-m]) / (2i) (row jb)
+  for (int e = threadIdx.x; e < NH * 16; e += blockDim.x) {
+    const int m = e >> 4, r = e & 15, q = r >> 1;
+    const cpx<double> Zm = zs[q * ZP + m];
+    const cpx<double> Zn = cconj(zs[q * ZP + (m == 0 ? 0 : N - m)]);
+    cpx<double> out;
+    if ((r & 1) == 0) out = cscale(cadd(Zm, Zn), 0.5);
+    else {
+      const cpx<double> d = csub(Zm, Zn);
+      out = cmake<double>(0.5 * d.y, -0.5 * d.x);
+    }
+    X[((size_t)m * nz + k) * ny + j0 + r] = out;
+  }
+}
+
+// Inverse real FFT along x of rows j0 .. j0+15 of plane k with the register
+// transform (nx = N1 * 16); writes p[k][j][i] (FP64).  Two rows travel as one
+// complex row Z = A + i B built from the half spectra (DC and Nyquist real).
+template <int N1>
+__global__ void __launch_bounds__(256) k_ifftx_reg(const cpx<double>* __restrict__ X, double* __restrict__ p,
+                                                  int ny, int nz, const cpx<double>* __restrict__ twx) {
+  using RF = RowFft<N1>;
+  constexpr int N = RF::N, NH = N / 2 + 1;
+  constexpr int SP = (NH + 7) / 8 * 8 + 1;                  // staging pitch
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cpx<double>* S = reinterpret_cast<cpx<double>*>(smraw);   // 16 rows x SP half spectra
+  cpx<double>* tiles = S + 16 * SP;                          // 8 packed rows x TILE
+  const int k = blockIdx.y, j0 = blockIdx.x * 16;
+  for (int e = threadIdx.x; e < NH * 16; e += blockDim.x) {
+    const int m = e >> 4, r = e & 15;
+    cpx<double> val = X[((size_t)m * nz + k) * ny + j0 + r];
+    if (m == 0 || 2 * m == N) val.y = 0.0;  // irfft ignores these imaginary parts
+    S[r * SP + m] = val;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
+  const int pr = warp * RF::RPW + sub;
+  const bool ok = sub < RF::RPW && pr < 8;
+  cpx<double>* tile = tiles + (size_t)(ok ? pr : 0) * RF::TILE;
+  const cpx<double>* A = S + (2 * (ok ? pr : 0)) * SP;
+  const cpx<double>* B = A + SP;
+  auto ld = [&](int m) -> cpx<double> {
+    cpx<double> a, bb;
+    if (m < NH) { a = A[m]; bb = B[m]; }
+    else { a = cconj(A[N - m]); bb = cconj(B[N - m]); }
+    return cmake<double>(a.x - bb.y, a.y + bb.x);  // A + i B
+  };
+  if (ok && l < RF::N2) rowfft_pass1<N1, true>(ld, l, tile, twx);
+  __syncwarp();
+  double* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
+  if (ok && l < N1)
+    rowfft_pass2<N1, true>([&](int i, cpx<double> z) { pa[i] = z.x; pa[N + i] = z.y; }, l, tile);
 }
 
 // Thomas sweep along z for every mode (kx, ky), one thread per mode
