@@ -210,6 +210,54 @@ int tc_timing_read(tc_ctx* ctx, double* ms_host, int* n_steps);
 /* Read and clear the device error word (syncs). */
 int tc_error(tc_ctx* ctx, int* code_host);
 
+/* ---- Adjoint of the IMEX step (FP64 contexts; TC_ERR_ARG otherwise) ------
+ * No counterpart in the reference, which has no adjoint.  Reverse-mode
+ * derivatives of solver.py:580-710 for gradients of an objective of the flow
+ * (e.g. a time-averaged kinetic energy) with respect to the initial field and
+ * a body-force field.  Arrays are in the internal layout: u and v hold nz
+ * planes of nx*ny values (x fastest), w holds nz+1 face planes whose wall
+ * planes 0 and nz stay 0; buffers of tc_internal_doubles' field size
+ * ((nz+1)*nx*ny) fit all three.  All calls are asynchronous on `stream`.
+ *
+ * tc_adjoint_scratch_bytes: size of the scratch every adjoint call takes
+ *   (16-byte aligned; the CN adjoint tables are cached in it per dt).
+ * tc_set_body_force: a body force F (caller-owned, internal layout) added to
+ *   the explicit right-hand side of every following step (R += F); null
+ *   pointers remove it.
+ * tc_internal_doubles / tc_save_internal / tc_load_internal: a flat record of
+ *   the step state (u, v, w, the AB2 history r_u, r_v, r_w, each
+ *   (nz+1)*nx*ny doubles, then the forcing) for checkpoints.
+ * tc_kinetic_energy: *acc += weight * (1/(2V)) sum W q^2 of the current state
+ *   (W = cell volume dx dy dz_f for u, v; face volume dx dy dz_c for w).
+ * tc_adjoint_ke_seed: lambda += weight * W q / V (the gradient of that term).
+ * tc_adjoint_rhs: lambda += (nu Dxy - dA[q])^T lambda_R, the transposed
+ *   linearised explicit right-hand side of operators.py:126-247, 474-548 at q.
+ * tc_adjoint_cn: lambda <- (Cz^-1 Bz)^T lambda, the transposed CN solve of
+ *   operators.py:563-811 for dt.
+ * tc_adjoint_project: lambda <- P^T lambda, P the FFT projection
+ *   (projection_fft.py, projection.py:143-165); P^T = W P W^-1.
+ * tc_adjoint_step: one reverse IMEX step.  In: q (the forward state before
+ *   the step), lambda (adjoint of the state after it), lambda_r (adjoint of
+ *   the history the step writes), mu (device scalar, adjoint of the forcing
+ *   after the step).  Out, in place: the adjoints of the state, history and
+ *   forcing before the step; lambda_F (optional) accumulates the body-force
+ *   gradient.  `first` marks a step taken without history (Euler start). */
+int tc_adjoint_scratch_bytes(tc_ctx* ctx, size_t* bytes);
+int tc_set_body_force(tc_ctx* ctx, const double* fu, const double* fv, const double* fw);
+int tc_internal_doubles(tc_ctx* ctx, size_t* n);
+int tc_save_internal(tc_ctx* ctx, double* dst, int* have_hist, void* stream);
+int tc_load_internal(tc_ctx* ctx, const double* src, int have_hist, void* stream);
+int tc_kinetic_energy(tc_ctx* ctx, double weight, double* acc, void* scratch, void* stream);
+int tc_adjoint_ke_seed(tc_ctx* ctx, double weight, const double* qu, const double* qv, const double* qw,
+                       double* lu, double* lv, double* lw, void* stream);
+int tc_adjoint_rhs(tc_ctx* ctx, const double* qu, const double* qv, const double* qw, const double* Ru,
+                   const double* Rv, const double* Rw, double* lu, double* lv, double* lw, void* stream);
+int tc_adjoint_cn(tc_ctx* ctx, double dt, double* lu, double* lv, double* lw, void* scratch, void* stream);
+int tc_adjoint_project(tc_ctx* ctx, double* lu, double* lv, double* lw, void* scratch, void* stream);
+int tc_adjoint_step(tc_ctx* ctx, double dt, int first, const double* qu, const double* qv, const double* qw,
+                    double* lu, double* lv, double* lw, double* lru, double* lrv, double* lrw,
+                    double* lFu, double* lFv, double* lFw, double* mu, void* scratch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

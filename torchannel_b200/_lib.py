@@ -63,6 +63,17 @@ SIGNATURES = [
     ("tc_timing_enable", _I, [_V, _I]),
     ("tc_timing_read", _I, [_V, _dp, ctypes.POINTER(_I)]),
     ("tc_error", _I, [_V, ctypes.POINTER(_I)]),
+    ("tc_adjoint_scratch_bytes", _I, [_V, ctypes.POINTER(ctypes.c_size_t)]),
+    ("tc_set_body_force", _I, [_V, _V, _V, _V]),
+    ("tc_internal_doubles", _I, [_V, ctypes.POINTER(ctypes.c_size_t)]),
+    ("tc_save_internal", _I, [_V, _V, ctypes.POINTER(_I), _V]),
+    ("tc_load_internal", _I, [_V, _V, _I, _V]),
+    ("tc_kinetic_energy", _I, [_V, _D, _V, _V, _V]),
+    ("tc_adjoint_ke_seed", _I, [_V, _D, _V, _V, _V, _V, _V, _V, _V]),
+    ("tc_adjoint_rhs", _I, [_V, _V, _V, _V, _V, _V, _V, _V, _V, _V, _V]),
+    ("tc_adjoint_cn", _I, [_V, _D, _V, _V, _V, _V, _V]),
+    ("tc_adjoint_project", _I, [_V, _V, _V, _V, _V, _V]),
+    ("tc_adjoint_step", _I, [_V, _D, _I] + [_V] * 15),
 ]
 
 

@@ -1,0 +1,193 @@
+"""Gradients of a time-averaged kinetic-energy objective of the IMEX channel
+with respect to the initial velocity field and a body-force field, from the
+hand-written CUDA adjoint of every substep (``tc_adjoint_*`` in
+``include/torchannel_b200.h``), with checkpointed recomputation of the step
+states.  FP64 contexts only.  The reference has no adjoint; the forward map
+differentiated is its IMEX step (``solver.py:580-710``) with an added body
+force F in the explicit right-hand side.
+
+Objective: J = sum over steps n in ``window`` of weight * KE(q^n), weight =
+1/len(window), KE(q) = (1/(2V)) sum W q^2 over the degrees of freedom (W = the
+cell volume dx dy dz_f for u and v, the face volume dx dy dz_c for w).
+
+Layouts: public arguments are reference-layout tensors (``u`` (nx+1, ny+2,
+nz+2), ``v`` (nx+2, ny+1, nz+2), ``w`` (nx+2, ny+2, nz+1), float64, on the
+device); gradients come back in the same layout on the degrees of freedom
+(ghost entries 0: the step overwrites ghosts before using them).  The C ABI
+works on the internal layout ([k][j][i]; u, v nz planes, w nz+1 face planes),
+converted here by index copies.
+"""
+import ctypes
+
+import torch
+
+from . import _lib as L
+from .core import _ptr, _stream
+
+
+def to_internal(ch, u, v, w):
+    """Degrees of freedom of reference-layout u, v, w as three internal fields
+    of (nz+1, ny, nx) (u and v with a zero top plane, w with zero walls)."""
+    nx, ny, nz = ch.nx, ch.ny, ch.nz
+    out = []
+    for a, kz in ((u, nz), (v, nz)):
+        t = torch.zeros(nz + 1, ny, nx, dtype=torch.float64, device="cuda")
+        t[:nz] = a[1:nx + 1, 1:ny + 1, 1:nz + 1].permute(2, 1, 0)
+        out.append(t)
+    t = torch.zeros(nz + 1, ny, nx, dtype=torch.float64, device="cuda")
+    t[1:nz] = w[1:nx + 1, 1:ny + 1, 1:nz].permute(2, 1, 0)
+    out.append(t)
+    return out
+
+
+def from_internal(ch, fu, fv, fw):
+    """Internal fields back to reference-layout tensors (ghosts 0)."""
+    nx, ny, nz = ch.nx, ch.ny, ch.nz
+    u = torch.zeros(nx + 1, ny + 2, nz + 2, dtype=torch.float64, device="cuda")
+    v = torch.zeros(nx + 2, ny + 1, nz + 2, dtype=torch.float64, device="cuda")
+    w = torch.zeros(nx + 2, ny + 2, nz + 1, dtype=torch.float64, device="cuda")
+    u[1:nx + 1, 1:ny + 1, 1:nz + 1] = fu[:nz].permute(2, 1, 0)
+    v[1:nx + 1, 1:ny + 1, 1:nz + 1] = fv[:nz].permute(2, 1, 0)
+    w[1:nx + 1, 1:ny + 1, 1:nz] = fw[1:nz].permute(2, 1, 0)
+    return u, v, w
+
+
+class AdjointRunner:
+    """Forward run of ``n_steps`` IMEX steps of ``dt`` from a fresh state
+    (Euler first step, as after ``tc_set_state``), accumulating the objective,
+    and the reverse sweep.  Checkpoints (the full step record: state, AB2
+    history, forcing) are kept every ``checkpoint_every`` steps; the reverse
+    sweep recomputes each segment from its checkpoint and then runs the
+    adjoint steps of the segment backwards."""
+
+    def __init__(self, ch, dt, n_steps, window, checkpoint_every=10):
+        if ch.precision != "fp64":
+            raise ValueError("the adjoint needs an FP64 channel")
+        self.ch, self.lib = ch, ch.lib
+        self.dt, self.N = float(dt), int(n_steps)
+        self.window = sorted(set(int(n) for n in window))
+        if not self.window or self.window[0] < 0 or self.window[-1] > self.N:
+            raise ValueError("window must be a non-empty subset of 0..n_steps")
+        self.weight = 1.0 / len(self.window)
+        self.C = max(1, int(checkpoint_every))
+        nb = ctypes.c_size_t()
+        L.check(self.lib.tc_adjoint_scratch_bytes(ch.ctx, ctypes.byref(nb)))
+        self.scratch = torch.empty(nb.value // 8 + 2, dtype=torch.float64, device="cuda")
+        nr = ctypes.c_size_t()
+        L.check(self.lib.tc_internal_doubles(ch.ctx, ctypes.byref(nr)))
+        self.nrec = nr.value
+        self.field = (ch.nz + 1) * ch.ny * ch.nx
+        self.ckpt = {}
+        self.body = None
+
+    # -- records ---------------------------------------------------------
+    def _save(self):
+        rec = torch.empty(self.nrec, dtype=torch.float64, device="cuda")
+        hh = ctypes.c_int()
+        L.check(self.lib.tc_save_internal(self.ch.ctx, _ptr(rec), ctypes.byref(hh), _stream()))
+        return rec, hh.value
+
+    def _load(self, rec, hh):
+        L.check(self.lib.tc_load_internal(self.ch.ctx, _ptr(rec), int(hh), _stream()))
+
+    def _q(self, rec):
+        f = self.field
+        return rec[0:f], rec[f:2 * f], rec[2 * f:3 * f]
+
+    def set_body_force(self, fu=None, fv=None, fw=None):
+        """Body force in the internal layout (kept alive here), or None."""
+        if fu is None:
+            self.body = None
+            L.check(self.lib.tc_set_body_force(self.ch.ctx, None, None, None))
+        else:
+            self.body = [t.contiguous() for t in (fu, fv, fw)]
+            L.check(self.lib.tc_set_body_force(self.ch.ctx, *[_ptr(t) for t in self.body]))
+
+    # -- forward -----------------------------------------------------------
+    def forward(self, u0, v0, w0, forcing0=0.0):
+        """Set the initial state (reference layout), run N steps; returns J as
+        a device tensor."""
+        ch = self.ch
+        ch.set_state(u0, v0, w0, forcing=forcing0)
+        J = torch.zeros(1, dtype=torch.float64, device="cuda")
+        self.ckpt = {}
+        if 0 in self.window:
+            self._ke(J)
+        for n in range(self.N):
+            if n % self.C == 0:
+                self.ckpt[n] = self._save()
+            ch.step("IMEX", self.dt)
+            if n + 1 in self.window:
+                self._ke(J)
+        return J
+
+    def _ke(self, J):
+        L.check(self.lib.tc_kinetic_energy(self.ch.ctx, self.weight, _ptr(J), _ptr(self.scratch), _stream()))
+
+    # -- reverse -----------------------------------------------------------
+    def backward(self, seed=1.0):
+        """Reverse sweep; returns (dJ/dq0, dJ/dF, dJ/dforcing0) with dJ/dq0 and
+        dJ/dF as internal fields (scaled by `seed`)."""
+        ch, lib, f = self.ch, self.lib, self.field
+        z = lambda: torch.zeros(f, dtype=torch.float64, device="cuda")  # noqa: E731
+        lam = [z(), z(), z()]
+        lr = [z(), z(), z()]
+        lF = [z(), z(), z()] if self.body is not None else None
+        mu = torch.zeros(1, dtype=torch.float64, device="cuda")
+        w = self.weight
+        first_hist = self.ckpt[0][1]
+        for s in sorted(self.ckpt, reverse=True):
+            e = min(s + self.C, self.N)
+            rec0, hh0 = self.ckpt[s]
+            self._load(rec0, hh0)
+            recs = {s: (rec0, hh0)}
+            for n in range(s, e):
+                ch.step("IMEX", self.dt)
+                recs[n + 1] = self._save()
+            for n in range(e - 1, s - 1, -1):
+                if n + 1 in self.window:
+                    qn1 = self._q(recs[n + 1][0])
+                    L.check(lib.tc_adjoint_ke_seed(ch.ctx, w, *[_ptr(t) for t in qn1],
+                                                   *[_ptr(t) for t in lam], _stream()))
+                q = self._q(recs[n][0])
+                first = int(recs[n][1] == 0)
+                Fp = [_ptr(t) for t in lF] if lF is not None else [None, None, None]
+                L.check(lib.tc_adjoint_step(ch.ctx, self.dt, first, *[_ptr(t) for t in q],
+                                            *[_ptr(t) for t in lam], *[_ptr(t) for t in lr], *Fp,
+                                            _ptr(mu), _ptr(self.scratch), _stream()))
+        if 0 in self.window:
+            q0 = self._q(self.ckpt[0][0])
+            L.check(lib.tc_adjoint_ke_seed(ch.ctx, w, *[_ptr(t) for t in q0], *[_ptr(t) for t in lam], _stream()))
+        del first_hist
+        shp = (ch.nz + 1, ch.ny, ch.nx)
+        gq = [t.view(shp) * seed for t in lam]
+        gF = [t.view(shp) * seed for t in lF] if lF is not None else None
+        return gq, gF, mu * seed
+
+
+class KineticEnergyObjective(torch.autograd.Function):
+    """J(u0, v0, w0, Fu, Fv, Fw): the runner's objective as an autograd
+    function of the reference-layout initial field and body force (all
+    float64 CUDA tensors).  Its backward is the CUDA adjoint."""
+
+    @staticmethod
+    def forward(ctx, u0, v0, w0, Fu, Fv, Fw, runner):
+        Fi = to_internal(runner.ch, Fu, Fv, Fw)
+        runner.set_body_force(*Fi)
+        J = runner.forward(u0, v0, w0)
+        ctx.runner = runner
+        return J[0].clone()
+
+    @staticmethod
+    def backward(ctx, gJ):
+        r = ctx.runner
+        gq, gF, _ = r.backward(seed=float(gJ))
+        gu, gv, gw = from_internal(r.ch, *gq)
+        fu, fv, fw = from_internal(r.ch, *gF)
+        return gu, gv, gw, fu, fv, fw, None
+
+
+def kinetic_energy_objective(ch, u0, v0, w0, Fu, Fv, Fw, dt, n_steps, window, checkpoint_every=10):
+    """Convenience: J as a differentiable tensor (see KineticEnergyObjective)."""
+    runner = AdjointRunner(ch, dt, n_steps, window, checkpoint_every)
+    return KineticEnergyObjective.apply(u0, v0, w0, Fu, Fv, Fw, runner)

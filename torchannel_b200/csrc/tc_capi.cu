@@ -15,6 +15,7 @@
 #include "tc_poisson.cuh"
 #include "tc_stats.cuh"
 #include "tc_step.cuh"
+#include "tc_adjoint.cuh"
 
 using namespace tc;
 
@@ -87,6 +88,11 @@ struct tc_ctx {
   size_t yz_smem;
   int cur, have_hist, state_set;
   double tab_dt;
+  // adjoint: body force of the forward step (caller-owned, FP64 internal
+  // layout, or null) and the dt of the CN adjoint tables in the scratch
+  const double* body[3];
+  double adj_tab_dt;
+  const void* adj_tab_ptr;
   // CUDA graph of two consecutive steps (tc_step replays it for n_steps >= 4)
   cudaStream_t cap_stream;
   cudaGraphExec_t gexec;
@@ -466,6 +472,9 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
   }
   if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "create sync"));
   c->tab_dt = -1.0;
+  c->adj_tab_dt = -1.0;
+  c->adj_tab_ptr = nullptr;
+  c->body[0] = c->body[1] = c->body[2] = nullptr;
   c->graphs_on = 1;
   *out = c;
   return TC_OK;
@@ -650,6 +659,15 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
     k_rhs_update<T, true, UPD_FE><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
                                                        c->scal + SC_FORCING, (T)dt, 0);
   TC_LAUNCHED();
+  if constexpr (sizeof(T) == 8) {
+    if (c->body[0]) {  // R += F: q* += c F, r += F (FP64 contexts only)
+      const double cq = (scheme == TC_FE || !c->have_hist) ? dt : 1.5 * dt;
+      k_add_body<<<dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz + 1), dim3(32, 8), 0, s>>>(
+          B[0], B[1], B[2], R[0], R[1], R[2], c->body[0], c->body[1], c->body[2], cq, scheme == TC_FE ? 0.0 : 1.0,
+          c->nx, c->ny, c->nz);
+      TC_LAUNCHED();
+    }
+  }
   mark(c, TC_PH_CN, s);
   if (scheme == TC_IMEX) {
     launch_cn<T>(c, B[0], B[1], B[2], s);
@@ -1294,4 +1312,226 @@ extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, doubl
   rc = poisson_impl<double>(&c, nullptr, nullptr, nullptr, field, field, 1.0 / ((double)nx * (double)ny), s);
   if (rc) return rc;
   return to_ref<double>(&c, field, p, FLD_P, s);
+}
+
+// ===========================================================================
+// Adjoint of the IMEX step (FP64 contexts).  Arrays are in the internal
+// layout: u, v nz planes of nx*ny (x fastest), w nz+1 face planes (walls 0).
+// ===========================================================================
+static size_t adj_field(const tc_ctx* c) { return (size_t)(c->nz + 1) * c->nx * c->ny; }
+static size_t adj_nblocks(const tc_ctx* c) {
+  return (size_t)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * (c->nz + 1);
+}
+// scratch: lambda_R (3 fields), A (3 fields), CN tables (12 nz + 1), partials
+struct AdjScratch {
+  double* R[3]; double* A[3]; double* tab; double* partials;
+};
+static size_t adj_scratch_doubles(const tc_ctx* c) { return 6 * adj_field(c) + 12 * (size_t)c->nz + 1 + adj_nblocks(c); }
+static AdjScratch adj_carve(const tc_ctx* c, void* scratch) {
+  AdjScratch a;
+  double* p = (double*)scratch;
+  const size_t f = adj_field(c);
+  for (int q = 0; q < 3; ++q) a.R[q] = p + q * f;
+  for (int q = 0; q < 3; ++q) a.A[q] = p + (3 + q) * f;
+  a.tab = p + 6 * f;
+  a.partials = a.tab + 12 * (size_t)c->nz + 1;
+  return a;
+}
+static int adj_check(const tc_ctx* c, const void* scratch) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (c->precision != TC_FP64) return fail(TC_ERR_ARG, "the adjoint needs an FP64 context");
+  if (scratch && ((uintptr_t)scratch & 15)) return fail(TC_ERR_WORKSPACE, "adjoint scratch must be 16-byte aligned");
+  return TC_OK;
+}
+static dim3 adj_grid(const tc_ctx* c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz + 1); }
+
+extern "C" int tc_adjoint_scratch_bytes(tc_ctx* c, size_t* bytes) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (!bytes) return fail(TC_ERR_ARG, "null bytes");
+  *bytes = adj_scratch_doubles(c) * sizeof(double);
+  return TC_OK;
+}
+
+extern "C" int tc_set_body_force(tc_ctx* c, const double* fu, const double* fv, const double* fw) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if ((fu || fv || fw) && !(fu && fv && fw)) return fail(TC_ERR_ARG, "body force needs all three components or none");
+  c->body[0] = fu; c->body[1] = fv; c->body[2] = fw;
+  if (c->g_valid) {  // captured steps hold the previous forcing
+    cudaGraphExecDestroy(c->gexec);
+    c->g_valid = 0;
+  }
+  return TC_OK;
+}
+
+extern "C" int tc_internal_doubles(tc_ctx* c, size_t* n) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (!n) return fail(TC_ERR_ARG, "null n");
+  *n = 6 * adj_field(c) + 1;
+  return TC_OK;
+}
+
+// state record: u, v, w, r_u, r_v, r_w (each adj_field doubles, u/v padded
+// with one zero plane), forcing.
+extern "C" int tc_save_internal(tc_ctx* c, double* dst, int* have_hist, void* stream) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (!dst || !have_hist) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  cudaStream_t s = ST(stream);
+  const size_t f = adj_field(c), pl = (size_t)c->nx * c->ny;
+  for (int q = 0; q < 3; ++q) {
+    const size_t n = (q < 2 ? (size_t)c->nz : (size_t)c->nz + 1) * pl;
+    TC_CUDA(cudaMemcpyAsync(dst + q * f, c->st[c->cur][q], n * 8, cudaMemcpyDeviceToDevice, s));
+    if (q < 2) TC_CUDA(cudaMemsetAsync(dst + q * f + n, 0, pl * 8, s));
+    TC_CUDA(cudaMemcpyAsync(dst + (3 + q) * f, c->rh[q], n * 8, cudaMemcpyDeviceToDevice, s));
+    if (q < 2) TC_CUDA(cudaMemsetAsync(dst + (3 + q) * f + n, 0, pl * 8, s));
+  }
+  TC_CUDA(cudaMemcpyAsync(dst + 6 * f, c->scal + SC_FORCING, 8, cudaMemcpyDeviceToDevice, s));
+  *have_hist = c->have_hist;
+  return TC_OK;
+}
+
+extern "C" int tc_load_internal(tc_ctx* c, const double* src, int have_hist, void* stream) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (!src) return fail(TC_ERR_ARG, "null argument");
+  cudaStream_t s = ST(stream);
+  const size_t f = adj_field(c), pl = (size_t)c->nx * c->ny;
+  for (int q = 0; q < 3; ++q) {
+    const size_t n = (q < 2 ? (size_t)c->nz : (size_t)c->nz + 1) * pl;
+    TC_CUDA(cudaMemcpyAsync(c->st[c->cur][q], src + q * f, n * 8, cudaMemcpyDeviceToDevice, s));
+    TC_CUDA(cudaMemcpyAsync(c->rh[q], src + (3 + q) * f, n * 8, cudaMemcpyDeviceToDevice, s));
+  }
+  TC_CUDA(cudaMemcpyAsync(c->scal + SC_FORCING, src + 6 * f, 8, cudaMemcpyDeviceToDevice, s));
+  c->have_hist = have_hist ? 1 : 0;
+  c->state_set = 1;
+  return TC_OK;
+}
+
+extern "C" int tc_kinetic_energy(tc_ctx* c, double weight, double* acc, void* scratch, void* stream) {
+  int rc = adj_check(c, scratch);
+  if (rc) return rc;
+  if (!acc || !scratch) return fail(TC_ERR_ARG, "null argument");
+  if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  cudaStream_t s = ST(stream);
+  AdjScratch a = adj_carve(c, scratch);
+  double** S = (double**)c->st[c->cur];
+  k_ke_partials<<<adj_grid(c), dim3(32, 8), 0, s>>>(S[0], S[1], S[2], c->dzf_d, c->dzc_d, a.partials, c->nx, c->ny,
+                                                   c->nz);
+  k_ke_finalize<<<1, 256, 0, s>>>(a.partials, (int)adj_nblocks(c), acc,
+                                  weight * c->dx * c->dy / (c->Lx * c->Ly * c->Lz));
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+extern "C" int tc_adjoint_ke_seed(tc_ctx* c, double weight, const double* qu, const double* qv, const double* qw,
+                                  double* lu, double* lv, double* lw, void* stream) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (!qu || !qv || !qw || !lu || !lv || !lw) return fail(TC_ERR_ARG, "null argument");
+  k_ke_seed<<<adj_grid(c), dim3(32, 8), 0, ST(stream)>>>(qu, qv, qw, lu, lv, lw, c->dzf_d, c->dzc_d,
+                                                         weight * c->dx * c->dy / (c->Lx * c->Ly * c->Lz), c->nx,
+                                                         c->ny, c->nz);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+static void adj_rhs_launch(tc_ctx* c, const double* qu, const double* qv, const double* qw, double* const* R,
+                           double* lu, double* lv, double* lw, cudaStream_t s) {
+  AdjRhsArgs a;
+  a.u = qu; a.v = qv; a.w = qw;
+  a.Ru = R[0]; a.Rv = R[1]; a.Rw = R[2];
+  a.lu = lu; a.lv = lv; a.lw = lw;
+  a.idzf = (const double*)c->idzf_t; a.idzc = (const double*)c->idzc_t;
+  a.idx = 1.0 / c->dx; a.idy = 1.0 / c->dy;
+  a.nu_idx2 = c->nu / (c->dx * c->dx); a.nu_idy2 = c->nu / (c->dy * c->dy);
+  a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.top_neumann = c->top_neumann; a.rhs_fused = c->rhs_fused;
+  k_adj_rhs<<<adj_grid(c), dim3(32, 8), 0, s>>>(a);
+}
+
+extern "C" int tc_adjoint_rhs(tc_ctx* c, const double* qu, const double* qv, const double* qw, const double* Ru,
+                              const double* Rv, const double* Rw, double* lu, double* lv, double* lw, void* stream) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (!qu || !qv || !qw || !Ru || !Rv || !Rw || !lu || !lv || !lw) return fail(TC_ERR_ARG, "null argument");
+  double* R[3] = {(double*)Ru, (double*)Rv, (double*)Rw};
+  adj_rhs_launch(c, qu, qv, qw, R, lu, lv, lw, ST(stream));
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+static void adj_cn_launch(tc_ctx* c, double dt, double* lu, double* lv, double* lw, const AdjScratch& a,
+                          cudaStream_t s) {
+  if (c->adj_tab_dt != dt || c->adj_tab_ptr != a.tab) {  // tables live in the caller's scratch
+    k_adj_cn_tables<<<1, 32, 0, s>>>(a.tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann);
+    c->adj_tab_dt = dt;
+    c->adj_tab_ptr = a.tab;
+  }
+  k_adj_cn<<<dim3((c->nx * c->ny + 127) / 128, 3), 128, 0, s>>>(lu, lv, lw, a.tab, c->nx, c->ny, c->nz);
+}
+
+extern "C" int tc_adjoint_cn(tc_ctx* c, double dt, double* lu, double* lv, double* lw, void* scratch,
+                             void* stream) {
+  int rc = adj_check(c, scratch);
+  if (rc) return rc;
+  if (!lu || !lv || !lw || !scratch || !(dt > 0)) return fail(TC_ERR_ARG, "null argument or dt <= 0");
+  adj_cn_launch(c, dt, lu, lv, lw, adj_carve(c, scratch), ST(stream));
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+// lambda <- W P W^-1 (lambda - cb mu grad ub / ...) : see k_adj_scale_in.
+static int adj_project_impl(tc_ctx* c, double* lu, double* lv, double* lw, const double* mu, double cb,
+                            const AdjScratch& a, cudaStream_t s) {
+  k_adj_scale_in<<<adj_grid(c), dim3(32, 8), 0, s>>>(lu, lv, lw, a.A[0], a.A[1], a.A[2], c->dzf_d, c->dzc_d, mu, cb,
+                                                    c->nx, c->ny, c->nz);
+  int rc = poisson_impl<double>(c, a.A[0], a.A[1], a.A[2], nullptr, c->p, 1.0 / ((double)c->nx * (double)c->ny), s);
+  if (rc) return rc;
+  k_adj_project_out<<<adj_grid(c), dim3(32, 8), 0, s>>>(a.A[0], a.A[1], a.A[2], c->p, lu, lv, lw, c->dzf_d,
+                                                       c->dzc_d, 1.0 / c->dx, 1.0 / c->dy, c->nx, c->ny, c->nz);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+extern "C" int tc_adjoint_project(tc_ctx* c, double* lu, double* lv, double* lw, void* scratch, void* stream) {
+  int rc = adj_check(c, scratch);
+  if (rc) return rc;
+  if (!lu || !lv || !lw || !scratch) return fail(TC_ERR_ARG, "null argument");
+  return adj_project_impl(c, lu, lv, lw, nullptr, 0.0, adj_carve(c, scratch), ST(stream));
+}
+
+extern "C" int tc_adjoint_step(tc_ctx* c, double dt, int first, const double* qu, const double* qv, const double* qw,
+                               double* lu, double* lv, double* lw, double* lru, double* lrv, double* lrw,
+                               double* lFu, double* lFv, double* lFw, double* mu, void* scratch, void* stream) {
+  int rc = adj_check(c, scratch);
+  if (rc) return rc;
+  if (!qu || !qv || !qw || !lu || !lv || !lw || !lru || !lrv || !lrw || !mu || !scratch || !(dt > 0))
+    return fail(TC_ERR_ARG, "null argument or dt <= 0");
+  if ((lFu || lFv || lFw) && !(lFu && lFv && lFw)) return fail(TC_ERR_ARG, "lambda_F needs all three or none");
+  cudaStream_t s = ST(stream);
+  AdjScratch a = adj_carve(c, scratch);
+  // bulk velocity / PI forcing, then the projection
+  const double cb = 0.1 / dt * c->dx * c->dy / (c->Lx * c->Ly * c->Lz);
+  if ((rc = adj_project_impl(c, lu, lv, lw, mu, cb, a, s))) return rc;
+  // Crank-Nicolson
+  adj_cn_launch(c, dt, lu, lv, lw, a, s);
+  // AB2 split, body force, forcing adjoint
+  AdjPrepArgs pa;
+  pa.l[0] = lu; pa.l[1] = lv; pa.l[2] = lw;
+  pa.lr[0] = lru; pa.lr[1] = lrv; pa.lr[2] = lrw;
+  for (int q = 0; q < 3; ++q) pa.R[q] = a.R[q];
+  pa.F[0] = lFu; pa.F[1] = lFv; pa.F[2] = lFw;
+  pa.partials = a.partials;
+  pa.c1 = first ? dt : 1.5 * dt;
+  pa.c2 = first ? 0.0 : -0.5 * dt;
+  pa.nx = c->nx; pa.ny = c->ny; pa.nz = c->nz;
+  k_adj_prep<<<adj_grid(c), dim3(32, 8), 0, s>>>(pa);
+  k_adj_mu<<<1, 256, 0, s>>>(a.partials, (int)adj_nblocks(c), mu);
+  // right-hand side
+  adj_rhs_launch(c, qu, qv, qw, a.R, lu, lv, lw, s);
+  TC_LAUNCHED();
+  return TC_OK;
 }
