@@ -50,9 +50,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "ensemble", "poisson"],
+    ap.add_argument("--workload", default="step", choices=["step", "ensemble", "poisson", "adjoint"],
                     help="step: the headline IMEX step; ensemble: 16 uneven channels (config 4); "
-                         "poisson: the FFT Poisson solve alone at 192x192x128 and 384x384x256 (config 2)")
+                         "poisson: the FFT Poisson solve alone at 192x192x128 and 384x384x256 (config 2); "
+                         "adjoint: gradient of a time-averaged kinetic energy, 96x96x64, 200 steps (config 3)")
+    ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -181,6 +183,12 @@ def run_b200(a):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    diag = ch.diagnostics()  # after 10 + warmup + steps steps, as the FP64 comparison below
+    stats = None
+    if not a.no_fp64_compare and a.precision == "mixed":
+        ch.stats_init(z_c, 180.0, 15.0)
+        ch.stats_accumulate()
+        stats = ch.stats_read()
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -207,15 +215,22 @@ def run_b200(a):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms2 = float(t.item())
         d2 = ch2.diagnostics()
+        ch2.stats_init(z_c, 180.0, 15.0)
+        ch2.stats_accumulate()
+        st2 = ch2.stats_read()
         other = {"value": NX * NY * NZ * a.steps * world / (ms2 / 1e3), "ms_per_step": ms2 / a.steps,
                  "max_div_after": d2["max_div"], "u_bulk": d2["u_bulk"], "u_tau": d2["u_tau"]}
+
+        def rerr(k):
+            return float(np.max(np.abs(stats[k] - st2[k])) / np.max(np.abs(st2[k])))
+        other["profile_rel_err"] = {"U": rerr("U_sum"), "uu": rerr("uu_sum"), "vv": rerr("vv_sum"),
+                                    "ww": rerr("ww_sum"), "uw": rerr("uw_sum"), "E_uu_2d": rerr("E_uu_2d_sum")}
         del ch2
     # per-phase timing (separate, instrumented pass of the same steps)
     ch.timing(True)
     ch.step("IMEX", dt, min(a.steps, L_RING))
     phases, nst = ch.timing_read()
     ch.timing(False)
-    diag = ch.diagnostics()
     # end-to-end through the public API with host buffers
     e2e = None if a.no_e2e else run_e2e(a, grid, (u0, v0, w0), dt)
     if world > 1:
@@ -260,8 +275,11 @@ def run_b200(a):
     if other is not None:
         line["fp64_plain"] = other
         line["mixed_speedup_over_fp64"] = value / other["value"]
-        line["mixed_vs_fp64_after_steps"] = {"u_bulk_abs_err": abs(diag["u_bulk"] - other["u_bulk"]),
-                                             "u_tau_rel_err": abs(diag["u_tau"] - other["u_tau"]) / other["u_tau"]}
+        line["mixed_vs_fp64_after_steps"] = {"steps": 10 + a.warmup + a.steps,
+                                             "max_div_mixed": diag["max_div"], "max_div_fp64": other["max_div_after"],
+                                             "u_bulk_abs_err": abs(diag["u_bulk"] - other["u_bulk"]),
+                                             "u_tau_rel_err": abs(diag["u_tau"] - other["u_tau"]) / other["u_tau"],
+                                             "profile_rel_err": other.pop("profile_rel_err")}
     print(json.dumps(line), flush=True)
 
 
@@ -490,6 +508,109 @@ def run_poisson(a):
                       "config": {"workload": "Poisson microbench"}, "results": res}), flush=True)
 
 
+def run_adjoint(a):
+    """Forward + adjoint of J = mean kinetic energy over steps 101..200 of 200
+    FP64 IMEX steps (dt 0.003) at 96x96x64 with a seeded 8-mode Fourier body
+    force (amplitude 0.01), gradients with respect to the initial field and the
+    body force; checked against central finite differences along 8 seeded
+    directions.  Replicas: every rank runs its own channel (seed = rank)."""
+    import torch
+    import torch.distributed as dist
+    from torchannel_b200.adjoint import AdjointRunner, fourier_body_force, to_internal
+    from torchannel_b200.core import Channel
+    from torchannel_b200.grid import generate_grid
+    from torchannel_b200.init import initialize_flow
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    nx, ny, nz, dt, N = 96, 96, 64, 0.003, 200
+    window = range(101, 201)
+    z_f, z_c, dz_f, dz_c = generate_grid(GAMMA, nz, LZ)
+    ch = Channel(nx, ny, nz, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision="fp64")
+    u, v, w, _ = initialize_flow(nx, ny, nz, z_c, LY, LZ, perturbation_intensity=0.1, seed=rank)
+    ch.set_state(u, v, w)
+    ub = ch.bulk_velocity()
+    ch.set_state(u * (1.0 / ub), v, w)
+    ch.project_initial()
+    q0 = [t.clone() for t in ch.get_state()[:3]]
+    F = fourier_body_force(ch, z_f, z_c, seed=100 + rank)
+    Fi = to_internal(ch, *F)
+    runner = AdjointRunner(ch, dt, N, window, checkpoint_every=a.checkpoint_every)
+    runner.set_body_force(*Fi)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    # plain forward (graph replay), the cost unit
+    for _ in range(max(a.warmup, 1)):
+        ch.set_state(*q0)
+        ch.step("IMEX", dt, N)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    ch.set_state(*q0)
+    e0.record()
+    ch.step("IMEX", dt, N)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    # forward with checkpoints + reverse sweep
+    J = runner.forward(*q0)
+    runner.backward()
+    torch.cuda.synchronize()
+    t0, t1, t2 = ev(), ev(), ev()
+    t0.record()
+    J = runner.forward(*q0)
+    t1.record()
+    gq, gF, gmu = runner.backward()
+    t2.record()
+    torch.cuda.synchronize()
+    fc_ms, bw_ms = t0.elapsed_time(t1), t1.elapsed_time(t2)
+    Jv = float(J)
+    # finite differences along seeded directions (initial field / body force)
+    g = torch.Generator(device="cpu").manual_seed(1234)
+    errs = []
+    eps = 1e-6
+    for trial in range(8):
+        d = [torch.randn(t.shape, generator=g, dtype=torch.float64).cuda() for t in gq]
+        for t in d:
+            t[nz] = 0
+        d[2][0] = 0
+        on_force = trial % 2 == 1
+        ad = sum(float((x * y).sum()) for x, y in zip(gF if on_force else gq, d))
+        vals = []
+        for sgn in (1.0, -1.0):
+            if on_force:
+                runner.set_body_force(*[f + sgn * eps * x for f, x in zip(Fi, d)])
+                vals.append(float(runner.forward(*q0)))
+            else:
+                from torchannel_b200.adjoint import from_internal
+                dq = from_internal(ch, *d)
+                vals.append(float(runner.forward(*[q + sgn * eps * x for q, x in zip(q0, dq)])))
+        runner.set_body_force(*Fi)
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        errs.append(abs(fd - ad) / abs(fd))
+    if world > 1:
+        t = torch.tensor([fwd_ms, fc_ms + bw_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fwd_ms, tot = float(t[0]), float(t[1])
+        dist.destroy_process_group()
+    else:
+        tot = fc_ms + bw_ms
+    if rank == 0:
+        npts = nx * ny * nz
+        print(json.dumps({
+            "metric": "forward+adjoint / forward cost ratio (96x96x64, 200 IMEX steps)",
+            "value": tot / fwd_ms, "unit": "ratio", "n_gpus": world, "steps": N, "warmup": a.warmup,
+            "ms_per_step": tot / N, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded laminar + 0.1 noise, projected; seeded 8-mode Fourier body force)",
+            "config": {"workload": "adjoint: J = mean KE over steps 101..200, gradients w.r.t. q0 and F",
+                       "nx": nx, "ny": ny, "nz": nz, "dt": dt, "checkpoint_every": a.checkpoint_every,
+                       "parallelism": f"replicas{world}"},
+            "forward_ms": fwd_ms, "forward_with_checkpoints_ms": fc_ms, "reverse_sweep_ms": bw_ms,
+            "forward_gpss": npts * N * world / (fwd_ms / 1e3),
+            "J": Jv, "grad_norm_q0": float(sum((t * t).sum() for t in gq)) ** 0.5,
+            "grad_norm_F": float(sum((t * t).sum() for t in gF)) ** 0.5,
+            "fd_rel_errors": errs, "fd_max_rel_error": max(errs), "fd_eps": eps}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -498,6 +619,8 @@ def main():
         run_ensemble(a)
     elif a.workload == "poisson":
         run_poisson(a)
+    elif a.workload == "adjoint":
+        run_adjoint(a)
     else:
         run_b200(a)
 

@@ -30,7 +30,7 @@ def to_internal(ch, u, v, w):
     of (nz+1, ny, nx) (u and v with a zero top plane, w with zero walls)."""
     nx, ny, nz = ch.nx, ch.ny, ch.nz
     out = []
-    for a, kz in ((u, nz), (v, nz)):
+    for a in (u, v):
         t = torch.zeros(nz + 1, ny, nx, dtype=torch.float64, device="cuda")
         t[:nz] = a[1:nx + 1, 1:ny + 1, 1:nz + 1].permute(2, 1, 0)
         out.append(t)
@@ -135,7 +135,6 @@ class AdjointRunner:
         lF = [z(), z(), z()] if self.body is not None else None
         mu = torch.zeros(1, dtype=torch.float64, device="cuda")
         w = self.weight
-        first_hist = self.ckpt[0][1]
         for s in sorted(self.ckpt, reverse=True):
             e = min(s + self.C, self.N)
             rec0, hh0 = self.ckpt[s]
@@ -158,7 +157,6 @@ class AdjointRunner:
         if 0 in self.window:
             q0 = self._q(self.ckpt[0][0])
             L.check(lib.tc_adjoint_ke_seed(ch.ctx, w, *[_ptr(t) for t in q0], *[_ptr(t) for t in lam], _stream()))
-        del first_hist
         shp = (ch.nz + 1, ch.ny, ch.nx)
         gq = [t.view(shp) * seed for t in lam]
         gF = [t.view(shp) * seed for t in lF] if lF is not None else None
@@ -191,3 +189,38 @@ def kinetic_energy_objective(ch, u0, v0, w0, Fu, Fv, Fw, dt, n_steps, window, ch
     """Convenience: J as a differentiable tensor (see KineticEnergyObjective)."""
     runner = AdjointRunner(ch, dt, n_steps, window, checkpoint_every)
     return KineticEnergyObjective.apply(u0, v0, w0, Fu, Fv, Fw, runner)
+
+
+def fourier_body_force(ch, z_f, z_c, n_modes=8, amplitude=0.01, seed=0):
+    """A seeded body force of ``n_modes`` Fourier modes per component:
+    F_c = amplitude * sum_m cos(2 pi (a_m x / Lx + b_m y / Ly) + phi_m)
+    sin(pi c_m z / Lz), a_m, b_m in 0..3, c_m in 1..3, phi_m in [0, 2 pi),
+    evaluated at each component's staggered positions (so it vanishes on the
+    walls).  Returns reference-layout tensors (ghosts 0)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = ch.nx, ch.ny, ch.nz
+    dx, dy = ch.Lx / nx, ch.Ly / ny
+    z_f = np.asarray(z_f, dtype=np.float64)
+    z_c = np.asarray(z_c, dtype=np.float64)
+    xs_face, xs_cell = (np.arange(nx) + 1.0) * dx, (np.arange(nx) + 0.5) * dx
+    ys_face, ys_cell = (np.arange(ny) + 1.0) * dy, (np.arange(ny) + 0.5) * dy
+    pos = {"u": (xs_face, ys_cell, z_c[1:nz + 1]), "v": (xs_cell, ys_face, z_c[1:nz + 1]),
+           "w": (xs_cell, ys_cell, z_f[1:nz])}
+    out = {}
+    for comp in "uvw":
+        x, y, z = pos[comp]
+        f = np.zeros((len(x), len(y), len(z)))
+        for _ in range(n_modes):
+            a, b, c = rng.integers(0, 4), rng.integers(0, 4), rng.integers(1, 4)
+            phi = rng.uniform(0.0, 2 * np.pi)
+            f += (amplitude * np.cos(2 * np.pi * (a * x[:, None, None] / ch.Lx + b * y[None, :, None] / ch.Ly) + phi)
+                  * np.sin(np.pi * c * z[None, None, :] / ch.Lz))
+        out[comp] = f
+    u = torch.zeros(nx + 1, ny + 2, nz + 2, dtype=torch.float64)
+    v = torch.zeros(nx + 2, ny + 1, nz + 2, dtype=torch.float64)
+    w = torch.zeros(nx + 2, ny + 2, nz + 1, dtype=torch.float64)
+    u[1:nx + 1, 1:ny + 1, 1:nz + 1] = torch.from_numpy(out["u"])
+    v[1:nx + 1, 1:ny + 1, 1:nz + 1] = torch.from_numpy(out["v"])
+    w[1:nx + 1, 1:ny + 1, 1:nz] = torch.from_numpy(out["w"])
+    return u.cuda(), v.cuda(), w.cuda()
