@@ -21,6 +21,7 @@ Multi-GPU: one process per GPU, each advancing its own independent channel
 grid-point-steps / max-over-ranks time.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -55,6 +56,7 @@ def parse():
                          "poisson: the FFT Poisson solve alone at 192x192x128 and 384x384x256 (config 2); "
                          "adjoint: gradient of a time-averaged kinetic energy, 96x96x64, 200 steps (config 3)")
     ap.add_argument("--checkpoint-every", type=int, default=20)
+    ap.add_argument("--adjoint-mode", default="auto", choices=["auto", "store", "recompute"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -517,6 +519,7 @@ def run_adjoint(a):
     import torch
     import torch.distributed as dist
     from torchannel_b200.adjoint import AdjointRunner, fourier_body_force, to_internal
+    from torchannel_b200 import _lib as L
     from torchannel_b200.core import Channel
     from torchannel_b200.grid import generate_grid
     from torchannel_b200.init import initialize_flow
@@ -536,10 +539,9 @@ def run_adjoint(a):
     q0 = [t.clone() for t in ch.get_state()[:3]]
     F = fourier_body_force(ch, z_f, z_c, seed=100 + rank)
     Fi = to_internal(ch, *F)
-    runner = AdjointRunner(ch, dt, N, window, checkpoint_every=a.checkpoint_every)
-    runner.set_body_force(*Fi)
+    L.check(ch.lib.tc_set_body_force(ch.ctx, *[ctypes.c_void_p(t.data_ptr()) for t in Fi]))
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    # plain forward (graph replay), the cost unit
+    # plain forward (graph replay, body force, no objective hooks), the cost unit
     for _ in range(max(a.warmup, 1)):
         ch.set_state(*q0)
         ch.step("IMEX", dt, N)
@@ -551,19 +553,27 @@ def run_adjoint(a):
     e1.record()
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1)
-    # forward with checkpoints + reverse sweep
-    J = runner.forward(*q0)
-    runner.backward()
-    torch.cuda.synchronize()
-    t0, t1, t2 = ev(), ev(), ev()
-    t0.record()
-    J = runner.forward(*q0)
-    t1.record()
-    gq, gF, gmu = runner.backward()
-    t2.record()
-    torch.cuda.synchronize()
-    fc_ms, bw_ms = t0.elapsed_time(t1), t1.elapsed_time(t2)
-    Jv = float(J)
+    def timed(mode):
+        r = AdjointRunner(ch, dt, N, window, checkpoint_every=a.checkpoint_every, mode=mode)
+        r.set_body_force(*Fi)
+        r.forward(*q0)
+        r.backward()  # captures the reverse segments
+        torch.cuda.synchronize()
+        t0, t1, t2 = ev(), ev(), ev()
+        t0.record()
+        J = r.forward(*q0)
+        t1.record()
+        gq, gF, _ = r.backward()
+        t2.record()
+        torch.cuda.synchronize()
+        return r, float(J), gq, gF, t0.elapsed_time(t1), t1.elapsed_time(t2)
+
+    # both reverse modes: recomputation from checkpoints and the stored tape
+    rr, Jr, gqr, gFr, fc_r, bw_r = timed("recompute")
+    rr.close()
+    del rr
+    runner, Jv, gq, gF, fc_ms, bw_ms = timed(a.adjoint_mode)
+    same = Jv == Jr and all(torch.equal(x, y) for x, y in zip(gq + gF, gqr + gFr))
     # finite differences along seeded directions (initial field / body force)
     g = torch.Generator(device="cpu").manual_seed(1234)
     errs = []
@@ -603,8 +613,13 @@ def run_adjoint(a):
             "dtype": "f64", "data": "synthetic (seeded laminar + 0.1 noise, projected; seeded 8-mode Fourier body force)",
             "config": {"workload": "adjoint: J = mean KE over steps 101..200, gradients w.r.t. q0 and F",
                        "nx": nx, "ny": ny, "nz": nz, "dt": dt, "checkpoint_every": a.checkpoint_every,
+                       "adjoint_mode": a.adjoint_mode,
                        "parallelism": f"replicas{world}"},
-            "forward_ms": fwd_ms, "forward_with_checkpoints_ms": fc_ms, "reverse_sweep_ms": bw_ms,
+            "adjoint_mode": runner.mode, "forward_ms": fwd_ms, "forward_with_hooks_ms": fc_ms,
+            "reverse_sweep_ms": bw_ms,
+            "recompute": {"checkpoint_every": a.checkpoint_every, "ratio": (fc_r + bw_r) / fwd_ms,
+                          "forward_with_checkpoints_ms": fc_r, "reverse_sweep_ms": bw_r},
+            "store_vs_recompute_bitwise_equal": same,
             "forward_gpss": npts * N * world / (fwd_ms / 1e3),
             "J": Jv, "grad_norm_q0": float(sum((t * t).sum() for t in gq)) ** 0.5,
             "grad_norm_F": float(sum((t * t).sum() for t in gF)) ** 0.5,

@@ -258,6 +258,19 @@ int tc_adjoint_step(tc_ctx* ctx, double dt, int first, const double* qu, const d
                     double* lu, double* lv, double* lw, double* lru, double* lrv, double* lrw,
                     double* lFu, double* lFv, double* lFw, double* mu, void* scratch, void* stream);
 
+/* Per-step hooks for the adjoint driver (FP64 contexts; no reference
+ * counterpart).  Both run inside tc_step (and its captured graphs) after the
+ * projection and read their switches from device memory, so changing the
+ * values needs no re-capture.
+ * tc_set_ke_accumulator: after every step, *acc += (*weight_dev) * KE(state)
+ *   (KE as tc_kinetic_energy; a zero weight skips the work); null acc removes
+ *   it.  The scratch holds the partial sums (tc_adjoint_scratch_bytes).
+ * tc_set_state_tape: after every step, when 0 <= *ctr_dev < nslots, copy
+ *   u, v, w of the new state into slot *ctr_dev of `tape` (slot stride
+ *   3 (nz+1) nx ny doubles) and increment *ctr_dev; null tape removes it. */
+int tc_set_ke_accumulator(tc_ctx* ctx, double* acc, const double* weight_dev, void* scratch);
+int tc_set_state_tape(tc_ctx* ctx, double* tape, int nslots, int* ctr_dev);
+
 #ifdef __cplusplus
 }
 #endif

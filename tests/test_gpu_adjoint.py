@@ -276,18 +276,25 @@ def test_objective_gradient_vs_finite_differences(torch_cuda):
 
 
 def test_checkpoint_interval_does_not_change_the_gradient(torch_cuda):
+    """Recomputation from checkpoints every 1, 4 or 20 steps and the stored
+    tape give the same objective and gradients bit for bit (second backward
+    of a runner replays the captured segments)."""
     torch = torch_cuda
     from torchannel_b200.adjoint import AdjointRunner, to_internal
     ch = _chan(32, 24, 16)
     q0 = _initial(torch, ch, 5)
     Fb = _body(torch, ch, 6)
     out = []
-    for C in (1, 4, 20):
-        r = AdjointRunner(ch, 0.003, 9, range(4, 10), checkpoint_every=C)
+    for C, mode in ((1, "recompute"), (4, "recompute"), (20, "recompute"), (4, "store")):
+        r = AdjointRunner(ch, 0.003, 9, range(4, 10), checkpoint_every=C, mode=mode)
         r.set_body_force(*to_internal(ch, *Fb))
         J = r.forward(*q0)
         gq, gF, mu = r.backward()
-        out.append((float(J), [t.cpu() for t in gq + gF], float(mu)))
+        res = (float(J), [t.cpu() for t in gq + gF], float(mu))
+        gq2, gF2, mu2 = r.backward()  # replayed graphs
+        for a, b in zip(res[1], gq2 + gF2):
+            assert torch.equal(a, b.cpu())
+        out.append(res)
     for o in out[1:]:
         assert o[0] == out[0][0]
         for a, b in zip(o[1], out[0][1]):

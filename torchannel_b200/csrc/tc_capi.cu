@@ -93,6 +93,10 @@ struct tc_ctx {
   const double* body[3];
   double adj_tab_dt;
   const void* adj_tab_ptr;
+  // per-step hooks of the adjoint driver (FP64): kinetic-energy accumulator
+  // (weight read from device memory) and state tape (slot counter on device)
+  double* ke_acc; const double* ke_w; double* ke_part;
+  double* tape; int* tape_ctr; int tape_slots;
   // CUDA graph of two consecutive steps (tc_step replays it for n_steps >= 4)
   cudaStream_t cap_stream;
   cudaGraphExec_t gexec;
@@ -474,6 +478,8 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
   c->tab_dt = -1.0;
   c->adj_tab_dt = -1.0;
   c->adj_tab_ptr = nullptr;
+  c->ke_acc = nullptr; c->ke_w = nullptr; c->ke_part = nullptr;
+  c->tape = nullptr; c->tape_ctr = nullptr; c->tape_slots = 0;
   c->body[0] = c->body[1] = c->body[2] = nullptr;
   c->graphs_on = 1;
   *out = c;
@@ -677,6 +683,22 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   if (rc) return rc;
   mark(c, TC_PH_PROJ, s);
   if ((rc = project_impl<T>(c, B, dt, scheme != TC_FE, s))) return rc;
+  if constexpr (sizeof(T) == 8) {
+    const dim3 ag((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz + 1);
+    if (c->ke_acc) {
+      k_ke_partials_w<<<ag, dim3(32, 8), 0, s>>>(B[0], B[1], B[2], c->dzf_d, c->dzc_d, c->ke_w, c->ke_part, c->nx,
+                                                 c->ny, c->nz);
+      k_ke_finalize_w<<<1, 256, 0, s>>>(c->ke_part, (int)(ag.x * ag.y * ag.z), c->ke_acc, c->ke_w,
+                                        c->dx * c->dy / (c->Lx * c->Ly * c->Lz));
+      TC_LAUNCHED();
+    }
+    if (c->tape) {
+      k_tape_copy<<<ag, dim3(32, 8), 0, s>>>(B[0], B[1], B[2], c->tape, c->tape_ctr, c->tape_slots, c->nx, c->ny,
+                                             c->nz);
+      k_tape_advance<<<1, 32, 0, s>>>(c->tape_ctr, c->tape_slots);
+      TC_LAUNCHED();
+    }
+  }
   mark(c, TC_PH_FIN, s);
   mark(c, TC_NPHASE, s);
   if (c->timing) {
@@ -1533,5 +1555,34 @@ extern "C" int tc_adjoint_step(tc_ctx* c, double dt, int first, const double* qu
   // right-hand side
   adj_rhs_launch(c, qu, qv, qw, a.R, lu, lv, lw, s);
   TC_LAUNCHED();
+  return TC_OK;
+}
+
+static void drop_graph(tc_ctx* c) {
+  if (c->g_valid) {
+    cudaGraphExecDestroy(c->gexec);
+    c->g_valid = 0;
+  }
+}
+
+extern "C" int tc_set_ke_accumulator(tc_ctx* c, double* acc, const double* weight_dev, void* scratch) {
+  int rc = adj_check(c, scratch);
+  if (rc) return rc;
+  if (acc && (!weight_dev || !scratch)) return fail(TC_ERR_ARG, "accumulator needs a weight and a scratch");
+  c->ke_acc = acc;
+  c->ke_w = acc ? weight_dev : nullptr;
+  c->ke_part = acc ? adj_carve(c, scratch).partials : nullptr;
+  drop_graph(c);
+  return TC_OK;
+}
+
+extern "C" int tc_set_state_tape(tc_ctx* c, double* tape, int nslots, int* ctr_dev) {
+  int rc = adj_check(c, nullptr);
+  if (rc) return rc;
+  if (tape && (!ctr_dev || nslots < 1)) return fail(TC_ERR_ARG, "tape needs a device counter and nslots >= 1");
+  c->tape = tape;
+  c->tape_ctr = tape ? ctr_dev : nullptr;
+  c->tape_slots = tape ? nslots : 0;
+  drop_graph(c);
   return TC_OK;
 }
