@@ -591,7 +591,8 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   const int nmodes = nxh * ny;
   mark(c, TC_PH_TRI, s);
   if (c->tri_rden)
-    k_tri_lu<<<(nmodes + 127) / 128, 128, 0, s>>>(X, c->tri_rden, c->tri_cp, tb, nxh, ny, nz);
+    k_tri_lu2<<<(2 * nmodes + 63) / 64, 64, 0, s>>>(reinterpret_cast<double*>(X), c->tri_rden, c->tri_cp, tb,
+                                                     nxh, ny, nz);
   else
     k_tri<<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, tb, nxh, ny, nz);
   mark(c, TC_PH_IFFTY, s);
@@ -636,7 +637,7 @@ static double bulk_scale(const tc_ctx* c) { return c->dx * c->dy / (c->Lx * c->L
 template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, int update_forcing, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
   BulkArgs ba{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, update_forcing};
-  dim3 grd((c->nx / 2 + 31) / 32, (c->ny + 7) / 8, c->nz);
+  dim3 grd((c->nx / 2 + 31) / 32, (c->ny + 7) / 8, (c->nz + PROJ_PK - 1) / PROJ_PK);
   k_project_bulk<T><<<grd, dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt, c->dzf_d, ba);
   TC_LAUNCHED();
   return TC_OK;

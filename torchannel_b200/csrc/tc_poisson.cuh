@@ -585,6 +585,73 @@ __global__ void __launch_bounds__(512) k_yz_solve(cpx<double>* __restrict__ X, c
   cluster.barrier_wait();
 }
 
+// k_tri_lu with the real and imaginary parts of a mode on two threads (the
+// factors are real, so the two recurrences are independent): twice the
+// threads in flight, half the registers per level, TRIP_B levels prefetched.
+#define TRIP_B 16
+__global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const double* __restrict__ rden_t,
+                                                 const double* __restrict__ cp_t, PoissonTabs tb, int nxh, int ny,
+                                                 int nz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mode = t >> 1, part = t & 1;
+  if (mode >= nxh * ny) return;
+  const int kx = mode / ny, ky = mode - kx * ny;
+  const size_t base = (size_t)kx * nz * ny + ky;
+  double* col = Xd + 2 * base + part;
+  const double* rd = rden_t + base;
+  const double* cpt = cp_t + base;
+  const size_t st = ny, st2 = 2 * (size_t)ny;
+  double dc[TRIP_B], dn[TRIP_B], fc[TRIP_B], fn[TRIP_B];
+#pragma unroll
+  for (int b = 0; b < TRIP_B; ++b) {
+    if (b < nz) { dc[b] = col[(size_t)b * st2]; fc[b] = ldg(rd + (size_t)b * st); }
+  }
+  double dp = 0.0;
+  for (int k0 = 0; k0 < nz; k0 += TRIP_B) {
+#pragma unroll
+    for (int b = 0; b < TRIP_B; ++b) {
+      const int kk = k0 + TRIP_B + b;
+      if (kk < nz) { dn[b] = col[(size_t)kk * st2]; fn[b] = ldg(rd + (size_t)kk * st); }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIP_B; ++b) {
+      const int k = k0 + b;
+      if (k < nz) {
+        const double a = (k == 0) ? 0.0 : tb.cl[k];
+        dp = (dc[b] - a * dp) * fc[b];
+        col[(size_t)k * st2] = dp;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIP_B; ++b) { dc[b] = dn[b]; fc[b] = fn[b]; }
+  }
+  double x = dp;
+  if (kx == 0 && ky == 0) x = 0.0;
+  col[(size_t)(nz - 1) * st2] = x;
+#pragma unroll
+  for (int b = 0; b < TRIP_B; ++b) {
+    const int k = nz - 2 - b;
+    if (k >= 0) { dc[b] = col[(size_t)k * st2]; fc[b] = ldg(cpt + (size_t)k * st); }
+  }
+  for (int k1 = nz - 2; k1 >= 0; k1 -= TRIP_B) {
+#pragma unroll
+    for (int b = 0; b < TRIP_B; ++b) {
+      const int k = k1 - TRIP_B - b;
+      if (k >= 0) { dn[b] = col[(size_t)k * st2]; fn[b] = ldg(cpt + (size_t)k * st); }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIP_B; ++b) {
+      const int k = k1 - b;
+      if (k >= 0) {
+        x = dc[b] - fc[b] * x;
+        col[(size_t)k * st2] = x;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < TRIP_B; ++b) { dc[b] = dn[b]; fc[b] = fn[b]; }
+  }
+}
+
 // Inverse real FFT along x of JT rows of plane k; writes p[k][j][i] (FP64).
 __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X, double* __restrict__ p, int nx,
                                                int ny, int nz, FftPlan plx, const cpx<double>* __restrict__ twx,

@@ -535,6 +535,7 @@ struct BulkArgs {
 // writes one partial sum and the last block to finish reduces them in a fixed
 // order.  p is FP64.  nx is even, so the pairs never straddle a row.
 // ---------------------------------------------------------------------------
+#define PROJ_PK 4  // planes per block of k_project_bulk
 template <class T> struct Vec2;
 template <> struct Vec2<double> { using t = double2; };
 template <> struct Vec2<float> { using t = float2; };
@@ -549,31 +550,40 @@ __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * PROJ_PK;  // planes k0 .. k0+PROJ_PK-1
   double acc = 0.0;
   if (i < nx && j < ny) {
     const int jp = wrap(j + 1, ny), ipp = wrap(i + 2, nx);
-    const size_t o = pidx(k, j, i, ny, nx);
-    const double2 P = *reinterpret_cast<const double2*>(p + o);
-    const double P2 = ldg(p + pidx(k, j, ipp, ny, nx));
-    const double2 Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
-    V2 uu = *reinterpret_cast<V2*>(u + o);
-    V2 vv = *reinterpret_cast<V2*>(v + o);
     const double cx = dt * (double)g.idx, cy = dt * (double)g.idy;
-    uu.x = (T)((double)uu.x - cx * (P.y - P.x));
-    uu.y = (T)((double)uu.y - cx * (P2 - P.y));
-    vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
-    vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
-    *reinterpret_cast<V2*>(u + o) = uu;
-    *reinterpret_cast<V2*>(v + o) = vv;
-    acc = ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
-    if (k >= 1) {
-      const double2 Pm = *reinterpret_cast<const double2*>(p + pidx(k - 1, j, i, ny, nx));
-      const double cz = dt * (double)g.idzc[k];
-      V2 ww = *reinterpret_cast<V2*>(w + o);
-      ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
-      ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
-      *reinterpret_cast<V2*>(w + o) = ww;
+    // p of the plane below k0 for w's face k0 (walls excluded below)
+    double2 Pm = make_double2(0.0, 0.0);
+    if (k0 >= 1) Pm = *reinterpret_cast<const double2*>(p + pidx(k0 - 1, j, i, ny, nx));
+#pragma unroll
+    for (int kk = 0; kk < PROJ_PK; ++kk) {
+      const int k = k0 + kk;
+      if (k < nz) {
+        const size_t o = pidx(k, j, i, ny, nx);
+        const double2 P = *reinterpret_cast<const double2*>(p + o);
+        const double P2 = ldg(p + pidx(k, j, ipp, ny, nx));
+        const double2 Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
+        V2 uu = *reinterpret_cast<V2*>(u + o);
+        V2 vv = *reinterpret_cast<V2*>(v + o);
+        uu.x = (T)((double)uu.x - cx * (P.y - P.x));
+        uu.y = (T)((double)uu.y - cx * (P2 - P.y));
+        vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
+        vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
+        *reinterpret_cast<V2*>(u + o) = uu;
+        *reinterpret_cast<V2*>(v + o) = vv;
+        acc += ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
+        if (k >= 1) {
+          const double cz = dt * (double)g.idzc[k];
+          V2 ww = *reinterpret_cast<V2*>(w + o);
+          ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
+          ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
+          *reinterpret_cast<V2*>(w + o) = ww;
+        }
+        Pm = P;
+      }
     }
   }
   double s = block_sum(acc, sh);
