@@ -438,6 +438,19 @@ def run_ensemble(a):
     torch.cuda.synchronize()
     ms_seq = (time.perf_counter() - t0) * 1e3
     value_seq, _, _ = aggregate(ens.points() * a.steps, ms_seq)
+    # autotuned shapes, then the whole ensemble step pair as one graph launch
+    tuning = ens.autotune()
+    ens.capture()
+    pairs = max(1, a.steps // 2)
+    ens.step_graph(1)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    ens.step_graph(pairs)
+    g1.record()
+    torch.cuda.synchronize()
+    ms_graph = g0.elapsed_time(g1)
+    value_graph, _, _ = aggregate(ens.points() * 2 * pairs, ms_graph)
     diag = ens.diagnostics()
     if world > 1:
         dist.destroy_process_group()
@@ -450,6 +463,9 @@ def run_ensemble(a):
                           "config": {"workload": "ensemble of 16 channels", "members": members,
                                      "parallelism": f"members over {world} rank(s), streams per member"},
                           "one_at_a_time": {"value": value_seq},
+                          "tuned_one_graph": {"value": value_graph, "ms_per_step": ms_graph / (2 * pairs),
+                                              "note": "autotuned member shapes; 2 steps of all members per graph launch"},
+                          "tuning": tuning,
                           "max_div_after": max(d["max_div"] for d in diag)}), flush=True)
 
 

@@ -271,6 +271,11 @@ int tc_adjoint_step(tc_ctx* ctx, double dt, int first, const double* qu, const d
 int tc_set_ke_accumulator(tc_ctx* ctx, double* acc, const double* weight_dev, void* scratch);
 int tc_set_state_tape(tc_ctx* ctx, double* tape, int nslots, int* ctr_dev);
 
+/* Tile shape of the CN solve along z: rows per chunk (16 or 32; 0 = by nz:
+ * 16 up to nz = 256, else 32).  Used by the ensemble autotuner; no reference
+ * counterpart.  TC_ERR_SIZE for 16 with nz > 256. */
+int tc_set_cn_chunk(tc_ctx* ctx, int rows);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,7 @@ SIGNATURES = [
     ("tc_adjoint_step", _I, [_V, _D, _I] + [_V] * 15),
     ("tc_set_ke_accumulator", _I, [_V, _V, _V, _V]),
     ("tc_set_state_tape", _I, [_V, _V, _I, _V]),
+    ("tc_set_cn_chunk", _I, [_V, _I]),
 ]
 
 

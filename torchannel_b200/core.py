@@ -142,6 +142,10 @@ class Channel:
     def use_graphs(self, on=True):
         L.check(self.lib.tc_use_graphs(self.ctx, int(bool(on))))
 
+    def set_cn_chunk(self, rows):
+        """Rows per chunk of the CN solve (16, 32, or 0 for the default)."""
+        L.check(self.lib.tc_set_cn_chunk(self.ctx, int(rows)))
+
     def use_fused_poisson(self, on=True):
         """One cluster kernel for the y transforms and the z solve (on) or three
         kernels (off); raises when the grid's cluster shape does not fit."""

@@ -85,6 +85,7 @@ struct tc_ctx {
   // FFT batch rows, threads, shared memory; yz_ok = launchable here
   int yz_CS, yz_P, yz_FB, yz_thr, yz_ok, yz_on;
   int nsm, yreg_blocks;  // SM count; resident-block cap of the y register FFT
+  int cn_L_force;        // CN chunk length chosen by tc_set_cn_chunk (0: by nz)
   size_t yz_smem;
   int cur, have_hist, state_set;
   double tab_dt;
@@ -611,7 +612,10 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
 
 // Chunk length of the CN solve: 16 rows up to nz = 256 (at most 16 warps),
 // 32 rows for deeper channels (nz <= 512).  The G/H tables follow it.
-static int cn_len(const tc_ctx* c) { return c->nz <= 256 ? 16 : 32; }
+static int cn_len(const tc_ctx* c) {
+  if (c->cn_L_force) return c->cn_L_force;
+  return c->nz <= 256 ? 16 : 32;
+}
 static int cn_chunks(const tc_ctx* c) { return (c->nz + cn_len(c) - 1) / cn_len(c); }
 template <class T> static size_t cn_smem(const tc_ctx* c) {
   const int vec = (cn_len(c) == 16 && sizeof(T) == 4) ? 2 : 1;
@@ -1585,5 +1589,17 @@ extern "C" int tc_set_state_tape(tc_ctx* c, double* tape, int nslots, int* ctr_d
   c->tape_ctr = tape ? ctr_dev : nullptr;
   c->tape_slots = tape ? nslots : 0;
   drop_graph(c);
+  return TC_OK;
+}
+
+extern "C" int tc_set_cn_chunk(tc_ctx* c, int rows) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (rows != 0 && rows != 16 && rows != 32) return fail(TC_ERR_ARG, "CN chunk length must be 0, 16 or 32");
+  if (rows == 16 && c->nz > 256) return fail(TC_ERR_SIZE, "16-row CN chunks need nz <= 256");
+  if (rows != c->cn_L_force) {
+    c->cn_L_force = rows;
+    c->tab_dt = -1.0;  // the chunk products of the tables follow the length
+    drop_graph(c);
+  }
   return TC_OK;
 }

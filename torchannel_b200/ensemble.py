@@ -4,7 +4,11 @@ Members are independent, so a multi-GPU ensemble shards them across ranks
 (one process per GPU, members assigned round-robin) with no collective on the
 hot path; the only collectives are host-side reductions of the timing and the
 per-member diagnostics after the steps.  On one GPU the members advance on
-their own CUDA streams so that small members overlap.
+their own CUDA streams so that small members overlap; ``Ensemble.capture``
+records two steps of every member (forked onto the member streams) as one
+CUDA graph, so an ensemble step pair is a single graph launch, and
+``Ensemble.autotune`` picks each member's kernel shapes (Poisson path, CN
+chunk length) by timing the candidates on that member.
 """
 import numpy as np
 
@@ -87,6 +91,98 @@ class Ensemble:
     def synchronize(self):
         for s in self.streams:
             s.synchronize()
+
+    # -- autotuning ------------------------------------------------------------
+    def _save(self, ch):
+        st = [t.clone() for t in ch.get_state()[:3]]
+        try:
+            hist = [t.clone() for t in ch.get_history()]
+        except RuntimeError:  # no history yet (no step taken)
+            hist = None
+        return st, hist, float(ch.scalars[0].item())
+
+    def _restore(self, ch, saved):
+        st, hist, f = saved
+        ch.set_state(*st, forcing=f)
+        if hist is not None:
+            ch.set_history(*hist)
+
+    def autotune(self, steps=6, repeats=2):
+        """For every member, time each candidate shape -- Poisson middle
+        (three register-FFT kernels or the fused cluster kernel) x CN chunk
+        length (16 or 32 rows) -- over `steps` steps (best of `repeats`), keep
+        the fastest, and restore the member's state, history and forcing.
+        Returns the chosen shapes and their step times (ms) per member."""
+        import torch
+        self.tuning = []
+        for ch, s, dt, m in zip(self.channels, self.streams, self.dts, self.members):
+            cands = []
+            for fused in (False, True):
+                for rows in (16, 32):
+                    if rows == 16 and m["nz"] > 256:
+                        continue
+                    cands.append((fused, rows))
+            best, times = None, {}
+            with torch.cuda.stream(s):
+                saved = self._save(ch)
+                for fused, rows in cands:
+                    try:
+                        ch.use_fused_poisson(fused)
+                    except RuntimeError:
+                        continue  # cluster shape not schedulable here
+                    ch.set_cn_chunk(rows)
+                    ch.step("IMEX", dt, 2)  # history, tables and graphs of this shape
+                    ms = []
+                    for _ in range(repeats):
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(s)
+                        ch.step("IMEX", dt, steps)
+                        e1.record(s)
+                        e1.synchronize()
+                        ms.append(e0.elapsed_time(e1) / steps)
+                    times[(fused, rows)] = min(ms)
+                    self._restore(ch, saved)
+                best = min(times, key=times.get)
+                ch.use_fused_poisson(best[0])
+                ch.set_cn_chunk(best[1])
+                s.synchronize()
+            self.tuning.append({"fused_poisson": best[0], "cn_rows": best[1],
+                                "ms_per_step": {f"{'fused' if k[0] else '3k'}/cn{k[1]}": v for k, v in times.items()}})
+        return self.tuning
+
+    # -- one graph for the whole ensemble ------------------------------------------
+    def capture(self):
+        """Record two IMEX steps of every member, each on its own stream forked
+        from and joined to one capture stream, as a single CUDA graph.  The
+        members need their AB2 history (one eager step) first; two steps keep
+        every member's buffer parity, so the graph can be replayed."""
+        import torch
+        for ch, s, dt in zip(self.channels, self.streams, self.dts):
+            with torch.cuda.stream(s):
+                ch.step("IMEX", dt, 1)  # history and CN tables in place
+        torch.cuda.synchronize()
+        main = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=main):
+            start = torch.cuda.Event()
+            start.record(main)
+            ends = []
+            for ch, s, dt in zip(self.channels, self.streams, self.dts):
+                s.wait_event(start)
+                with torch.cuda.stream(s):
+                    ch.step("IMEX", dt, 2)
+                e = torch.cuda.Event()
+                e.record(s)
+                ends.append(e)
+            for e in ends:
+                main.wait_event(e)
+        self.graph, self.graph_stream = g, main
+        return g
+
+    def step_graph(self, n_pairs):
+        """Advance every member by 2 * n_pairs steps: n_pairs graph launches."""
+        for _ in range(n_pairs):
+            self.graph.replay()
 
     def diagnostics(self):
         import torch
