@@ -84,6 +84,8 @@ struct tc_ctx {
   // fused y/z Poisson middle (k_yz_solve): cluster size, planes per CTA,
   // FFT batch rows, threads, shared memory; yz_ok = launchable here
   int yz_CS, yz_P, yz_FB, yz_thr, yz_ok, yz_on;
+  int yzr_thr, yzr_ok;  // register-FFT form of the fused kernel (k_yz_solve_reg)
+  size_t yzr_smem;
   int nsm, yreg_blocks;  // SM count; resident-block cap of the y register FFT
   int cn_L_force;        // CN chunk length chosen by tc_set_cn_chunk (0: by nz)
   size_t yz_smem;
@@ -335,6 +337,23 @@ static void ifftx_reg(const tc_ctx* c, const cpx<double>* X, double* p, cudaStre
   });
 }
 
+// Fused y/z middle with register transforms: threads (one per column ky, at
+// least 8 warps) and shared memory (rows, per-warp transpose tiles, chunk ends).
+template <int N1> static size_t yzr_bytes(int P, int thr) {
+  using RF = RowFft<N1>;
+  return ((size_t)P * RF::N + (size_t)(thr / 32) * RF::RPW * RF::TILE + 2 * (size_t)RF::N) * sizeof(cpx<double>) +
+         2 * (size_t)RF::N * sizeof(double);
+}
+template <int N1, int PM> static void* yzr_kernel() { return (void*)k_yz_solve_reg<N1, PM>; }
+static void* yzr_fn(const tc_ctx* c) {
+  void* f = nullptr;
+  for_each_n1(c->ny, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    f = c->yz_P <= 16 ? yzr_kernel<N1, 16>() : yzr_kernel<N1, 32>();
+  });
+  return f;
+}
+
 static cudaLaunchConfig_t yz_config(const tc_ctx* c, cudaLaunchAttribute* at, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(c->nxh * c->yz_CS, 1, 1);
@@ -348,6 +367,35 @@ static cudaLaunchConfig_t yz_config(const tc_ctx* c, cudaLaunchAttribute* at, cu
   cfg.attrs = at;
   cfg.numAttrs = 1;
   return cfg;
+}
+
+// Whether the cluster shape of k_yz_solve_reg can be resident on this device
+// (sets its attributes first).
+static int yzr_probe(tc_ctx* c) {
+  if (!rowfft_supported(c->ny) || c->yz_P > 32) return 0;
+  c->yzr_thr = ((c->ny + 31) / 32) * 32;
+  if (c->yzr_thr < 256) c->yzr_thr = 256;
+  for_each_n1(c->ny, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    c->yzr_smem = yzr_bytes<N1>(c->yz_P, c->yzr_thr);
+  });
+  if (c->yzr_thr > 512 || c->yzr_smem > 200 * 1024) return 0;
+  void* f = yzr_fn(c);
+  if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+      cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = yz_config(c, at, 0);
+  cfg.blockDim = dim3(c->yzr_thr, 1, 1);
+  cfg.dynamicSmemBytes = c->yzr_smem;
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, f, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return ncl > 0;
 }
 
 // Whether the cluster shape of k_yz_solve can be resident on this device.
@@ -468,6 +516,7 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
   }
   c->yz_ok = yz_probe(c);
+  c->yzr_ok = c->yz_ok ? yzr_probe(c) : 0;
   c->yz_on = 0;  // the three-kernel path with register FFTs is faster
   if (c->yz_ok) {
     PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
@@ -567,7 +616,21 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
     cudaLaunchAttribute at[1];
     cudaLaunchConfig_t cfg = yz_config(c, at, s);
     PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
-    if (c->yz_P <= 16)
+    if (c->yzr_ok) {
+      cfg.blockDim = dim3(c->yzr_thr, 1, 1);
+      cfg.dynamicSmemBytes = c->yzr_smem;
+      int rc2 = TC_OK;
+      for_each_n1(ny, [&](auto I) {
+        constexpr int N1 = decltype(I)::value;
+        cudaError_t e = c->yz_P <= 16
+                            ? cudaLaunchKernelEx(&cfg, k_yz_solve_reg<N1, 16>, X, (const double*)c->tri_cpb, tb,
+                                                 (const cpx<double>*)c->twy_d, nz, c->yz_P)
+                            : cudaLaunchKernelEx(&cfg, k_yz_solve_reg<N1, 32>, X, (const double*)c->tri_cpb, tb,
+                                                 (const cpx<double>*)c->twy_d, nz, c->yz_P);
+        if (e != cudaSuccess) rc2 = fail(TC_ERR_CUDA, std::string("k_yz_solve_reg: ") + cudaGetErrorString(e));
+      });
+      if (rc2) return rc2;
+    } else if (c->yz_P <= 16)
       TC_CUDA(cudaLaunchKernelEx(&cfg, k_yz_solve<16>, X, (const double*)c->tri_cpb, tb, c->plany,
                                  (const cpx<double>*)c->twy_d, ny, nz, c->yz_P, c->yz_FB));
     else

@@ -652,6 +652,169 @@ __global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const d
   }
 }
 
+// k_yz_solve with the register-resident row transforms (ny = N1 * 16): the
+// CTA's rows sit unpadded in shared memory, each warp transforms RowFft::RPW
+// rows at a time through its own transpose tile (twiddles from the global
+// table), and the chunk scans read the lower / upper chunks' values four at a
+// time.
+// Otherwise the same stitched chunk solve and cluster barriers as k_yz_solve.
+template <int N1, int PM>
+__global__ void __launch_bounds__(512) k_yz_solve_reg(cpx<double>* __restrict__ X, const double* __restrict__ cpb,
+                                                      PoissonTabs tb, const cpx<double>* __restrict__ twy, int nz,
+                                                      int P) {
+  using RF = RowFft<N1>;
+  constexpr int ny = RF::N;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int CS = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int kx = blockIdx.x / CS;
+  const int tid = threadIdx.x, nthr = blockDim.x, nwarp = nthr >> 5;
+  cpx<double>* R = reinterpret_cast<cpx<double>*>(smraw);        // P rows of ny
+  cpx<double>* tiles = R + (size_t)P * ny;                          // nwarp * RPW tiles
+  cpx<double>* eV = tiles + (size_t)nwarp * RF::RPW * RF::TILE;    // ny
+  cpx<double>* sZ = eV + ny;                                        // ny
+  double* eG = reinterpret_cast<double*>(sZ + ny);                  // ny
+  double* sH = eG + ny;                                             // ny
+  const int k0 = rank * P;
+  const int nr = max(0, min(P, nz - k0));
+  cpx<double>* slab = X + ((size_t)kx * nz + k0) * ny;
+#pragma unroll 4
+  for (int e = tid; e < nr * ny; e += nthr) R[e] = slab[e];
+  __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
+  cpx<double>* tile = tiles + (size_t)(warp * RF::RPW + (sub < RF::RPW ? sub : 0)) * RF::TILE;
+  auto rows_fft = [&](auto inv) {
+    constexpr bool INV = decltype(inv)::value;
+    for (int r0 = warp * RF::RPW; r0 < nr; r0 += nwarp * RF::RPW) {
+      const int row = r0 + sub;
+      const bool ok = sub < RF::RPW && row < nr;
+      cpx<double>* x = R + (size_t)(ok ? row : 0) * ny;
+      if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
+      __syncwarp();
+      if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+      __syncwarp();
+    }
+  };
+  rows_fft(std::integral_constant<bool, false>{});
+  __syncthreads();
+
+  // one column per thread (blockDim >= ny); factors rebuilt on the fly
+  const int j = tid;
+  const bool colt = j < ny;
+  const double K2 = colt ? tb.k2x[kx] + tb.k2y[j] : 0.0;
+  double cpv[PM], gv[PM];
+  cpx<double>* col = R + (colt ? j : 0);
+  if (colt) {
+    double cprev = cpb[((size_t)kx * CS + rank) * ny + j];
+    double yr = 0.0, yi = 0.0, g = 1.0;
+#pragma unroll
+    for (int r = 0; r < PM; ++r) {
+      if (r < nr) {
+        const int k = k0 + r;
+        const double cl = tb.cl[k], cr = tb.cr[k];
+        const double a = (k == 0) ? 0.0 : cl;
+        double bb = -(cl + cr + K2);
+        if (k == 0) bb += cl;
+        if (k == nz - 1) bb += cr;
+        const double c = (k == nz - 1) ? 0.0 : cr;
+        const double rd = 1.0 / (bb - a * cprev);
+        const double cpk = (k == nz - 1) ? 0.0 : c * rd;
+        const cpx<double> d = col[(size_t)r * ny];
+        yr = (d.x - a * yr) * rd;
+        yi = (d.y - a * yi) * rd;
+        col[(size_t)r * ny] = cpx<double>{yr, yi};
+        g *= -a * rd;
+        gv[r] = g;
+        cpv[r] = cpk;
+        cprev = cpk;
+      }
+    }
+    eV[j] = cpx<double>{yr, yi};
+    eG[j] = g;
+  }
+  cluster.sync();
+  if (colt) {
+    // d'(start-1) from the lower chunks, remote reads four at a time
+    double dr = 0.0, di = 0.0;
+    for (int c0 = 0; c0 < rank; c0 += 4) {
+      cpx<double> vv[4];
+      double gg[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (c0 + q < rank) {
+          vv[q] = *cluster.map_shared_rank(eV + j, c0 + q);
+          gg[q] = *cluster.map_shared_rank(eG + j, c0 + q);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (c0 + q < rank) {
+          dr = vv[q].x + gg[q] * dr;
+          di = vv[q].y + gg[q] * di;
+        }
+      }
+    }
+    const bool gauge = (kx == 0) && (j == 0);
+    double zr = 0.0, zi = 0.0, h = 1.0;
+#pragma unroll
+    for (int r = PM - 1; r >= 0; --r) {
+      if (r < nr) {
+        const int k = k0 + r;
+        const cpx<double> y = col[(size_t)r * ny];
+        double vr = y.x + gv[r] * dr, vi = y.y + gv[r] * di;
+        if (gauge && k == nz - 1) { vr = 0.0; vi = 0.0; }
+        zr = vr - cpv[r] * zr;
+        zi = vi - cpv[r] * zi;
+        col[(size_t)r * ny] = cpx<double>{zr, zi};
+        h *= -cpv[r];
+        gv[r] = h;
+      }
+    }
+    sZ[j] = cpx<double>{zr, zi};
+    sH[j] = h;
+  }
+  cluster.sync();
+  if (colt) {
+    // x(end+1) from the upper chunks, top down, remote reads four at a time
+    double xr = 0.0, xi = 0.0;
+    for (int c0 = CS - 1; c0 > rank; c0 -= 4) {
+      cpx<double> vv[4];
+      double hh[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (c0 - q > rank) {
+          vv[q] = *cluster.map_shared_rank(sZ + j, c0 - q);
+          hh[q] = *cluster.map_shared_rank(sH + j, c0 - q);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (c0 - q > rank) {
+          xr = vv[q].x + hh[q] * xr;
+          xi = vv[q].y + hh[q] * xi;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < PM; ++r) {
+      if (r < nr) {
+        const cpx<double> z = col[(size_t)r * ny];
+        col[(size_t)r * ny] = cpx<double>{z.x + gv[r] * xr, z.y + gv[r] * xi};
+      }
+    }
+  }
+  cluster.barrier_arrive();  // this CTA reads no peer memory after here
+  __syncthreads();
+  rows_fft(std::integral_constant<bool, true>{});
+  __syncthreads();
+#pragma unroll 4
+  for (int e = tid; e < nr * ny; e += nthr) slab[e] = R[e];
+  cluster.barrier_wait();
+}
+
 // Inverse real FFT along x of JT rows of plane k; writes p[k][j][i] (FP64).
 __global__ void __launch_bounds__(256) k_ifftx(const cpx<double>* __restrict__ X, double* __restrict__ p, int nx,
                                                int ny, int nz, FftPlan plx, const cpx<double>* __restrict__ twx,
