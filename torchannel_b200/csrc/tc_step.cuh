@@ -236,7 +236,8 @@ __global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const
 // G_m = prod_{j = chunk start .. m} f_j and H_m = prod_{j = m .. chunk end}
 // (-cp_j), a chunk swept from zero boundary values is corrected by
 // d'_m += G_m d'_(start-1) and x_m += H_m x_(end+1).
-// Table layout per system: 8 arrays of length nz: a, inv_den, cp, cA, cB, cC, G, H.
+// Table layout per system: 8 arrays of length nz: a, inv_den, cp, cA, cB, cC, G, H;
+// after cn_fold, a holds f and cA, cB, cC the folded coefficients.
 // ---------------------------------------------------------------------------
 struct CnTab {
   double* uv;  // 8*nz
@@ -253,6 +254,21 @@ __device__ __forceinline__ void cn_chunk_products(double* a, double* iv, double*
   for (int m = n - 1; m >= 0; --m) {
     const int e = min((m / L + 1) * L, n) - 1;
     H[m] = (m == e) ? -cp[m] : H[m + 1] * (-cp[m]);
+  }
+}
+
+// Fold the explicit half and the forward elimination of a row into four
+// coefficients, d'_m = eA s_{-1} + eB s_0 + eC s_{+1} + f d'_{m-1}, with
+// f = -a_m rden_m, eX = rden_m (beta cX_m + [X is the row's own point]); the
+// own point is s_0 for u/v and s_{+1} for w (stored over a, cA, cB, cC).
+__device__ __forceinline__ void cn_fold(double* a, const double* iv, double* cA, double* cB, double* cC, int n,
+                                        double beta, bool w_rows) {
+  for (int m = 0; m < n; ++m) {
+    const double r = iv[m];
+    a[m] = -a[m] * r;
+    cA[m] = r * (beta * cA[m]);
+    cB[m] = r * (beta * cB[m] + (w_rows ? 0.0 : 1.0));
+    cC[m] = r * (beta * cC[m] + (w_rows ? 1.0 : 0.0));
   }
 }
 
@@ -288,6 +304,7 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
     }
     cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz, L);
     *t.beta = (1.0 - theta) * dt * nu;
+    cn_fold(a, iv, cA, cB, cC, nz, (1.0 - theta) * dt * nu, false);
   } else if (sys == 1) {
     const int n = nz - 1;
     double* a = t.w; double* iv = a + nz; double* cp = iv + nz;
@@ -308,6 +325,7 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
       cA[m] = ea; cB[m] = eb; cC[m] = ec;
     }
     cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n, L);
+    cn_fold(a, iv, cA, cB, cC, n, (1.0 - theta) * dt * nu, true);
   }
 }
 
@@ -384,7 +402,6 @@ __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restr
   const double* a = tab; const double* iv = a + nz; const double* cp = iv + nz;
   const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
   const double* G = cC + nz; const double* H = G + nz;
-  const double beta = *t.beta;
   // base profile of window entry tt (u/v planes in range; zero for w)
   auto wb = [&](int tt) -> double {
     const int pl = s0 - 1 + tt;
@@ -404,13 +421,11 @@ __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restr
       const int m = s0 + tt;
       if (m < e0) {
         const double bp = wb(tt + 2);
-        const double am = a[m], ivm = iv[m], ca = cA[m], cb = cB[m], cc = cC[m];
+        const double f = a[m], ea = cA[m], eb = cB[m], ec = cC[m];
 #pragma unroll
         for (int c = 0; c < VEC; ++c) {
           const double sm = (double)wv[tt][c] + bm, sc = (double)wv[tt + 1][c] + bc, sp = (double)wv[tt + 2][c] + bp;
-          const double own = comp < 2 ? sc : sp;
-          const double d = own + beta * (ca * sm + cb * sc + cc * sp);
-          yp[c] = (d - am * yp[c]) * ivm;
+          yp[c] = fma(ea, sm, fma(eb, sc, fma(ec, sp, f * yp[c])));
           y[tt][c] = yp[c];
         }
         bm = bc; bc = bp;
