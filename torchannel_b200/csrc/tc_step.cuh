@@ -550,7 +550,7 @@ struct BulkArgs {
 // writes one partial sum and the last block to finish reduces them in a fixed
 // order.  p is FP64.  nx is even, so the pairs never straddle a row.
 // ---------------------------------------------------------------------------
-#define PROJ_PK 8  // planes per block of k_project_bulk
+#define PROJ_PK 16  // planes per block of k_project_bulk
 template <class T> struct Vec2;
 template <> struct Vec2<double> { using t = double2; };
 template <> struct Vec2<float> { using t = float2; };
