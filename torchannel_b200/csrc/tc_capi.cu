@@ -262,19 +262,22 @@ template <class F> static void for_each_n1(int n, F&& f) {
     default: f(std::integral_constant<int, 24>{}); break;
   }
 }
+// rows per block of the register x transforms
+#define XROWS 16
 template <int N1> static size_t fftx_reg_smem() {
-  return (size_t)8 * ((RowFft<N1>::TILE + 7) / 8 * 8 + 1) * sizeof(cpx<double>);
+  return (size_t)(XROWS / 2) * ((RowFft<N1>::TILE + 7) / 8 * 8 + 1) * sizeof(cpx<double>);
 }
 template <int N1> static size_t ifftx_reg_smem() {
   constexpr int NH = RowFft<N1>::N / 2 + 1;
-  return ((size_t)16 * ((NH + 7) / 8 * 8 + 1) + (size_t)8 * RowFft<N1>::TILE) * sizeof(cpx<double>);
+  return ((size_t)XROWS * ((NH + 7) / 8 * 8 + 1) + (size_t)(XROWS / 2) * RowFft<N1>::TILE) * sizeof(cpx<double>);
 }
+template <int N1> static int xreg_threads() { return 16 * XROWS / RowFft<N1>::RPW; }
 template <int N1> static size_t ffty_reg_smem() {
   return (size_t)4 * RowFft<N1>::RPW * RowFft<N1>::TILE * sizeof(cpx<double>);
 }
 // x transforms take the register path for supported nx when ny is a multiple
 // of 16 (16 rows a block); y transforms for supported ny.
-static bool xreg_ok(const tc_ctx* c) { return rowfft_supported(c->nx) && c->ny % 16 == 0; }
+static bool xreg_ok(const tc_ctx* c) { return rowfft_supported(c->nx) && c->ny % XROWS == 0; }
 static bool yreg_ok(const tc_ctx* c) { return rowfft_supported(c->ny); }
 
 // Shared-memory opt-in and the resident-block count of the y kernel.
@@ -283,9 +286,9 @@ template <class T> static int reg_fft_setup(tc_ctx* c) {
   if (xreg_ok(c)) {
     for_each_n1(c->nx, [&](auto I) {
       constexpr int N1 = decltype(I)::value;
-      if (cudaFuncSetAttribute(k_div_fftx_reg<T, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      if (cudaFuncSetAttribute(k_div_fftx_reg<T, N1, XROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)fftx_reg_smem<N1>()) != cudaSuccess ||
-          cudaFuncSetAttribute(k_ifftx_reg<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          cudaFuncSetAttribute(k_ifftx_reg<N1, XROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)ifftx_reg_smem<N1>()) != cudaSuccess)
         rc = fail(TC_ERR_CUDA, "register x FFT attributes");
     });
@@ -324,7 +327,7 @@ static void fftx_reg(const tc_ctx* c, Grid<T> g, const T* u, const T* v, const T
                      cpx<double>* X, double scale, cudaStream_t s) {
   for_each_n1(c->nx, [&](auto I) {
     constexpr int N1 = decltype(I)::value;
-    k_div_fftx_reg<T, N1><<<dim3(c->ny / 16, c->nz), 32 * 8 / RowFft<N1>::RPW, fftx_reg_smem<N1>(), s>>>(
+    k_div_fftx_reg<T, N1, XROWS><<<dim3(c->ny / XROWS, c->nz), xreg_threads<N1>(), fftx_reg_smem<N1>(), s>>>(
         g, u, v, w, field, X, c->twx_d, scale);
   });
 }
@@ -332,7 +335,7 @@ static void fftx_reg(const tc_ctx* c, Grid<T> g, const T* u, const T* v, const T
 static void ifftx_reg(const tc_ctx* c, const cpx<double>* X, double* p, cudaStream_t s) {
   for_each_n1(c->nx, [&](auto I) {
     constexpr int N1 = decltype(I)::value;
-    k_ifftx_reg<N1><<<dim3(c->ny / 16, c->nz), 32 * 8 / RowFft<N1>::RPW, ifftx_reg_smem<N1>(), s>>>(
+    k_ifftx_reg<N1, XROWS><<<dim3(c->ny / XROWS, c->nz), xreg_threads<N1>(), ifftx_reg_smem<N1>(), s>>>(
         X, p, c->ny, c->nz, c->twx_d);
   });
 }
@@ -716,8 +719,8 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   T** A = (T**)c->st[c->cur];
   T** B = (T**)c->st[nxt];
   T** R = (T**)c->rh;
-  dim3 blk(RHS_TX, RHS_TY);
-  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
+  dim3 blk(RHS_TX, rhs_ty<T>());
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>(), (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (scheme == TC_IMEX && c->tab_dt != dt) {
     k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c));
     c->tab_dt = dt;
@@ -844,12 +847,12 @@ template <class T> static int rhs_hook_impl(tc_ctx* c, int full, double* ru, dou
   T** B = (T**)c->st[c->cur ^ 1];  // scratch: the next buffer is free between steps
   const size_t ncell = (size_t)c->nx * c->ny * c->nz;
   cudaMemsetAsync(B[2], 0, ncell / c->nz * (c->nz + 1) * sizeof(T), s);
-  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + RHS_TY - 1) / RHS_TY, (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
+  dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>(), (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (full)
-    k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, RHS_TY), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+    k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, rhs_ty<T>()), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                    B[0], B[1], B[2], c->scal, (T)0, 0);
   else
-    k_rhs_update<T, false, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, RHS_TY), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+    k_rhs_update<T, false, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, rhs_ty<T>()), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                     B[0], B[1], B[2], c->scal, (T)0, 0);
   TC_LAUNCHED();
   int rc;

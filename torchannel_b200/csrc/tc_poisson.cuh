@@ -130,13 +130,13 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
   }
 }
 
-// Divergence (as k_div_fftx) of rows j0 .. j0+15 of plane k and forward real
-// FFT along x with the register transform (nx = N1 * 16); two real rows
-// travel as one complex row, RowFft<N1>::RPW such rows per warp (8 / RPW
+// Divergence (as k_div_fftx) of rows j0 .. j0+XR-1 of plane k and forward
+// real FFT along x with the register transform (nx = N1 * 16); two real rows
+// travel as one complex row, RowFft<N1>::RPW such rows per warp (XR / 2 / RPW
 // warps a block).  The unpacked half spectra are written transposed,
 // X[m][k][j], as in k_div_fftx.
-template <class T, int N1>
-__global__ void __launch_bounds__(256) k_div_fftx_reg(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+template <class T, int N1, int XR>
+__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
                                                      const T* __restrict__ w, const double* __restrict__ field,
                                                      cpx<double>* __restrict__ X,
                                                      const cpx<double>* __restrict__ twx, double scale) {
@@ -144,13 +144,13 @@ __global__ void __launch_bounds__(256) k_div_fftx_reg(Grid<T> g, const T* __rest
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int ZP = (RF::TILE + 7) / 8 * 8 + 1;          // row pitch of the spectra (16 B mod 128 B)
   extern __shared__ __align__(16) unsigned char smraw[];
-  cpx<double>* zs = reinterpret_cast<cpx<double>*>(smraw);  // 8 packed rows x ZP
+  cpx<double>* zs = reinterpret_cast<cpx<double>*>(smraw);  // XR/2 packed rows x ZP
   const int ny = g.ny, nz = g.nz;
-  const int k = blockIdx.y, j0 = blockIdx.x * 16;
+  const int k = blockIdx.y, j0 = blockIdx.x * XR;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
   const int pr = warp * RF::RPW + sub;                      // packed row: j = j0 + 2 pr, +1
-  const bool ok = sub < RF::RPW && pr < 8;
+  const bool ok = sub < RF::RPW && pr < XR / 2;
   cpx<double>* tile = zs + (size_t)(ok ? pr : 0) * ZP;
   const double idx = (double)g.idx, idy = (double)g.idy;
   const double idzf = (u != nullptr) ? (double)g.idzf[k] : 0.0;
@@ -183,8 +183,8 @@ __global__ void __launch_bounds__(256) k_div_fftx_reg(Grid<T> g, const T* __rest
   }
   __syncthreads();
   // unpack: A = (Z[m] + conj Z[N-m]) / 2 (row ja), B = (Z[m] - conj Z[N-m]) / (2i) (row jb)
-  for (int e = threadIdx.x; e < NH * 16; e += blockDim.x) {
-    const int m = e >> 4, r = e & 15, q = r >> 1;
+  for (int e = threadIdx.x; e < NH * XR; e += blockDim.x) {
+    const int m = e / XR, r = e % XR, q = r >> 1;
     const cpx<double> Zm = zs[q * ZP + m];
     const cpx<double> Zn = cconj(zs[q * ZP + (m == 0 ? 0 : N - m)]);
     cpx<double> out;
@@ -197,21 +197,22 @@ __global__ void __launch_bounds__(256) k_div_fftx_reg(Grid<T> g, const T* __rest
   }
 }
 
-// Inverse real FFT along x of rows j0 .. j0+15 of plane k with the register
-// transform (nx = N1 * 16); writes p[k][j][i] (FP64).  Two rows travel as one
-// complex row Z = A + i B built from the half spectra (DC and Nyquist real).
-template <int N1>
-__global__ void __launch_bounds__(256) k_ifftx_reg(const cpx<double>* __restrict__ X, double* __restrict__ p,
+// Inverse real FFT along x of rows j0 .. j0+XR-1 of plane k with the
+// register transform (nx = N1 * 16); writes p[k][j][i] (FP64).  Two rows
+// travel as one complex row Z = A + i B built from the half spectra (DC and
+// Nyquist real).
+template <int N1, int XR>
+__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_ifftx_reg(const cpx<double>* __restrict__ X, double* __restrict__ p,
                                                   int ny, int nz, const cpx<double>* __restrict__ twx) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int SP = (NH + 7) / 8 * 8 + 1;                  // staging pitch
   extern __shared__ __align__(16) unsigned char smraw[];
-  cpx<double>* S = reinterpret_cast<cpx<double>*>(smraw);   // 16 rows x SP half spectra
-  cpx<double>* tiles = S + 16 * SP;                          // 8 packed rows x TILE
-  const int k = blockIdx.y, j0 = blockIdx.x * 16;
-  for (int e = threadIdx.x; e < NH * 16; e += blockDim.x) {
-    const int m = e >> 4, r = e & 15;
+  cpx<double>* S = reinterpret_cast<cpx<double>*>(smraw);   // XR rows x SP half spectra
+  cpx<double>* tiles = S + XR * SP;                          // XR/2 packed rows x TILE
+  const int k = blockIdx.y, j0 = blockIdx.x * XR;
+  for (int e = threadIdx.x; e < NH * XR; e += blockDim.x) {
+    const int m = e / XR, r = e % XR;
     cpx<double> val = X[((size_t)m * nz + k) * ny + j0 + r];
     if (m == 0 || 2 * m == N) val.y = 0.0;  // irfft ignores these imaginary parts
     S[r * SP + m] = val;
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(256) k_ifftx_reg(const cpx<double>* __restrict
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
   const int pr = warp * RF::RPW + sub;
-  const bool ok = sub < RF::RPW && pr < 8;
+  const bool ok = sub < RF::RPW && pr < XR / 2;
   cpx<double>* tile = tiles + (size_t)(ok ? pr : 0) * RF::TILE;
   const cpx<double>* A = S + (2 * (ok ? pr : 0)) * SP;
   const cpx<double>* B = A + SP;

@@ -42,7 +42,7 @@ enum : int {
 // (:1037-1225) and _v2 (:818-1034), AB2 combine solver.py:626-651.
 // FULL=false: IMEX (x/y diffusion only); FULL=true: full Laplacian (AB2/FE).
 //
-// A block owns a RHS_TX x RHS_TY tile and RHS_KB (rhs_kb<T>()) consecutive
+// A block owns a RHS_TX x RHS_TY (rhs_ty<T>()) tile and RHS_KB (rhs_kb<T>()) consecutive
 // planes k = kb..kb+RHS_KB-1 (u, v at cell k, w at face k).  It first stages the u,
 // v, w planes kb-1 .. kb+RHS_KB with a one-cell periodic halo (z ghosts
 // applied, u with its base profile added) in shared memory -- every load of
@@ -53,23 +53,24 @@ enum : int {
 // keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
 // ---------------------------------------------------------------------------
 #define RHS_TX 32
-#define RHS_TY 8
-// planes per block: 4 in FP32, 3 in FP64 (static shared memory <= 48 KB)
+// tile rows and planes per block: 8 x 4 in FP32, 8 x 3 in FP64 (static
+// shared memory <= 48 KB)
+template <class T> __host__ __device__ constexpr int rhs_ty() { return 8; }
 template <class T> __host__ __device__ constexpr int rhs_kb() { return sizeof(T) == 8 ? 3 : 4; }
 #define RHS_HX (RHS_TX + 2)
-#define RHS_HY (RHS_TY + 2)
-#define RHS_NH (RHS_HX * RHS_HY)
 
 template <class T, bool FULL, int UPD>
-__global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const T* __restrict__ u,
+__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, const T* __restrict__ u,
                                                                 const T* __restrict__ v, const T* __restrict__ w,
                                                                 T* __restrict__ us, T* __restrict__ vs,
                                                                 T* __restrict__ ws, T* __restrict__ ru,
                                                                 T* __restrict__ rv, T* __restrict__ rw,
                                                                 const double* __restrict__ forcing_dev, T dt,
                                                                 int have_hist) {
+  constexpr int RHS_TY = rhs_ty<T>(), RHS_HY = RHS_TY + 2, RHS_NH = RHS_HX * RHS_HY;
   constexpr int RHS_KB = rhs_kb<T>();
   constexpr int RHS_NS = RHS_KB + 2;
+  static_assert(RHS_NH <= 2 * RHS_TX * RHS_TY, "two halo elements per thread at most");
   __shared__ T su[RHS_NS][RHS_HY][RHS_HX];
   __shared__ T sv[RHS_NS][RHS_HY][RHS_HX];
   __shared__ T sw[RHS_NS][RHS_HY][RHS_HX];
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(RHS_TX * RHS_TY) k_rhs_update(Grid<T> g, const
   const T h = T(0.5);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
   const T* __restrict__ base = g.ubase_t;
-  // halo elements of this thread: e0 = tid, e1 = tid + 256 (if < RHS_NH)
+  // halo elements of this thread: e0 = tid, e1 = tid + block size (if < RHS_NH)
   const int e1 = tid + RHS_TX * RHS_TY;
   const bool has1 = e1 < RHS_NH;
   size_t off[2];
