@@ -276,6 +276,41 @@ int tc_set_state_tape(tc_ctx* ctx, double* tape, int nslots, int* ctr_dev);
  * counterpart.  TC_ERR_SIZE for 16 with nz > 256. */
 int tc_set_cn_chunk(tc_ctx* ctx, int rows);
 
+/* ---------------------------------------------------------------------------
+ * Ensembles: one launch per substep for every member.
+ *
+ * No reference counterpart (the reference steps one ChannelFlow at a time;
+ * an ensemble there is a loop of ChannelFlow.step_imex calls,
+ * solver.py:580-710).  An ensemble groups up to 64 existing contexts of one
+ * precision on one device whose nx and ny are 64, 96, 128, 192 or 256; each
+ * substep (RHS, CN, x / y transforms, z solve, inverse transforms,
+ * projection) of every member runs as ONE persistent launch over the
+ * concatenated work of all members, and tc_batch_step with n_steps >= 4
+ * replays two such steps as one CUDA graph.  Each member advances exactly
+ * as tc_step would advance it (same kernels' tile code; bit-identical with
+ * the same CN chunk length), its scalars, statistics and state entries stay
+ * per context, and members may still be stepped on their own between
+ * ensemble calls (the ensemble rebuilds its tables when it notices).
+ * The caller owns the member-table memory (device, 16-byte aligned, size
+ * from tc_batch_table_bytes); all calls on one stream.
+ * tc_batch_set_shape: CN rows per chunk (16 or 32; the members' tables follow)
+ *   and persistent CTAs per SM (0 = occupancy limit), the ensemble
+ *   autotuner's knobs.
+ * tc_batch_step: dts = host array of one dt per member; members without AB2
+ *   history start with a forward step as tc_step does.  Members may carry no
+ *   adjoint hooks (TC_ERR_ARG).
+ * tc_batch_info: shape = {cn rows, ctas per SM, tables built}; units and
+ *   grids = work units and CTAs of the seven launches (RHS, CN, x transform,
+ *   y transform, z solve, inverse x transform, projection). */
+typedef struct tc_batch tc_batch;
+int tc_batch_table_bytes(int n_members, int precision, size_t* bytes);
+int tc_batch_create(tc_ctx* const* members, int n_members, void* table, size_t table_bytes, tc_batch** out);
+int tc_batch_destroy(tc_batch* b);
+int tc_batch_set_shape(tc_batch* b, int cn_rows, int ctas_per_sm);
+int tc_batch_use_graphs(tc_batch* b, int on);
+int tc_batch_step(tc_batch* b, int scheme, const double* dts, int n_steps, void* stream);
+int tc_batch_info(tc_batch* b, int* shape, int* units, int* grids);
+
 #ifdef __cplusplus
 }
 #endif

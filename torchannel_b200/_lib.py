@@ -77,6 +77,13 @@ SIGNATURES = [
     ("tc_set_ke_accumulator", _I, [_V, _V, _V, _V]),
     ("tc_set_state_tape", _I, [_V, _V, _I, _V]),
     ("tc_set_cn_chunk", _I, [_V, _I]),
+    ("tc_batch_table_bytes", _I, [_I, _I, ctypes.POINTER(ctypes.c_size_t)]),
+    ("tc_batch_create", _I, [ctypes.POINTER(_V), _I, _V, ctypes.c_size_t, ctypes.POINTER(_V)]),
+    ("tc_batch_destroy", _I, [_V]),
+    ("tc_batch_set_shape", _I, [_V, _I, _I]),
+    ("tc_batch_use_graphs", _I, [_V, _I]),
+    ("tc_batch_step", _I, [_V, _I, _dp, _I, _V]),
+    ("tc_batch_info", _I, [_V, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
 ]
 
 

@@ -1,0 +1,231 @@
+// Ensemble kernels: one persistent launch per substep for every member of an
+// ensemble of independent channels with uneven grids.
+//
+// A launch's work is the concatenation of the members' work units (the
+// blocks -- or, for the y transforms, the warp tasks -- each member's own
+// kernel would run); member m owns units [BMember::u0[K], u0[K] + count).  A
+// fixed grid of CTAs (a multiple of the SM count) strides over the units, so
+// the launch is persistent and small members fill the SMs together.  Each unit
+// runs the same tile function as the single-channel kernel (rhs_tile,
+// cn_tile, fftx_tile, ffty_rows, tri_lu2_thread, ifftx_tile, project_tile), so
+// a member's results are bit-identical to stepping it alone with the same
+// CN chunk length.  Units that share the block's shared memory are separated
+// by a barrier.
+#pragma once
+#include "tc_common.cuh"
+#include "tc_poisson.cuh"
+#include "tc_step.cuh"
+
+namespace tc {
+
+enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT };
+#define TC_BATCH_MAX 64  // members per ensemble launch
+
+template <class T> struct BMember {
+  Grid<T> g;
+  T* A[3];                 // state at the start of the step
+  T* B[3];                 // u*, then u**, then the new state
+  T* R[3];                 // AB2 history
+  const double* forcing;   // device forcing scalar of the member
+  T dt;
+  int have_hist;
+  CnTab tab;
+  const double* ubase;     // FP64 base profile of u (mixed) or null
+  cpx<double>* X;
+  const cpx<double>* twx;
+  const cpx<double>* twy;
+  double scale;            // 1 / (dt nx ny)
+  const double* rden;
+  const double* cpt;
+  PoissonTabs tb;
+  double* p;
+  const double* dzf;
+  BulkArgs ba;
+  int n1x, n1y, nxh, nrows;
+  int rgx, rgy, rgz;       // block grid of k_rhs_update
+  int cgx;                 // column blocks per component of k_cn_solve
+  int xgx;                 // row blocks per plane of the x transforms
+  int pgx, pgy, pgz;       // block grid of k_project_bulk
+  int u0[BK_COUNT];        // first unit of the member in each launch
+};
+
+// Stage the members' first units of launch K (and the total) in shared memory.
+template <class T>
+__device__ __forceinline__ void batch_starts(const BMember<T>* __restrict__ M, int nm, int K, int total, int* st) {
+  for (int m = threadIdx.x + blockDim.x * threadIdx.y; m < nm; m += blockDim.x * blockDim.y) st[m] = M[m].u0[K];
+  if (threadIdx.x == 0 && threadIdx.y == 0) st[nm] = total;
+  __syncthreads();
+}
+
+__device__ __forceinline__ int batch_member(const int* st, int nm, int w) {
+  int m = 0;
+  while (m + 1 < nm && w >= st[m + 1]) ++m;
+  return m;
+}
+
+template <class T, bool FULL, int UPD>
+__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) kb_rhs(const BMember<T>* __restrict__ M, int nm, int total) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_RHS, total, st);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int m = batch_member(st, nm, w);
+    const BMember<T>& b = M[m];
+    int l = w - st[m];
+    const int bx = l % b.rgx;
+    l /= b.rgx;
+    const int by = l % b.rgy, bz = l / b.rgy;
+    rhs_tile<T, FULL, UPD>(b.g, b.A[0], b.A[1], b.A[2], b.B[0], b.B[1], b.B[2], b.R[0], b.R[1], b.R[2], b.forcing,
+                           b.dt, UPD == UPD_FE ? 0 : b.have_hist, bx, by, bz);
+    __syncthreads();
+  }
+}
+
+// Register allocation of the unit loops.  Inlining every transform length
+// into one switch makes the x transform spill heavily, so that tile is a
+// called function (TC_BATCH_FX_CALL); the CN tile is inlined with no register
+// cap below the block's (TC_BATCH_CN_CALL, TC_BATCH_CN_MINB).
+#ifndef TC_BATCH_FX_CALL
+#define TC_BATCH_FX_CALL __noinline__
+#endif
+#ifndef TC_BATCH_CN_CALL
+#define TC_BATCH_CN_CALL __forceinline__
+#endif
+#ifndef TC_BATCH_CN_MINB
+#define TC_BATCH_CN_MINB 1
+#endif
+#ifndef TC_BATCH_FFT_MINB
+#define TC_BATCH_FFT_MINB 4
+#endif
+template <class T, int L, int VEC>
+__device__ TC_BATCH_CN_CALL void batch_cn_call(const BMember<T>* __restrict__ bp, int bx, int comp) {
+  const BMember<T>& b = *bp;
+  cn_tile<T, L, VEC>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.g.nx, b.g.ny, b.g.nz, bx, comp);
+}
+
+// blockDim = (32, chunks of the deepest member) <= MAXT threads
+template <class T, int L, int VEC, int MAXT>
+__global__ void __launch_bounds__(MAXT, TC_BATCH_CN_MINB) kb_cn(const BMember<T>* __restrict__ M, int nm, int total) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_CN, total, st);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int m = batch_member(st, nm, w);
+    const int l = w - st[m];
+    batch_cn_call<T, L, VEC>(M + m, l % M[m].cgx, l / M[m].cgx);
+    __syncthreads();
+  }
+}
+
+// Register-FFT lengths of the ensemble kernels: N = 16 N1, N1 in {4, 6, 8, 12, 16}
+// (64 .. 256 points), all with two rows per warp (128-thread x blocks).  The
+// FFT kernels come in two sets, NMAX = 8 (every member's N1 <= 8) and
+// NMAX = 16, since a kernel's registers are those of its longest transform.
+__host__ __device__ constexpr bool batch_n1_ok(int n1) { return n1 == 4 || n1 == 6 || n1 == 8 || n1 == 12 || n1 == 16; }
+
+template <int NMAX, class F> __device__ __forceinline__ void batch_n1_switch(int n1, F&& f) {
+  if constexpr (NMAX <= 8) {
+    switch (n1) {
+      case 4: f(std::integral_constant<int, 4>{}); break;
+      case 6: f(std::integral_constant<int, 6>{}); break;
+      default: f(std::integral_constant<int, 8>{}); break;
+    }
+  } else {
+    switch (n1) {
+      case 4: f(std::integral_constant<int, 4>{}); break;
+      case 6: f(std::integral_constant<int, 6>{}); break;
+      case 8: f(std::integral_constant<int, 8>{}); break;
+      case 12: f(std::integral_constant<int, 12>{}); break;
+      default: f(std::integral_constant<int, 16>{}); break;
+    }
+  }
+}
+
+template <class T, int N1>
+__device__ TC_BATCH_FX_CALL void batch_fftx_call(const BMember<T>* __restrict__ bp, int bx, int k) {
+  const BMember<T>& b = *bp;
+  fftx_tile<T, N1, XROWS>(b.g, b.B[0], b.B[1], b.B[2], nullptr, b.X, b.twx, b.scale, bx, k);
+}
+template <class T, int N1>
+__device__ __forceinline__ void batch_ifftx_call(const BMember<T>* __restrict__ bp, int bx, int k) {
+  const BMember<T>& b = *bp;
+  ifftx_tile<N1, XROWS>(b.X, b.p, b.g.ny, b.g.nz, b.twx, bx, k);
+}
+template <class T, int N1, bool INV>
+__device__ __forceinline__ void batch_ffty_call(const BMember<T>* __restrict__ bp, int row0, cpx<double>* tiles) {
+  const BMember<T>& b = *bp;
+  ffty_rows<N1, INV>(b.X, b.nrows, b.twy, row0, tiles);
+}
+
+template <class T, int NMAX>
+__global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_fftx(const BMember<T>* __restrict__ M, int nm, int total) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_FX, total, st);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int m = batch_member(st, nm, w);
+    const BMember<T>& b = M[m];
+    const int l = w - st[m];
+    batch_n1_switch<NMAX>(b.n1x, [&](auto I) { batch_fftx_call<T, decltype(I)::value>(&b, l % b.xgx, l / b.xgx); });
+    __syncthreads();
+  }
+}
+
+// Units are warp tasks of two rows; no block barrier.
+template <class T, int NMAX, bool INV>
+__global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_ffty(const BMember<T>* __restrict__ M, int nm, int total, int tile_elems) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_FY, total, st);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  cpx<double>* tiles = reinterpret_cast<cpx<double>*>(smraw) + (size_t)warp * 2 * tile_elems;
+  for (int w = blockIdx.x * wpb + warp; w < total; w += gridDim.x * wpb) {
+    const int m = batch_member(st, nm, w);
+    const BMember<T>& b = M[m];
+    const int row0 = (w - st[m]) * 2;
+    batch_n1_switch<NMAX>(b.n1y, [&](auto I) { batch_ffty_call<T, decltype(I)::value, INV>(&b, row0, tiles); });
+  }
+}
+
+// Units are 64-thread groups of the z sweeps.
+template <class T>
+__global__ void __launch_bounds__(64) kb_tri(const BMember<T>* __restrict__ M, int nm, int total) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_TRI, total, st);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int m = batch_member(st, nm, w);
+    const BMember<T>& b = M[m];
+    tri_lu2_thread(reinterpret_cast<double*>(b.X), b.rden, b.cpt, b.tb, b.nxh, b.g.ny, b.g.nz,
+                   (w - st[m]) * 64 + threadIdx.x);
+  }
+}
+
+template <class T, int NMAX>
+__global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_ifftx(const BMember<T>* __restrict__ M, int nm, int total) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_IFX, total, st);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int m = batch_member(st, nm, w);
+    const BMember<T>& b = M[m];
+    const int l = w - st[m];
+    batch_n1_switch<NMAX>(b.n1x, [&](auto I) { batch_ifftx_call<T, decltype(I)::value>(&b, l % b.xgx, l / b.xgx); });
+    __syncthreads();
+  }
+}
+
+// The member's last block (atomic ticket, per member) reduces its partials
+// and updates its forcing, as in k_project_bulk.
+template <class T>
+__global__ void __launch_bounds__(256) kb_proj(const BMember<T>* __restrict__ M, int nm, int total) {
+  __shared__ int st[TC_BATCH_MAX + 1];
+  batch_starts(M, nm, BK_PROJ, total, st);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int m = batch_member(st, nm, w);
+    const BMember<T>& b = M[m];
+    int l = w - st[m];
+    const int bx = l % b.pgx;
+    l /= b.pgx;
+    const int by = l % b.pgy, bz = l / b.pgy;
+    project_tile<T>(b.g, b.B[0], b.B[1], b.B[2], b.p, (double)b.ba.dt, b.dzf, b.ba, bx, by, bz, b.pgx, b.pgy, b.pgz);
+    __syncthreads();
+  }
+}
+
+}  // namespace tc

@@ -2,7 +2,9 @@
 // workspace carving, launch configuration and the extern "C" entry points.
 // The library never allocates device memory; every buffer is carved from the
 // caller's workspace.
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -16,6 +18,7 @@
 #include "tc_stats.cuh"
 #include "tc_step.cuh"
 #include "tc_adjoint.cuh"
+#include "tc_batch.cuh"
 
 using namespace tc;
 
@@ -262,8 +265,6 @@ template <class F> static void for_each_n1(int n, F&& f) {
     default: f(std::integral_constant<int, 24>{}); break;
   }
 }
-// rows per block of the register x transforms
-#define XROWS 16
 template <int N1> static size_t fftx_reg_smem() {
   return (size_t)(XROWS / 2) * ((RowFft<N1>::TILE + 7) / 8 * 8 + 1) * sizeof(cpx<double>);
 }
@@ -1666,6 +1667,390 @@ extern "C" int tc_set_cn_chunk(tc_ctx* c, int rows) {
     c->cn_L_force = rows;
     c->tab_dt = -1.0;  // the chunk products of the tables follow the length
     drop_graph(c);
+  }
+  return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ensembles: one persistent launch per substep for all members (tc_batch.cuh)
+// ---------------------------------------------------------------------------
+struct tc_batch {
+  int n, precision, dev, nsm;
+  std::vector<tc_ctx*> m;
+  void* table;               // caller memory: 3 tables of n member records
+  size_t rec;                // bytes of one member record
+  int cn_L, ctas_per_sm;     // tuned shapes: CN chunk length, CTAs per SM (0: occupancy limit)
+  int valid, scheme;         // tables match the members' parity, dt, scheme and shapes
+  std::vector<double> dts;
+  std::vector<int> cur0;
+  int q;                     // steps since the tables were built, mod 2
+  int total[BK_COUNT], grid[BK_COUNT];
+  int cn_y, cn_maxt, nmax, fy_tile;
+  size_t smem_cn, smem_fx, smem_ifx, smem_fy;
+  int graphs_on;
+  cudaStream_t cap_stream;
+  cudaGraphExec_t gexec;
+  int g_valid, g_scheme, g_q;
+};
+
+static bool batch_grid_ok(const tc_ctx* c) {
+  return c->nx % 16 == 0 && c->ny % 16 == 0 && batch_n1_ok(c->nx / 16) && batch_n1_ok(c->ny / 16) &&
+         c->ny % XROWS == 0 && c->tri_rden != nullptr;
+}
+
+extern "C" int tc_batch_table_bytes(int n, int precision, size_t* bytes) {
+  if (!bytes) return fail(TC_ERR_ARG, "null bytes");
+  if (n < 1 || n > TC_BATCH_MAX) return fail(TC_ERR_ARG, "ensemble size must be 1 .. 64");
+  if (precision != TC_FP64 && precision != TC_MIXED) return fail(TC_ERR_ARG, "bad precision");
+  const size_t rec = precision == TC_FP64 ? sizeof(BMember<double>) : sizeof(BMember<float>);
+  *bytes = 3 * (size_t)n * rec;
+  return TC_OK;
+}
+
+static void batch_drop_graph(tc_batch* b) {
+  if (b->g_valid) {
+    cudaGraphExecDestroy(b->gexec);
+    b->g_valid = 0;
+  }
+}
+
+extern "C" int tc_batch_create(tc_ctx* const* members, int n, void* table, size_t bytes, tc_batch** out) {
+  if (!members || !out || !table) return fail(TC_ERR_ARG, "null argument");
+  if (n < 1 || n > TC_BATCH_MAX) return fail(TC_ERR_ARG, "ensemble size must be 1 .. 64");
+  if (reinterpret_cast<uintptr_t>(table) % 16) return fail(TC_ERR_WORKSPACE, "table must be 16-byte aligned");
+  const int prec = members[0] ? members[0]->precision : -1;
+  size_t need = 0;
+  int rc = tc_batch_table_bytes(n, prec, &need);
+  if (rc) return rc;
+  if (bytes < need) return fail(TC_ERR_WORKSPACE, "ensemble table too small");
+  for (int i = 0; i < n; ++i) {
+    const tc_ctx* c = members[i];
+    if (!c) return fail(TC_ERR_ARG, "null member");
+    if (c->precision != prec) return fail(TC_ERR_ARG, "members must share the precision");
+    if (c->dev != members[0]->dev) return fail(TC_ERR_ARG, "members must share the device");
+    for (int k = 0; k < i; ++k)
+      if (members[k] == c) return fail(TC_ERR_ARG, "a context appears twice in the ensemble");
+    if (!batch_grid_ok(c))
+      return fail(TC_ERR_SIZE, "ensemble launches need nx, ny in {64, 96, 128, 192, 256}");
+  }
+  tc_batch* b = new tc_batch();
+  b->n = n; b->precision = prec; b->dev = members[0]->dev; b->nsm = members[0]->nsm;
+  b->m.assign(members, members + n);
+  b->table = table;
+  b->rec = prec == TC_FP64 ? sizeof(BMember<double>) : sizeof(BMember<float>);
+  int maxnz = 0;
+  for (auto* c : b->m) maxnz = std::max(maxnz, c->nz);
+  b->cn_L = maxnz <= 256 ? 16 : 32;
+  b->ctas_per_sm = 0;
+  b->graphs_on = 1;
+  *out = b;
+  return TC_OK;
+}
+
+extern "C" int tc_batch_destroy(tc_batch* b) {
+  if (!b) return TC_OK;
+  batch_drop_graph(b);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  delete b;
+  return TC_OK;
+}
+
+extern "C" int tc_batch_set_shape(tc_batch* b, int cn_rows, int ctas_per_sm) {
+  if (!b) return fail(TC_ERR_ARG, "null ensemble");
+  if (cn_rows != 16 && cn_rows != 32) return fail(TC_ERR_ARG, "CN chunk length must be 16 or 32");
+  for (auto* c : b->m)
+    if (cn_rows == 16 && c->nz > 256) return fail(TC_ERR_SIZE, "16-row CN chunks need nz <= 256");
+  if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(TC_ERR_ARG, "ctas_per_sm must be 0 .. 32");
+  if (cn_rows != b->cn_L || ctas_per_sm != b->ctas_per_sm) {
+    b->cn_L = cn_rows;
+    b->ctas_per_sm = ctas_per_sm;
+    b->valid = 0;
+    batch_drop_graph(b);
+  }
+  return TC_OK;
+}
+
+extern "C" int tc_batch_use_graphs(tc_batch* b, int on) {
+  if (!b) return fail(TC_ERR_ARG, "null ensemble");
+  b->graphs_on = on ? 1 : 0;
+  return TC_OK;
+}
+
+template <class T> static constexpr int batch_cn_vec(int L) { return (L == 16 && sizeof(T) == 4) ? 2 : 1; }
+
+template <class T>
+static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int scheme, int L) {
+  BMember<T> r;
+  std::memset(&r, 0, sizeof(r));
+  r.g = make_grid<T>(c);
+  T** A = (T**)c->st[cur];
+  T** Bn = (T**)c->st[cur ^ 1];
+  for (int i = 0; i < 3; ++i) { r.A[i] = A[i]; r.B[i] = Bn[i]; r.R[i] = (T*)c->rh[i]; }
+  r.forcing = c->scal + SC_FORCING;
+  r.dt = (T)dt;
+  r.have_hist = hist;
+  r.tab = c->tab;
+  r.ubase = ubase_of(c);
+  r.X = c->X; r.twx = c->twx_d; r.twy = c->twy_d;
+  r.scale = 1.0 / (dt * (double)c->nx * (double)c->ny);
+  r.rden = c->tri_rden; r.cpt = c->tri_cp;
+  r.tb = PoissonTabs{c->k2x, c->k2y, c->cl, c->cr};
+  r.p = c->p; r.dzf = c->dzf_d;
+  r.ba = BulkArgs{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, scheme != TC_FE};
+  r.n1x = c->nx / 16; r.n1y = c->ny / 16; r.nxh = c->nxh; r.nrows = c->nxh * c->nz;
+  r.rgx = (c->nx + RHS_TX - 1) / RHS_TX;
+  r.rgy = (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>();
+  r.rgz = (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>();
+  const int V = batch_cn_vec<T>(L);
+  r.cgx = (c->nx * c->ny / V + 31) / 32;
+  r.xgx = c->ny / XROWS;
+  r.pgx = (c->nx / 2 + 31) / 32; r.pgy = (c->ny + 7) / 8; r.pgz = (c->nz + PROJ_PK - 1) / PROJ_PK;
+  return r;
+}
+
+template <class T> static void batch_units(const BMember<T>& r, const tc_ctx* c, int cnt[BK_COUNT]) {
+  cnt[BK_RHS] = r.rgx * r.rgy * r.rgz;
+  cnt[BK_CN] = 3 * r.cgx;
+  cnt[BK_FX] = r.xgx * c->nz;
+  cnt[BK_FY] = (r.nrows + 1) / 2;
+  cnt[BK_TRI] = (2 * c->nxh * c->ny + 63) / 64;
+  cnt[BK_IFX] = r.xgx * c->nz;
+  cnt[BK_PROJ] = r.pgx * r.pgy * r.pgz;
+}
+
+template <class T, class K> static int batch_grid(const tc_batch* b, K kernel, int threads, size_t smem, int total,
+                                                  int* grid) {
+  int occ = 0;
+  TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem));
+  if (occ < 1) return fail(TC_ERR_SIZE, "ensemble kernel does not fit on an SM");
+  const int per = b->ctas_per_sm ? std::min(occ, b->ctas_per_sm) : occ;
+  *grid = std::max(1, std::min(total, per * b->nsm));
+  return TC_OK;
+}
+
+// Shared-memory opt-in and persistent grid of every ensemble kernel.
+template <class T, int L, int MAXT> static int batch_cn_shape(tc_batch* b) {
+  constexpr int V = batch_cn_vec<T>(L);
+  TC_CUDA(cudaFuncSetAttribute(kb_cn<T, L, V, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_cn));
+  return batch_grid<T>(b, kb_cn<T, L, V, MAXT>, 32 * b->cn_y, b->smem_cn, b->total[BK_CN], &b->grid[BK_CN]);
+}
+template <class T, int NMAX> static int batch_fft_shapes(tc_batch* b) {
+  TC_CUDA(cudaFuncSetAttribute(kb_fftx<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fx));
+  TC_CUDA(cudaFuncSetAttribute(kb_ifftx<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_ifx));
+  TC_CUDA(cudaFuncSetAttribute(kb_ffty<T, NMAX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fy));
+  TC_CUDA(cudaFuncSetAttribute(kb_ffty<T, NMAX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fy));
+  int rc = batch_grid<T>(b, kb_fftx<T, NMAX>, 128, b->smem_fx, b->total[BK_FX], &b->grid[BK_FX]);
+  if (!rc) rc = batch_grid<T>(b, kb_ffty<T, NMAX, false>, 128, b->smem_fy, (b->total[BK_FY] + 3) / 4, &b->grid[BK_FY]);
+  if (!rc) rc = batch_grid<T>(b, kb_ifftx<T, NMAX>, 128, b->smem_ifx, b->total[BK_IFX], &b->grid[BK_IFX]);
+  return rc;
+}
+template <class T> static int batch_shapes(tc_batch* b, int scheme) {
+  int rc;
+  if (b->cn_L == 16)
+    rc = b->cn_maxt == 256 ? batch_cn_shape<T, 16, 256>(b) : batch_cn_shape<T, 16, 512>(b);
+  else
+    rc = b->cn_maxt == 256 ? batch_cn_shape<T, 32, 256>(b) : batch_cn_shape<T, 32, 512>(b);
+  if (rc) return rc;
+  rc = b->nmax == 8 ? batch_fft_shapes<T, 8>(b) : batch_fft_shapes<T, 16>(b);
+  if (rc) return rc;
+  const int rthr = RHS_TX * rhs_ty<T>();
+  if (scheme == TC_IMEX)
+    rc = batch_grid<T>(b, kb_rhs<T, false, UPD_AB2>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
+  else if (scheme == TC_AB2)
+    rc = batch_grid<T>(b, kb_rhs<T, true, UPD_AB2>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
+  else
+    rc = batch_grid<T>(b, kb_rhs<T, true, UPD_FE>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
+  if (!rc) rc = batch_grid<T>(b, kb_tri<T>, 64, 0, b->total[BK_TRI], &b->grid[BK_TRI]);
+  if (!rc) rc = batch_grid<T>(b, kb_proj<T>, 256, 0, b->total[BK_PROJ], &b->grid[BK_PROJ]);
+  return rc;
+}
+
+template <class T> static int batch_build_impl(tc_batch* b, int scheme, const double* dts, cudaStream_t s) {
+  const int n = b->n, L = b->cn_L;
+  constexpr int VL16 = sizeof(T) == 4 ? 2 : 1;
+  std::vector<BMember<T>> tab(3 * (size_t)n);
+  int run[BK_COUNT] = {0, 0, 0, 0, 0, 0, 0};
+  int maxnz = 0, maxchunks = 0;
+  size_t fx = 0, ifx = 0;
+  int fyt = 0;
+  for (int i = 0; i < n; ++i) {
+    tc_ctx* c = b->m[i];
+    if (c->cn_L_force != L) {  // the members' CN tables follow the ensemble's chunk length
+      c->cn_L_force = L;
+      c->tab_dt = -1.0;
+      drop_graph(c);
+    }
+    if (scheme == TC_IMEX && c->tab_dt != dts[i]) {
+      k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dts[i], c->top_neumann, L);
+      TC_LAUNCHED();
+      c->tab_dt = dts[i];
+    }
+    const int hist = scheme == TC_FE ? 0 : c->have_hist;
+    tab[i] = batch_record<T>(c, c->cur, dts[i], 1, scheme, L);
+    tab[n + i] = batch_record<T>(c, c->cur ^ 1, dts[i], 1, scheme, L);
+    tab[2 * n + i] = batch_record<T>(c, c->cur, dts[i], hist, scheme, L);
+    int cnt[BK_COUNT];
+    batch_units<T>(tab[i], c, cnt);
+    for (int k = 0; k < BK_COUNT; ++k) {
+      tab[i].u0[k] = tab[n + i].u0[k] = tab[2 * n + i].u0[k] = run[k];
+      run[k] += cnt[k];
+    }
+    maxnz = std::max(maxnz, c->nz);
+    maxchunks = std::max(maxchunks, (c->nz + L - 1) / L);
+    for_each_n1(c->nx, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      fx = std::max(fx, fftx_reg_smem<N1>());
+      ifx = std::max(ifx, ifftx_reg_smem<N1>());
+    });
+    for_each_n1(c->ny, [&](auto I) { fyt = std::max(fyt, RowFft<decltype(I)::value>::TILE); });
+  }
+  for (int k = 0; k < BK_COUNT; ++k) b->total[k] = run[k];
+  const int V = L == 16 ? VL16 : 1;
+  b->cn_y = maxchunks;
+  b->smem_cn = (size_t)(9 * maxnz + 2 * maxchunks * 32 * V) * 8;
+  b->smem_fx = fx; b->smem_ifx = ifx;
+  b->fy_tile = fyt;
+  b->smem_fy = (size_t)4 * 2 * fyt * sizeof(cpx<double>);
+  b->cn_maxt = 32 * b->cn_y <= 256 ? 256 : 512;
+  int n1max = 0;
+  for (auto* c : b->m) n1max = std::max(n1max, std::max(c->nx, c->ny) / 16);
+  b->nmax = n1max <= 8 ? 8 : 16;
+  int rc = batch_shapes<T>(b, scheme);
+  if (rc) return rc;
+  // pageable copy: returns once the records are staged
+  TC_CUDA(cudaMemcpyAsync(b->table, tab.data(), tab.size() * sizeof(BMember<T>), cudaMemcpyHostToDevice, s));
+  b->dts.assign(dts, dts + n);
+  b->cur0.resize(n);
+  for (int i = 0; i < n; ++i) b->cur0[i] = b->m[i]->cur;
+  b->q = 0;
+  b->scheme = scheme;
+  b->valid = 1;
+  batch_drop_graph(b);
+  return TC_OK;
+}
+
+template <class T, int NMAX> static void batch_poisson(const tc_batch* b, const BMember<T>* M, cudaStream_t s) {
+  const int n = b->n;
+  kb_fftx<T, NMAX><<<b->grid[BK_FX], 128, b->smem_fx, s>>>(M, n, b->total[BK_FX]);
+  kb_ffty<T, NMAX, false><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
+  kb_tri<T><<<b->grid[BK_TRI], 64, 0, s>>>(M, n, b->total[BK_TRI]);
+  kb_ffty<T, NMAX, true><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
+  kb_ifftx<T, NMAX><<<b->grid[BK_IFX], 128, b->smem_ifx, s>>>(M, n, b->total[BK_IFX]);
+}
+
+// One step of every member with table `ti` (0, 1: parity; 2: first step).
+template <class T> static int batch_step_impl(tc_batch* b, int scheme, int ti, cudaStream_t s) {
+  const BMember<T>* M = reinterpret_cast<const BMember<T>*>(b->table) + (size_t)ti * b->n;
+  const int n = b->n;
+  const dim3 rb(RHS_TX, rhs_ty<T>());
+  if (scheme == TC_IMEX)
+    kb_rhs<T, false, UPD_AB2><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
+  else if (scheme == TC_AB2)
+    kb_rhs<T, true, UPD_AB2><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
+  else
+    kb_rhs<T, true, UPD_FE><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
+  if (scheme == TC_IMEX) {
+    const dim3 cb(32, b->cn_y);
+    constexpr int V16 = batch_cn_vec<T>(16);
+    if (b->cn_L == 16 && b->cn_maxt == 256)
+      kb_cn<T, 16, V16, 256><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
+    else if (b->cn_L == 16)
+      kb_cn<T, 16, V16, 512><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
+    else if (b->cn_maxt == 256)
+      kb_cn<T, 32, 1, 256><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
+    else
+      kb_cn<T, 32, 1, 512><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
+  }
+  if (b->nmax == 8)
+    batch_poisson<T, 8>(b, M, s);
+  else
+    batch_poisson<T, 16>(b, M, s);
+  kb_proj<T><<<b->grid[BK_PROJ], dim3(32, 8), 0, s>>>(M, n, b->total[BK_PROJ]);
+  TC_LAUNCHED();
+  return TC_OK;
+}
+
+static void batch_advance(tc_batch* b, int scheme) {
+  for (auto* c : b->m) {
+    c->cur ^= 1;
+    if (scheme != TC_FE) c->have_hist = 1;
+  }
+  b->q ^= 1;
+}
+
+#define BDISPATCH(b, fn, ...) ((b)->precision == TC_FP64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+static int batch_build_graph(tc_batch* b, int scheme) {
+  batch_drop_graph(b);
+  if (!b->cap_stream) TC_CUDA(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+  TC_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int rc = TC_OK;
+  for (int k = 0; k < 2 && rc == TC_OK; ++k) rc = BDISPATCH(b, batch_step_impl, b, scheme, b->q ^ k, b->cap_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->cap_stream, &graph);
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  b->g_valid = 1; b->g_scheme = scheme; b->g_q = b->q;
+  return TC_OK;
+}
+
+extern "C" int tc_batch_step(tc_batch* b, int scheme, const double* dts, int n_steps, void* stream) {
+  if (!b || !dts) return fail(TC_ERR_ARG, "null argument");
+  if (scheme != TC_IMEX && scheme != TC_AB2 && scheme != TC_FE) return fail(TC_ERR_ARG, "bad scheme");
+  if (n_steps < 0) return fail(TC_ERR_ARG, "n_steps must be >= 0");
+  const cudaStream_t s = ST(stream);
+  bool rebuild = !b->valid || b->scheme != scheme;
+  bool lack = false;
+  for (int i = 0; i < b->n; ++i) {
+    const tc_ctx* c = b->m[i];
+    if (!c->state_set) return fail(TC_ERR_STATE, "member without a state");
+    if (!(dts[i] > 0)) return fail(TC_ERR_ARG, "dt must be > 0");
+    if (c->body[0] || c->ke_acc || c->tape) return fail(TC_ERR_ARG, "ensemble launches take no adjoint hooks");
+    if (b->valid && (b->dts[i] != dts[i] || c->cur != (b->cur0[i] ^ b->q))) rebuild = true;
+    if (scheme == TC_IMEX && (c->cn_L_force != b->cn_L || c->tab_dt != dts[i])) rebuild = true;
+    lack = lack || (scheme != TC_FE && !c->have_hist);
+  }
+  if (lack && b->valid && b->q != 0) rebuild = true;
+  if (n_steps == 0) return TC_OK;
+  if (rebuild) {
+    int rc = BDISPATCH(b, batch_build_impl, b, scheme, dts, s);
+    if (rc) return rc;
+  }
+  int k = 0;
+  if (lack) {  // first step: members without history take a forward-Euler-style start
+    int rc = BDISPATCH(b, batch_step_impl, b, scheme, 2, s);
+    if (rc) return rc;
+    batch_advance(b, scheme);
+    ++k;
+  }
+  if (b->graphs_on && n_steps - k >= 4) {
+    if (!b->g_valid || b->g_scheme != scheme || b->g_q != b->q) {
+      int rc = batch_build_graph(b, scheme);
+      if (rc) return rc;
+    }
+    for (; k + 2 <= n_steps; k += 2) {
+      TC_CUDA(cudaGraphLaunch(b->gexec, s));
+      batch_advance(b, scheme);
+      batch_advance(b, scheme);
+    }
+  }
+  for (; k < n_steps; ++k) {
+    int rc = BDISPATCH(b, batch_step_impl, b, scheme, b->q, s);
+    if (rc) return rc;
+    batch_advance(b, scheme);
+  }
+  return TC_OK;
+}
+
+extern "C" int tc_batch_info(tc_batch* b, int* shape, int* units, int* grids) {
+  if (!b) return fail(TC_ERR_ARG, "null ensemble");
+  if (shape) { shape[0] = b->cn_L; shape[1] = b->ctas_per_sm; shape[2] = b->valid; }
+  for (int k = 0; k < BK_COUNT; ++k) {
+    if (units) units[k] = b->valid ? b->total[k] : 0;
+    if (grids) grids[k] = b->valid ? b->grid[k] : 0;
   }
   return TC_OK;
 }

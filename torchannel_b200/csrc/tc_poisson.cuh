@@ -109,6 +109,24 @@ __global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int n
 // In-place complex FFT along y of the rows X[kx][k][:] with the register
 // transform (ny = N1 * 16): RowFft<N1>::RPW rows per warp, each row read and
 // written once, no block barrier; warps stride over the rows.
+// Rows row0 .. row0+RPW-1 (< nrows) by one warp, as one pass of the
+// k_ffty_reg loop below; `tiles` holds the warp's RPW transpose tiles.
+template <int N1, bool INV>
+__device__ __forceinline__ void ffty_rows(cpx<double>* __restrict__ X, int nrows, const cpx<double>* __restrict__ twy,
+                                          int row0, cpx<double>* tiles) {
+  using RF = RowFft<N1>;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;   // row of the warp, lane in the row
+  cpx<double>* tile = tiles + (size_t)sub * RF::TILE;
+  const int row = row0 + sub;
+  const bool ok = sub < RF::RPW && row < nrows;
+  cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
+  if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
+  __syncwarp();
+  if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+  __syncwarp();
+}
+
 template <int N1, bool INV>
 __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, int nrows,
                                                  const cpx<double>* __restrict__ twy) {
@@ -135,18 +153,23 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
 // travel as one complex row, RowFft<N1>::RPW such rows per warp (XR / 2 / RPW
 // warps a block).  The unpacked half spectra are written transposed,
 // X[m][k][j], as in k_div_fftx.
+// rows per block of the register x transforms (XR below)
+#define XROWS 16
+
+// Rows j0 = bx * XR .. of plane k; blockDim.x may exceed the warps the rows
+// need (ensemble kernel), the extra warps only take part in the barrier.
 template <class T, int N1, int XR>
-__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
-                                                     const T* __restrict__ w, const double* __restrict__ field,
-                                                     cpx<double>* __restrict__ X,
-                                                     const cpx<double>* __restrict__ twx, double scale) {
+__device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
+                                          const T* __restrict__ w, const double* __restrict__ field,
+                                          cpx<double>* __restrict__ X, const cpx<double>* __restrict__ twx,
+                                          double scale, int bx, int k) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int ZP = (RF::TILE + 7) / 8 * 8 + 1;          // row pitch of the spectra (16 B mod 128 B)
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<double>* zs = reinterpret_cast<cpx<double>*>(smraw);  // XR/2 packed rows x ZP
   const int ny = g.ny, nz = g.nz;
-  const int k = blockIdx.y, j0 = blockIdx.x * XR;
+  const int j0 = bx * XR;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
   const int pr = warp * RF::RPW + sub;                      // packed row: j = j0 + 2 pr, +1
@@ -197,20 +220,28 @@ __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid
   }
 }
 
+template <class T, int N1, int XR>
+__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+                                                     const T* __restrict__ w, const double* __restrict__ field,
+                                                     cpx<double>* __restrict__ X,
+                                                     const cpx<double>* __restrict__ twx, double scale) {
+  fftx_tile<T, N1, XR>(g, u, v, w, field, X, twx, scale, blockIdx.x, blockIdx.y);
+}
+
 // Inverse real FFT along x of rows j0 .. j0+XR-1 of plane k with the
 // register transform (nx = N1 * 16); writes p[k][j][i] (FP64).  Two rows
 // travel as one complex row Z = A + i B built from the half spectra (DC and
 // Nyquist real).
 template <int N1, int XR>
-__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_ifftx_reg(const cpx<double>* __restrict__ X, double* __restrict__ p,
-                                                  int ny, int nz, const cpx<double>* __restrict__ twx) {
+__device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, double* __restrict__ p, int ny, int nz,
+                                           const cpx<double>* __restrict__ twx, int bx, int k) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int SP = (NH + 7) / 8 * 8 + 1;                  // staging pitch
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<double>* S = reinterpret_cast<cpx<double>*>(smraw);   // XR rows x SP half spectra
   cpx<double>* tiles = S + XR * SP;                          // XR/2 packed rows x TILE
-  const int k = blockIdx.y, j0 = blockIdx.x * XR;
+  const int j0 = bx * XR;
   for (int e = threadIdx.x; e < NH * XR; e += blockDim.x) {
     const int m = e / XR, r = e % XR;
     cpx<double> val = X[((size_t)m * nz + k) * ny + j0 + r];
@@ -236,6 +267,12 @@ __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_ifftx_reg(const c
   double* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
   if (ok && l < N1)
     rowfft_pass2<N1, true>([&](int i, cpx<double> z) { pa[i] = z.x; pa[N + i] = z.y; }, l, tile);
+}
+
+template <int N1, int XR>
+__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_ifftx_reg(const cpx<double>* __restrict__ X, double* __restrict__ p,
+                                                  int ny, int nz, const cpx<double>* __restrict__ twx) {
+  ifftx_tile<N1, XR>(X, p, ny, nz, twx, blockIdx.x, blockIdx.y);
 }
 
 // Thomas sweep along z for every mode (kx, ky), one thread per mode
@@ -590,10 +627,10 @@ __global__ void __launch_bounds__(512) k_yz_solve(cpx<double>* __restrict__ X, c
 // factors are real, so the two recurrences are independent): twice the
 // threads in flight, half the registers per level, TRIP_B levels prefetched.
 #define TRIP_B 16
-__global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const double* __restrict__ rden_t,
-                                                 const double* __restrict__ cp_t, PoissonTabs tb, int nxh, int ny,
-                                                 int nz) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// Thread t of the sweep (mode t / 2, part t % 2).
+__device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const double* __restrict__ rden_t,
+                                               const double* __restrict__ cp_t, const PoissonTabs& tb, int nxh,
+                                               int ny, int nz, int t) {
   const int mode = t >> 1, part = t & 1;
   if (mode >= nxh * ny) return;
   const int kx = mode / ny, ky = mode - kx * ny;
@@ -651,6 +688,12 @@ __global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const d
 #pragma unroll
     for (int b = 0; b < TRIP_B; ++b) { dc[b] = dn[b]; fc[b] = fn[b]; }
   }
+}
+
+__global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const double* __restrict__ rden_t,
+                                                 const double* __restrict__ cp_t, PoissonTabs tb, int nxh, int ny,
+                                                 int nz) {
+  tri_lu2_thread(Xd, rden_t, cp_t, tb, nxh, ny, nz, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // k_yz_solve with the register-resident row transforms (ny = N1 * 16): the

@@ -59,14 +59,15 @@ template <class T> __host__ __device__ constexpr int rhs_ty() { return 8; }
 template <class T> __host__ __device__ constexpr int rhs_kb() { return sizeof(T) == 8 ? 3 : 4; }
 #define RHS_HX (RHS_TX + 2)
 
+// The tile (bx, by, bz) of the block grid above; k_rhs_update runs one tile
+// per block, the ensemble kernel of tc_batch.cuh loops over the tiles of all
+// members (the shared tile is reused: callers separate tiles by a barrier).
 template <class T, bool FULL, int UPD>
-__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, const T* __restrict__ u,
-                                                                const T* __restrict__ v, const T* __restrict__ w,
-                                                                T* __restrict__ us, T* __restrict__ vs,
-                                                                T* __restrict__ ws, T* __restrict__ ru,
-                                                                T* __restrict__ rv, T* __restrict__ rw,
-                                                                const double* __restrict__ forcing_dev, T dt,
-                                                                int have_hist) {
+__device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
+                                         const T* __restrict__ w, T* __restrict__ us, T* __restrict__ vs,
+                                         T* __restrict__ ws, T* __restrict__ ru, T* __restrict__ rv,
+                                         T* __restrict__ rw, const double* __restrict__ forcing_dev, T dt,
+                                         int have_hist, int bx, int by, int bz) {
   constexpr int RHS_TY = rhs_ty<T>(), RHS_HY = RHS_TY + 2, RHS_NH = RHS_HX * RHS_HY;
   constexpr int RHS_KB = rhs_kb<T>();
   constexpr int RHS_NS = RHS_KB + 2;
@@ -77,10 +78,10 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, 
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx;
-  const int i0 = blockIdx.x * RHS_TX, j0 = blockIdx.y * RHS_TY;
+  const int i0 = bx * RHS_TX, j0 = by * RHS_TY;
   const int i = i0 + tx, j = j0 + ty;
   const bool active = (i < nx) && (j < ny);
-  const int kb = blockIdx.z * RHS_KB;  // planes kb .. kb+RHS_KB-1 (<= nz)
+  const int kb = bz * RHS_KB;  // planes kb .. kb+RHS_KB-1 (<= nz)
   const T top = g.top_neumann ? T(1) : T(-1);
   const T h = T(0.5);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
@@ -225,6 +226,18 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, 
   }
 }
 
+template <class T, bool FULL, int UPD>
+__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, const T* __restrict__ u,
+                                                                const T* __restrict__ v, const T* __restrict__ w,
+                                                                T* __restrict__ us, T* __restrict__ vs,
+                                                                T* __restrict__ ws, T* __restrict__ ru,
+                                                                T* __restrict__ rv, T* __restrict__ rw,
+                                                                const double* __restrict__ forcing_dev, T dt,
+                                                                int have_hist) {
+  rhs_tile<T, FULL, UPD>(g, u, v, w, us, vs, ws, ru, rv, rw, forcing_dev, dt, have_hist, blockIdx.x, blockIdx.y,
+                         blockIdx.z);
+}
+
 // ---------------------------------------------------------------------------
 // Crank-Nicolson tables.  Row m of a system:
 //   a_m x_{m-1} + b_m x_m + c_m x_{m+1} = q_m + beta (cA_m s_{-1} + cB_m s_0 + cC_m s_{+1})
@@ -361,12 +374,13 @@ template <> struct CnVec<float, 2> {
     *reinterpret_cast<float2*>(p) = make_float2((float)o[0], (float)o[1]);
   }
 };
-template <class T, int L, int VEC, int MAXT>
-__global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
-                                                   CnTab t, const double* __restrict__ ubase, int nx, int ny,
-                                                   int nz) {
+// Column block bx of component comp (the block grid above); blockDim.y may
+// exceed the chunks of this system (ensemble kernel: the deepest member's
+// count), the extra warps only take part in the barriers.
+template <class T, int L, int VEC>
+__device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, const CnTab& t,
+                                        const double* __restrict__ ubase, int nx, int ny, int nz, int bx, int comp) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int comp = blockIdx.z;
   const int lane = threadIdx.x, chunk = threadIdx.y, nchunk = blockDim.y;
   const int tid = chunk * 32 + lane, nthr = 32 * nchunk;
   double* tab = reinterpret_cast<double*>(smraw);           // 8*nz
@@ -376,7 +390,7 @@ __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restr
   for (int e = tid; e < 8 * nz; e += nthr) tab[e] = src[e];
   for (int e = tid; e < nz; e += nthr) shb[e] = (comp == 0 && ubase) ? ubase[e] : 0.0;
   // nx*ny is even, so with VEC = 2 a pair of columns is valid as a whole
-  const int col = (blockIdx.x * 32 + lane) * VEC;
+  const int col = (bx * 32 + lane) * VEC;
   const int ncols = nx * ny;
   const bool colok = col < ncols;
   const size_t plane = (size_t)ncols;
@@ -502,6 +516,13 @@ __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restr
   }
 }
 
+template <class T, int L, int VEC, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+                                                   CnTab t, const double* __restrict__ ubase, int nx, int ny,
+                                                   int nz) {
+  cn_tile<T, L, VEC>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z);
+}
+
 // Scalars slot layout (FP64, device).
 enum : int {
   SC_FORCING = 0,
@@ -556,17 +577,19 @@ template <class T> struct Vec2;
 template <> struct Vec2<double> { using t = double2; };
 template <> struct Vec2<float> { using t = float2; };
 
+// Block (bx, by, bz) of a grid of gx x gy x gz blocks of 32 x 8 threads.
 template <class T>
-__global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
-                                                      T* __restrict__ w, const double* __restrict__ p, double dt,
-                                                      const double* __restrict__ dzf, BulkArgs ba) {
+__device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u, T* __restrict__ v,
+                                             T* __restrict__ w, const double* __restrict__ p, double dt,
+                                             const double* __restrict__ dzf, const BulkArgs& ba, int bx, int by,
+                                             int bz, int gx, int gy, int gz) {
   using V2 = typename Vec2<T>::t;
   __shared__ double sh[32];
   __shared__ int last;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k0 = blockIdx.z * PROJ_PK;  // planes k0 .. k0+PROJ_PK-1
+  const int i = 2 * (bx * 32 + threadIdx.x);
+  const int j = by * 8 + threadIdx.y;
+  const int k0 = bz * PROJ_PK;  // planes k0 .. k0+PROJ_PK-1
   double acc = 0.0;
   if (i < nx && j < ny) {
     const int jp = wrap(j + 1, ny), ipp = wrap(i + 2, nx);
@@ -603,9 +626,9 @@ __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__
     }
   }
   double s = block_sum(acc, sh);
-  const int nb = gridDim.x * gridDim.y * gridDim.z;
+  const int nb = gx * gy * gz;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
-    ba.partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+    ba.partials[((size_t)bz * gy + by) * gx + bx] = s;
     __threadfence();
     unsigned int t = atomicAdd(ba.ticket, 1u);
     last = (t == (unsigned)nb - 1u);
@@ -616,6 +639,13 @@ __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__
     bulk_reduce_block(ba.partials, nb, ba.scal, ba.scale, ba.U_target, ba.dt, ba.update_forcing, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) *ba.ticket = 0u;
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
+                                                      T* __restrict__ w, const double* __restrict__ p, double dt,
+                                                      const double* __restrict__ dzf, BulkArgs ba) {
+  project_tile<T>(g, u, v, w, p, dt, dzf, ba, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z);
 }
 
 // Bulk sum over all DOFs without projection (set-up and diagnostics).

@@ -3,13 +3,21 @@
 Members are independent, so a multi-GPU ensemble shards them across ranks
 (one process per GPU, members assigned round-robin) with no collective on the
 hot path; the only collectives are host-side reductions of the timing and the
-per-member diagnostics after the steps.  On one GPU the members advance on
-their own CUDA streams so that small members overlap; ``Ensemble.capture``
-records two steps of every member (forked onto the member streams) as one
-CUDA graph, so an ensemble step pair is a single graph launch, and
-``Ensemble.autotune`` picks each member's kernel shapes (Poisson path, CN
-chunk length) by timing the candidates on that member.
+per-member diagnostics after the steps.
+
+On one GPU there are two ways to advance the members:
+* ``ChannelBatch`` (``Ensemble.batch``): every substep of every member is ONE
+  persistent launch over the concatenated work of all members
+  (``tc_batch_*``), two steps replayed as one CUDA graph;
+  ``Ensemble.autotune_batch`` picks its shapes (CN rows per chunk, CTAs per
+  SM) by timing them on the ensemble.
+* per-member launches on per-member streams (``Ensemble.step``);
+  ``Ensemble.capture`` records two steps of every member (forked onto the
+  member streams) as one CUDA graph, and ``Ensemble.autotune`` picks each
+  member's kernel shapes (Poisson path, CN chunk length).
 """
+import ctypes
+
 import numpy as np
 
 
@@ -45,6 +53,61 @@ def aggregate(local_points, local_ms):
         dist.all_reduce(m, op=dist.ReduceOp.MAX)
         pts, ms = float(t.item()), float(m.item())
     return pts / (ms / 1e3), pts, ms
+
+
+class ChannelBatch:
+    """Channels (one precision, one device; nx, ny in {64, 96, 128, 192,
+    256}) stepped together: one persistent launch per substep for all of
+    them (``tc_batch_step``).  Each member advances as ``Channel.step``
+    would; its state, scalars and statistics stay on its own ``Channel``."""
+
+    def __init__(self, channels):
+        import torch
+        from . import _lib as L
+        self.L = L
+        self.lib = L.lib()
+        self.channels = list(channels)  # keeps the contexts alive
+        n = len(self.channels)
+        prec = self.channels[0]._desc.precision
+        nb = ctypes.c_size_t()
+        L.check(self.lib.tc_batch_table_bytes(n, prec, ctypes.byref(nb)))
+        self._table = torch.empty(nb.value + 16, dtype=torch.uint8, device="cuda")
+        base = (self._table.data_ptr() + 15) & ~15
+        arr = (ctypes.c_void_p * n)(*[c.ctx.value for c in self.channels])
+        b = ctypes.c_void_p()
+        L.check(self.lib.tc_batch_create(arr, n, ctypes.c_void_p(base), nb.value, ctypes.byref(b)))
+        self.b = b
+
+    def __del__(self):
+        try:
+            if getattr(self, "b", None) is not None and self.b.value:
+                import torch
+                torch.cuda.synchronize()
+                self.lib.tc_batch_destroy(self.b)
+                self.b = None
+        except Exception:
+            pass
+
+    def set_shape(self, cn_rows=16, ctas_per_sm=0):
+        self.L.check(self.lib.tc_batch_set_shape(self.b, int(cn_rows), int(ctas_per_sm)))
+
+    def use_graphs(self, on=True):
+        self.L.check(self.lib.tc_batch_use_graphs(self.b, int(bool(on))))
+
+    def step(self, scheme, dts, n_steps=1):
+        import torch
+        from .core import SCHEMES
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dts, dtype=np.float64), (len(self.channels),)))
+        self.L.check(self.lib.tc_batch_step(self.b, SCHEMES[scheme] if isinstance(scheme, str) else int(scheme),
+                                            d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(n_steps),
+                                            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    def info(self):
+        shape, units, grids = (ctypes.c_int * 3)(), (ctypes.c_int * 7)(), (ctypes.c_int * 7)()
+        self.L.check(self.lib.tc_batch_info(self.b, shape, units, grids))
+        names = ["rhs", "cn", "fftx", "ffty", "tri", "ifftx", "proj"]
+        return {"cn_rows": shape[0], "ctas_per_sm": shape[1], "built": bool(shape[2]),
+                "units": dict(zip(names, list(units))), "ctas": dict(zip(names, list(grids)))}
 
 
 class Ensemble:
@@ -183,6 +246,53 @@ class Ensemble:
         """Advance every member by 2 * n_pairs steps: n_pairs graph launches."""
         for _ in range(n_pairs):
             self.graph.replay()
+
+    # -- one launch per substep for all members ----------------------------------
+    def batch(self):
+        """Group the members into a ChannelBatch (kept as ``self.batched``)."""
+        import torch
+        torch.cuda.synchronize()  # the members were set up on their own streams
+        self.batched = ChannelBatch(self.channels)
+        return self.batched
+
+    def step_batch(self, n_steps, scheme="IMEX"):
+        """Advance every member by n_steps with the ensemble launches (on the
+        current stream)."""
+        self.batched.step(scheme, self.dts, n_steps)
+
+    def autotune_batch(self, steps=8, repeats=2, rows=(16, 32), ctas=(0, 1, 2, 4)):
+        """Time every (CN rows per chunk, persistent CTAs per SM) shape of the
+        ensemble launches over `steps` steps (best of `repeats`), keep the
+        fastest, and restore every member's state, history and forcing.
+        Returns the chosen shape and the step time (ms) of each candidate."""
+        import torch
+        b = self.batched
+        saved = [self._save(ch) for ch in self.channels]
+        deep = max(m["nz"] for m in self.members) > 256
+        times = {}
+        for r in rows:
+            if r == 16 and deep:
+                continue
+            for c in ctas:
+                b.set_shape(r, c)
+                b.step("IMEX", self.dts, 2)  # tables, history and graph of this shape
+                ms = []
+                for _ in range(repeats):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    b.step("IMEX", self.dts, steps)
+                    e1.record()
+                    e1.synchronize()
+                    ms.append(e0.elapsed_time(e1) / steps)
+                times[(r, c)] = min(ms)
+                for ch, sv in zip(self.channels, saved):
+                    self._restore(ch, sv)
+        best = min(times, key=times.get)
+        b.set_shape(*best)
+        torch.cuda.synchronize()
+        self.batch_tuning = {"cn_rows": best[0], "ctas_per_sm": best[1],
+                             "ms_per_step": {f"cn{k[0]}/ctas{k[1]}": v for k, v in times.items()}}
+        return self.batch_tuning
 
     def diagnostics(self):
         import torch
