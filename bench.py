@@ -453,6 +453,19 @@ def run_ensemble(a):
     torch.cuda.synchronize()
     ms_graph = g0.elapsed_time(g1)
     value_graph, _, _ = aggregate(ens.points() * 2 * pairs, ms_graph)
+    # one persistent launch per substep for all members, tuned shape
+    ens.batch()
+    btun = ens.autotune_batch()
+    ens.step_batch(2)
+    torch.cuda.synchronize()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record()
+    ens.step_batch(2 * pairs)
+    b1.record()
+    torch.cuda.synchronize()
+    ms_batch = b0.elapsed_time(b1)
+    value_batch, _, _ = aggregate(ens.points() * 2 * pairs, ms_batch)
+    binfo = ens.batched.info()
     diag = ens.diagnostics()
     if world > 1:
         dist.destroy_process_group()
@@ -468,6 +481,11 @@ def run_ensemble(a):
                           "tuned_one_graph": {"value": value_graph, "ms_per_step": ms_graph / (2 * pairs),
                                               "note": "autotuned member shapes; 2 steps of all members per graph launch"},
                           "tuning": tuning,
+                          "batched": {"value": value_batch, "ms_per_step": ms_batch / (2 * pairs),
+                                      "launches_per_step": 8, "shape": btun, "units": binfo["units"],
+                                      "ctas": binfo["ctas"],
+                                      "note": "one persistent launch per substep for all members, "
+                                              "two steps per graph launch (tc_batch_step)"},
                           "max_div_after": max(d["max_div"] for d in diag)}), flush=True)
 
 

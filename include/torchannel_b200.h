@@ -271,9 +271,10 @@ int tc_adjoint_step(tc_ctx* ctx, double dt, int first, const double* qu, const d
 int tc_set_ke_accumulator(tc_ctx* ctx, double* acc, const double* weight_dev, void* scratch);
 int tc_set_state_tape(tc_ctx* ctx, double* tape, int nslots, int* ctr_dev);
 
-/* Tile shape of the CN solve along z: rows per chunk (16 or 32; 0 = by nz:
- * 16 up to nz = 256, else 32).  Used by the ensemble autotuner; no reference
- * counterpart.  TC_ERR_SIZE for 16 with nz > 256. */
+/* Tile shape of the CN solve along z: rows per chunk (1 .. 32; 0 = by nz:
+ * 16 up to nz = 256, else 32).  Used by the autotuners and the ensemble
+ * launches; no reference counterpart.  TC_ERR_SIZE when a column would need
+ * more than 16 chunks. */
 int tc_set_cn_chunk(tc_ctx* ctx, int rows);
 
 /* ---------------------------------------------------------------------------
@@ -293,13 +294,17 @@ int tc_set_cn_chunk(tc_ctx* ctx, int rows);
  * ensemble calls (the ensemble rebuilds its tables when it notices).
  * The caller owns the member-table memory (device, 16-byte aligned, size
  * from tc_batch_table_bytes); all calls on one stream.
- * tc_batch_set_shape: CN rows per chunk (16 or 32; the members' tables follow)
- *   and persistent CTAs per SM (0 = occupancy limit), the ensemble
+ * tc_batch_set_shape: CN rows per chunk bound (16 or 32: the deepest
+ *   member's chunk count fixes the CN block, every member's chunk length
+ *   becomes ceil(nz / chunks) and its tables follow) and persistent CTAs per
+ *   SM (0 = occupancy limit, -1 = one CTA per work unit), the ensemble
  *   autotuner's knobs.
  * tc_batch_step: dts = host array of one dt per member; members without AB2
  *   history start with a forward step as tc_step does.  Members may carry no
  *   adjoint hooks (TC_ERR_ARG).
- * tc_batch_info: shape = {cn rows, ctas per SM, tables built}; units and
+ * tc_batch_info: shape = {cn rows (the shape's bound), ctas per SM (-1: one
+ *   CTA per work unit), tables built, CN chunks per column}; every member
+ *   then solves CN in chunks of ceil(nz / chunks) rows; units and
  *   grids = work units and CTAs of the seven launches (RHS, CN, x transform,
  *   y transform, z solve, inverse x transform, projection). */
 typedef struct tc_batch tc_batch;

@@ -34,9 +34,15 @@ def _same(torch, ea, eb):
         assert torch.equal(ca.scalars[:2], cb.scalars[:2])
 
 
-def _step_members(torch, e, n, scheme="IMEX", rows=16):
-    for ch, dt in zip(e.channels, e.dts):
-        ch.set_cn_chunk(rows)
+def _rows(e, bound=16):
+    """Each member's CN chunk length under the ensemble shape bound."""
+    chunks = -(-max(c.nz for c in e.channels) // bound)
+    return [-(-c.nz // chunks) for c in e.channels]
+
+
+def _step_members(torch, e, n, scheme="IMEX", bound=16):
+    for ch, dt, r in zip(e.channels, e.dts, _rows(e, bound)):
+        ch.set_cn_chunk(r)
         ch.step(scheme, dt, n)
     torch.cuda.synchronize()
 
@@ -66,22 +72,26 @@ def test_batch_explicit_schemes(torch_cuda, scheme):
     _same(torch, a, b)
 
 
-@pytest.mark.parametrize("rows,ctas", [(32, 0), (16, 1), (32, 3)])
+@pytest.mark.parametrize("rows,ctas", [(32, 0), (16, 1), (32, 3), (16, -1)])
 def test_batch_shapes(torch_cuda, rows, ctas):
     torch = torch_cuda
     a, b = _pair("mixed")
     a.batch().set_shape(rows, ctas)
     a.step_batch(7)
     torch.cuda.synchronize()
-    _step_members(torch, b, 7, rows=rows)
+    _step_members(torch, b, 7, bound=rows)
     _same(torch, a, b)
     info = a.batched.info()
     assert info["cn_rows"] == rows and info["ctas_per_sm"] == ctas and info["built"]
+    assert a.batched.member_cn_rows() == _rows(b, rows)
+    assert info["cn_chunks"] == -(-max(c.nz for c in a.channels) // rows)
     nsm = torch.cuda.get_device_properties(0).multi_processor_count
     for k, g in info["ctas"].items():
-        assert 1 <= g <= info["units"][k] or (k == "ffty" and g * 4 >= 1)
-        if ctas:
+        assert 1 <= g <= info["units"][k]
+        if ctas > 0:
             assert g <= ctas * nsm
+        if ctas < 0 and k != "ffty":
+            assert g == info["units"][k]
 
 
 def test_batch_interleaved_with_member_steps(torch_cuda):
@@ -97,8 +107,8 @@ def test_batch_interleaved_with_member_steps(torch_cuda):
     a.dts = b.dts = [0.9 * dt for dt in old]
     a.step_batch(5)
     torch.cuda.synchronize()
-    for i, (ch, dt0, dt) in enumerate(zip(b.channels, old, b.dts)):
-        ch.set_cn_chunk(16)
+    for i, (ch, dt0, dt, r) in enumerate(zip(b.channels, old, b.dts, _rows(b))):
+        ch.set_cn_chunk(r)
         ch.step("IMEX", dt0, 4)
         if i == 1:
             ch.step("IMEX", dt0, 1)
@@ -119,7 +129,7 @@ def test_batch_uneven_large_members(torch_cuda):
     assert a.batched.info()["cn_rows"] == 32
     a.step_batch(6)
     torch.cuda.synchronize()
-    _step_members(torch, b, 6, rows=32)
+    _step_members(torch, b, 6, bound=32)
     _same(torch, a, b)
 
 
@@ -141,7 +151,7 @@ def test_batch_autotune_restores_state(torch_cuda):
     torch = torch_cuda
     a, b = _pair("mixed")
     a.batch()
-    tun = a.autotune_batch(steps=4, repeats=1, ctas=(0, 2))
+    tun = a.autotune_batch(steps=4, repeats=1, ctas=(-1, 2))
     assert tun["cn_rows"] in (16, 32) and len(tun["ms_per_step"]) == 4
     a.batched.set_shape(16, 0)
     a.step_batch(4)
@@ -162,3 +172,15 @@ def test_batch_stays_divergence_free(torch_cuda):
     torch.cuda.synchronize()
     for d in e.diagnostics():
         assert np.isfinite(d["max_div"]) and d["max_div"] < 1e-5
+
+
+def test_autotune_mode_restores_state(torch_cuda):
+    torch = torch_cuda
+    from torchannel_b200.ensemble import Ensemble
+    e = Ensemble(_members(3, seed=5), precision="fp64")
+    before = [[t.clone() for t in ch.get_state()[:3]] for ch in e.channels]
+    times = e.autotune_mode(steps=2, repeats=1)
+    assert set(times) == {"batch", "streams"} and e.mode in times
+    for ch, b in zip(e.channels, before):
+        for x, y in zip(ch.get_state()[:3], b):
+            assert torch.equal(x, y)

@@ -21,6 +21,34 @@ namespace tc {
 enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT };
 #define TC_BATCH_MAX 64  // members per ensemble launch
 
+// Register allocation of the unit loops.  Inlining every transform length
+// into one switch makes the x transform spill heavily, so that tile is a
+// called function (TC_BATCH_FX_CALL) over TC_BATCH_XP planes per unit (the
+// call's register saves are paid once per group).  The other loops inline
+// their tiles under occupancy-driven register caps (minimum resident blocks
+// per SM below).
+#ifndef TC_BATCH_FX_CALL
+#define TC_BATCH_FX_CALL __noinline__
+#endif
+#ifndef TC_BATCH_CN_CALL
+#define TC_BATCH_CN_CALL __forceinline__
+#endif
+#ifndef TC_BATCH_FFT_MINB
+#define TC_BATCH_FFT_MINB 4
+#endif
+#ifndef TC_BATCH_RHS_MINB
+#define TC_BATCH_RHS_MINB 6
+#endif
+#ifndef TC_BATCH_TRI_MINB
+#define TC_BATCH_TRI_MINB 6
+#endif
+#ifndef TC_BATCH_XP
+#define TC_BATCH_XP 4
+#endif
+#ifndef TC_BATCH_CN_CAP
+#define TC_BATCH_CN_CAP 1  // CN: cap at 128 registers (two 256-thread blocks per SM)
+#endif
+
 template <class T> struct BMember {
   Grid<T> g;
   T* A[3];                 // state at the start of the step
@@ -44,7 +72,9 @@ template <class T> struct BMember {
   int n1x, n1y, nxh, nrows;
   int rgx, rgy, rgz;       // block grid of k_rhs_update
   int cgx;                 // column blocks per component of k_cn_solve
+  int cn_lr;               // CN rows per chunk of this member (its tables' length)
   int xgx;                 // row blocks per plane of the x transforms
+  int xpg;                 // plane groups of the forward x transform
   int pgx, pgy, pgz;       // block grid of k_project_bulk
   int u0[BK_COUNT];        // first unit of the member in each launch
 };
@@ -57,14 +87,19 @@ __device__ __forceinline__ void batch_starts(const BMember<T>* __restrict__ M, i
   __syncthreads();
 }
 
+// Member owning unit w: the last m with st[m] <= w (binary search).
 __device__ __forceinline__ int batch_member(const int* st, int nm, int w) {
-  int m = 0;
-  while (m + 1 < nm && w >= st[m + 1]) ++m;
-  return m;
+  int lo = 0, hi = nm - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (st[mid] <= w) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 template <class T, bool FULL, int UPD>
-__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) kb_rhs(const BMember<T>* __restrict__ M, int nm, int total) {
+__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>(), TC_BATCH_RHS_MINB) kb_rhs(const BMember<T>* __restrict__ M, int nm, int total) {
   __shared__ int st[TC_BATCH_MAX + 1];
   batch_starts(M, nm, BK_RHS, total, st);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -80,31 +115,15 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) kb_rhs(const BMember<T>*
   }
 }
 
-// Register allocation of the unit loops.  Inlining every transform length
-// into one switch makes the x transform spill heavily, so that tile is a
-// called function (TC_BATCH_FX_CALL); the CN tile is inlined with no register
-// cap below the block's (TC_BATCH_CN_CALL, TC_BATCH_CN_MINB).
-#ifndef TC_BATCH_FX_CALL
-#define TC_BATCH_FX_CALL __noinline__
-#endif
-#ifndef TC_BATCH_CN_CALL
-#define TC_BATCH_CN_CALL __forceinline__
-#endif
-#ifndef TC_BATCH_CN_MINB
-#define TC_BATCH_CN_MINB 1
-#endif
-#ifndef TC_BATCH_FFT_MINB
-#define TC_BATCH_FFT_MINB 4
-#endif
 template <class T, int L, int VEC>
 __device__ TC_BATCH_CN_CALL void batch_cn_call(const BMember<T>* __restrict__ bp, int bx, int comp) {
   const BMember<T>& b = *bp;
-  cn_tile<T, L, VEC>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.g.nx, b.g.ny, b.g.nz, bx, comp);
+  cn_tile<T, L, VEC>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.g.nx, b.g.ny, b.g.nz, bx, comp, b.cn_lr);
 }
 
 // blockDim = (32, chunks of the deepest member) <= MAXT threads
 template <class T, int L, int VEC, int MAXT>
-__global__ void __launch_bounds__(MAXT, TC_BATCH_CN_MINB) kb_cn(const BMember<T>* __restrict__ M, int nm, int total) {
+__global__ void __launch_bounds__(MAXT, TC_BATCH_CN_CAP ? 512 / MAXT : 1) kb_cn(const BMember<T>* __restrict__ M, int nm, int total) {
   __shared__ int st[TC_BATCH_MAX + 1];
   batch_starts(M, nm, BK_CN, total, st);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -140,9 +159,13 @@ template <int NMAX, class F> __device__ __forceinline__ void batch_n1_switch(int
 }
 
 template <class T, int N1>
-__device__ TC_BATCH_FX_CALL void batch_fftx_call(const BMember<T>* __restrict__ bp, int bx, int k) {
+__device__ TC_BATCH_FX_CALL void batch_fftx_call(const BMember<T>* __restrict__ bp, int bx, int k0) {
   const BMember<T>& b = *bp;
-  fftx_tile<T, N1, XROWS>(b.g, b.B[0], b.B[1], b.B[2], nullptr, b.X, b.twx, b.scale, bx, k);
+  const int k1 = min(k0 + TC_BATCH_XP, b.g.nz);
+  for (int k = k0; k < k1; ++k) {
+    if (k > k0) __syncthreads();  // the previous plane's spectra are read
+    fftx_tile<T, N1, XROWS>(b.g, b.B[0], b.B[1], b.B[2], nullptr, b.X, b.twx, b.scale, bx, k);
+  }
 }
 template <class T, int N1>
 __device__ __forceinline__ void batch_ifftx_call(const BMember<T>* __restrict__ bp, int bx, int k) {
@@ -163,7 +186,9 @@ __global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_fftx(const BMember<
     const int m = batch_member(st, nm, w);
     const BMember<T>& b = M[m];
     const int l = w - st[m];
-    batch_n1_switch<NMAX>(b.n1x, [&](auto I) { batch_fftx_call<T, decltype(I)::value>(&b, l % b.xgx, l / b.xgx); });
+    batch_n1_switch<NMAX>(b.n1x, [&](auto I) {
+      batch_fftx_call<T, decltype(I)::value>(&b, l % b.xgx, (l / b.xgx) * TC_BATCH_XP);
+    });
     __syncthreads();
   }
 }
@@ -186,7 +211,7 @@ __global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_ffty(const BMember<
 
 // Units are 64-thread groups of the z sweeps.
 template <class T>
-__global__ void __launch_bounds__(64) kb_tri(const BMember<T>* __restrict__ M, int nm, int total) {
+__global__ void __launch_bounds__(64, TC_BATCH_TRI_MINB) kb_tri(const BMember<T>* __restrict__ M, int nm, int total) {
   __shared__ int st[TC_BATCH_MAX + 1];
   batch_starts(M, nm, BK_TRI, total, st);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {

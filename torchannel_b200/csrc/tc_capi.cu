@@ -428,9 +428,11 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   TC_CUDA(cudaFuncSetAttribute(k_yz_solve<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   TC_CUDA(cudaFuncSetAttribute(k_yz_solve<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_yz_solve<32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, sizeof(T) == 4 ? 2 : 1, 512>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  constexpr int V16 = sizeof(T) == 4 ? 2 : 1;
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   (void)c;
@@ -685,19 +687,27 @@ static int cn_len(const tc_ctx* c) {
 }
 static int cn_chunks(const tc_ctx* c) { return (c->nz + cn_len(c) - 1) / cn_len(c); }
 template <class T> static size_t cn_smem(const tc_ctx* c) {
-  const int vec = (cn_len(c) == 16 && sizeof(T) == 4) ? 2 : 1;
+  const int vec = (cn_len(c) <= 16 && sizeof(T) == 4) ? 2 : 1;
   return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32 * vec) * 8;
 }
 template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s) {
   const int ncol = c->nx * c->ny;
   const dim3 blk(32, cn_chunks(c));
-  if (cn_len(c) == 16) {
+  const int Lr = cn_len(c);
+  const size_t sm = cn_smem<T>(c);
+  if (Lr <= 16) {
     constexpr int V = sizeof(T) == 4 ? 2 : 1;
     const dim3 grid((ncol / V + 31) / 32, 1, 3);
-    k_cn_solve<T, 16, V, 512><<<grid, blk, cn_smem<T>(c), s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz);
+    if (Lr == 16)
+      k_cn_solve<T, 16, V, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
+    else
+      k_cn_solve<T, 16, V, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
   } else {
     const dim3 grid((ncol + 31) / 32, 1, 3);
-    k_cn_solve<T, 32, 1, 512><<<grid, blk, cn_smem<T>(c), s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz);
+    if (Lr == 32)
+      k_cn_solve<T, 32, 1, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
+    else
+      k_cn_solve<T, 32, 1, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
   }
 }
 
@@ -1661,8 +1671,8 @@ extern "C" int tc_set_state_tape(tc_ctx* c, double* tape, int nslots, int* ctr_d
 
 extern "C" int tc_set_cn_chunk(tc_ctx* c, int rows) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
-  if (rows != 0 && rows != 16 && rows != 32) return fail(TC_ERR_ARG, "CN chunk length must be 0, 16 or 32");
-  if (rows == 16 && c->nz > 256) return fail(TC_ERR_SIZE, "16-row CN chunks need nz <= 256");
+  if (rows < 0 || rows > 32) return fail(TC_ERR_ARG, "CN chunk length must be 0 .. 32");
+  if (rows > 0 && (c->nz + rows - 1) / rows > 16) return fail(TC_ERR_SIZE, "CN chunks of this length exceed 16 per column");
   if (rows != c->cn_L_force) {
     c->cn_L_force = rows;
     c->tab_dt = -1.0;  // the chunk products of the tables follow the length
@@ -1760,7 +1770,7 @@ extern "C" int tc_batch_set_shape(tc_batch* b, int cn_rows, int ctas_per_sm) {
   if (cn_rows != 16 && cn_rows != 32) return fail(TC_ERR_ARG, "CN chunk length must be 16 or 32");
   for (auto* c : b->m)
     if (cn_rows == 16 && c->nz > 256) return fail(TC_ERR_SIZE, "16-row CN chunks need nz <= 256");
-  if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(TC_ERR_ARG, "ctas_per_sm must be 0 .. 32");
+  if (ctas_per_sm < -1 || ctas_per_sm > 32) return fail(TC_ERR_ARG, "ctas_per_sm must be -1 .. 32");
   if (cn_rows != b->cn_L || ctas_per_sm != b->ctas_per_sm) {
     b->cn_L = cn_rows;
     b->ctas_per_sm = ctas_per_sm;
@@ -1779,7 +1789,7 @@ extern "C" int tc_batch_use_graphs(tc_batch* b, int on) {
 template <class T> static constexpr int batch_cn_vec(int L) { return (L == 16 && sizeof(T) == 4) ? 2 : 1; }
 
 template <class T>
-static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int scheme, int L) {
+static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int scheme, int L, int Lr) {
   BMember<T> r;
   std::memset(&r, 0, sizeof(r));
   r.g = make_grid<T>(c);
@@ -1803,7 +1813,9 @@ static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int sche
   r.rgz = (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>();
   const int V = batch_cn_vec<T>(L);
   r.cgx = (c->nx * c->ny / V + 31) / 32;
+  r.cn_lr = Lr;
   r.xgx = c->ny / XROWS;
+  r.xpg = (c->nz + TC_BATCH_XP - 1) / TC_BATCH_XP;
   r.pgx = (c->nx / 2 + 31) / 32; r.pgy = (c->ny + 7) / 8; r.pgz = (c->nz + PROJ_PK - 1) / PROJ_PK;
   return r;
 }
@@ -1811,7 +1823,7 @@ static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int sche
 template <class T> static void batch_units(const BMember<T>& r, const tc_ctx* c, int cnt[BK_COUNT]) {
   cnt[BK_RHS] = r.rgx * r.rgy * r.rgz;
   cnt[BK_CN] = 3 * r.cgx;
-  cnt[BK_FX] = r.xgx * c->nz;
+  cnt[BK_FX] = r.xgx * r.xpg;
   cnt[BK_FY] = (r.nrows + 1) / 2;
   cnt[BK_TRI] = (2 * c->nxh * c->ny + 63) / 64;
   cnt[BK_IFX] = r.xgx * c->nz;
@@ -1823,6 +1835,10 @@ template <class T, class K> static int batch_grid(const tc_batch* b, K kernel, i
   int occ = 0;
   TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem));
   if (occ < 1) return fail(TC_ERR_SIZE, "ensemble kernel does not fit on an SM");
+  if (b->ctas_per_sm < 0) {  // one CTA per work unit: the hardware scheduler refills the SMs
+    *grid = std::max(1, total);
+    return TC_OK;
+  }
   const int per = b->ctas_per_sm ? std::min(occ, b->ctas_per_sm) : occ;
   *grid = std::max(1, std::min(total, per * b->nsm));
   return TC_OK;
@@ -1870,33 +1886,36 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   constexpr int VL16 = sizeof(T) == 4 ? 2 : 1;
   std::vector<BMember<T>> tab(3 * (size_t)n);
   int run[BK_COUNT] = {0, 0, 0, 0, 0, 0, 0};
-  int maxnz = 0, maxchunks = 0;
+  int maxnz = 0;
+  for (auto* c : b->m) maxnz = std::max(maxnz, c->nz);
+  // one CN block of cn_y chunk warps for every member: member chunks of
+  // ceil(nz / cn_y) <= L rows fill all of its warps
+  const int maxchunks = (maxnz + L - 1) / L;
   size_t fx = 0, ifx = 0;
   int fyt = 0;
   for (int i = 0; i < n; ++i) {
     tc_ctx* c = b->m[i];
-    if (c->cn_L_force != L) {  // the members' CN tables follow the ensemble's chunk length
-      c->cn_L_force = L;
+    const int Lr = (c->nz + maxchunks - 1) / maxchunks;
+    if (c->cn_L_force != Lr) {  // the member's CN tables follow its chunk length
+      c->cn_L_force = Lr;
       c->tab_dt = -1.0;
       drop_graph(c);
     }
     if (scheme == TC_IMEX && c->tab_dt != dts[i]) {
-      k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dts[i], c->top_neumann, L);
+      k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dts[i], c->top_neumann, Lr);
       TC_LAUNCHED();
       c->tab_dt = dts[i];
     }
     const int hist = scheme == TC_FE ? 0 : c->have_hist;
-    tab[i] = batch_record<T>(c, c->cur, dts[i], 1, scheme, L);
-    tab[n + i] = batch_record<T>(c, c->cur ^ 1, dts[i], 1, scheme, L);
-    tab[2 * n + i] = batch_record<T>(c, c->cur, dts[i], hist, scheme, L);
+    tab[i] = batch_record<T>(c, c->cur, dts[i], 1, scheme, L, Lr);
+    tab[n + i] = batch_record<T>(c, c->cur ^ 1, dts[i], 1, scheme, L, Lr);
+    tab[2 * n + i] = batch_record<T>(c, c->cur, dts[i], hist, scheme, L, Lr);
     int cnt[BK_COUNT];
     batch_units<T>(tab[i], c, cnt);
     for (int k = 0; k < BK_COUNT; ++k) {
       tab[i].u0[k] = tab[n + i].u0[k] = tab[2 * n + i].u0[k] = run[k];
       run[k] += cnt[k];
     }
-    maxnz = std::max(maxnz, c->nz);
-    maxchunks = std::max(maxchunks, (c->nz + L - 1) / L);
     for_each_n1(c->nx, [&](auto I) {
       constexpr int N1 = decltype(I)::value;
       fx = std::max(fx, fftx_reg_smem<N1>());
@@ -2010,7 +2029,7 @@ extern "C" int tc_batch_step(tc_batch* b, int scheme, const double* dts, int n_s
     if (!(dts[i] > 0)) return fail(TC_ERR_ARG, "dt must be > 0");
     if (c->body[0] || c->ke_acc || c->tape) return fail(TC_ERR_ARG, "ensemble launches take no adjoint hooks");
     if (b->valid && (b->dts[i] != dts[i] || c->cur != (b->cur0[i] ^ b->q))) rebuild = true;
-    if (scheme == TC_IMEX && (c->cn_L_force != b->cn_L || c->tab_dt != dts[i])) rebuild = true;
+    if (scheme == TC_IMEX && c->tab_dt != dts[i]) rebuild = true;
     lack = lack || (scheme != TC_FE && !c->have_hist);
   }
   if (lack && b->valid && b->q != 0) rebuild = true;
@@ -2047,7 +2066,7 @@ extern "C" int tc_batch_step(tc_batch* b, int scheme, const double* dts, int n_s
 
 extern "C" int tc_batch_info(tc_batch* b, int* shape, int* units, int* grids) {
   if (!b) return fail(TC_ERR_ARG, "null ensemble");
-  if (shape) { shape[0] = b->cn_L; shape[1] = b->ctas_per_sm; shape[2] = b->valid; }
+  if (shape) { shape[0] = b->cn_L; shape[1] = b->ctas_per_sm; shape[2] = b->valid; shape[3] = b->valid ? b->cn_y : 0; }
   for (int k = 0; k < BK_COUNT; ++k) {
     if (units) units[k] = b->valid ? b->total[k] : 0;
     if (grids) grids[k] = b->valid ? b->grid[k] : 0;

@@ -374,12 +374,15 @@ template <> struct CnVec<float, 2> {
     *reinterpret_cast<float2*>(p) = make_float2((float)o[0], (float)o[1]);
   }
 };
-// Column block bx of component comp (the block grid above); blockDim.y may
-// exceed the chunks of this system (ensemble kernel: the deepest member's
-// count), the extra warps only take part in the barriers.
-template <class T, int L, int VEC>
+// Column block bx of component comp (the block grid above), chunks of Lr <= L
+// rows (the tables' chunk length; L sizes the register windows; FIXED: Lr is
+// L, known at compile time); blockDim.y may exceed the chunks of this
+// system, the extra warps only take part in the barriers.
+template <class T, int L, int VEC, bool FIXED = false>
 __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, const CnTab& t,
-                                        const double* __restrict__ ubase, int nx, int ny, int nz, int bx, int comp) {
+                                        const double* __restrict__ ubase, int nx, int ny, int nz, int bx, int comp,
+                                        int Lr_arg) {
+  const int Lr = FIXED ? L : Lr_arg;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x, chunk = threadIdx.y, nchunk = blockDim.y;
   const int tid = chunk * 32 + lane, nthr = 32 * nchunk;
@@ -396,7 +399,7 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   const size_t plane = (size_t)ncols;
   T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + (colok ? col : 0);
   const int n = comp < 2 ? nz : nz - 1;
-  const int s0 = chunk * L, e0 = min(s0 + L, n);            // rows [s0, e0)
+  const int s0 = chunk * Lr, e0 = min(s0 + Lr, n);          // rows [s0, e0)
   const bool act = s0 < n;
   // window: stencil sources of rows s0..e0-1 = planes (u/v) or faces (w)
   // s0-1 .. e0; row m uses wv[m-s0], wv[m-s0+1], wv[m-s0+2]; the unknown of
@@ -406,7 +409,7 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
   for (int tt = 0; tt < L + 2; ++tt) {
     const int pl = s0 - 1 + tt;
-    if (act && colok && pl >= 0 && pl <= plmax) {
+    if (act && colok && pl >= 0 && pl <= plmax && tt < Lr + 2) {
       CnVec<T, VEC>::ld(q + (size_t)pl * plane, wv[tt]);
     } else {
 #pragma unroll
@@ -457,7 +460,7 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
   for (int c = 0; c < VEC; ++c) Din[c] = 0.0;
   for (int k = 0; k < chunk; ++k) {
-    const double g = G[min(k * L + L, n) - 1];
+    const double g = G[min(k * Lr + Lr, n) - 1];
 #pragma unroll
     for (int c = 0; c < VEC; ++c) Din[c] = bnd[(k * VEC + c) * 32 + lane] + g * Din[c];
   }
@@ -492,7 +495,7 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
   for (int c = 0; c < VEC; ++c) Xin[c] = 0.0;
   for (int k = nchunk - 1; k > chunk; --k) {
-    const int cs = k * L;
+    const int cs = k * Lr;
     if (cs < n) {
       const double h = H[cs];
 #pragma unroll
@@ -516,11 +519,11 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   }
 }
 
-template <class T, int L, int VEC, int MAXT>
+template <class T, int L, int VEC, int MAXT, bool FIXED>
 __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
                                                    CnTab t, const double* __restrict__ ubase, int nx, int ny,
-                                                   int nz) {
-  cn_tile<T, L, VEC>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z);
+                                                   int nz, int Lr) {
+  cn_tile<T, L, VEC, FIXED>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr);
 }
 
 // Scalars slot layout (FP64, device).

@@ -88,6 +88,13 @@ class ChannelBatch:
         except Exception:
             pass
 
+    def member_cn_rows(self, cn_rows=None):
+        """CN rows per chunk each member uses under the shape bound cn_rows
+        (default: the current shape)."""
+        L = cn_rows or self.info()["cn_rows"]
+        chunks = -(-max(c.nz for c in self.channels) // L)
+        return [-(-c.nz // chunks) for c in self.channels]
+
     def set_shape(self, cn_rows=16, ctas_per_sm=0):
         self.L.check(self.lib.tc_batch_set_shape(self.b, int(cn_rows), int(ctas_per_sm)))
 
@@ -103,10 +110,10 @@ class ChannelBatch:
                                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
     def info(self):
-        shape, units, grids = (ctypes.c_int * 3)(), (ctypes.c_int * 7)(), (ctypes.c_int * 7)()
+        shape, units, grids = (ctypes.c_int * 4)(), (ctypes.c_int * 7)(), (ctypes.c_int * 7)()
         self.L.check(self.lib.tc_batch_info(self.b, shape, units, grids))
         names = ["rhs", "cn", "fftx", "ffty", "tri", "ifftx", "proj"]
-        return {"cn_rows": shape[0], "ctas_per_sm": shape[1], "built": bool(shape[2]),
+        return {"cn_rows": shape[0], "ctas_per_sm": shape[1], "built": bool(shape[2]), "cn_chunks": shape[3],
                 "units": dict(zip(names, list(units))), "ctas": dict(zip(names, list(grids)))}
 
 
@@ -260,7 +267,7 @@ class Ensemble:
         current stream)."""
         self.batched.step(scheme, self.dts, n_steps)
 
-    def autotune_batch(self, steps=8, repeats=2, rows=(16, 32), ctas=(0, 1, 2, 4)):
+    def autotune_batch(self, steps=8, repeats=2, rows=(16, 32), ctas=(-1, 0, 2)):
         """Time every (CN rows per chunk, persistent CTAs per SM) shape of the
         ensemble launches over `steps` steps (best of `repeats`), keep the
         fastest, and restore every member's state, history and forcing.
@@ -293,6 +300,37 @@ class Ensemble:
         self.batch_tuning = {"cn_rows": best[0], "ctas_per_sm": best[1],
                              "ms_per_step": {f"cn{k[0]}/ctas{k[1]}": v for k, v in times.items()}}
         return self.batch_tuning
+
+    def autotune_mode(self, steps=8, repeats=2):
+        """Choose between the ensemble launches (tuned shape) and per-member
+        launches on per-member streams (one graph, tuned member shapes): time
+        both over `steps` steps and keep the faster as ``self.mode``
+        ("batch" or "streams"), restoring every member's state.  Returns the
+        two step times (ms)."""
+        import torch
+        saved = [self._save(ch) for ch in self.channels]
+        if getattr(self, "batched", None) is None:
+            self.batch()
+        self.autotune_batch(steps=steps, repeats=repeats)
+        times = {"batch": min(self.batch_tuning["ms_per_step"].values())}
+        for ch, sv in zip(self.channels, saved):
+            self._restore(ch, sv)
+        self.autotune(steps=steps, repeats=repeats)
+        self.capture()
+        ms = []
+        for _ in range(repeats):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.step_graph(max(1, steps // 2))
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1) / (2 * max(1, steps // 2)))
+        times["streams"] = min(ms)
+        for ch, sv in zip(self.channels, saved):
+            self._restore(ch, sv)
+        torch.cuda.synchronize()
+        self.mode = min(times, key=times.get)
+        return times
 
     def diagnostics(self):
         import torch
