@@ -655,8 +655,10 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
     for (int b = 0; b < TRIP_B; ++b) {
       const int k = k0 + b;
       if (k < nz) {
+        // d'_k = (d_k - a_k d'_{k-1}) rden_k with the products formed off the
+        // recurrence: one dependent FMA per level
         const double a = (k == 0) ? 0.0 : tb.cl[k];
-        dp = (dc[b] - a * dp) * fc[b];
+        dp = fma(-(a * fc[b]), dp, dc[b] * fc[b]);
         col[(size_t)k * st2] = dp;
       }
     }

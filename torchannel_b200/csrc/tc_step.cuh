@@ -443,7 +443,9 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
         for (int c = 0; c < VEC; ++c) {
           const double sm = (double)wv[tt][c] + bm, sc = (double)wv[tt + 1][c] + bc, sp = (double)wv[tt + 2][c] + bp;
-          yp[c] = fma(ea, sm, fma(eb, sc, fma(ec, sp, f * yp[c])));
+          // the explicit part first: one dependent FMA per row on the recurrence
+          const double E = fma(ea, sm, fma(eb, sc, ec * sp));
+          yp[c] = fma(f, yp[c], E);
           y[tt][c] = yp[c];
         }
         bm = bc; bc = bp;
