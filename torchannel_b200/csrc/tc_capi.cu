@@ -172,6 +172,7 @@ static size_t carve(tc_ctx* c, char* base) {
   c->tab.uv = cv.take<double>(8 * c->nz * 8);
   c->tab.w = cv.take<double>(8 * c->nz * 8);
   c->tab.beta = cv.take<double>(8);
+  c->tab.corr = cv.take<double>(c->nz * 8);
   const int gx = (c->nx + 31) / 32, gy = (c->ny + 7) / 8;
   c->npart = gx * gy * (c->nz + 1);
   c->partials = cv.take<double>((size_t)c->npart * 8);
@@ -733,7 +734,8 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   dim3 blk(RHS_TX, rhs_ty<T>());
   dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>(), (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (scheme == TC_IMEX && c->tab_dt != dt) {
-    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c));
+    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c),
+                                 ubase_of(c));
     c->tab_dt = dt;
   }
   mark(c, TC_PH_RHS, s);
@@ -888,6 +890,7 @@ extern "C" int tc_set_state(tc_ctx* c, const double* u, const double* v, const d
   TC_CUDA(cudaMemsetAsync(c->p, 0, (size_t)c->nx * c->ny * c->nz * 8, ST(stream)));
   c->have_hist = 0;
   c->state_set = 1;
+  if (c->precision == TC_MIXED) c->tab_dt = -1.0;  // the CN tables carry the new base profile
   return TC_OK;
 }
 
@@ -1126,7 +1129,8 @@ extern "C" int tc_explicit_rhs(tc_ctx* c, int full, double* ru, double* rv, doub
 template <class T> static int cn_hook_impl(tc_ctx* c, double dt, cudaStream_t s) {
   T** A = (T**)c->st[c->cur];
   if (c->tab_dt != dt) {
-    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c));
+    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c),
+                                 ubase_of(c));
     c->tab_dt = dt;
   }
   launch_cn<T>(c, A[0], A[1], A[2], s);
@@ -1902,7 +1906,8 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
       drop_graph(c);
     }
     if (scheme == TC_IMEX && c->tab_dt != dts[i]) {
-      k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dts[i], c->top_neumann, Lr);
+      k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dts[i], c->top_neumann, Lr,
+                                   ubase_of(c));
       TC_LAUNCHED();
       c->tab_dt = dts[i];
     }

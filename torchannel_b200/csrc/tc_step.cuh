@@ -254,9 +254,10 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, 
 // after cn_fold, a holds f and cA, cB, cC the folded coefficients.
 // ---------------------------------------------------------------------------
 struct CnTab {
-  double* uv;  // 8*nz
-  double* w;   // 8*nz (first nz-1 rows used)
+  double* uv;    // 8*nz
+  double* w;     // 8*nz (first nz-1 rows used)
   double* beta;
+  double* corr;  // nz: S(U0) - U0 of the u system (FP32-arithmetic sweeps of u - U0)
 };
 
 __device__ __forceinline__ void cn_chunk_products(double* a, double* iv, double* cp, double* G, double* H, int n,
@@ -287,7 +288,7 @@ __device__ __forceinline__ void cn_fold(double* a, const double* iv, double* cA,
 }
 
 __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const double* __restrict__ dzc, int nz,
-                            double nu, double dt, int top_neumann, int L) {
+                            double nu, double dt, int top_neumann, int L, const double* __restrict__ ubase) {
   const double theta = 0.5;
   const double alpha = theta * dt * nu;
   const int sys = threadIdx.x;
@@ -319,6 +320,23 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
     cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz, L);
     *t.beta = (1.0 - theta) * dt * nu;
     cn_fold(a, iv, cA, cB, cC, nz, (1.0 - theta) * dt * nu, false);
+    // CN image of the base profile minus itself (zero without a base):
+    // unchunked sweeps with the folded rows, FP64
+    if (ubase) {
+      double dp = 0.0;
+      for (int m = 0; m < nz; ++m) {
+        const double sm = m > 0 ? ubase[m - 1] : 0.0, sp = m + 1 < nz ? ubase[m + 1] : 0.0;
+        dp = a[m] * dp + (cA[m] * sm + cB[m] * ubase[m] + cC[m] * sp);
+        t.corr[m] = dp;
+      }
+      double x = 0.0;
+      for (int m = nz - 1; m >= 0; --m) {
+        x = t.corr[m] - cp[m] * x;
+        t.corr[m] = x - ubase[m];
+      }
+    } else {
+      for (int m = 0; m < nz; ++m) t.corr[m] = 0.0;
+    }
   } else if (sys == 1) {
     const int n = nz - 1;
     double* a = t.w; double* iv = a + nz; double* cp = iv + nz;
@@ -359,21 +377,28 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
 template <class T, int VEC> struct CnVec;
 template <> struct CnVec<double, 1> {
   static __device__ __forceinline__ void ld(const double* p, double (&o)[1]) { o[0] = *p; }
-  static __device__ __forceinline__ void st(double* p, const double (&o)[1]) { *p = o[0]; }
+  template <class A> static __device__ __forceinline__ void st(double* p, const A (&o)[1]) { *p = (double)o[0]; }
 };
 template <> struct CnVec<float, 1> {
   static __device__ __forceinline__ void ld(const float* p, float (&o)[1]) { o[0] = *p; }
-  static __device__ __forceinline__ void st(float* p, const double (&o)[1]) { *p = (float)o[0]; }
+  template <class A> static __device__ __forceinline__ void st(float* p, const A (&o)[1]) { *p = (float)o[0]; }
 };
 template <> struct CnVec<float, 2> {
   static __device__ __forceinline__ void ld(const float* p, float (&o)[2]) {
     const float2 x = *reinterpret_cast<const float2*>(p);
     o[0] = x.x; o[1] = x.y;
   }
-  static __device__ __forceinline__ void st(float* p, const double (&o)[2]) {
+  template <class A> static __device__ __forceinline__ void st(float* p, const A (&o)[2]) {
     *reinterpret_cast<float2*>(p) = make_float2((float)o[0], (float)o[1]);
   }
 };
+// Arithmetic of the sweeps: FP64 for FP64 storage; FP32 for FP32 storage,
+// where u is solved as its stored deviation u - U0 (the system is linear:
+// S(u' + U0) - U0 = S(u') + (S(U0) - U0), the last column tabulated in FP64
+// by k_cn_tables as CnTab::corr) so that no FP32 sum carries the O(1) base.
+template <class T> struct CnArith { using type = double; };
+template <> struct CnArith<float> { using type = float; };
+
 // Column block bx of component comp (the block grid above), chunks of Lr <= L
 // rows (the tables' chunk length; L sizes the register windows; FIXED: Lr is
 // L, known at compile time); blockDim.y may exceed the chunks of this
@@ -382,16 +407,19 @@ template <class T, int L, int VEC, bool FIXED = false>
 __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, const CnTab& t,
                                         const double* __restrict__ ubase, int nx, int ny, int nz, int bx, int comp,
                                         int Lr_arg) {
+  using A = typename CnArith<T>::type;
+  constexpr bool F32 = sizeof(A) == 4;
   const int Lr = FIXED ? L : Lr_arg;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x, chunk = threadIdx.y, nchunk = blockDim.y;
   const int tid = chunk * 32 + lane, nthr = 32 * nchunk;
-  double* tab = reinterpret_cast<double*>(smraw);           // 8*nz
-  double* shb = tab + 8 * nz;                                // nz (base, u only)
-  double* bnd = shb + nz;                                    // 2 * nchunk * 32 * VEC
+  A* tab = reinterpret_cast<A*>(smraw);                      // 8*nz
+  A* shb = tab + 8 * nz;                                     // nz: base (FP64) or its CN correction (FP32), u only
+  A* bnd = shb + nz;                                         // 2 * nchunk * 32 * VEC
   const double* src = comp == 2 ? t.w : t.uv;
-  for (int e = tid; e < 8 * nz; e += nthr) tab[e] = src[e];
-  for (int e = tid; e < nz; e += nthr) shb[e] = (comp == 0 && ubase) ? ubase[e] : 0.0;
+  for (int e = tid; e < 8 * nz; e += nthr) tab[e] = (A)src[e];
+  for (int e = tid; e < nz; e += nthr)
+    shb[e] = (comp == 0 && ubase) ? (A)(F32 ? t.corr[e] : ubase[e]) : A(0);
   // nx*ny is even, so with VEC = 2 a pair of columns is valid as a whole
   const int col = (bx * 32 + lane) * VEC;
   const int ncols = nx * ny;
@@ -417,34 +445,39 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
     }
   }
   __syncthreads();  // tables staged
-  const double* a = tab; const double* iv = a + nz; const double* cp = iv + nz;
-  const double* cA = cp + nz; const double* cB = cA + nz; const double* cC = cB + nz;
-  const double* G = cC + nz; const double* H = G + nz;
-  // base profile of window entry tt (u/v planes in range; zero for w)
-  auto wb = [&](int tt) -> double {
-    const int pl = s0 - 1 + tt;
-    return (comp < 2 && pl >= 0 && pl < nz) ? shb[pl] : 0.0;
+  const A* a = tab; const A* iv = a + nz; const A* cp = iv + nz;
+  const A* cA = cp + nz; const A* cB = cA + nz; const A* cC = cB + nz;
+  const A* G = cC + nz; const A* H = G + nz;
+  (void)iv;
+  // base profile of window entry tt (FP64 sweeps of u: planes in range; else 0)
+  auto wb = [&](int tt) -> A {
+    if constexpr (F32) {
+      return A(0);
+    } else {
+      const int pl = s0 - 1 + tt;
+      return (comp < 2 && pl >= 0 && pl < nz) ? shb[pl] : A(0);
+    }
   };
-  double y[L][VEC];
-  double yend[VEC];
+  A y[L][VEC];
+  A yend[VEC];
 #pragma unroll
-  for (int c = 0; c < VEC; ++c) yend[c] = 0.0;
+  for (int c = 0; c < VEC; ++c) yend[c] = A(0);
   if (act) {
-    double yp[VEC];
+    A yp[VEC];
 #pragma unroll
-    for (int c = 0; c < VEC; ++c) yp[c] = 0.0;
-    double bm = wb(0), bc = wb(1);
+    for (int c = 0; c < VEC; ++c) yp[c] = A(0);
+    A bm = wb(0), bc = wb(1);
 #pragma unroll
     for (int tt = 0; tt < L; ++tt) {
       const int m = s0 + tt;
       if (m < e0) {
-        const double bp = wb(tt + 2);
-        const double f = a[m], ea = cA[m], eb = cB[m], ec = cC[m];
+        const A bp = wb(tt + 2);
+        const A f = a[m], ea = cA[m], eb = cB[m], ec = cC[m];
 #pragma unroll
         for (int c = 0; c < VEC; ++c) {
-          const double sm = (double)wv[tt][c] + bm, sc = (double)wv[tt + 1][c] + bc, sp = (double)wv[tt + 2][c] + bp;
+          const A sm = (A)wv[tt][c] + bm, sc = (A)wv[tt + 1][c] + bc, sp = (A)wv[tt + 2][c] + bp;
           // the explicit part first: one dependent FMA per row on the recurrence
-          const double E = fma(ea, sm, fma(eb, sc, ec * sp));
+          const A E = fma(ea, sm, fma(eb, sc, ec * sp));
           yp[c] = fma(f, yp[c], E);
           y[tt][c] = yp[c];
         }
@@ -458,27 +491,27 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   for (int c = 0; c < VEC; ++c) bnd[(chunk * VEC + c) * 32 + lane] = yend[c];
   __syncthreads();
   // true d' entering this chunk: scan the chunk ends below it
-  double Din[VEC];
+  A Din[VEC];
 #pragma unroll
-  for (int c = 0; c < VEC; ++c) Din[c] = 0.0;
+  for (int c = 0; c < VEC; ++c) Din[c] = A(0);
   for (int k = 0; k < chunk; ++k) {
-    const double g = G[min(k * Lr + Lr, n) - 1];
+    const A g = G[min(k * Lr + Lr, n) - 1];
 #pragma unroll
     for (int c = 0; c < VEC; ++c) Din[c] = bnd[(k * VEC + c) * 32 + lane] + g * Din[c];
   }
-  double zstart[VEC];
+  A zstart[VEC];
 #pragma unroll
-  for (int c = 0; c < VEC; ++c) zstart[c] = 0.0;
+  for (int c = 0; c < VEC; ++c) zstart[c] = A(0);
   if (act) {
     // backward from a zero value beyond the chunk end, with the d' shift
-    double zn[VEC];
+    A zn[VEC];
 #pragma unroll
-    for (int c = 0; c < VEC; ++c) zn[c] = 0.0;
+    for (int c = 0; c < VEC; ++c) zn[c] = A(0);
 #pragma unroll
     for (int tt = L - 1; tt >= 0; --tt) {
       const int m = s0 + tt;
       if (m < e0) {
-        const double g = G[m], cpm = cp[m];
+        const A g = G[m], cpm = cp[m];
 #pragma unroll
         for (int c = 0; c < VEC; ++c) {
           zn[c] = (y[tt][c] + g * Din[c]) - cpm * zn[c];
@@ -493,13 +526,13 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   for (int c = 0; c < VEC; ++c) bnd[((nchunk + chunk) * VEC + c) * 32 + lane] = zstart[c];
   __syncthreads();
   // true x just beyond this chunk: scan the chunk starts above it
-  double Xin[VEC];
+  A Xin[VEC];
 #pragma unroll
-  for (int c = 0; c < VEC; ++c) Xin[c] = 0.0;
+  for (int c = 0; c < VEC; ++c) Xin[c] = A(0);
   for (int k = nchunk - 1; k > chunk; --k) {
     const int cs = k * Lr;
     if (cs < n) {
-      const double h = H[cs];
+      const A h = H[cs];
 #pragma unroll
       for (int c = 0; c < VEC; ++c) Xin[c] = bnd[((nchunk + k) * VEC + c) * 32 + lane] + h * Xin[c];
     }
@@ -509,11 +542,11 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
     for (int tt = 0; tt < L; ++tt) {
       const int m = s0 + tt;
       if (m < e0) {
-        const double h = H[m];
-        const double bs = comp < 2 ? shb[m] : 0.0;
-        double o[VEC];
+        const A h = H[m];
+        const A bs = comp < 2 ? shb[m] : A(0);
+        A o[VEC];
 #pragma unroll
-        for (int c = 0; c < VEC; ++c) o[c] = (y[tt][c] + h * Xin[c]) - bs;
+        for (int c = 0; c < VEC; ++c) o[c] = F32 ? (y[tt][c] + h * Xin[c]) + bs : (y[tt][c] + h * Xin[c]) - bs;
         const int pl = comp < 2 ? m : m + 1;
         CnVec<T, VEC>::st(q + (size_t)pl * plane, o);
       }
