@@ -105,6 +105,21 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
       hyx[q][0] = hy; hyx[q][1] = hx;
     }
   }
+  // AB2 history and the stored u of this thread's points, loaded with the
+  // staging so that their latency overlaps it; one plane consumed per
+  // iteration (shifted down)
+  T pf_ru[RHS_KB], pf_rv[RHS_KB], pf_rw[RHS_KB], pf_u[RHS_KB];
+#pragma unroll
+  for (int q = 0; q < RHS_KB; ++q) {
+    const int k = kb + q;
+    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+    const bool cell = active && k < nz, face = active && k >= 1 && k <= nz - 1;
+    const bool hist = UPD == UPD_AB2 && have_hist;
+    pf_ru[q] = (cell && hist) ? ru[o] : T(0);
+    pf_rv[q] = (cell && hist) ? rv[o] : T(0);
+    pf_rw[q] = (face && hist) ? rw[o] : T(0);
+    pf_u[q] = (cell && base && UPD != UPD_RHS_ONLY) ? ldg(u + o) : T(0);
+  }
   // stage planes p = kb-1 .. kb+RHS_KB into slots 0 .. RHS_NS-1
 #pragma unroll
   for (int sl = 0; sl < RHS_NS; ++sl) {
@@ -158,13 +173,13 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
         if (UPD == UPD_RHS_ONLY) {
           ru[o] = r;
         } else {
-          const T Uraw = base ? ldg(u + o) : U0;  // stored value (u - U0[k] in mixed precision)
+          const T Uraw = base ? pf_u[0] : U0;  // stored value (u - U0[k] in mixed precision)
           if (UPD == UPD_FE) {
             T q = Uraw + dt * r;
             us[o] = q + dt * T(1);
           } else {
             r += forcing;
-            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * ru[o]) : Uraw + dt * r;
+            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * pf_ru[0]) : Uraw + dt * r;
             ru[o] = r;
           }
         }
@@ -193,7 +208,7 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
         } else if (UPD == UPD_FE) {
           vs[o] = V0 + dt * r;
         } else {
-          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * rv[o]) : V0 + dt * r;
+          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * pf_rv[0]) : V0 + dt * r;
           rv[o] = r;
         }
       }
@@ -218,11 +233,14 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
       } else if (UPD == UPD_FE) {
         ws[o] = W0 + dt * r;
       } else {
-        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * rw[o]) : W0 + dt * r;
+        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * pf_rw[0]) : W0 + dt * r;
         rw[o] = r;
       }
     }
-
+#pragma unroll
+    for (int q = 0; q + 1 < RHS_KB; ++q) {
+      pf_ru[q] = pf_ru[q + 1]; pf_rv[q] = pf_rv[q + 1]; pf_rw[q] = pf_rw[q + 1]; pf_u[q] = pf_u[q + 1];
+    }
   }
 }
 
@@ -635,31 +653,77 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
     // p of the plane below k0 for w's face k0 (walls excluded below)
     double2 Pm = make_double2(0.0, 0.0);
     if (k0 >= 1) Pm = *reinterpret_cast<const double2*>(p + pidx(k0 - 1, j, i, ny, nx));
-#pragma unroll
-    for (int kk = 0; kk < PROJ_PK; ++kk) {
-      const int k = k0 + kk;
-      if (k < nz) {
+    if constexpr (sizeof(T) == 4) {
+      // FP32 storage: the next plane's loads are issued before this plane's
+      // stores (the FP64 form has no registers to spare for it)
+      struct Ld { double2 P, Py; double P2; V2 uu, vv, ww; };
+      auto load = [&](int k) {
+        Ld l;
         const size_t o = pidx(k, j, i, ny, nx);
-        const double2 P = *reinterpret_cast<const double2*>(p + o);
-        const double P2 = ldg(p + pidx(k, j, ipp, ny, nx));
-        const double2 Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
-        V2 uu = *reinterpret_cast<V2*>(u + o);
-        V2 vv = *reinterpret_cast<V2*>(v + o);
-        uu.x = (T)((double)uu.x - cx * (P.y - P.x));
-        uu.y = (T)((double)uu.y - cx * (P2 - P.y));
-        vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
-        vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
-        *reinterpret_cast<V2*>(u + o) = uu;
-        *reinterpret_cast<V2*>(v + o) = vv;
-        acc += ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
-        if (k >= 1) {
-          const double cz = dt * (double)g.idzc[k];
-          V2 ww = *reinterpret_cast<V2*>(w + o);
-          ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
-          ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
-          *reinterpret_cast<V2*>(w + o) = ww;
+        l.P = *reinterpret_cast<const double2*>(p + o);
+        l.P2 = ldg(p + pidx(k, j, ipp, ny, nx));
+        l.Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
+        l.uu = *reinterpret_cast<const V2*>(u + o);
+        l.vv = *reinterpret_cast<const V2*>(v + o);
+        l.ww = *reinterpret_cast<const V2*>(w + o);
+        return l;
+      };
+      Ld cur = load(min(k0, nz - 1));
+#pragma unroll
+      for (int kk = 0; kk < PROJ_PK; ++kk) {
+        const int k = k0 + kk;
+        if (k < nz) {
+          Ld nxt = cur;
+          if (kk + 1 < PROJ_PK && k + 1 < nz) nxt = load(k + 1);
+          const size_t o = pidx(k, j, i, ny, nx);
+          const double2 P = cur.P, Py = cur.Py;
+          const double P2 = cur.P2;
+          V2 uu = cur.uu, vv = cur.vv;
+          uu.x = (T)((double)uu.x - cx * (P.y - P.x));
+          uu.y = (T)((double)uu.y - cx * (P2 - P.y));
+          vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
+          vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
+          *reinterpret_cast<V2*>(u + o) = uu;
+          *reinterpret_cast<V2*>(v + o) = vv;
+          acc += ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
+          if (k >= 1) {
+            const double cz = dt * (double)g.idzc[k];
+            V2 ww = cur.ww;
+            ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
+            ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
+            *reinterpret_cast<V2*>(w + o) = ww;
+          }
+          Pm = P;
+          cur = nxt;
         }
-        Pm = P;
+      }
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < PROJ_PK; ++kk) {
+        const int k = k0 + kk;
+        if (k < nz) {
+          const size_t o = pidx(k, j, i, ny, nx);
+          const double2 P = *reinterpret_cast<const double2*>(p + o);
+          const double P2 = ldg(p + pidx(k, j, ipp, ny, nx));
+          const double2 Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
+          V2 uu = *reinterpret_cast<V2*>(u + o);
+          V2 vv = *reinterpret_cast<V2*>(v + o);
+          uu.x = (T)((double)uu.x - cx * (P.y - P.x));
+          uu.y = (T)((double)uu.y - cx * (P2 - P.y));
+          vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
+          vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
+          *reinterpret_cast<V2*>(u + o) = uu;
+          *reinterpret_cast<V2*>(v + o) = vv;
+          acc += ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
+          if (k >= 1) {
+            const double cz = dt * (double)g.idzc[k];
+            V2 ww = *reinterpret_cast<V2*>(w + o);
+            ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
+            ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
+            *reinterpret_cast<V2*>(w + o) = ww;
+          }
+          Pm = P;
+        }
       }
     }
   }
