@@ -9,10 +9,10 @@ Workload (one "step" = one IMEX time step of the channel):
 Metric: grid-point-steps/s = nx*ny*nz*steps / seconds (whole job, all ranks).
 
 Arms:
-  default           this repo's CUDA path, mixed precision (FP32 velocity fields
-                    and history; FP64 Poisson, tridiagonal arithmetic, bulk
-                    forcing); the plain FP64 form is timed in the same run as
-                    "fp64_plain" (--precision fp64 makes it the headline)
+  default           this repo's CUDA path, mixed precision (FP32 velocity fields,
+                    history, stencils and CN sweeps; FP64 Poisson, CN tables,
+                    bulk forcing); the plain FP64 form is timed in the same run
+                    as "fp64_plain" (--precision fp64 makes it the headline)
   --impl reference  the CPU oracle (numpy FP64 restatement of the reference
                     step, oracle/) on the host cores, bounded sample
 
