@@ -34,8 +34,9 @@ class _DevArray:
 class Channel:
     """One channel on the current CUDA device.
 
-    precision: "fp64" (plain) or "mixed" (FP32 fields, FP64 tridiagonal
-    arithmetic, bulk forcing and statistics sums).
+    precision: "fp64" (plain) or "mixed" (FP32 fields, stencils and CN
+    sweeps of the deviation from the base profile; FP64 Poisson solve, CN
+    tables, bulk forcing and statistics sums).
     rhs_path: "separate" (reference CPU-path semantics, default) or "fused"
     (reference CUDA-path semantics for the duplicate planes u[nx], v[:, ny]).
     """
