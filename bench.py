@@ -51,10 +51,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "ensemble", "poisson", "adjoint"],
+    ap.add_argument("--run-steps", type=int, default=2000, help="steps of --workload config1")
+    ap.add_argument("--workload", default="step", choices=["step", "ensemble", "poisson", "adjoint", "config1"],
                     help="step: the headline IMEX step; ensemble: 16 uneven channels (config 4); "
                          "poisson: the FFT Poisson solve alone at 192x192x128 and 384x384x256 (config 2); "
-                         "adjoint: gradient of a time-averaged kinetic energy, 96x96x64, 200 steps (config 3)")
+                         "adjoint: gradient of a time-averaged kinetic energy, 96x96x64, 200 steps (config 3); "
+                         "config1: the 2000-step run of config 1 through the drop-in solver, FP64 and mixed")
     ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--adjoint-mode", default="auto", choices=["auto", "store", "recompute"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
@@ -665,6 +667,80 @@ def run_adjoint(a):
             "fd_rel_errors": errs, "fd_max_rel_error": max(errs), "fd_eps": eps}), flush=True)
 
 
+def run_config1(a):
+    """Config 1 as a run: 192x192x128, seeded laminar + 0.1 noise, adaptive dt
+    (CFL 0.25, every 10 steps, the 5% rule), --run-steps IMEX steps,
+    statistics every 200 steps from t = 0, diagnostics every 100 steps,
+    through ChannelFlowB200.run_simulation, once in plain FP64 and once in
+    mixed precision.  Throughput is grid points x steps / wall time of the
+    step loop (host loop, dt updates, diagnostics and statistics included;
+    the final field files excluded).  The two runs' statistics are compared
+    at the end."""
+    import shutil
+    import tempfile
+    import torch
+    import yaml
+    from torchannel_b200.solver import ChannelFlowB200
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    out = {}
+    tmp = tempfile.mkdtemp(prefix="tc_config1_")
+    try:
+        for prec in ("fp64", "mixed"):
+            res = os.path.join(tmp, prec)
+            cfg = {
+                "grid": {"nx": NX, "ny": NY, "nz": NZ},
+                "domain": {"Lx": float(LX), "Ly": float(LY), "Lz": float(LZ), "stretching_type": "symmetric"},
+                "flow": {"Re": RE, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": GAMMA},
+                "boundary_conditions": {"top_wall": {"type": "dirichlet"}},
+                "initialization": {"type": "parabolic", "perturbation_intensity": 0.1},
+                "solver": {"type": "fft"},
+                "time": {"dt": 0.002, "n_steps": a.run_steps, "CFL_target": CFL, "dt_update_interval": 10,
+                         "dt_max": DT_MAX, "dt_min": DT_MIN, "scheme": "IMEX"},
+                "compute": {"device": "cuda", "precision": prec},
+                "output": {"results_folder": res, "n_out": 100, "n_save": a.run_steps + 1},
+                "statistics": {"n_stats": 200, "t_stats": 0.0, "z_plus_target": 15.0},
+            }
+            os.makedirs(res, exist_ok=True)
+            path = os.path.join(res, "config.yaml")
+            with open(path, "w") as f:
+                yaml.safe_dump(cfg, f)
+            cf = ChannelFlowB200(path, seed=0, verbose=False)
+            torch.cuda.synchronize()
+            cf.run_simulation()
+            torch.cuda.synchronize()
+            st = cf.turbulence_stats.finalize_statistics()
+            d = cf.ch.diagnostics()
+            out[prec] = {"seconds": cf.loop_seconds, "value": NX * NY * NZ * a.run_steps / cf.loop_seconds,
+                         "time": cf.time, "final_dt": cf.dt, "max_div": d["max_div"], "u_bulk": d["u_bulk"],
+                         "u_tau_stats": st["u_tau"], "n_samples": int(st["n_samples"]), "stats": st}
+            del cf
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    f64, mix = out["fp64"]["stats"], out["mixed"]["stats"]
+
+    def rel(k):
+        return float(np.max(np.abs(mix[k] - f64[k])) / max(np.max(np.abs(f64[k])), 1e-300))
+    m, d64 = out["mixed"], out["fp64"]
+    line = {"metric": f"grid-point-steps/s, config 1 run ({a.run_steps} IMEX steps, adaptive dt, statistics)",
+            "value": m["value"], "unit": "grid-point-steps/s", "n_gpus": 1, "steps": a.run_steps, "warmup": 0,
+            "ms_per_step": m["seconds"] / a.run_steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded laminar profile + 0.1 uniform noise)",
+            "config": {"workload": "config 1 run through ChannelFlowB200.run_simulation", "nx": NX, "ny": NY,
+                       "nz": NZ, "cfl": CFL, "dt_update_interval": 10, "n_stats": 200},
+            "fp64_plain": {k: d64[k] for k in ("value", "seconds", "time", "final_dt", "max_div", "u_bulk",
+                                                "u_tau_stats", "n_samples")},
+            "mixed": {k: m[k] for k in ("seconds", "time", "final_dt", "max_div", "u_bulk", "u_tau_stats",
+                                         "n_samples")},
+            "mixed_speedup_over_fp64": m["value"] / d64["value"],
+            "stats_rel_diff_mixed_vs_fp64": {k: rel(k) for k in ("U_mean", "uu_mean", "vv_mean", "ww_mean",
+                                                                  "uw_mean", "E_uu_2d")},
+            "u_tau_rel_diff": abs(m["u_tau_stats"] - d64["u_tau_stats"]) / d64["u_tau_stats"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -673,6 +749,8 @@ def main():
         run_ensemble(a)
     elif a.workload == "poisson":
         run_poisson(a)
+    elif a.workload == "config1":
+        run_config1(a)
     elif a.workload == "adjoint":
         run_adjoint(a)
     else:
