@@ -269,7 +269,7 @@ def run_b200(a):
         "data": "synthetic (seeded laminar profile + 0.1 uniform noise, projected)",
         "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "scheme": "IMEX",
                    "precision": a.precision, "dt": dt, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (state + history > 126 MB)"},
+                   "l2": "inputs larger than L2 (a step touches both state buffers, the history, the spectrum and p: > 126 MB)"},
         "roofline": roof, "step_roofline": step_roof, "kernels": kern,
         "cpu_baseline": cpu, "e2e": e2e,
         "clocks": clk.summary(),
