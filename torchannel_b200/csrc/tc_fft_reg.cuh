@@ -164,6 +164,20 @@ __device__ __forceinline__ void rowfft_pass1(LD ld, int n2, cpx<double>* tile, c
   }
 }
 
+// Pass 1 on values already in registers: v[n1] = x[N2 n1 + n2].
+template <int N1, bool INV>
+__device__ __forceinline__ void rowfft_pass1_regs(cpx<double> (&v)[N1], int n2, cpx<double>* tile,
+                                                  const cpx<double>* __restrict__ tw) {
+  using RF = RowFft<N1>;
+  Dft<N1, INV>::run(v);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    cpx<double> w = tw[n2 * k1];
+    if (INV) w.y = -w.y;
+    tile[k1 * RF::TP + n2] = k1 == 0 ? v[0] : cmul(v[k1], w);
+  }
+}
+
 // Pass 2 for lane k1: b[n2] = tile[k1 * TP + n2] -> DFT_16; `st(e, val)`
 // receives element e = k1 + N1 k2 of the transformed row.
 template <int N1, bool INV, class ST>

@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(256) k_ffty(cpx<double>* __restrict__ X, int n
 
 // In-place complex FFT along y of the rows X[kx][k][:] with the register
 // transform (ny = N1 * 16): RowFft<N1>::RPW rows per warp, each row read and
-// written once, no block barrier; warps stride over the rows.
+// written once, no block barrier; warps stride over the rows, loading the
+// next rows while transforming the current ones.
 // Rows row0 .. row0+RPW-1 (< nrows) by one warp, as one pass of the
 // k_ffty_reg loop below; `tiles` holds the warp's RPW transpose tiles.
 template <int N1, bool INV>
@@ -137,14 +138,31 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
   const int wpb = blockDim.x >> 5;
   cpx<double>* tile = reinterpret_cast<cpx<double>*>(smraw) + (size_t)(warp * RF::RPW + sub) * RF::TILE;
   const int rstep = gridDim.x * wpb * RF::RPW;
-  for (int row0 = (blockIdx.x * wpb + warp) * RF::RPW; row0 < nrows; row0 += rstep) {
+  // the next rows' values are loaded before this row's transform
+  const bool lane_ld = sub < RF::RPW && l < RF::N2;
+  int row0 = (blockIdx.x * wpb + warp) * RF::RPW;
+  cpx<double> v[N1];
+  auto ldrow = [&](int r0, cpx<double> (&o)[N1]) {
+    const int row = r0 + sub;
+    if (lane_ld && row < nrows) {
+      const cpx<double>* x = X + (size_t)row * RF::N;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) o[n1] = x[RF::N2 * n1 + l];
+    }
+  };
+  ldrow(row0, v);
+  for (; row0 < nrows; row0 += rstep) {
     const int row = row0 + sub;
     const bool ok = sub < RF::RPW && row < nrows;
     cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
-    if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
+    cpx<double> vn[N1];
+    ldrow(row0 + rstep, vn);
+    if (ok && l < RF::N2) rowfft_pass1_regs<N1, INV>(v, l, tile, twy);
     __syncwarp();
     if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
     __syncwarp();
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = vn[n1];
   }
 }
 
