@@ -270,8 +270,7 @@ template <int N1> static size_t fftx_reg_smem() {
   return (size_t)(XROWS / 2) * ((RowFft<N1>::TILE + 7) / 8 * 8 + 1) * sizeof(cpx<double>);
 }
 template <int N1> static size_t ifftx_reg_smem() {
-  constexpr int NH = RowFft<N1>::N / 2 + 1;
-  return ((size_t)XROWS * ((NH + 7) / 8 * 8 + 1) + (size_t)(XROWS / 2) * RowFft<N1>::TILE) * sizeof(cpx<double>);
+  return (size_t)XROWS * ifftx_pitch<N1>() * sizeof(cpx<double>);
 }
 template <int N1> static int xreg_threads() { return 16 * XROWS / RowFft<N1>::RPW; }
 template <int N1> static size_t ffty_reg_smem() {

@@ -250,15 +250,21 @@ __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid
 // register transform (nx = N1 * 16); writes p[k][j][i] (FP64).  Two rows
 // travel as one complex row Z = A + i B built from the half spectra (DC and
 // Nyquist real).
+// Row pitch of the staged half spectra of the inverse x transform: odd in
+// 16-byte words, and two rows hold one transpose tile.
+template <int N1> __host__ __device__ constexpr int ifftx_pitch() {
+  constexpr int NH = RowFft<N1>::N / 2 + 1, HT = (RowFft<N1>::TILE + 1) / 2;
+  return ((NH > HT ? NH : HT) + 7) / 8 * 8 + 1;
+}
+
 template <int N1, int XR>
 __device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, double* __restrict__ p, int ny, int nz,
                                            const cpx<double>* __restrict__ twx, int bx, int k) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
-  constexpr int SP = (NH + 7) / 8 * 8 + 1;                  // staging pitch
+  constexpr int SP = ifftx_pitch<N1>();                      // staging pitch
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<double>* S = reinterpret_cast<cpx<double>*>(smraw);   // XR rows x SP half spectra
-  cpx<double>* tiles = S + XR * SP;                          // XR/2 packed rows x TILE
   const int j0 = bx * XR;
   for (int e = threadIdx.x; e < NH * XR; e += blockDim.x) {
     const int m = e / XR, r = e % XR;
@@ -271,16 +277,24 @@ __device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, do
   const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
   const int pr = warp * RF::RPW + sub;
   const bool ok = sub < RF::RPW && pr < XR / 2;
-  cpx<double>* tile = tiles + (size_t)(ok ? pr : 0) * RF::TILE;
+  // a packed row's transpose tile overlays the two staged rows it reads
+  // (the warp reads them all before any lane writes its tile)
   const cpx<double>* A = S + (2 * (ok ? pr : 0)) * SP;
   const cpx<double>* B = A + SP;
+  cpx<double>* tile = S + (2 * (ok ? pr : 0)) * SP;
   auto ld = [&](int m) -> cpx<double> {
     cpx<double> a, bb;
     if (m < NH) { a = A[m]; bb = B[m]; }
     else { a = cconj(A[N - m]); bb = cconj(B[N - m]); }
     return cmake<double>(a.x - bb.y, a.y + bb.x);  // A + i B
   };
-  if (ok && l < RF::N2) rowfft_pass1<N1, true>(ld, l, tile, twx);
+  cpx<double> vr[N1];
+  if (ok && l < RF::N2) {
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) vr[n1] = ld(RF::N2 * n1 + l);
+  }
+  __syncwarp();
+  if (ok && l < RF::N2) rowfft_pass1_regs<N1, true>(vr, l, tile, twx);
   __syncwarp();
   double* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
   if (ok && l < N1)
