@@ -73,18 +73,21 @@ def test_implicit_diffusion(torch_cuda, nx, ny, nz, top):
 
 def _fused(ch, fused, nz):
     """Select the Poisson path; the fused cluster kernel must be available for
-    portable cluster sizes (nz <= 128: at most 8 CTAs of 16 planes)."""
+    portable cluster sizes (nz <= 128: at most 8 CTAs of 16 planes) and y
+    rows of at most 384 points (it holds whole rows of its planes in shared
+    memory)."""
     try:
         ch.use_fused_poisson(fused)
     except Exception:
-        if nz <= 128:
+        if nz <= 128 and ch.ny <= 384:
             raise
-        pytest.skip("16-CTA cluster not schedulable on this device")
+        pytest.skip("fused y/z kernel not schedulable for this shape")
 
 
 # (32,24,128): 8 CTAs of 16 planes; (16,12,100): 8 CTAs, ragged last chunk;
 # (16,12,200): 16-CTA cluster
-POISSON_SIZES = SIZES + [(64, 64, 48), (96, 48, 32), (32, 24, 128), (16, 12, 100), (16, 12, 200)]
+POISSON_SIZES = SIZES + [(64, 64, 48), (96, 48, 32), (32, 24, 128), (16, 12, 100), (16, 12, 200),
+                         (768, 32, 8), (32, 768, 8), (512, 48, 6), (48, 512, 6)]  # 768 = 24 x 32, 512 = 32 x 16 splits
 
 
 @pytest.mark.parametrize("nx,ny,nz", POISSON_SIZES)
@@ -219,6 +222,22 @@ def test_steps_vs_oracle(torch_cuda, scheme, path, top, nx, ny, nz):
         assert abs(sc[1] - ub) < 1e-13
         if scheme != "FE":
             assert abs(sc[0] - f) < 1e-9 * max(1.0, abs(f))
+        assert ch.diagnostics()["max_div"] < 1e-12
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(768, 32, 8), (32, 768, 8), (512, 48, 6), (48, 512, 6)])
+def test_steps_vs_oracle_long_rows(torch_cuda, nx, ny, nz):
+    """Register transforms of 768 (24 x 32 split) and 512 (32 x 16) points in x
+    and in y, through full IMEX steps."""
+    oc = make_oracle(nx, ny, nz, seed=12)
+    ch = make_gpu(oc)
+    ch.set_state(oc.u, oc.v, oc.w, forcing=0.0)
+    for s in range(3):
+        ub, f = oc.step_imex(0.002)
+        ch.step("IMEX", 0.002)
+        gu, gv, gw, gp = ch.get_state()
+        for name, g, r in zip("uvw", (gu, gv, gw), (oc.u, oc.v, oc.w)):
+            assert rel(np_(g), r) < TOL, (s, name, rel(np_(g), r))
         assert ch.diagnostics()["max_div"] < 1e-12
 
 

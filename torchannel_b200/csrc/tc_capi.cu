@@ -255,7 +255,7 @@ extern "C" int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes) {
   return TC_OK;
 }
 
-// ---- register-FFT launches (lengths N1 * 16, N1 in 4, 6, 8, 12, 16, 24) ----
+// ---- register-FFT launches (lengths 16 K, K in 4, 6, 8, 12, 16, 24, 32, 48) ----
 template <class F> static void for_each_n1(int n, F&& f) {
   switch (n / 16) {
     case 4: f(std::integral_constant<int, 4>{}); break;
@@ -263,7 +263,9 @@ template <class F> static void for_each_n1(int n, F&& f) {
     case 8: f(std::integral_constant<int, 8>{}); break;
     case 12: f(std::integral_constant<int, 12>{}); break;
     case 16: f(std::integral_constant<int, 16>{}); break;
-    default: f(std::integral_constant<int, 24>{}); break;
+    case 24: f(std::integral_constant<int, 24>{}); break;
+    case 32: f(std::integral_constant<int, 32>{}); break;
+    default: f(std::integral_constant<int, 48>{}); break;
   }
 }
 template <int N1> static size_t fftx_reg_smem() {

@@ -137,27 +137,31 @@ template <int N, bool INV> struct Dft {
   }
 };
 
-// ---- row transform of length N = N1 * 16 -----------------------------------
-template <int N1> struct RowFft {
-  static constexpr int N2 = 16;
+// ---- row transform of length N = 16 K -----------------------------------
+// Split N = N1 N2 with N1 = K, N2 = 16 for K <= 32, and N1 = 24, N2 = 32 for
+// K = 48 (N = 768), so that a row's lanes, max(N1, N2), fit in a warp.
+template <int K> struct RowFft {
+  static constexpr int N1 = K == 48 ? 24 : K;
+  static constexpr int N2 = K == 48 ? 32 : 16;
   static constexpr int N = N1 * N2;
   static constexpr int LANES = N1 > N2 ? N1 : N2;         // lanes a row needs
   static constexpr int RPW = 32 / LANES;                  // rows per warp
   static constexpr int TP = N2 + 1;                       // tile pitch (complex)
   static constexpr int TILE = N1 * TP;                    // tile size per row (complex)
+  static_assert(N == 16 * K && LANES <= 32, "unsupported row length");
 };
 
 // Pass 1 for lane n2: v[n1] = x[N2 n1 + n2] -> DFT_N1 -> times W_N^(n2 k1),
 // stored to tile[k1 * TP + n2].  `ld(e)` returns element e of the row.
-template <int N1, bool INV, class LD>
+template <int K, bool INV, class LD>
 __device__ __forceinline__ void rowfft_pass1(LD ld, int n2, cpx<double>* tile, const cpx<double>* __restrict__ tw) {
-  using RF = RowFft<N1>;
-  cpx<double> v[N1];
+  using RF = RowFft<K>;
+  cpx<double> v[RF::N1];
 #pragma unroll
-  for (int n1 = 0; n1 < N1; ++n1) v[n1] = ld(RF::N2 * n1 + n2);
-  Dft<N1, INV>::run(v);
+  for (int n1 = 0; n1 < RF::N1; ++n1) v[n1] = ld(RF::N2 * n1 + n2);
+  Dft<RF::N1, INV>::run(v);
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1) {
+  for (int k1 = 0; k1 < RF::N1; ++k1) {
     cpx<double> w = tw[n2 * k1];
     if (INV) w.y = -w.y;
     tile[k1 * RF::TP + n2] = k1 == 0 ? v[0] : cmul(v[k1], w);
@@ -165,35 +169,35 @@ __device__ __forceinline__ void rowfft_pass1(LD ld, int n2, cpx<double>* tile, c
 }
 
 // Pass 1 on values already in registers: v[n1] = x[N2 n1 + n2].
-template <int N1, bool INV>
-__device__ __forceinline__ void rowfft_pass1_regs(cpx<double> (&v)[N1], int n2, cpx<double>* tile,
+template <int K, bool INV>
+__device__ __forceinline__ void rowfft_pass1_regs(cpx<double> (&v)[RowFft<K>::N1], int n2, cpx<double>* tile,
                                                   const cpx<double>* __restrict__ tw) {
-  using RF = RowFft<N1>;
-  Dft<N1, INV>::run(v);
+  using RF = RowFft<K>;
+  Dft<RF::N1, INV>::run(v);
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1) {
+  for (int k1 = 0; k1 < RF::N1; ++k1) {
     cpx<double> w = tw[n2 * k1];
     if (INV) w.y = -w.y;
     tile[k1 * RF::TP + n2] = k1 == 0 ? v[0] : cmul(v[k1], w);
   }
 }
 
-// Pass 2 for lane k1: b[n2] = tile[k1 * TP + n2] -> DFT_16; `st(e, val)`
+// Pass 2 for lane k1: b[n2] = tile[k1 * TP + n2] -> DFT_N2; `st(e, val)`
 // receives element e = k1 + N1 k2 of the transformed row.
-template <int N1, bool INV, class ST>
+template <int K, bool INV, class ST>
 __device__ __forceinline__ void rowfft_pass2(ST st, int k1, const cpx<double>* tile) {
-  using RF = RowFft<N1>;
+  using RF = RowFft<K>;
   cpx<double> b[RF::N2];
 #pragma unroll
   for (int n2 = 0; n2 < RF::N2; ++n2) b[n2] = tile[k1 * RF::TP + n2];
   Dft<RF::N2, INV>::run(b);
 #pragma unroll
-  for (int k2 = 0; k2 < RF::N2; ++k2) st(k1 + N1 * k2, b[k2]);
+  for (int k2 = 0; k2 < RF::N2; ++k2) st(k1 + RF::N1 * k2, b[k2]);
 }
 
-// Lengths with a register transform: N1 = N / 16 in {4, 6, 8, 12, 16, 24}.
+// Lengths with a register transform: K = N / 16 in {4, 6, 8, 12, 16, 24, 32, 48}.
 __host__ __device__ inline bool rowfft_supported(int n) {
-  return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 384;
+  return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512 || n == 768;
 }
 
 }  // namespace tc

@@ -124,7 +124,7 @@ __device__ __forceinline__ void ffty_rows(cpx<double>* __restrict__ X, int nrows
   cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
   if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
   __syncwarp();
-  if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+  if (ok && l < RF::N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
   __syncwarp();
 }
 
@@ -141,13 +141,13 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
   // the next rows' values are loaded before this row's transform
   const bool lane_ld = sub < RF::RPW && l < RF::N2;
   int row0 = (blockIdx.x * wpb + warp) * RF::RPW;
-  cpx<double> v[N1];
-  auto ldrow = [&](int r0, cpx<double> (&o)[N1]) {
+  cpx<double> v[RF::N1];
+  auto ldrow = [&](int r0, cpx<double> (&o)[RF::N1]) {
     const int row = r0 + sub;
     if (lane_ld && row < nrows) {
       const cpx<double>* x = X + (size_t)row * RF::N;
 #pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) o[n1] = x[RF::N2 * n1 + l];
+      for (int n1 = 0; n1 < RF::N1; ++n1) o[n1] = x[RF::N2 * n1 + l];
     }
   };
   ldrow(row0, v);
@@ -155,14 +155,14 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
     const int row = row0 + sub;
     const bool ok = sub < RF::RPW && row < nrows;
     cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
-    cpx<double> vn[N1];
+    cpx<double> vn[RF::N1];
     ldrow(row0 + rstep, vn);
     if (ok && l < RF::N2) rowfft_pass1_regs<N1, INV>(v, l, tile, twy);
     __syncwarp();
-    if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+    if (ok && l < RF::N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
     __syncwarp();
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[n1] = vn[n1];
+    for (int n1 = 0; n1 < RF::N1; ++n1) v[n1] = vn[n1];
   }
 }
 
@@ -212,15 +212,15 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
     rowfft_pass1<N1, false>([&](int i) { return cmake<double>(divv(ja, i), divv(jb, i)); }, l, tile, twx);
   __syncwarp();
   cpx<double> b[RF::N2];
-  if (ok && l < N1) {
+  if (ok && l < RF::N1) {
 #pragma unroll
     for (int n2 = 0; n2 < RF::N2; ++n2) b[n2] = tile[l * RF::TP + n2];
   }
   __syncwarp();
-  if (ok && l < N1) {
+  if (ok && l < RF::N1) {
     Dft<RF::N2, false>::run(b);
 #pragma unroll
-    for (int k2 = 0; k2 < RF::N2; ++k2) tile[l + N1 * k2] = b[k2];  // Z[m], natural order
+    for (int k2 = 0; k2 < RF::N2; ++k2) tile[l + RF::N1 * k2] = b[k2];  // Z[m], natural order
   }
   __syncthreads();
   // unpack: A = (Z[m] + conj Z[N-m]) / 2 (row ja), B = (Z[m] - conj Z[N-m]) / (2i) (row jb)
@@ -288,16 +288,16 @@ __device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, do
     else { a = cconj(A[N - m]); bb = cconj(B[N - m]); }
     return cmake<double>(a.x - bb.y, a.y + bb.x);  // A + i B
   };
-  cpx<double> vr[N1];
+  cpx<double> vr[RF::N1];
   if (ok && l < RF::N2) {
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) vr[n1] = ld(RF::N2 * n1 + l);
+    for (int n1 = 0; n1 < RF::N1; ++n1) vr[n1] = ld(RF::N2 * n1 + l);
   }
   __syncwarp();
   if (ok && l < RF::N2) rowfft_pass1_regs<N1, true>(vr, l, tile, twx);
   __syncwarp();
   double* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
-  if (ok && l < N1)
+  if (ok && l < RF::N1)
     rowfft_pass2<N1, true>([&](int i, cpx<double> z) { pa[i] = z.x; pa[N + i] = z.y; }, l, tile);
 }
 
@@ -772,7 +772,7 @@ __global__ void __launch_bounds__(512) k_yz_solve_reg(cpx<double>* __restrict__ 
       cpx<double>* x = R + (size_t)(ok ? row : 0) * ny;
       if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
       __syncwarp();
-      if (ok && l < N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+      if (ok && l < RF::N1) rowfft_pass2<N1, INV>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
       __syncwarp();
     }
   };
