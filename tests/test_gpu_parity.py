@@ -87,7 +87,8 @@ def _fused(ch, fused, nz):
 # (32,24,128): 8 CTAs of 16 planes; (16,12,100): 8 CTAs, ragged last chunk;
 # (16,12,200): 16-CTA cluster
 POISSON_SIZES = SIZES + [(64, 64, 48), (96, 48, 32), (32, 24, 128), (16, 12, 100), (16, 12, 200),
-                         (768, 32, 8), (32, 768, 8), (512, 48, 6), (48, 512, 6)]  # 768 = 24 x 32, 512 = 32 x 16 splits
+                         (768, 32, 8), (32, 768, 8), (512, 48, 6), (48, 512, 6),  # 768 = 24 x 32, 512 = 32 x 16
+                         (144, 288, 6), (1024, 16, 4), (16, 576, 4)]               # 9 x 16, 18 x 16, 32 x 32, 18 x 32
 
 
 @pytest.mark.parametrize("nx,ny,nz", POISSON_SIZES)
@@ -225,10 +226,14 @@ def test_steps_vs_oracle(torch_cuda, scheme, path, top, nx, ny, nz):
         assert ch.diagnostics()["max_div"] < 1e-12
 
 
-@pytest.mark.parametrize("nx,ny,nz", [(768, 32, 8), (32, 768, 8), (512, 48, 6), (48, 512, 6)])
+@pytest.mark.parametrize("nx,ny,nz", [(768, 32, 8), (32, 768, 8), (512, 48, 6), (48, 512, 6),
+                                      (144, 288, 6), (288, 144, 6), (1024, 16, 4), (16, 1024, 4), (576, 32, 4),
+                                      (32, 576, 4)])
 def test_steps_vs_oracle_long_rows(torch_cuda, nx, ny, nz):
-    """Register transforms of 768 (24 x 32 split) and 512 (32 x 16) points in x
-    and in y, through full IMEX steps."""
+    """Register transforms of every supported split beyond 384 points (512 =
+    32 x 16, 576 = 18 x 32, 768 = 24 x 32, 1024 = 32 x 32) and of the odd
+    radix-3 lengths 144 = 9 x 16 and 288 = 18 x 16, in x and in y, through full
+    IMEX steps."""
     oc = make_oracle(nx, ny, nz, seed=12)
     ch = make_gpu(oc)
     ch.set_state(oc.u, oc.v, oc.w, forcing=0.0)

@@ -255,17 +255,21 @@ extern "C" int tc_workspace_bytes(const tc_grid_desc* g, size_t* bytes) {
   return TC_OK;
 }
 
-// ---- register-FFT launches (lengths 16 K, K in 4, 6, 8, 12, 16, 24, 32, 48) ----
+// ---- register-FFT launches (lengths 16 K, K as rowfft_supported) ----
 template <class F> static void for_each_n1(int n, F&& f) {
   switch (n / 16) {
     case 4: f(std::integral_constant<int, 4>{}); break;
     case 6: f(std::integral_constant<int, 6>{}); break;
     case 8: f(std::integral_constant<int, 8>{}); break;
     case 12: f(std::integral_constant<int, 12>{}); break;
+    case 9: f(std::integral_constant<int, 9>{}); break;
     case 16: f(std::integral_constant<int, 16>{}); break;
+    case 18: f(std::integral_constant<int, 18>{}); break;
     case 24: f(std::integral_constant<int, 24>{}); break;
     case 32: f(std::integral_constant<int, 32>{}); break;
-    default: f(std::integral_constant<int, 48>{}); break;
+    case 36: f(std::integral_constant<int, 36>{}); break;
+    case 48: f(std::integral_constant<int, 48>{}); break;
+    default: f(std::integral_constant<int, 64>{}); break;
   }
 }
 template <int N1> static size_t fftx_reg_smem() {

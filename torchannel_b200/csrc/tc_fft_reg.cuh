@@ -138,11 +138,12 @@ template <int N, bool INV> struct Dft {
 };
 
 // ---- row transform of length N = 16 K -----------------------------------
-// Split N = N1 N2 with N1 = K, N2 = 16 for K <= 32, and N1 = 24, N2 = 32 for
-// K = 48 (N = 768), so that a row's lanes, max(N1, N2), fit in a warp.
+// Split N = N1 N2 with N1 = K, N2 = 16 for K <= 32, and N1 = K / 2, N2 = 32
+// above (N = 576, 768, 1024), so that a row's lanes, max(N1, N2), fit in a
+// warp.
 template <int K> struct RowFft {
-  static constexpr int N1 = K == 48 ? 24 : K;
-  static constexpr int N2 = K == 48 ? 32 : 16;
+  static constexpr int N1 = K <= 32 ? K : K / 2;
+  static constexpr int N2 = K <= 32 ? 16 : 32;
   static constexpr int N = N1 * N2;
   static constexpr int LANES = N1 > N2 ? N1 : N2;         // lanes a row needs
   static constexpr int RPW = 32 / LANES;                  // rows per warp
@@ -195,9 +196,16 @@ __device__ __forceinline__ void rowfft_pass2(ST st, int k1, const cpx<double>* t
   for (int k2 = 0; k2 < RF::N2; ++k2) st(k1 + RF::N1 * k2, b[k2]);
 }
 
-// Lengths with a register transform: K = N / 16 in {4, 6, 8, 12, 16, 24, 32, 48}.
+// Lengths with a register transform: K = N / 16 in {4, 6, 8, 9, 12, 16, 18,
+// 24, 32, 36, 48, 64} (N = 64 .. 1024).
 __host__ __device__ inline bool rowfft_supported(int n) {
-  return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512 || n == 768;
+  if (n % 16) return false;
+  switch (n / 16) {
+    case 4: case 6: case 8: case 9: case 12: case 16: case 18: case 24: case 32: case 36: case 48: case 64:
+      return true;
+    default:
+      return false;
+  }
 }
 
 }  // namespace tc
