@@ -745,13 +745,13 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   }
   mark(c, TC_PH_RHS, s);
   if (scheme == TC_IMEX)
-    k_rhs_update<T, false, UPD_AB2><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
+    RhsKernel<T, false, UPD_AB2>::fn<<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
                                                          c->scal + SC_FORCING, (T)dt, c->have_hist);
   else if (scheme == TC_AB2)
-    k_rhs_update<T, true, UPD_AB2><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
+    RhsKernel<T, true, UPD_AB2>::fn<<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
                                                         c->scal + SC_FORCING, (T)dt, c->have_hist);
   else
-    k_rhs_update<T, true, UPD_FE><<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
+    RhsKernel<T, true, UPD_FE>::fn<<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
                                                        c->scal + SC_FORCING, (T)dt, 0);
   TC_LAUNCHED();
   if constexpr (sizeof(T) == 8) {
@@ -867,10 +867,10 @@ template <class T> static int rhs_hook_impl(tc_ctx* c, int full, double* ru, dou
   cudaMemsetAsync(B[2], 0, ncell / c->nz * (c->nz + 1) * sizeof(T), s);
   dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>(), (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (full)
-    k_rhs_update<T, true, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, rhs_ty<T>()), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+    RhsKernel<T, true, UPD_RHS_ONLY>::fn<<<grd, dim3(RHS_TX, rhs_ty<T>()), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                    B[0], B[1], B[2], c->scal, (T)0, 0);
   else
-    k_rhs_update<T, false, UPD_RHS_ONLY><<<grd, dim3(RHS_TX, rhs_ty<T>()), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
+    RhsKernel<T, false, UPD_RHS_ONLY>::fn<<<grd, dim3(RHS_TX, rhs_ty<T>()), 0, s>>>(g, A[0], A[1], A[2], nullptr, nullptr, nullptr,
                                                                     B[0], B[1], B[2], c->scal, (T)0, 0);
   TC_LAUNCHED();
   int rc;

@@ -83,7 +83,6 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
   const bool active = (i < nx) && (j < ny);
   const int kb = bz * RHS_KB;  // planes kb .. kb+RHS_KB-1 (<= nz)
   const T top = g.top_neumann ? T(1) : T(-1);
-  const T h = T(0.5);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
   const T* __restrict__ base = g.ubase_t;
   // halo elements of this thread: e0 = tid, e1 = tid + block size (if < RHS_NH)
@@ -143,6 +142,11 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
   }
   __syncthreads();
   const int cx = tx + 1, cy = ty + 1;
+  // Every advective flux is a product of two interpolations 0.5(a + b); the
+  // sums are multiplied unscaled and the two factors 0.5 are folded into the
+  // difference quotient as 0.25 / delta.  Scaling by powers of two is exact,
+  // so the fluxes are the same numbers as with the interpolations formed.
+  const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
 #pragma unroll 1
   for (int kk = 0; kk < RHS_KB; ++kk) {
     const int k = kb + kk;
@@ -151,6 +155,7 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
     if (active && k < nz) {
       const size_t o = (size_t)k * plane + (size_t)j * nx + i;
       const T idzf = g.idzf[k];
+      const T qzf = T(0.25) * idzf;
       // ---------------- u at cell k ----------------
       {
         const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
@@ -163,12 +168,12 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
           if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
         }
         if (!edge) {
-          const T duudx = (sq(h * (U0 + Uxp)) - sq(h * (Uxm + U0))) * g.idx;
-          const T vu_t = h * (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (h * (U0 + Uyp));
-          const T vu_b = h * (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (h * (Uym + U0));
-          const T wu_t = h * (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (h * (U0 + Uzp));
-          const T wu_b = h * (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (h * (Uzm + U0));
-          r -= duudx + (vu_t - vu_b) * g.idy + (wu_t - wu_b) * idzf;
+          const T duudx = (sq(U0 + Uxp) - sq(Uxm + U0)) * qx;
+          const T vu_t = (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (U0 + Uyp);
+          const T vu_b = (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (Uym + U0);
+          const T wu_t = (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (U0 + Uzp);
+          const T wu_b = (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (Uzm + U0);
+          r -= duudx + (vu_t - vu_b) * qy + (wu_t - wu_b) * qzf;
         }
         if (UPD == UPD_RHS_ONLY) {
           ru[o] = r;
@@ -196,12 +201,12 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
           if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
         }
         if (!edge) {
-          const T uv_r = h * (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (h * (V0 + Vxp));
-          const T uv_l = h * (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (h * (Vxm + V0));
-          const T dvvdy = (sq(h * (V0 + Vyp)) - sq(h * (Vym + V0))) * g.idy;
-          const T wv_t = h * (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (h * (V0 + Vzp));
-          const T wv_b = h * (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (h * (Vzm + V0));
-          r -= (uv_r - uv_l) * g.idx + dvvdy + (wv_t - wv_b) * idzf;
+          const T uv_r = (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (V0 + Vxp);
+          const T uv_l = (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (Vxm + V0);
+          const T dvvdy = (sq(V0 + Vyp) - sq(Vym + V0)) * qy;
+          const T wv_t = (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (V0 + Vzp);
+          const T wv_b = (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (Vzm + V0);
+          r -= (uv_r - uv_l) * qx + dvvdy + (wv_t - wv_b) * qzf;
         }
         if (UPD == UPD_RHS_ONLY) {
           rv[o] = r;
@@ -222,12 +227,12 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
       T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
       // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
       if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
-      const T uw_r = h * (su[sm][cy][cx] + su[s0][cy][cx]) * (h * (W0 + Wxp));
-      const T uw_l = h * (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (h * (Wxm + W0));
-      const T vw_t = h * (sv[sm][cy][cx] + sv[s0][cy][cx]) * (h * (W0 + Wyp));
-      const T vw_b = h * (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (h * (Wym + W0));
-      const T dwwdz = (sq(h * (W0 + Wzp)) - sq(h * (Wzm + W0))) * g.idzc[k];
-      r -= (uw_r - uw_l) * g.idx + (vw_t - vw_b) * g.idy + dwwdz;
+      const T uw_r = (su[sm][cy][cx] + su[s0][cy][cx]) * (W0 + Wxp);
+      const T uw_l = (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (Wxm + W0);
+      const T vw_t = (sv[sm][cy][cx] + sv[s0][cy][cx]) * (W0 + Wyp);
+      const T vw_b = (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (Wym + W0);
+      const T dwwdz = (sq(W0 + Wzp) - sq(Wzm + W0)) * (T(0.25) * g.idzc[k]);
+      r -= (uw_r - uw_l) * qx + (vw_t - vw_b) * qy + dwwdz;
       if (UPD == UPD_RHS_ONLY) {
         rw[o] = r;
       } else if (UPD == UPD_FE) {
@@ -244,6 +249,9 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
   }
 }
 
+// FP32 storage: the compiler's own register choice (48 in the IMEX form, 5
+// blocks per SM); bounding it to 5 blocks gives the same count and a slower
+// schedule.
 template <class T, bool FULL, int UPD>
 __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, const T* __restrict__ u,
                                                                 const T* __restrict__ v, const T* __restrict__ w,
@@ -255,6 +263,26 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>()) k_rhs_update(Grid<T> g, 
   rhs_tile<T, FULL, UPD>(g, u, v, w, us, vs, ws, ru, rv, rw, forcing_dev, dt, have_hist, blockIdx.x, blockIdx.y,
                          blockIdx.z);
 }
+
+// FP64 storage: bounded to 4 blocks per SM (64 registers, no spills); left
+// free the compiler takes 74 and 3 blocks fit.
+template <bool FULL, int UPD>
+__global__ void __launch_bounds__(RHS_TX * rhs_ty<double>(), 4) k_rhs_update_f64(
+    Grid<double> g, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+    double* __restrict__ us, double* __restrict__ vs, double* __restrict__ ws, double* __restrict__ ru,
+    double* __restrict__ rv, double* __restrict__ rw, const double* __restrict__ forcing_dev, double dt,
+    int have_hist) {
+  rhs_tile<double, FULL, UPD>(g, u, v, w, us, vs, ws, ru, rv, rw, forcing_dev, dt, have_hist, blockIdx.x,
+                              blockIdx.y, blockIdx.z);
+}
+
+// The RHS kernel for storage type T.
+template <class T, bool FULL, int UPD> struct RhsKernel {
+  static constexpr auto fn = k_rhs_update<T, FULL, UPD>;
+};
+template <bool FULL, int UPD> struct RhsKernel<double, FULL, UPD> {
+  static constexpr auto fn = k_rhs_update_f64<FULL, UPD>;
+};
 
 // ---------------------------------------------------------------------------
 // Crank-Nicolson tables.  Row m of a system:
