@@ -217,8 +217,8 @@ __global__ void __launch_bounds__(64, TC_BATCH_TRI_MINB) kb_tri(const BMember<T>
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
     const int m = batch_member(st, nm, w);
     const BMember<T>& b = M[m];
-    tri_lu2_thread(reinterpret_cast<double*>(b.X), b.rden, b.cpt, b.tb, b.nxh, b.g.ny, b.g.nz,
-                   (w - st[m]) * 64 + threadIdx.x);
+    tri_lu2_thread<8>(reinterpret_cast<double*>(b.X), b.rden, b.cpt, b.tb, b.nxh, b.g.ny, b.g.nz,
+                      (w - st[m]) * 64 + threadIdx.x);
   }
 }
 

@@ -90,6 +90,7 @@ struct tc_ctx {
   int yzr_thr, yzr_ok;  // register-FFT form of the fused kernel (k_yz_solve_reg)
   size_t yzr_smem;
   int nsm, yreg_blocks;  // SM count; resident-block cap of the y register FFT
+  int tri16_blocks;      // resident blocks of k_tri_lu2<16> on the device
   int cn_L_force;        // CN chunk length chosen by tc_set_cn_chunk (0: by nz)
   size_t yz_smem;
   int cur, have_hist, state_set;
@@ -316,6 +317,12 @@ template <class T> static int reg_fft_setup(tc_ctx* c) {
     });
   }
   if (c->yreg_blocks < 1) c->yreg_blocks = 1;
+  {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tri_lu2<16>, 64, 0) != cudaSuccess)
+      rc = fail(TC_ERR_CUDA, "z solve occupancy");
+    c->tri16_blocks = nb * c->nsm;
+  }
   return rc;
 }
 
@@ -666,10 +673,13 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
   const int nmodes = nxh * ny;
   mark(c, TC_PH_TRI, s);
-  if (c->tri_rden)
-    k_tri_lu2<<<(2 * nmodes + 63) / 64, 64, 0, s>>>(reinterpret_cast<double*>(X), c->tri_rden, c->tri_cp, tb,
-                                                     nxh, ny, nz);
-  else
+  if (c->tri_rden) {
+    const int nb = (2 * nmodes + 63) / 64;
+    if (nb <= c->tri16_blocks)
+      k_tri_lu2<16><<<nb, 64, 0, s>>>(reinterpret_cast<double*>(X), c->tri_rden, c->tri_cp, tb, nxh, ny, nz);
+    else
+      k_tri_lu2<8><<<nb, 64, 0, s>>>(reinterpret_cast<double*>(X), c->tri_rden, c->tri_cp, tb, nxh, ny, nz);
+  } else
     k_tri<<<(nmodes + c->tri_bt - 1) / c->tri_bt, c->tri_bt, (size_t)c->tri_bt * nz * 8, s>>>(X, tb, nxh, ny, nz);
   mark(c, TC_PH_IFFTY, s);
   if (yreg)

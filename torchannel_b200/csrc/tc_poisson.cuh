@@ -659,7 +659,87 @@ __global__ void __launch_bounds__(512) k_yz_solve(cpx<double>* __restrict__ X, c
 // factors are real, so the two recurrences are independent): twice the
 // threads in flight, half the registers per level, TRIP_B levels prefetched.
 #define TRIP_B 16
-// Thread t of the sweep (mode t / 2, part t % 2).
+
+// The sweeps of tri_lu2_thread for nz a multiple of 2 LB (LB levels per
+// block), with the same arithmetic: 32-bit running offsets (one multiply-add
+// per address), the level coefficients at constant offsets from a block's
+// first level, no per-level guards, and two prefetch buffers used in turn
+// instead of one that is shifted.  Integer work was most of the general form's instructions, and
+// with two warps per scheduler each level costs its instructions' latencies.
+// The backward sweep starts at level nz-1 (x = d' there) so that it too
+// covers whole blocks; the gauged (0,0) mode has 0 stored there first.
+template <int LB>
+__device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const double* __restrict__ rd,
+                                             const double* __restrict__ cpt, const double* __restrict__ cl,
+                                             unsigned st, int nz, bool gauge) {
+  const unsigned st2 = 2u * st;
+  double da[LB], fa[LB], db[LB], fb[LB];
+  // levels k0 .. k0+LB-1 of d and of a factor table
+  auto load_up = [&](double (&d)[LB], double (&f)[LB], const double* __restrict__ tab, int k0) {
+    unsigned o = (unsigned)k0 * st2, q = (unsigned)k0 * st;
+#pragma unroll
+    for (int b = 0; b < LB; ++b) {
+      d[b] = col[o];
+      f[b] = ldg(tab + q);
+      o += st2;
+      q += st;
+    }
+  };
+  // levels k1, k1-1, .. k1-LB+1
+  auto load_dn = [&](double (&d)[LB], double (&f)[LB], const double* __restrict__ tab, int k1) {
+    unsigned o = (unsigned)k1 * st2, q = (unsigned)k1 * st;
+#pragma unroll
+    for (int b = 0; b < LB; ++b) {
+      d[b] = col[o];
+      f[b] = ldg(tab + q);
+      o -= st2;
+      q -= st;
+    }
+  };
+  double dp = 0.0;
+  auto sweep_up = [&](const double (&d)[LB], const double (&f)[LB], int k0) {
+    unsigned o = (unsigned)k0 * st2;
+    const double* a = cl + k0;
+#pragma unroll
+    for (int b = 0; b < LB; ++b) {
+      const double ak = (b == 0 && k0 == 0) ? 0.0 : ldg(a + b);
+      dp = fma(-(ak * f[b]), dp, d[b] * f[b]);
+      col[o] = dp;
+      o += st2;
+    }
+  };
+  load_up(da, fa, rd, 0);
+  for (int k0 = 0; k0 < nz; k0 += 2 * LB) {
+    load_up(db, fb, rd, k0 + LB);
+    sweep_up(da, fa, k0);
+    if (k0 + 2 * LB < nz) load_up(da, fa, rd, k0 + 2 * LB);
+    sweep_up(db, fb, k0 + LB);
+  }
+  if (gauge) col[(unsigned)(nz - 1) * st2] = 0.0;
+  double x = 0.0;
+  auto sweep_dn = [&](const double (&d)[LB], const double (&f)[LB], int k1) {
+    unsigned o = (unsigned)k1 * st2;
+#pragma unroll
+    for (int b = 0; b < LB; ++b) {
+      // level nz-1 is d' itself: its table entry c_{nz-1} rden_{nz-1} is 0,
+      // or not finite for the singular (0,0) mode
+      x = (b == 0 && k1 == nz - 1) ? d[b] : d[b] - f[b] * x;
+      col[o] = x;
+      o -= st2;
+    }
+  };
+  load_dn(da, fa, cpt, nz - 1);
+  for (int k1 = nz - 1; k1 >= 0; k1 -= 2 * LB) {
+    load_dn(db, fb, cpt, k1 - LB);
+    sweep_dn(da, fa, k1);
+    if (k1 - 2 * LB >= 0) load_dn(da, fa, cpt, k1 - 2 * LB);
+    sweep_dn(db, fb, k1 - LB);
+  }
+}
+
+// Thread t of the sweep (mode t / 2, part t % 2); LEAN_B > 0: tri_lu2_lean
+// with LEAN_B levels per block where nz is a multiple of 2 LEAN_B.
+template <int LEAN_B>
 __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const double* __restrict__ rden_t,
                                                const double* __restrict__ cp_t, const PoissonTabs& tb, int nxh,
                                                int ny, int nz, int t) {
@@ -670,6 +750,12 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
   double* col = Xd + 2 * base + part;
   const double* rd = rden_t + base;
   const double* cpt = cp_t + base;
+  if constexpr (LEAN_B > 0) {
+    if (nz % (2 * LEAN_B) == 0) {
+      tri_lu2_lean<LEAN_B>(col, rd, cpt, tb.cl, (unsigned)ny, nz, kx == 0 && ky == 0);
+      return;
+    }
+  }
   const size_t st = ny, st2 = 2 * (size_t)ny;
   double dc[TRIP_B], dn[TRIP_B], fc[TRIP_B], fn[TRIP_B];
 #pragma unroll
@@ -724,10 +810,13 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
   }
 }
 
+// LEAN_B = 16 holds 254 registers (4 blocks per SM), LEAN_B = 8 166 (6):
+// the deeper form where the whole launch is resident at once.
+template <int LEAN_B>
 __global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const double* __restrict__ rden_t,
                                                  const double* __restrict__ cp_t, PoissonTabs tb, int nxh, int ny,
                                                  int nz) {
-  tri_lu2_thread(Xd, rden_t, cp_t, tb, nxh, ny, nz, blockIdx.x * blockDim.x + threadIdx.x);
+  tri_lu2_thread<LEAN_B>(Xd, rden_t, cp_t, tb, nxh, ny, nz, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // k_yz_solve with the register-resident row transforms (ny = N1 * 16): the
