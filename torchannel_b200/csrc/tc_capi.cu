@@ -196,6 +196,10 @@ static int validate(const tc_grid_desc* g) {
   if (!fft_make_plan(g->nx, &a) || !fft_make_plan(g->ny, &b))
     return fail(TC_ERR_SIZE, "nx and ny must factor into 2 and 3 only");
   if (g->nx > 4096 || g->ny > 4096) return fail(TC_ERR_SIZE, "nx, ny must be <= 4096");
+  // kernels index within a field in 32 bits; such a grid (> 200 GB of state)
+  // does not fit on one device in any case
+  if ((uint64_t)g->nx * g->ny * (g->nz + 1) >= (1ull << 32))
+    return fail(TC_ERR_SIZE, "nx * ny * (nz + 1) must be below 2^32");
   if (g->precision != TC_FP64 && g->precision != TC_MIXED) return fail(TC_ERR_ARG, "bad precision");
   if (!g->dz_f || !g->dz_c) return fail(TC_ERR_ARG, "null dz_f / dz_c");
   if (!(g->Lx > 0 && g->Ly > 0 && g->Lz > 0 && g->nu > 0)) return fail(TC_ERR_ARG, "non-positive domain or viscosity");
