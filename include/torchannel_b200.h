@@ -31,7 +31,8 @@ extern "C" {
 enum {
   TC_OK = 0,
   TC_ERR_ARG = 1,         /* bad argument / null pointer */
-  TC_ERR_SIZE = 2,        /* unsupported grid size (nx, ny even, >= 8, factors 2 and 3 only; 4 <= nz <= 512) */
+  TC_ERR_SIZE = 2,        /* unsupported grid size (nx, ny even, >= 8, factors 2 and 3 only; 4 <= nz <= 512;
+                             nx * ny * (nz + 1) < 2^32) */
   TC_ERR_CUDA = 3,        /* a CUDA runtime call failed */
   TC_ERR_WORKSPACE = 4,   /* workspace too small or misaligned */
   TC_ERR_STATE = 5,       /* call needs a state set with tc_set_state first */

@@ -306,12 +306,18 @@ __global__ void k_adj_cn_tables(double* tab, const double* __restrict__ dzf, con
 // faces m-1, m, m+1 (the reference's index convention), so face g of the
 // result collects y_{g-1} (its own row) and beta (cC_{g-1} y_{g-1} + cB_g y_g +
 // cA_{g+1} y_{g+1}); the wall faces take nothing.  One thread per column.
+// Each pass reads a column it is rewriting, so its loads are taken in blocks
+// of ADJ_CN_B rows, the next block's before this block's stores (a load after
+// a store to the same column would wait for it); the arithmetic is that of
+// the one-row-at-a-time form.
+#define ADJ_CN_B 8
 __global__ void __launch_bounds__(128) k_adj_cn(double* lu, double* lv, double* lw, const double* __restrict__ tab,
                                                 int nx, int ny, int nz) {
+  constexpr int B = ADJ_CN_B;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int comp = blockIdx.y;
   if (col >= nx * ny) return;
-  const size_t pl = (size_t)nx * ny;
+  const unsigned pl = (unsigned)nx * (unsigned)ny;  // a field has fewer than 2^32 elements
   const double* t = tab + (size_t)(comp == 2 ? 1 : 0) * 6 * nz;
   const double* aT = t; const double* ivT = t + nz; const double* cpT = t + 2 * nz;
   const double* eA = t + 3 * nz; const double* eB = t + 4 * nz; const double* eC = t + 5 * nz;
@@ -319,42 +325,91 @@ __global__ void __launch_bounds__(128) k_adj_cn(double* lu, double* lv, double* 
   double* q = (comp == 0 ? lu : (comp == 1 ? lv : lw)) + col;
   const int n = comp < 2 ? nz : nz - 1;
   const int off = comp < 2 ? 0 : 1;  // row m lives at plane m + off
+  auto row = [&](int m) -> double { return (m >= 0 && m < n) ? q[(unsigned)(m + off) * pl] : 0.0; };
+  double buf[B], nxt[B];
   // forward sweep
   double yp = 0.0;
-  for (int m = 0; m < n; ++m) {
-    double* e = q + (size_t)(m + off) * pl;
-    yp = (*e - aT[m] * yp) * ivT[m];
-    *e = yp;
+#pragma unroll
+  for (int b = 0; b < B; ++b) buf[b] = row(b);
+  for (int m0 = 0; m0 < n; m0 += B) {
+#pragma unroll
+    for (int b = 0; b < B; ++b) nxt[b] = row(m0 + B + b);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const int m = m0 + b;
+      if (m < n) {
+        yp = (buf[b] - aT[m] * yp) * ivT[m];
+        q[(unsigned)(m + off) * pl] = yp;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) buf[b] = nxt[b];
   }
   // backward sweep
   double x = 0.0;
-  for (int m = n - 1; m >= 0; --m) {
-    double* e = q + (size_t)(m + off) * pl;
-    x = *e - cpT[m] * x;
-    *e = x;
+#pragma unroll
+  for (int b = 0; b < B; ++b) buf[b] = row(n - 1 - b);
+  for (int m1 = n - 1; m1 >= 0; m1 -= B) {
+#pragma unroll
+    for (int b = 0; b < B; ++b) nxt[b] = row(m1 - B - b);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const int m = m1 - b;
+      if (m >= 0) {
+        x = buf[b] - cpT[m] * x;
+        q[(unsigned)(m + off) * pl] = x;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) buf[b] = nxt[b];
   }
   // explicit transpose, ascending, from a window of rows m-1, m, m+1
   if (comp < 2) {
-    double ym = 0.0, y0 = q[0], yn;
-    for (int m = 0; m < n; ++m) {
-      yn = (m + 1 < n) ? q[(size_t)(m + 1) * pl] : 0.0;
-      double s = eB[m] * y0;
-      if (m > 0) s += eC[m - 1] * ym;
-      if (m + 1 < n) s += eA[m + 1] * yn;
-      q[(size_t)m * pl] = y0 + beta * s;
-      ym = y0; y0 = yn;
+    double ym = 0.0;
+#pragma unroll
+    for (int b = 0; b < B; ++b) buf[b] = row(b);
+    for (int m0 = 0; m0 < n; m0 += B) {
+#pragma unroll
+      for (int b = 0; b < B; ++b) nxt[b] = row(m0 + B + b);
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int m = m0 + b;
+        if (m < n) {
+          const double y0 = buf[b], yn = (b + 1 < B) ? buf[b + 1] : nxt[0];
+          double s = eB[m] * y0;
+          if (m > 0) s += eC[m - 1] * ym;
+          if (m + 1 < n) s += eA[m + 1] * yn;
+          q[(unsigned)m * pl] = y0 + beta * s;
+          ym = y0;
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) buf[b] = nxt[b];
     }
   } else {
-    // Y(m) sits at face m+1; output face g in [1, nz-1] overwrites Y(g-1)
-    double Yg1 = q[pl];                   // Y(g-1) at g = 1
-    double Yg = (n > 1) ? q[2 * pl] : 0.0;  // Y(g)
-    for (int g = 1; g <= nz - 1; ++g) {
-      const double Yg2 = (g + 1 <= n - 1) ? q[(size_t)(g + 2) * pl] : 0.0;  // Y(g+1) at face g+2
-      double s = eC[g - 1] * Yg1;                       // row g-1 uses face g as its +1 point
-      if (g <= n - 1) s += eB[g] * Yg;                  // row g uses face g as its centre
-      if (g + 1 <= n - 1) s += eA[g + 1] * Yg2;         // row g+1 uses face g as its -1 point
-      q[(size_t)g * pl] = Yg1 + beta * s;
-      Yg1 = Yg; Yg = Yg2;
+    // Y(m) sits at face m+1 (F(f) below, 0 past face n); output face g in
+    // [1, nz-1] overwrites Y(g-1) and reads Y(g-1), Y(g), Y(g+1)
+    auto F = [&](int f) -> double { return (f >= 1 && f <= n) ? q[(unsigned)f * pl] : 0.0; };
+#pragma unroll
+    for (int b = 0; b < B; ++b) buf[b] = F(1 + b);
+    for (int g0 = 1; g0 <= nz - 1; g0 += B) {
+#pragma unroll
+      for (int b = 0; b < B; ++b) nxt[b] = F(g0 + B + b);
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int g = g0 + b;
+        if (g <= nz - 1) {
+          const double Yg1 = buf[b];
+          const double Yg = (b + 1 < B) ? buf[b + 1] : nxt[b + 1 - B];
+          const double Yg2 = (b + 2 < B) ? buf[b + 2] : nxt[b + 2 - B];
+          double s = eC[g - 1] * Yg1;                       // row g-1 uses face g as its +1 point
+          if (g <= n - 1) s += eB[g] * Yg;                  // row g uses face g as its centre
+          if (g + 1 <= n - 1) s += eA[g + 1] * Yg2;         // row g+1 uses face g as its -1 point
+          q[(unsigned)g * pl] = Yg1 + beta * s;
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) buf[b] = nxt[b];
     }
   }
 }
