@@ -3,7 +3,7 @@ spectrum / pressure / tridiagonal arithmetic / bulk forcing / statistics sums)
 against the FP64 oracle.  Tolerances are stated per quantity:
 
 * u, v, w after 20 IMEX steps: <= 2e-5 relative (FP32 storage, ~1e-7 per step)
-* post-projection max|div| <= 1e-6 (north-star bound for the mixed step)
+* post-projection max|div| <= 1e-6 (the bound the mixed step is built to)
 * u_bulk <= 1e-9 absolute; U(z) <= 1e-6 relative (0.5% allowed)
 * statistics sums <= 1e-5 relative
 """
