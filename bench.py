@@ -64,6 +64,11 @@ def parse():
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-only", default=None, metavar="ROWS,CTAS",
+                    help="--workload ensemble: only the ensemble launches, with this fixed shape (CN rows bound, "
+                         "CTAs per SM) and graphs off, every launch visible to a profiler")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the forward+adjoint cost ratio (96x96x64, 200 steps) of the step line")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
 
@@ -238,6 +243,9 @@ def run_b200(a):
     ch.timing(False)
     # end-to-end through the public API with host buffers
     e2e = None if a.no_e2e else run_e2e(a, grid, (u0, v0, w0), dt)
+    # the second half of the metric: forward + adjoint cost over a forward run
+    del ch
+    adj = None if a.no_adjoint else measure_adjoint(a, rank, world)["summary"]
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -276,6 +284,7 @@ def run_b200(a):
         "clocks": clk.summary(),
         "gpu_launches": LAUNCHES_PER_STEP * a.steps,
         "max_div_after": diag["max_div"],
+        "adjoint": adj,
     }
     if other is not None:
         line["fp64_plain"] = other
@@ -474,6 +483,29 @@ def run_ensemble(a):
     members = make_members(16, seed=0)
     mine = [members[m] for m in partition(len(members), world, rank)]
     ens = Ensemble(mine, precision=a.precision)
+    if a.batch_only:
+        rows, ctas = (int(x) for x in a.batch_only.split(","))
+        b = ens.batch()
+        b.set_shape(rows, ctas)
+        b.use_graphs(False)
+        ens.step_batch(a.warmup)
+        torch.cuda.synchronize()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record()
+        ens.step_batch(a.steps)
+        b1.record()
+        torch.cuda.synchronize()
+        ms_b = b0.elapsed_time(b1)
+        value_b, _, max_ms = aggregate(ens.points() * a.steps, ms_b)
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": "grid-point-steps/s, 16-member uneven ensemble, ensemble launches only",
+                              "value": value_b, "unit": "grid-point-steps/s", "n_gpus": world, "steps": a.steps,
+                              "warmup": a.warmup, "ms_per_step": max_ms / a.steps, "higher_is_better": True,
+                              "config": {"workload": "ensemble of 16 channels", "shape": [rows, ctas],
+                                         "graphs": False}, "info": b.info()}), flush=True)
+        return
     ens.step(a.warmup)
     ens.synchronize()
     torch.cuda.synchronize()
@@ -604,15 +636,28 @@ def run_adjoint(a):
     directions.  Replicas: every rank runs its own channel (seed = rank)."""
     import torch
     import torch.distributed as dist
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    r = measure_adjoint(a, rank, world)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(r["line"]), flush=True)
+
+
+def measure_adjoint(a, rank, world):
+    """The adjoint workload (see run_adjoint) on this rank; every rank takes
+    the same collective steps.  Returns {"line": the workload's JSON line,
+    "summary": the keys the step bench line carries}."""
+    import torch
+    import torch.distributed as dist
     from torchannel_b200.adjoint import AdjointRunner, fourier_body_force, to_internal
     from torchannel_b200 import _lib as L
     from torchannel_b200.core import Channel
     from torchannel_b200.grid import generate_grid
     from torchannel_b200.init import initialize_flow
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     nx, ny, nz, dt, N = 96, 96, 64, 0.003, 200
     window = range(101, 201)
     z_f, z_c, dz_f, dz_c = generate_grid(GAMMA, nz, LZ)
@@ -687,12 +732,17 @@ def run_adjoint(a):
         t = torch.tensor([fwd_ms, fc_ms + bw_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         fwd_ms, tot = float(t[0]), float(t[1])
-        dist.destroy_process_group()
     else:
         tot = fc_ms + bw_ms
-    if rank == 0:
-        npts = nx * ny * nz
-        print(json.dumps({
+    runner.close()
+    npts = nx * ny * nz
+    summary = {"workload": "96x96x64, 200 FP64 IMEX steps (dt 0.003), J = mean KE over steps 101..200, "
+                           "gradients w.r.t. the initial field and an 8-mode body force",
+               "adjoint_over_forward": tot / fwd_ms, "mode": runner.mode, "forward_ms": fwd_ms,
+               "forward_with_hooks_ms": fc_ms, "reverse_sweep_ms": bw_ms,
+               "recompute_ratio": (fc_r + bw_r) / fwd_ms, "fd_directions": len(errs),
+               "fd_max_rel_error": max(errs), "fd_eps": eps, "store_vs_recompute_bitwise_equal": same}
+    line = {
             "metric": "forward+adjoint / forward cost ratio (96x96x64, 200 IMEX steps)",
             "value": tot / fwd_ms, "unit": "ratio", "n_gpus": world, "steps": N, "warmup": a.warmup,
             "ms_per_step": tot / N, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -709,7 +759,8 @@ def run_adjoint(a):
             "forward_gpss": npts * N * world / (fwd_ms / 1e3),
             "J": Jv, "grad_norm_q0": float(sum((t * t).sum() for t in gq)) ** 0.5,
             "grad_norm_F": float(sum((t * t).sum() for t in gF)) ** 0.5,
-            "fd_rel_errors": errs, "fd_max_rel_error": max(errs), "fd_eps": eps}), flush=True)
+            "fd_rel_errors": errs, "fd_max_rel_error": max(errs), "fd_eps": eps}
+    return {"line": line, "summary": summary}
 
 
 def run_config1(a):

@@ -167,12 +167,18 @@ int tc_poisson_solve(tc_ctx* ctx, const double* rhs, double* p, void* stream);
  * they must not risk the device-wide synchronisation of cudaMalloc/cudaFree):
  * no context, no workspace, and no allocation of any kind.  No counterpart in
  * the reference.  dz_f (nz) and dz_c (nz+1) are DEVICE arrays; rhs and p as in
- * tc_poisson_solve; FP64.  The scratch is one static 64 MiB array in device
- * memory per GPU that loads the library, held until the process exits; grids
- * needing more (about nx*ny*nz*16 bytes, e.g. above 128x128x128) get
- * TC_ERR_SIZE.  The first call on each device looks the array up and sets
- * kernel attributes there: make that first call before any stream capture.
- * All calls share the array, so calls that overlap on the GPU (other streams,
+ * tc_poisson_solve; FP64; all four must be device (or managed) memory of the
+ * current device, else TC_ERR_ARG before any launch.  The scratch is one
+ * static 64 MiB (67108864-byte) array in device memory per GPU that loads the
+ * library, held until the process exits.  A grid needs
+ * nx*ny*nz*8 + (nx/2+1)*ny*nz*16 bytes plus six small tables (each region
+ * rounded up to 256 bytes), about 16.1 bytes per grid point: 160x160x160
+ * (65955328 bytes) fits, 162x162x162 or 128x128x256 do not and get
+ * TC_ERR_SIZE before any GPU work.  The first call in each CUDA context (per
+ * device, and again in a context made after cudaDeviceReset) sets kernel
+ * attributes and reads occupancy figures there: make that first call before
+ * any stream capture.  The array's address is looked up on every call.  All
+ * calls share the array, so calls that overlap on the GPU (other streams,
  * other host threads) race; serialise them. */
 int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, double Ly, const double* dz_f,
                              const double* dz_c, const double* rhs, double* p, void* stream);

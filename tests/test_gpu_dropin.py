@@ -129,3 +129,24 @@ def test_field_accessors_and_schemes(torch_cuda, tmp_path):
         cf.step_rk3(0.001)
     dt = cf.compute_cfl_dt()
     assert cf.dt_min <= dt <= cf.dt_max
+
+
+def test_nonfinite_state_writes_error_file_and_stops(torch_cuda, tmp_path):
+    """A NaN in the field is caught at the next save point: fields_error.npz
+    is written with the reference's keys and the loop stops there
+    (solver.py:862-881); no fields.npz is written for that step."""
+    from torchannel_b200.solver import ChannelFlowB200
+    res = str(tmp_path / "e")
+    cf = ChannelFlowB200(_cfg(str(tmp_path / "e.yaml"), res, 24, 16, 12, time__n_steps=20,
+                              time__dt_update_interval=0, output__n_save=4, output__n_out=2,
+                              statistics__n_stats=0), verbose=False)
+    u = cf.u.cpu().numpy()
+    u[5, 6, 7] = np.nan
+    cf.set_fields(u, cf.v, cf.w)
+    last = cf.run_simulation()
+    assert last == 4 and cf.current_step == 4
+    err = np.load(os.path.join(res, "fields_error.npz"))
+    assert set(err.files) == {"u", "v", "w", "p", "z_c", "z_f", "Lx", "Ly", "step", "time", "u_tau", "forcing"}
+    assert int(err["step"]) == 4
+    assert not np.all(np.isfinite(err["u"]))
+    assert not os.path.exists(os.path.join(res, "fields.npz"))

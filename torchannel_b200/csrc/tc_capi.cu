@@ -1314,6 +1314,7 @@ extern "C" int tc_error(tc_ctx* c, int* code) {
 // spectral intermediate and the small tables live in one fixed-size array in
 // device global memory that the library owns for the life of the process.
 // ---------------------------------------------------------------------------
+#include <cuda.h>  // CUcontext and CUresult only: the driver calls are looked up at run time
 #include <mutex>
 
 #define TC_NOALLOC_SCRATCH_BYTES (64ull << 20)
@@ -1321,22 +1322,116 @@ extern "C" int tc_error(tc_ctx* c, int* code) {
 
 static __device__ __align__(256) unsigned char tc_noalloc_scratch[TC_NOALLOC_SCRATCH_BYTES];
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[TC_NOALLOC_MAX_DEVICES];
-
-// The host-side name tc_noalloc_scratch is not a device address: look the
-// address up once per device (with that device current) and pass it on.
-static int noalloc_setup(int dev, unsigned char** out) {
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, tc_noalloc_scratch);
-    if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    int r = set_smem_attrs<double>(nullptr);
-    if (r) return r;
-    g_noalloc_ptr[dev] = ptr;
+// Register-FFT lengths 16 N1 (rowfft_supported) and an index per N1 for the
+// per-context occupancy cache below.
+static constexpr int kNoallocN1[12] = {4, 6, 8, 9, 12, 16, 18, 24, 32, 36, 48, 64};
+static int noalloc_n1_index(int n1) {
+  for (int e = 0; e < 12; ++e)
+    if (kNoallocN1[e] == n1) return e;
+  return -1;
+}
+template <int E = 0, class F> static void for_all_n1(F&& f) {
+  if constexpr (E < 12) {
+    f(std::integral_constant<int, kNoallocN1[E]>{}, E);
+    for_all_n1<E + 1>(f);
   }
-  *out = (unsigned char*)g_noalloc_ptr[dev];
+}
+
+// What the set-up of a device's context leaves for later calls: the context
+// it ran in (a unique id, so that a context created after cudaDeviceReset is
+// set up again), the SM count and the resident-block counts of the
+// register y transform (per length) and of the 16-level z solve.
+struct NoallocDev {
+  unsigned long long ctx_id;
+  int nsm;
+  int ffty_nb[12];
+  int tri16_nb;
+};
+static std::mutex g_noalloc_mu;
+static NoallocDev g_noalloc_dev[TC_NOALLOC_MAX_DEVICES];
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (driver calls found
+// through the runtime, so the library needs no link-time libcuda).
+static int noalloc_ctx_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_cur || !get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1) {
+      cudaGetLastError();
+      return fail(TC_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId not found");
+    }
+    get_cur = (CtxGetCurrentFn)f0;
+    get_id = (CtxGetIdFn)f1;
+  }
+  CUcontext ctx = nullptr;
+  if (get_cur(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS)
+    return fail(TC_ERR_CUDA, "no current CUDA context");
+  return TC_OK;
+}
+
+// The host-side name tc_noalloc_scratch is not a device address: its
+// address is looked up on every call (a cheap query in the current context).
+// Kernel attributes and occupancy figures are set up once per context, in the
+// first call made in it.
+static int noalloc_setup(int dev, unsigned char** out, NoallocDev* info) {
+  void* ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, tc_noalloc_scratch);
+  if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  unsigned long long id = 0;
+  int rc = noalloc_ctx_id(&id);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoallocDev& d = g_noalloc_dev[dev];
+  if (d.ctx_id != id) {
+    NoallocDev n{};
+    if ((rc = set_smem_attrs<double>(nullptr))) return rc;
+    TC_CUDA(cudaDeviceGetAttribute(&n.nsm, cudaDevAttrMultiProcessorCount, dev));
+    for_all_n1([&](auto I, int idx) {
+      constexpr int N1 = decltype(I)::value;
+      int nb = 0;
+      if (cudaFuncSetAttribute(k_div_fftx_reg<double, N1, XROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fftx_reg_smem<N1>()) != cudaSuccess ||
+          cudaFuncSetAttribute(k_ifftx_reg<N1, XROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ifftx_reg_smem<N1>()) != cudaSuccess ||
+          cudaFuncSetAttribute(k_ffty_reg<N1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ffty_reg_smem<N1>()) != cudaSuccess ||
+          cudaFuncSetAttribute(k_ffty_reg<N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ffty_reg_smem<N1>()) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ffty_reg<N1, false>, 128, ffty_reg_smem<N1>()) !=
+              cudaSuccess)
+        rc = fail(TC_ERR_CUDA, "register FFT attributes");
+      n.ffty_nb[idx] = nb;
+    });
+    if (rc) return rc;
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n.tri16_nb, k_tri_lu2<16>, 64, 0));
+    n.ctx_id = id;
+    d = n;
+  }
+  *info = d;
+  *out = (unsigned char*)ptr;
+  return TC_OK;
+}
+
+// A caller's array must be device (or managed) memory of the current device:
+// a host pointer handed to the kernels would fault instead of failing here.
+static int noalloc_check_ptr(const void* p, int dev, const char* name) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(TC_ERR_ARG, std::string(name) + ": not a CUDA pointer");
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return fail(TC_ERR_ARG, std::string(name) + " must be device memory (got host or unregistered memory)");
+  if (a.type == cudaMemoryTypeDevice && a.device != dev)
+    return fail(TC_ERR_ARG, std::string(name) + " belongs to another device");
   return TC_OK;
 }
 
@@ -1410,9 +1505,13 @@ extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, doubl
   int dev = 0;
   TC_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= TC_NOALLOC_MAX_DEVICES) return fail(TC_ERR_ARG, "device index out of range");
+  int rc;
+  if ((rc = noalloc_check_ptr(dz_f, dev, "dz_f")) || (rc = noalloc_check_ptr(dz_c, dev, "dz_c")) ||
+      (rc = noalloc_check_ptr(rhs, dev, "rhs")) || (rc = noalloc_check_ptr(p, dev, "p")))
+    return rc;
   unsigned char* base = nullptr;
-  int rc = noalloc_setup(dev, &base);
-  if (rc) return rc;
+  NoallocDev info{};
+  if ((rc = noalloc_setup(dev, &base, &info))) return rc;
   cudaStream_t s = ST(stream);
   // a context view over the static scratch (launch shapes as tc_create picks them)
   tc_grid_desc g{};
@@ -1420,9 +1519,13 @@ extern "C" int tc_poisson_solve_noalloc(int nx, int ny, int nz, double Lx, doubl
   tc_ctx c{};
   fill_basic(&c, &g);
   c.dev = dev;
-  TC_CUDA(cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, dev));
-  rc = reg_fft_setup<double>(&c);
-  if (rc) return rc;
+  c.nsm = info.nsm;
+  c.yreg_blocks = c.nsm;
+  if (yreg_ok(&c)) {
+    const int nb = info.ffty_nb[noalloc_n1_index(ny / 16)];
+    if (nb > 0) c.yreg_blocks = nb * c.nsm;
+  }
+  c.tri16_blocks = info.tri16_nb * c.nsm;
   double* field = (double*)(base + off[0]);
   c.X = (cpx<double>*)(base + off[1]);
   c.k2x = (double*)(base + off[2]); c.k2y = (double*)(base + off[3]);

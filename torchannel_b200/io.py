@@ -11,6 +11,7 @@
 """
 import csv
 import os
+import zipfile
 
 import numpy as np
 
@@ -38,16 +39,39 @@ def save_flow_fields(u, v, w, p, z_c, z_f, Lx, Ly, step, time, u_tau, forcing, r
     return path
 
 
+FIELD_KEYS = ("u", "v", "w", "p", "z_c", "z_f", "Lx", "Ly", "step", "time", "u_tau", "forcing")
+
+
 def load_flow_fields(filepath):
+    """Read a ``fields*.npz`` (``utils.py:402-444``).  A missing file raises
+    FileNotFoundError as in the reference; a truncated or corrupt archive, a
+    missing key, or a field with an inconsistent shape raises ValueError
+    naming the file, instead of the reference's unchecked ``np.load``
+    indexing (which fails late or not at all)."""
     if not os.path.exists(filepath):
         raise FileNotFoundError(f"Field file not found: {filepath}")
-    data = np.load(filepath)
-    out = {k: data[k] for k in ("u", "v", "w", "p", "z_c", "z_f")}
-    out.update(Lx=float(data["Lx"]), Ly=float(data["Ly"]), step=int(data["step"]), time=float(data["time"]),
-               u_tau=float(data["u_tau"]), forcing=float(data["forcing"]))
-    for k in data.files:
-        if k not in out:
-            out[k] = data[k]
+    try:
+        with np.load(filepath) as data:
+            missing = [k for k in FIELD_KEYS if k not in data.files]
+            if missing:
+                raise ValueError(f"missing keys {missing}")
+            out = {k: np.array(data[k]) for k in ("u", "v", "w", "p", "z_c", "z_f")}
+            out.update(Lx=float(data["Lx"]), Ly=float(data["Ly"]), step=int(data["step"]),
+                       time=float(data["time"]), u_tau=float(data["u_tau"]), forcing=float(data["forcing"]))
+            for k in data.files:
+                if k not in out:
+                    out[k] = np.array(data[k])
+    except (zipfile.BadZipFile, EOFError, OSError, ValueError, KeyError) as e:
+        raise ValueError(f"Cannot read field file {filepath}: {e}") from e
+    u, v, w, p = out["u"], out["v"], out["w"], out["p"]
+    if u.ndim != 3 or v.ndim != 3 or w.ndim != 3 or p.ndim != 3:
+        raise ValueError(f"Field file {filepath}: u, v, w, p must be 3-D")
+    nx, ny, nz = u.shape[0] - 1, u.shape[1] - 2, u.shape[2] - 2
+    want = {"v": (nx + 2, ny + 1, nz + 2), "w": (nx + 2, ny + 2, nz + 1), "p": (nx + 2, ny + 2, nz + 2)}
+    for k, s in want.items():
+        if out[k].shape != s:
+            raise ValueError(f"Field file {filepath}: {k} has shape {out[k].shape}, expected {s} for "
+                             f"u of shape {u.shape}")
     return out
 
 
