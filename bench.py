@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--batch-only", default=None, metavar="ROWS,CTAS",
                     help="--workload ensemble: only the ensemble launches, with this fixed shape (CN rows bound, "
                          "CTAs per SM) and graphs off, every launch visible to a profiler")
+    ap.add_argument("--no-fp32-poisson", action="store_true",
+                    help="skip the mixed step with the single-precision Poisson solve")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the forward+adjoint cost ratio (96x96x64, 200 steps) of the step line")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -236,6 +238,12 @@ def run_b200(a):
         other["profile_rel_err"] = {"U": rerr("U_sum"), "uu": rerr("uu_sum"), "vv": rerr("vv_sum"),
                                     "ww": rerr("ww_sum"), "uw": rerr("uw_sum"), "E_uu_2d": rerr("E_uu_2d_sum")}
         del ch2
+    # mixed precision with the single-precision Poisson step (FP32 spectrum,
+    # FP64 low modes, increment over the previous pressure; the 10 set-up
+    # steps use the FP64 solve), same state and dt
+    psp = None
+    if a.precision == "mixed" and not a.no_fp32_poisson:
+        psp = time_fp32_poisson(a, grid, (u0, v0, w0), dt, world, stats)
     # per-phase timing (separate, instrumented pass of the same steps)
     ch.timing(True)
     ch.step("IMEX", dt, min(a.steps, L_RING))
@@ -285,6 +293,7 @@ def run_b200(a):
         "gpu_launches": LAUNCHES_PER_STEP * a.steps,
         "max_div_after": diag["max_div"],
         "adjoint": adj,
+        "mixed_fp32_poisson": psp,
     }
     if other is not None:
         line["fp64_plain"] = other
@@ -295,6 +304,60 @@ def run_b200(a):
                                              "u_tau_rel_err": abs(diag["u_tau"] - other["u_tau"]) / other["u_tau"],
                                              "profile_rel_err": other.pop("profile_rel_err")}
     print(json.dumps(line), flush=True)
+
+
+def time_fp32_poisson(a, grid, fields, dt, world, stats_mixed):
+    """The mixed step with the single-precision Poisson solve: set-up as the
+    headline run (initial projection, 10 steps, which are the FP64 warm-up of
+    the increment's base), warm-up, then K timed steps; returns its speed,
+    divergence, per-kernel table and its statistics' distance from the FP64
+    Poisson run's."""
+    import torch
+    import torch.distributed as dist
+    from torchannel_b200.core import Channel
+    z_f, z_c, dz_f, dz_c = grid
+    u0, v0, w0 = fields
+    ch = Channel(NX, NY, NZ, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision="mixed")
+    ch.set_state(u0, v0, w0)
+    ub = ch.bulk_velocity()
+    ch.set_state(u0 * (1.0 / ub), v0, w0)
+    ch.project_initial()
+    ch.use_fp32_poisson(True, warm_steps=10)
+    ch.step("IMEX", dt, 10 + a.warmup)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ch.step("IMEX", dt, a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    d = ch.diagnostics()
+    out = {"value": NX * NY * NZ * a.steps * world / (ms / 1e3), "ms_per_step": ms / a.steps,
+           "max_div_after": d["max_div"], "u_bulk": d["u_bulk"], "u_tau": d["u_tau"],
+           "error_word": ch.error_word()}
+    if stats_mixed is not None:
+        ch.stats_init(z_c, 180.0, 15.0)
+        ch.stats_accumulate()
+        st = ch.stats_read()
+
+        def rerr(k):
+            return float(np.max(np.abs(st[k] - stats_mixed[k])) / np.max(np.abs(stats_mixed[k])))
+        out["profile_rel_err_vs_fp64_poisson"] = {"U": rerr("U_sum"), "uu": rerr("uu_sum"), "ww": rerr("ww_sum"),
+                                                  "uw": rerr("uw_sum")}
+    ch.timing(True)
+    ch.step("IMEX", dt, min(a.steps, L_RING))
+    phases, nst = ch.timing_read()
+    ch.timing(False)
+    out["kernels_ms"] = {k: v / max(nst, 1) for k, v in phases.items()}
+    out["note"] = ("FP32 spectrum (x transform, fused y transform / z solve / inverse y transform per kx slab in "
+                   "shared memory, inverse x transform), FP64 for the (0,0) mode and kx < 3, |ky| < 3; solves for "
+                   "the increment over the previous step's pressure; the first 10 steps use the FP64 solve")
+    return out
 
 
 L_RING = 64

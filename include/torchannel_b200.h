@@ -118,6 +118,24 @@ int tc_use_graphs(tc_ctx* ctx, int on);
  * counterpart. */
 int tc_use_fused_poisson(tc_ctx* ctx, int on);
 
+/* Single-precision Poisson step (TC_MIXED contexts; TC_ERR_ARG otherwise):
+ * the pressure solve of every step (projection_fft.py:101-215) with an FP32
+ * spectrum -- x transform, y transforms and the z tridiagonal solves of all
+ * but the lowest wavenumbers in FP32, the (kx, ky) = (0,0) mode and the
+ * modes with kx < 3 and |ky| < 3 solved in FP64 -- for the increment of p
+ * over the previous step's pressure: the right-hand side becomes
+ * div(u**)/dt - L p_prev, so FP32 rounding scales with the change of p over
+ * one step, not with p (whose FP32 rounding alone would leave a
+ * post-projection divergence of about 1e-5 on stretched grids).  The first
+ * `warm_steps` steps after tc_set_state (and every step until a previous
+ * pressure exists) use the FP64 solve.  y transform, z solve and inverse y
+ * transform run as one kernel per kx slab with the slab in shared memory:
+ * TC_ERR_SIZE unless nx has a register transform, ny = 16 K (K <= 24) and
+ * ny * nz * 8 bytes fit one CTA's shared memory (e.g. 192 x 128).  p from
+ * tc_get_state is then FP32-rounded.  No reference counterpart (the
+ * reference solves in its field precision, FP64). */
+int tc_use_fp32_poisson(tc_ctx* ctx, int on, int warm_steps);
+
 /* Initial projection of a fresh field: div -> Poisson -> u -= grad p
  * (dt = 1) (solver.py:345-370). */
 int tc_project_initial(tc_ctx* ctx, void* stream);
@@ -172,9 +190,10 @@ int tc_poisson_solve(tc_ctx* ctx, const double* rhs, double* p, void* stream);
  * static 64 MiB (67108864-byte) array in device memory per GPU that loads the
  * library, held until the process exits.  A grid needs
  * nx*ny*nz*8 + (nx/2+1)*ny*nz*16 bytes plus six small tables (each region
- * rounded up to 256 bytes), about 16.1 bytes per grid point: 160x160x160
- * (65955328 bytes) fits, 162x162x162 or 128x128x256 do not and get
- * TC_ERR_SIZE before any GPU work.  The first call in each CUDA context (per
+ * rounded up to 256 bytes), about 16.1 bytes per grid point: 144x144x192
+ * (64153088 bytes) and 162x128x201 (exactly 67108864) fit, 162x128x202,
+ * 162x162x162 or 128x128x256 do not and get TC_ERR_SIZE before any GPU
+ * work.  The first call in each CUDA context (per
  * device, and again in a context made after cudaDeviceReset) sets kernel
  * attributes and reads occupancy figures there: make that first call before
  * any stream capture.  The array's address is looked up on every call.  All

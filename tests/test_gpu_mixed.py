@@ -106,3 +106,62 @@ def test_mixed_other_schemes(torch_cuda, scheme):
     for name, g, r in zip("uvw", (gu, gv, gw), (oc.u, oc.v, oc.w)):
         assert rel(dof(name, np_(g), nx, ny, nz), dof(name, r, nx, ny, nz)) < 2e-5, name
     assert ch.diagnostics()["max_div"] <= 1e-6
+
+
+# ---- single-precision Poisson step (FP32 spectrum, FP64 low modes, increment
+# over the previous pressure) -------------------------------------------------
+FP32P_SIZES = [(64, 64, 48), (96, 64, 40), (128, 96, 24), (192, 192, 16)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", FP32P_SIZES)
+def test_fp32_poisson_steps_vs_fp64_oracle(torch_cuda, nx, ny, nz):
+    """20 IMEX steps with the single-precision Poisson solve from step 3 on,
+    against the FP64 oracle: u, v, w <= 2e-5 relative (as the mixed form),
+    u_bulk <= 1e-9, U(z) <= 1e-6 relative; the post-projection divergence is
+    printed (FP32 rounding of the increment) and bounded by 1e-5."""
+    oc = make_oracle(nx, ny, nz, seed=41)
+    ch = make_gpu(oc, precision="mixed")
+    ch.set_state(oc.u, oc.v, oc.w)
+    ch.use_fp32_poisson(True, warm_steps=2)
+    dt = 0.004
+    divs = []
+    for s in range(20):
+        ub, f = oc.step_imex(dt)
+        ch.step("IMEX", dt)
+        divs.append(ch.diagnostics()["max_div"])
+    gu, gv, gw, gp = ch.get_state()
+    for name, g, r in zip("uvw", (gu, gv, gw), (oc.u, oc.v, oc.w)):
+        assert rel(dof(name, np_(g), nx, ny, nz), dof(name, r, nx, ny, nz)) < 2e-5, name
+    assert rel(dof("p", np_(gp), nx, ny, nz), dof("p", oc.p, nx, ny, nz)) < 1e-3
+    d = ch.diagnostics()
+    print(f"{nx}x{ny}x{nz} FP32 Poisson: max|div| per step {['%.1e' % x for x in divs]}")
+    assert max(divs) <= 1e-5 and not d["nonfinite"], divs
+    assert abs(d["u_bulk"] - ub) < 1e-9
+    Ug = np_(gu)[1:nx + 1, 1:ny + 1, 1:nz + 1].mean(axis=(0, 1))
+    Ur = oc.u[1:nx + 1, 1:ny + 1, 1:nz + 1].mean(axis=(0, 1))
+    assert np.max(np.abs(Ug - Ur)) / np.max(np.abs(Ur)) < 1e-6
+    assert ch.error_word() == 0
+
+
+def test_fp32_poisson_graph_replay_is_bitwise_identical(torch_cuda):
+    nx, ny, nz = 64, 64, 24
+    oc = make_oracle(nx, ny, nz, seed=42)
+    a, b = make_gpu(oc, "mixed"), make_gpu(oc, "mixed")
+    a.use_graphs(False)
+    for ch in (a, b):
+        ch.set_state(oc.u, oc.v, oc.w)
+        ch.use_fp32_poisson(True, warm_steps=3)
+        ch.step("IMEX", 0.003, 9)       # 3 FP64 warm-up steps, then graph pairs + remainder
+        ch.step("IMEX", 0.002, 7)
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(np_(x), np_(y))
+    assert np.array_equal(np_(a.scalars), np_(b.scalars))
+
+
+def test_fp32_poisson_refused_where_unavailable(torch_cuda):
+    from torchannel_b200._lib import TCError
+    oc = make_oracle(32, 48, 16)                    # ny = 48: no register transform of the fused kernel
+    with pytest.raises(TCError):
+        make_gpu(oc, "mixed").use_fp32_poisson(True)
+    with pytest.raises(TCError):
+        make_gpu(make_oracle(64, 64, 16), "fp64").use_fp32_poisson(True)

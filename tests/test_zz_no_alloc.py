@@ -46,11 +46,11 @@ def _scratch_bytes(nx, ny, nz):
     return o
 
 
-@pytest.mark.parametrize("nx,ny,nz", [(192, 192, 128), (128, 128, 256), (162, 162, 162)])
+@pytest.mark.parametrize("nx,ny,nz", [(192, 192, 128), (128, 128, 256), (162, 162, 162), (162, 128, 202)])
 def test_noalloc_rejects_oversize_grid(nx, ny, nz):
     """Grids whose scratch exceeds the static array get TC_ERR_SIZE (no GPU
-    work is attempted before the size check); (128, 128, 256) and 162^3 are
-    the first sizes just over the limit."""
+    work is attempted before the size check); (162, 128, 202) is one plane
+    more than a grid that needs exactly the whole array."""
     assert _scratch_bytes(nx, ny, nz) > LIMIT
     lib = L.load()
     rc = lib.tc_poisson_solve_noalloc(nx, ny, nz, 1.0, 1.0, ctypes.c_void_p(8), ctypes.c_void_p(8),
@@ -60,17 +60,18 @@ def test_noalloc_rejects_oversize_grid(nx, ny, nz):
 
 
 def test_noalloc_limit_examples():
-    """The documented examples: 160^3 fits, 128x128x240 fits."""
-    assert _scratch_bytes(160, 160, 160) == 65955328 <= LIMIT
-    assert _scratch_bytes(128, 128, 240) <= LIMIT
+    """The documented examples: 144x144x192 fits, 162x128x201 needs exactly
+    the whole array."""
+    assert _scratch_bytes(144, 144, 192) == 64153088 <= LIMIT
+    assert _scratch_bytes(162, 128, 201) == LIMIT
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nx,ny,nz", [(32, 24, 16), (96, 96, 64), (160, 160, 160)])
+@pytest.mark.parametrize("nx,ny,nz", [(32, 24, 16), (96, 96, 64), (162, 128, 201)])
 def test_noalloc_matches_workspace_solve(nx, ny, nz):
-    """(160, 160, 160) needs 65955328 of the 67108864 bytes: its tables end
-    close to the end of the static array (and 160 takes the shared-memory
-    Stockham transforms, 96 the register ones)."""
+    """(162, 128, 201) needs exactly the 67108864 bytes of the static array:
+    its last table ends at the array's last byte (162 takes the shared-memory
+    Stockham transforms along x, 128 and 96 the register ones)."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")

@@ -152,6 +152,14 @@ class Channel:
         kernels (off); raises when the grid's cluster shape does not fit."""
         L.check(self.lib.tc_use_fused_poisson(self.ctx, int(bool(on))))
 
+    def use_fp32_poisson(self, on=True, warm_steps=10):
+        """Single-precision Poisson step (mixed precision): FP32 spectrum,
+        FP64 for the (0,0) and lowest modes, solving for the increment of p
+        over the previous step's pressure; the first `warm_steps` steps after
+        set_state use the FP64 solve.  Raises for FP64 contexts and for grids
+        whose kx slab does not fit one CTA's shared memory."""
+        L.check(self.lib.tc_use_fp32_poisson(self.ctx, int(bool(on)), int(warm_steps)))
+
     def project_initial(self):
         L.check(self.lib.tc_project_initial(self.ctx, _stream()))
 

@@ -15,6 +15,7 @@
 #include "tc_common.cuh"
 #include "tc_fft.cuh"
 #include "tc_poisson.cuh"
+#include "tc_poisson32.cuh"
 #include "tc_stats.cuh"
 #include "tc_step.cuh"
 #include "tc_adjoint.cuh"
@@ -95,6 +96,19 @@ struct tc_ctx {
   size_t yz_smem;
   int cur, have_hist, state_set;
   double tab_dt;
+  // single-precision Poisson step (mixed contexts, tc_use_fp32_poisson): FP32
+  // pressure pair (pf[pcur] = the last step's p, the base of the next solve;
+  // the projection writes the new p into the other), FP32 factor tables and
+  // y twiddles, FP64 scratch of the low modes; the FP32 spectrum and the
+  // increment dp overlay X and p
+  float* pf[2];
+  float* rden32; float* cp32;
+  cpx<float>* twy32;
+  double* lowbuf;
+  int pcur, p_hist, p_f32;  // pf[pcur] holds p; p of the last step is in pf (else in p)
+  int psp_on, psp_ok, psp_warm, nlow, since_set;
+  int yz32_thr;
+  size_t yz32_smem;
   // adjoint: body force of the forward step (caller-owned, FP64 internal
   // layout, or null) and the dt of the CN adjoint tables in the scratch
   const double* body[3];
@@ -107,7 +121,7 @@ struct tc_ctx {
   // CUDA graph of two consecutive steps (tc_step replays it for n_steps >= 4)
   cudaStream_t cap_stream;
   cudaGraphExec_t gexec;
-  int g_valid, g_scheme, g_cur;
+  int g_valid, g_scheme, g_cur, g_pcur, g_psp;
   double g_dt;
   int graphs_on;
   // per-phase timing ring (tc_timing_enable)
@@ -137,6 +151,10 @@ template <class T> static Grid<T> make_grid(const tc_ctx* c, int which_unused = 
   g.ubase_d = mixed ? c->ubase_d : nullptr;
   return g;
 }
+
+// Lowest wavenumbers solved in FP64 by the single-precision Poisson step:
+// kx < PSP_NLOW and |ky| < PSP_NLOW (the (0,0) mode among them).
+#define PSP_NLOW 3
 
 static size_t carve(tc_ctx* c, char* base) {
   Carver cv; cv.base = base;
@@ -184,6 +202,14 @@ static size_t carve(tc_ctx* c, char* base) {
   c->st_spec = cv.take<double>((size_t)4 * (c->nx / 2) * (c->ny / 2) * 8);
   c->st_means = cv.take<double>(3 * c->nz * 8);
   c->st_S = cv.take<cpx<double>>(3 * n * 16);
+  if (c->precision == TC_MIXED) {
+    c->pf[0] = cv.take<float>(ncell * 4);
+    c->pf[1] = cv.take<float>(ncell * 4);
+    c->rden32 = cv.take<float>(nspec * 4);
+    c->cp32 = cv.take<float>(nspec * 4);
+    c->twy32 = cv.take<cpx<float>>((size_t)c->ny * 8);
+    c->lowbuf = cv.take<double>(yz32_lowbuf_doubles(PSP_NLOW, c->nz) * 8);
+  }
   return cv.off + 256;
 }
 
@@ -456,6 +482,24 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   return TC_OK;
 }
 
+// ---- single-precision Poisson step (mixed contexts) ----------------------
+// k_yz32 lengths: ny = 16 K with a register transform and K <= 24 (N <= 384).
+template <class F> static void for_each_yz32(int n, F&& f) {
+  switch (n / 16) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 9: f(std::integral_constant<int, 9>{}); break;
+    case 12: f(std::integral_constant<int, 12>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    case 18: f(std::integral_constant<int, 18>{}); break;
+    case 24: f(std::integral_constant<int, 24>{}); break;
+    default: break;
+  }
+}
+static bool yz32_len_ok(int ny) { return rowfft_supported(ny) && ny / 16 <= 24; }
+static bool psp_ready(const tc_ctx* c) { return c->psp_on && c->p_hist >= 1 && c->since_set >= c->psp_warm; }
+
 template <class T> static void to_t(const std::vector<double>& src, std::vector<unsigned char>& dst) {
   dst.resize(src.size() * sizeof(T));
   T* d = reinterpret_cast<T*>(dst.data());
@@ -483,6 +527,43 @@ static std::vector<double> twiddles(int n) {
     t[2 * m + 1] = std::sin(ang);
   }
   return t;
+}
+
+// Whether the single-precision Poisson step can run on this grid (register x
+// transforms, a k_yz32 length, the kx slab within a CTA's shared memory),
+// and its tables and kernel attributes.
+static int psp_setup(tc_ctx* c, const std::vector<double>& twy) {
+  c->psp_ok = 0; c->psp_on = 0; c->psp_warm = 10; c->nlow = PSP_NLOW;
+  if (c->precision != TC_MIXED || !xreg_ok(c) || !yz32_len_ok(c->ny)) return TC_OK;
+  int optin = 0;
+  TC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+  c->yz32_smem = yz32_smem_bytes(c->ny, c->nz);
+  if (c->yz32_smem > (size_t)optin) return TC_OK;
+  int rc = TC_OK;
+  for_each_yz32(c->ny, [&](auto I) {
+    constexpr int K = decltype(I)::value;
+    c->yz32_thr = yz32_threads<K>();
+    if (cudaFuncSetAttribute(k_yz32<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->yz32_smem) !=
+        cudaSuccess)
+      rc = fail(TC_ERR_CUDA, "k_yz32 attributes");
+  });
+  if (rc) return rc;
+  for_each_n1(c->nx, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    if (cudaFuncSetAttribute(k_div_fftx_reg32<float, N1, XROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fftx_reg_smem<N1>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_ifftx_reg32<N1, XROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ifftx_reg_smem<N1>()) != cudaSuccess)
+      rc = fail(TC_ERR_CUDA, "single-precision x transform attributes");
+  });
+  if (rc) return rc;
+  const size_t nspec = (size_t)c->nxh * c->nz * c->ny;
+  k_tri_factors32<<<(unsigned)((nspec + 255) / 256 < 4096 ? (nspec + 255) / 256 : 4096), 256>>>(
+      c->tri_rden, c->tri_cp, c->rden32, c->cp32, nspec);
+  if (cudaGetLastError() != cudaSuccess) return fail(TC_ERR_CUDA, "FP32 factor tables launch");
+  if ((rc = upload(c->twy32, twy, 4))) return rc;
+  c->psp_ok = 1;
+  return TC_OK;
 }
 
 extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, tc_ctx** out) {
@@ -538,6 +619,7 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     k_tri_factors<<<(nmodes + 127) / 128, 128>>>(tb, c->tri_rden, c->tri_cp, c->nxh, c->ny, c->nz);
     if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
   }
+  if ((r2 = psp_setup(c, twy))) return bail(r2);
   c->yz_ok = yz_probe(c);
   c->yzr_ok = c->yz_ok ? yzr_probe(c) : 0;
   c->yz_on = 0;  // the three-kernel path with register FFTs is faster
@@ -699,6 +781,46 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   return TC_OK;
 }
 
+// The single-precision Poisson solve of a step: L dp = div(u**)/dt - L pf[pcur]
+// with the FP32 spectrum (x transform with the base's Laplacian, the fused
+// y / z / inverse-y slab kernel, inverse x transform into dp = c->p as FP32).
+template <class T> static int poisson32_impl(tc_ctx* c, const T* u, const T* v, const T* w, double dt,
+                                             cudaStream_t s) {
+  if constexpr (sizeof(T) != 4) {
+    return fail(TC_ERR_ARG, "the single-precision Poisson step needs a mixed-precision context");
+  } else {
+    Grid<float> g = make_grid<float>(c);
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    cpx<float>* Xf = reinterpret_cast<cpx<float>*>(c->X);
+    float* dpf = reinterpret_cast<float*>(c->p);
+    const BaseLap bl{c->pf[c->pcur], 1.0 / (c->dx * c->dx), 1.0 / (c->dy * c->dy), c->cl, c->cr,
+                     1.0 / ((double)nx * (double)ny)};
+    const double scale = 1.0 / (dt * (double)nx * (double)ny);
+    mark(c, TC_PH_FFTX, s);
+    for_each_n1(nx, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      k_div_fftx_reg32<float, N1, XROWS><<<dim3(ny / XROWS, nz), xreg_threads<N1>(), fftx_reg_smem<N1>(), s>>>(
+          g, u, v, w, Xf, c->twx_d, scale, bl);
+    });
+    mark(c, TC_PH_FFTY, s);
+    for_each_yz32(ny, [&](auto I) {
+      constexpr int K = decltype(I)::value;
+      k_yz32<K><<<c->nxh, c->yz32_thr, c->yz32_smem, s>>>(Xf, c->rden32, c->cp32, c->tri_rden, c->tri_cp, c->cl,
+                                                         c->twy32, nz, c->nlow, c->lowbuf, c->err);
+    });
+    mark(c, TC_PH_TRI, s);
+    mark(c, TC_PH_IFFTY, s);
+    mark(c, TC_PH_IFFTX, s);
+    for_each_n1(nx, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      k_ifftx_reg32<N1, XROWS><<<dim3(ny / XROWS, nz), xreg_threads<N1>(), ifftx_reg_smem<N1>(), s>>>(
+          Xf, dpf, ny, nz, c->twx_d);
+    });
+    TC_LAUNCHED();
+    return TC_OK;
+  }
+}
+
 // Chunk length of the CN solve: 16 rows up to nz = 256 (at most 16 warps),
 // 32 rows for deeper channels (nz <= 512).  The G/H tables follow it.
 static int cn_len(const tc_ctx* c) {
@@ -735,13 +857,17 @@ static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, 
 
 static double bulk_scale(const tc_ctx* c) { return c->dx * c->dy / (c->Lx * c->Ly * c->Lz); }
 
-template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, int update_forcing, cudaStream_t s) {
+template <class T, class PS>
+static int project_impl_ps(tc_ctx* c, T* const* S, const PS& ps, double dt, int update_forcing, cudaStream_t s) {
   Grid<T> g = make_grid<T>(c);
   BulkArgs ba{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, update_forcing};
   dim3 grd((c->nx / 2 + 31) / 32, (c->ny + 7) / 8, (c->nz + PROJ_PK - 1) / PROJ_PK);
-  k_project_bulk<T><<<grd, dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], c->p, dt, c->dzf_d, ba);
+  k_project_bulk<T, PS><<<grd, dim3(32, 8), 0, s>>>(g, S[0], S[1], S[2], ps, dt, c->dzf_d, ba);
   TC_LAUNCHED();
   return TC_OK;
+}
+template <class T> static int project_impl(tc_ctx* c, T* const* S, double dt, int update_forcing, cudaStream_t s) {
+  return project_impl_ps<T, PSrc64>(c, S, PSrc64{c->p, nullptr}, dt, update_forcing, s);
 }
 
 template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaStream_t s) {
@@ -782,10 +908,29 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
     launch_cn<T>(c, B[0], B[1], B[2], s);
     TC_LAUNCHED();
   }
-  int rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
+  // single-precision Poisson: the increment over pf[pcur] once a base exists
+  // and the warm-up steps after set_state are done; before that the FP64
+  // solve, whose p (rounded) becomes the base
+  const bool psp_now = psp_ready(c);
+  int rc;
+  if (psp_now)
+    rc = poisson32_impl<T>(c, B[0], B[1], B[2], dt, s);
+  else
+    rc = poisson_impl<T>(c, B[0], B[1], B[2], nullptr, c->p, 1.0 / (dt * (double)c->nx * (double)c->ny), s);
   if (rc) return rc;
   mark(c, TC_PH_PROJ, s);
-  if ((rc = project_impl<T>(c, B, dt, scheme != TC_FE, s))) return rc;
+  if constexpr (sizeof(T) == 4) {
+    if (psp_now)
+      rc = project_impl_ps<T, PSrcInc>(c, B, PSrcInc{c->pf[c->pcur], reinterpret_cast<const float*>(c->p),
+                                                       c->pf[c->pcur ^ 1]},
+                                       dt, scheme != TC_FE, s);
+    else
+      rc = project_impl_ps<T, PSrc64>(c, B, PSrc64{c->p, c->psp_on ? c->pf[c->pcur ^ 1] : nullptr}, dt,
+                                      scheme != TC_FE, s);
+  } else {
+    rc = project_impl<T>(c, B, dt, scheme != TC_FE, s);
+  }
+  if (rc) return rc;
   if constexpr (sizeof(T) == 8) {
     const dim3 ag((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz + 1);
     if (c->ke_acc) {
@@ -810,6 +955,12 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   }
   c->cur = nxt;
   if (scheme != TC_FE) c->have_hist = 1;
+  if (c->psp_on) {
+    c->pcur ^= 1;
+    c->p_hist = 1;
+  }
+  c->p_f32 = psp_now;
+  c->since_set++;
   return TC_OK;
 }
 
@@ -846,7 +997,11 @@ template <class T> static int diag_impl(tc_ctx* c, cudaStream_t s) {
   dim3 grd = grid3(c, c->nz);
   const int nb = grd.x * grd.y * grd.z;
   // nb = gx*gy*nz <= npart: one partials buffer each for the max and the flag
-  k_diag_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], c->p, c->partials2, c->partials);
+  if (c->p_f32)
+    k_diag_partials<T, float><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], c->pf[c->pcur], c->partials2,
+                                                          c->partials);
+  else
+    k_diag_partials<T><<<grd, dim3(32, 8), 0, s>>>(g, A[0], A[1], A[2], c->p, c->partials2, c->partials);
   k_max_finalize<<<1, 256, 0, s>>>(c->partials2, nb, c->scal + SC_MAXDIV);
   k_max_finalize<<<1, 256, 0, s>>>(c->partials, nb, c->scal + SC_NONFINITE);
   k_utau_sums<T><<<2, 256, 0, s>>>(g, A[0], c->scal);
@@ -909,6 +1064,9 @@ extern "C" int tc_set_state(tc_ctx* c, const double* u, const double* v, const d
   TC_CUDA(cudaMemsetAsync(c->p, 0, (size_t)c->nx * c->ny * c->nz * 8, ST(stream)));
   c->have_hist = 0;
   c->state_set = 1;
+  c->p_hist = 0;   // no pressure base for a single-precision solve yet
+  c->p_f32 = 0;
+  c->since_set = 0;
   if (c->precision == TC_MIXED) c->tab_dt = -1.0;  // the CN tables carry the new base profile
   return TC_OK;
 }
@@ -927,7 +1085,8 @@ template <class T> static int get_state_impl(tc_ctx* c, double* u, double* v, do
   if (u && (rc = to_ref<T>(c, A[0], u, FLD_U, s, ubase_of(c)))) return rc;
   if (v && (rc = to_ref<T>(c, A[1], v, FLD_V, s))) return rc;
   if (w && (rc = to_ref<T>(c, A[2], w, FLD_W, s))) return rc;
-  if (p && (rc = to_ref<double>(c, c->p, p, FLD_P, s))) return rc;
+  if (p && c->p_f32 && (rc = to_ref<float>(c, c->pf[c->pcur], p, FLD_P, s))) return rc;
+  if (p && !c->p_f32 && (rc = to_ref<double>(c, c->p, p, FLD_P, s))) return rc;
   return TC_OK;
 }
 
@@ -982,6 +1141,8 @@ static int build_graph(tc_ctx* c, int scheme, double dt) {
   }
   if (!c->cap_stream) TC_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
   const int cur0 = c->cur, hist0 = c->have_hist;
+  const int pcur0 = c->pcur, phist0 = c->p_hist, pf320 = c->p_f32, since0 = c->since_set;
+  const int psp0 = psp_ready(c);
   TC_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
   int rc = TC_OK;
   for (int q = 0; q < 2 && rc == TC_OK; ++q) rc = DISPATCH(c, step_impl, c, scheme, dt, c->cap_stream);
@@ -989,12 +1150,14 @@ static int build_graph(tc_ctx* c, int scheme, double dt) {
   cudaError_t e = cudaStreamEndCapture(c->cap_stream, &graph);
   c->cur = cur0;  // capture launched nothing: restore the host-side state
   c->have_hist = hist0;
+  c->pcur = pcur0; c->p_hist = phist0; c->p_f32 = pf320; c->since_set = since0;
   if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
   if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   e = cudaGraphInstantiate(&c->gexec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return fail(TC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   c->g_valid = 1; c->g_scheme = scheme; c->g_dt = dt; c->g_cur = cur0;
+  c->g_pcur = pcur0; c->g_psp = psp0;
   return TC_OK;
 }
 
@@ -1006,17 +1169,21 @@ extern "C" int tc_step(tc_ctx* c, int scheme, double dt, int n_steps, void* stre
   int n = 0;
   // plain launches until the history exists and the CN tables match dt
   while (n < n_steps && (!c->have_hist || (scheme == TC_IMEX && c->tab_dt != dt) || c->timing || !c->graphs_on ||
-                         n_steps - n < 4)) {
+                         (c->psp_on && !psp_ready(c)) || n_steps - n < 4)) {
     int rc = DISPATCH(c, step_impl, c, scheme, dt, ST(stream));
     if (rc) return rc;
     ++n;
   }
   if (n_steps - n >= 2) {
-    if (!c->g_valid || c->g_scheme != scheme || c->g_dt != dt || c->g_cur != c->cur) {
+    if (!c->g_valid || c->g_scheme != scheme || c->g_dt != dt || c->g_cur != c->cur || c->g_pcur != c->pcur ||
+        c->g_psp != (int)psp_ready(c)) {
       int rc = build_graph(c, scheme, dt);
       if (rc) return rc;
     }
-    for (; n + 2 <= n_steps; n += 2) TC_CUDA(cudaGraphLaunch(c->gexec, ST(stream)));
+    for (; n + 2 <= n_steps; n += 2) {
+      TC_CUDA(cudaGraphLaunch(c->gexec, ST(stream)));
+      c->since_set += 2;
+    }
   }
   for (; n < n_steps; ++n) {
     int rc = DISPATCH(c, step_impl, c, scheme, dt, ST(stream));
@@ -1044,9 +1211,29 @@ extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
   return TC_OK;
 }
 
+extern "C" int tc_use_fp32_poisson(tc_ctx* c, int on, int warm_steps) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (warm_steps < 0) return fail(TC_ERR_ARG, "warm_steps must be >= 0");
+  if (on && c->precision != TC_MIXED) return fail(TC_ERR_ARG, "the single-precision Poisson step needs TC_MIXED");
+  if (on && !c->psp_ok)
+    return fail(TC_ERR_SIZE, "single-precision Poisson step not available for this grid (register-transform nx, "
+                             "ny = 16 K with K <= 24, and a kx slab of ny * nz * 8 bytes within shared memory)");
+  const int was = c->psp_on;
+  c->psp_on = on ? 1 : 0;
+  c->psp_warm = warm_steps;
+  if (c->psp_on && !was) c->p_hist = 0;  // the ring holds no base yet
+  if (c->g_valid) {  // the captured steps hold the other path
+    cudaGraphExecDestroy(c->gexec);
+    c->g_valid = 0;
+  }
+  return TC_OK;
+}
+
 extern "C" int tc_project_initial(tc_ctx* c, void* stream) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
   if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  c->p_hist = 0;  // the dt = 1 pressure of this projection is no base for a step
+  c->p_f32 = 0;
   return DISPATCH(c, project_initial_impl, c, ST(stream));
 }
 
@@ -1197,6 +1384,7 @@ template <class T> static int project_hook_impl(tc_ctx* c, const double* p, doub
 extern "C" int tc_project(tc_ctx* c, const double* p, double dt, void* stream) {
   if (!c || !p) return fail(TC_ERR_ARG, "null argument");
   if (!c->state_set) return fail(TC_ERR_STATE, "no state");
+  c->p_f32 = 0;  // the given p (in the FP64 buffer) is the current one
   return DISPATCH(c, project_hook_impl, c, p, dt, ST(stream));
 }
 
@@ -2155,6 +2343,7 @@ extern "C" int tc_batch_step(tc_batch* b, int scheme, const double* dts, int n_s
     if (!c->state_set) return fail(TC_ERR_STATE, "member without a state");
     if (!(dts[i] > 0)) return fail(TC_ERR_ARG, "dt must be > 0");
     if (c->body[0] || c->ke_acc || c->tape) return fail(TC_ERR_ARG, "ensemble launches take no adjoint hooks");
+    if (c->psp_on) return fail(TC_ERR_ARG, "ensemble launches take no single-precision Poisson members");
     if (b->valid && (b->dts[i] != dts[i] || c->cur != (b->cur0[i] ^ b->q))) rebuild = true;
     if (scheme == TC_IMEX && c->tab_dt != dts[i]) rebuild = true;
     lack = lack || (scheme != TC_FE && !c->have_hist);

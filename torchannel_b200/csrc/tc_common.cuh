@@ -99,6 +99,7 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
 enum : int {
   TCE_NONFINITE = 1,
   TCE_BOUNDS = 2,
+  TCE_TIMEOUT = 4,  // a bounded wait for a bulk copy ran out
 };
 
 }  // namespace tc

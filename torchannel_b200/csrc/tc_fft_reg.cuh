@@ -62,22 +62,23 @@ constexpr CxCS cx_cossin(int e, int n) {
 }
 
 // a * W_N^E with W_N = exp(-2 pi i / N) (forward) or its conjugate (inverse);
-// exact for the multiples of a quarter turn.
-template <int E, int N, bool INV> __device__ __forceinline__ cpx<double> twc(cpx<double> a) {
+// exact for the multiples of a quarter turn.  T = double or float (the
+// constants are rounded once to T).
+template <int E, int N, bool INV, class T = double> __device__ __forceinline__ cpx<T> twc(cpx<T> a) {
   constexpr int e = ((E % N) + N) % N;
   if constexpr (e == 0) {
     return a;
   } else if constexpr (4 * e == N) {
-    return mul_mi<double, INV>(a);
+    return mul_mi<T, INV>(a);
   } else if constexpr (2 * e == N) {
-    return cmake<double>(-a.x, -a.y);
+    return cmake<T>(-a.x, -a.y);
   } else if constexpr (4 * e == 3 * N) {
-    return mul_mi<double, !INV>(a);
+    return mul_mi<T, !INV>(a);
   } else {
     constexpr CxCS w = cx_cossin(e, N);
-    constexpr double c = w.c, s = w.s;
-    return INV ? cmake<double>(a.x * c - a.y * s, a.x * s + a.y * c)
-               : cmake<double>(a.x * c + a.y * s, a.y * c - a.x * s);
+    constexpr T c = (T)w.c, s = (T)w.s;
+    return INV ? cmake<T>(a.x * c - a.y * s, a.x * s + a.y * c)
+               : cmake<T>(a.x * c + a.y * s, a.y * c - a.x * s);
   }
 }
 
@@ -89,48 +90,48 @@ template <int B, int E, class F> __device__ __forceinline__ void static_for(F&& 
 }
 
 // ---- small DFTs in registers (natural order in and out) -------------------
-template <int N, bool INV> struct Dft;
-template <bool INV> struct Dft<1, INV> { static __device__ __forceinline__ void run(cpx<double>*) {} };
-template <bool INV> struct Dft<2, INV> {
-  static __device__ __forceinline__ void run(cpx<double>* v) { dft2<double, INV>(v); }
+template <int N, bool INV, class T = double> struct Dft;
+template <bool INV, class T> struct Dft<1, INV, T> { static __device__ __forceinline__ void run(cpx<T>*) {} };
+template <bool INV, class T> struct Dft<2, INV, T> {
+  static __device__ __forceinline__ void run(cpx<T>* v) { dft2<T, INV>(v); }
 };
-template <bool INV> struct Dft<3, INV> {
-  static __device__ __forceinline__ void run(cpx<double>* v) { dft3<double, INV>(v); }
+template <bool INV, class T> struct Dft<3, INV, T> {
+  static __device__ __forceinline__ void run(cpx<T>* v) { dft3<T, INV>(v); }
 };
-template <bool INV> struct Dft<4, INV> {
-  static __device__ __forceinline__ void run(cpx<double>* v) { dft4<double, INV>(v); }
+template <bool INV, class T> struct Dft<4, INV, T> {
+  static __device__ __forceinline__ void run(cpx<T>* v) { dft4<T, INV>(v); }
 };
-template <bool INV> struct Dft<8, INV> {
-  static __device__ __forceinline__ void run(cpx<double>* v) { dft8<double, INV>(v); }
+template <bool INV, class T> struct Dft<8, INV, T> {
+  static __device__ __forceinline__ void run(cpx<T>* v) { dft8<T, INV>(v); }
 };
 // N = R M: R-point DFTs of the stride-M subsets, twiddles W_N^(n2 k1), then
 // M-point DFTs; output index k1 + R k2.
 template <int N> constexpr int dft_first_radix() {
   return (N % 8 == 0 && N > 8) ? 8 : (N % 4 == 0) ? 4 : (N % 3 == 0) ? 3 : 2;
 }
-template <int N, bool INV> struct Dft {
-  static __device__ __forceinline__ void run(cpx<double>* v) {
+template <int N, bool INV, class T> struct Dft {
+  static __device__ __forceinline__ void run(cpx<T>* v) {
     constexpr int R = dft_first_radix<N>();
     constexpr int M = N / R;
     static_assert(R * M == N, "unsupported DFT length");
-    cpx<double> t[N];
+    cpx<T> t[N];
     static_for<0, M>([&](auto I2) {
       constexpr int n2 = decltype(I2)::value;
-      cpx<double> a[R];
+      cpx<T> a[R];
 #pragma unroll
       for (int n1 = 0; n1 < R; ++n1) a[n1] = v[M * n1 + n2];
-      Dft<R, INV>::run(a);
+      Dft<R, INV, T>::run(a);
       static_for<0, R>([&](auto K1) {
         constexpr int k1 = decltype(K1)::value;
-        t[k1 * M + n2] = twc<n2 * k1, N, INV>(a[k1]);
+        t[k1 * M + n2] = twc<n2 * k1, N, INV, T>(a[k1]);
       });
     });
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
-      cpx<double> b[M];
+      cpx<T> b[M];
 #pragma unroll
       for (int n2 = 0; n2 < M; ++n2) b[n2] = t[k1 * M + n2];
-      Dft<M, INV>::run(b);
+      Dft<M, INV, T>::run(b);
 #pragma unroll
       for (int k2 = 0; k2 < M; ++k2) v[k1 + R * k2] = b[k2];
     }

@@ -174,13 +174,42 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
 // rows per block of the register x transforms (XR below)
 #define XROWS 16
 
+// Pressure base of the single-precision Poisson step: the right-hand side
+// becomes div(u**)/dt - L p_b (L the discrete operator the solve inverts:
+// 3-point periodic x/y differences and the z rows of projection_fft.py:44-82
+// with their Neumann closures), so that the solve returns the increment
+// p - p_b.  p == nullptr: no base.
+struct BaseLap {
+  const float* p;      // p_b, [nz][ny][nx]
+  double idx2, idy2;   // 1/dx^2, 1/dy^2
+  const double* cl;    // nz: 1/(dz_c[k] dz_f[k])
+  const double* cr;    // nz: 1/(dz_c[k+1] dz_f[k])
+  double scale;        // factor of L p_b in the transformed field (1/(nx ny))
+};
+
+// L p_b at (i, j, k) in FP64 from the FP32 values.
+__device__ __forceinline__ double base_lap(const BaseLap& bl, int i, int j, int k, int nx, int ny, int nz) {
+  const float* p = bl.p;
+  const double c = (double)p[pidx(k, j, i, ny, nx)];
+  const double xm = (double)p[pidx(k, j, i == 0 ? nx - 1 : i - 1, ny, nx)];
+  const double xp = (double)p[pidx(k, j, i == nx - 1 ? 0 : i + 1, ny, nx)];
+  const double ym = (double)p[pidx(k, j == 0 ? ny - 1 : j - 1, i, ny, nx)];
+  const double yp = (double)p[pidx(k, j == ny - 1 ? 0 : j + 1, i, ny, nx)];
+  double l = (xp - 2.0 * c + xm) * bl.idx2 + (yp - 2.0 * c + ym) * bl.idy2;
+  if (k < nz - 1) l += bl.cr[k] * ((double)p[pidx(k + 1, j, i, ny, nx)] - c);
+  if (k > 0) l -= bl.cl[k] * (c - (double)p[pidx(k - 1, j, i, ny, nx)]);
+  return l;
+}
+
 // Rows j0 = bx * XR .. of plane k; blockDim.x may exceed the warps the rows
 // need (ensemble kernel), the extra warps only take part in the barrier.
-template <class T, int N1, int XR>
+// XT: element type of the written spectrum (double, or float for the
+// single-precision Poisson step, whose base pressure `bl` is subtracted).
+template <class T, int N1, int XR, class XT = double>
 __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
                                           const T* __restrict__ w, const double* __restrict__ field,
-                                          cpx<double>* __restrict__ X, const cpx<double>* __restrict__ twx,
-                                          double scale, int bx, int k) {
+                                          cpx<XT>* __restrict__ X, const cpx<double>* __restrict__ twx,
+                                          double scale, int bx, int k, const BaseLap& bl = BaseLap{}) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int ZP = (RF::TILE + 7) / 8 * 8 + 1;          // row pitch of the spectra (16 B mod 128 B)
@@ -206,7 +235,9 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
     } else {
       val = field[pidx(k, j, i, ny, N)];
     }
-    return val * scale;
+    val *= scale;
+    if (bl.p != nullptr) val -= base_lap(bl, i, j, k, N, ny, nz) * bl.scale;
+    return val;
   };
   if (ok && l < RF::N2)
     rowfft_pass1<N1, false>([&](int i) { return cmake<double>(divv(ja, i), divv(jb, i)); }, l, tile, twx);
@@ -234,7 +265,7 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
       const cpx<double> d = csub(Zm, Zn);
       out = cmake<double>(0.5 * d.y, -0.5 * d.x);
     }
-    X[((size_t)m * nz + k) * ny + j0 + r] = out;
+    X[((size_t)m * nz + k) * ny + j0 + r] = cmake<XT>((XT)out.x, (XT)out.y);
   }
 }
 
@@ -244,6 +275,18 @@ __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid
                                                      cpx<double>* __restrict__ X,
                                                      const cpx<double>* __restrict__ twx, double scale) {
   fftx_tile<T, N1, XR>(g, u, v, w, field, X, twx, scale, blockIdx.x, blockIdx.y);
+}
+
+// The x transform of the single-precision Poisson step: divergence minus the
+// base pressure's Laplacian, FP64 arithmetic, FP32 spectrum out.
+template <class T, int N1, int XR>
+__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg32(Grid<T> g, const T* __restrict__ u,
+                                                                             const T* __restrict__ v,
+                                                                             const T* __restrict__ w,
+                                                                             cpx<float>* __restrict__ X,
+                                                                             const cpx<double>* __restrict__ twx,
+                                                                             double scale, BaseLap bl) {
+  fftx_tile<T, N1, XR, float>(g, u, v, w, nullptr, X, twx, scale, blockIdx.x, blockIdx.y, bl);
 }
 
 // Inverse real FFT along x of rows j0 .. j0+XR-1 of plane k with the
@@ -257,8 +300,11 @@ template <int N1> __host__ __device__ constexpr int ifftx_pitch() {
   return ((NH > HT ? NH : HT) + 7) / 8 * 8 + 1;
 }
 
-template <int N1, int XR>
-__device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, double* __restrict__ p, int ny, int nz,
+// XT / PT: element types of the spectrum read and of the field written
+// (double / double, or float / float for the increment of the
+// single-precision Poisson step; the transform itself runs in FP64).
+template <int N1, int XR, class XT = double, class PT = double>
+__device__ __forceinline__ void ifftx_tile(const cpx<XT>* __restrict__ X, PT* __restrict__ p, int ny, int nz,
                                            const cpx<double>* __restrict__ twx, int bx, int k) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
@@ -268,7 +314,8 @@ __device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, do
   const int j0 = bx * XR;
   for (int e = threadIdx.x; e < NH * XR; e += blockDim.x) {
     const int m = e / XR, r = e % XR;
-    cpx<double> val = X[((size_t)m * nz + k) * ny + j0 + r];
+    const cpx<XT> x = X[((size_t)m * nz + k) * ny + j0 + r];
+    cpx<double> val = cmake<double>((double)x.x, (double)x.y);
     if (m == 0 || 2 * m == N) val.y = 0.0;  // irfft ignores these imaginary parts
     S[r * SP + m] = val;
   }
@@ -296,15 +343,24 @@ __device__ __forceinline__ void ifftx_tile(const cpx<double>* __restrict__ X, do
   __syncwarp();
   if (ok && l < RF::N2) rowfft_pass1_regs<N1, true>(vr, l, tile, twx);
   __syncwarp();
-  double* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
+  PT* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
   if (ok && l < RF::N1)
-    rowfft_pass2<N1, true>([&](int i, cpx<double> z) { pa[i] = z.x; pa[N + i] = z.y; }, l, tile);
+    rowfft_pass2<N1, true>([&](int i, cpx<double> z) { pa[i] = (PT)z.x; pa[N + i] = (PT)z.y; }, l, tile);
 }
 
 template <int N1, int XR>
 __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_ifftx_reg(const cpx<double>* __restrict__ X, double* __restrict__ p,
                                                   int ny, int nz, const cpx<double>* __restrict__ twx) {
   ifftx_tile<N1, XR>(X, p, ny, nz, twx, blockIdx.x, blockIdx.y);
+}
+
+// Inverse x transform of the single-precision Poisson step: FP32 spectrum
+// in, FP64 transform, FP32 pressure increment out.
+template <int N1, int XR>
+__global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_ifftx_reg32(const cpx<float>* __restrict__ X,
+                                                                          float* __restrict__ dp, int ny, int nz,
+                                                                          const cpx<double>* __restrict__ twx) {
+  ifftx_tile<N1, XR, float, float>(X, dp, ny, nz, twx, blockIdx.x, blockIdx.y);
 }
 
 // Thomas sweep along z for every mode (kx, ky), one thread per mode

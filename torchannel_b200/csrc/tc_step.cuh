@@ -689,12 +689,43 @@ template <class T> struct Vec2;
 template <> struct Vec2<double> { using t = double2; };
 template <> struct Vec2<float> { using t = float2; };
 
+// Sources of the pressure the projection applies.  PSrc64: an FP64 p (out,
+// when set, receives p rounded to FP32 as the base of a following
+// single-precision Poisson step).  PSrcInc: the single-precision Poisson
+// step's base p_b plus its increment dp, both FP32 and summed in FP64 (the
+// gradient of p_b + dp is exact to FP64 rounding, whatever the FP32 rounding
+// of p_b); out receives p_b + dp rounded to FP32, the next step's base.
+// pair(o) = p at o and o + 1, one(o) = p at o, keep(o, P) stores the pair P
+// the thread applied at its own points.
+struct PSrc64 {
+  const double* p;
+  float* out;
+  __device__ __forceinline__ double2 pair(size_t o) const { return *reinterpret_cast<const double2*>(p + o); }
+  __device__ __forceinline__ double one(size_t o) const { return ldg(p + o); }
+  __device__ __forceinline__ void keep(size_t o, double2 P) const {
+    if (out) *reinterpret_cast<float2*>(out + o) = make_float2((float)P.x, (float)P.y);
+  }
+};
+struct PSrcInc {
+  const float* pb;
+  const float* dp;
+  float* out;
+  __device__ __forceinline__ double2 pair(size_t o) const {
+    const float2 a = *reinterpret_cast<const float2*>(pb + o), b = *reinterpret_cast<const float2*>(dp + o);
+    return make_double2((double)a.x + (double)b.x, (double)a.y + (double)b.y);
+  }
+  __device__ __forceinline__ double one(size_t o) const { return (double)ldg(pb + o) + (double)ldg(dp + o); }
+  __device__ __forceinline__ void keep(size_t o, double2 P) const {
+    *reinterpret_cast<float2*>(out + o) = make_float2((float)P.x, (float)P.y);
+  }
+};
+
 // Block (bx, by, bz) of a grid of gx x gy x gz blocks of 32 x 8 threads.
-template <class T>
-__device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u, T* __restrict__ v,
-                                             T* __restrict__ w, const double* __restrict__ p, double dt,
-                                             const double* __restrict__ dzf, const BulkArgs& ba, int bx, int by,
-                                             int bz, int gx, int gy, int gz) {
+template <class T, class PS>
+__device__ __forceinline__ void project_tile_ps(const Grid<T>& g, T* __restrict__ u, T* __restrict__ v,
+                                                T* __restrict__ w, const PS& ps, double dt,
+                                                const double* __restrict__ dzf, const BulkArgs& ba, int bx, int by,
+                                                int bz, int gx, int gy, int gz) {
   using V2 = typename Vec2<T>::t;
   __shared__ double sh[32];
   __shared__ int last;
@@ -708,7 +739,7 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
     const double cx = dt * (double)g.idx, cy = dt * (double)g.idy;
     // p of the plane below k0 for w's face k0 (walls excluded below)
     double2 Pm = make_double2(0.0, 0.0);
-    if (k0 >= 1) Pm = *reinterpret_cast<const double2*>(p + pidx(k0 - 1, j, i, ny, nx));
+    if (k0 >= 1) Pm = ps.pair(pidx(k0 - 1, j, i, ny, nx));
     if constexpr (sizeof(T) == 4) {
       // FP32 storage: the next plane's loads are issued before this plane's
       // stores (the FP64 form has no registers to spare for it)
@@ -716,9 +747,9 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
       auto load = [&](int k) {
         Ld l;
         const size_t o = pidx(k, j, i, ny, nx);
-        l.P = *reinterpret_cast<const double2*>(p + o);
-        l.P2 = ldg(p + pidx(k, j, ipp, ny, nx));
-        l.Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
+        l.P = ps.pair(o);
+        l.P2 = ps.one(pidx(k, j, ipp, ny, nx));
+        l.Py = ps.pair(pidx(k, jp, i, ny, nx));
         l.uu = *reinterpret_cast<const V2*>(u + o);
         l.vv = *reinterpret_cast<const V2*>(v + o);
         l.ww = *reinterpret_cast<const V2*>(w + o);
@@ -749,6 +780,7 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
             ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
             *reinterpret_cast<V2*>(w + o) = ww;
           }
+          ps.keep(o, P);
           Pm = P;
           cur = nxt;
         }
@@ -759,9 +791,9 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
         const int k = k0 + kk;
         if (k < nz) {
           const size_t o = pidx(k, j, i, ny, nx);
-          const double2 P = *reinterpret_cast<const double2*>(p + o);
-          const double P2 = ldg(p + pidx(k, j, ipp, ny, nx));
-          const double2 Py = *reinterpret_cast<const double2*>(p + pidx(k, jp, i, ny, nx));
+          const double2 P = ps.pair(o);
+          const double P2 = ps.one(pidx(k, j, ipp, ny, nx));
+          const double2 Py = ps.pair(pidx(k, jp, i, ny, nx));
           V2 uu = *reinterpret_cast<V2*>(u + o);
           V2 vv = *reinterpret_cast<V2*>(v + o);
           uu.x = (T)((double)uu.x - cx * (P.y - P.x));
@@ -778,6 +810,7 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
             ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
             *reinterpret_cast<V2*>(w + o) = ww;
           }
+          ps.keep(o, P);
           Pm = P;
         }
       }
@@ -799,11 +832,21 @@ __device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u
   }
 }
 
+// The projection with an FP64 pressure p.
 template <class T>
+__device__ __forceinline__ void project_tile(const Grid<T>& g, T* __restrict__ u, T* __restrict__ v,
+                                             T* __restrict__ w, const double* __restrict__ p, double dt,
+                                             const double* __restrict__ dzf, const BulkArgs& ba, int bx, int by,
+                                             int bz, int gx, int gy, int gz) {
+  project_tile_ps<T, PSrc64>(g, u, v, w, PSrc64{p, nullptr}, dt, dzf, ba, bx, by, bz, gx, gy, gz);
+}
+
+template <class T, class PS>
 __global__ void __launch_bounds__(256) k_project_bulk(Grid<T> g, T* __restrict__ u, T* __restrict__ v,
-                                                      T* __restrict__ w, const double* __restrict__ p, double dt,
+                                                      T* __restrict__ w, PS ps, double dt,
                                                       const double* __restrict__ dzf, BulkArgs ba) {
-  project_tile<T>(g, u, v, w, p, dt, dzf, ba, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z);
+  project_tile_ps<T, PS>(g, u, v, w, ps, dt, dzf, ba, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y,
+                         gridDim.z);
 }
 
 // Bulk sum over all DOFs without projection (set-up and diagnostics).
@@ -879,9 +922,9 @@ __global__ void k_max_finalize(const double* __restrict__ partials, int n, doubl
 // (solver.py:865-868) -> per-block partials (max, flag).  The base profile of
 // u cancels in the x difference.
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, class PT = double>
 __global__ void __launch_bounds__(256) k_diag_partials(Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
-                                                       const T* __restrict__ w, const double* __restrict__ p,
+                                                       const T* __restrict__ w, const PT* __restrict__ p,
                                                        double* __restrict__ pmax, double* __restrict__ pflag) {
   __shared__ double sh[32];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -895,7 +938,7 @@ __global__ void __launch_bounds__(256) k_diag_partials(Grid<T> g, const T* __res
     double dv = ((double)v[o] - (double)v[pidx(k, wrap(j - 1, ny), i, ny, nx)]) * (double)g.idy;
     double dw = ((double)w[pidx(k + 1, j, i, ny, nx)] - (double)w[o]) * (double)g.idzf[k];
     m = fabs(du + dv + dw);
-    double s = (double)u[o] + (double)v[o] + (double)w[pidx(k + 1, j, i, ny, nx)] + p[o];
+    double s = (double)u[o] + (double)v[o] + (double)w[pidx(k + 1, j, i, ny, nx)] + (double)p[o];
     if (!isfinite(s)) bad = 1.0;
     if (!isfinite(m)) m = INFINITY;
   }
