@@ -118,22 +118,33 @@ int tc_use_graphs(tc_ctx* ctx, int on);
  * counterpart. */
 int tc_use_fused_poisson(tc_ctx* ctx, int on);
 
+/* Staging of the explicit-RHS kernel: on (the default where the grid allows
+ * it: x rows a multiple of 16 bytes, nx >= 64, ny >= 16), its u, v, w tiles
+ * reach shared memory by 3-D tensor copies of the tensor memory accelerator
+ * in a persistent two-stage pipeline; off, by per-thread loads.  Same
+ * arithmetic, bit-identical results.  TC_ERR_SIZE when `on` is asked where it
+ * is not available.  No reference counterpart. */
+int tc_use_tma_rhs(tc_ctx* ctx, int on);
+
 /* Single-precision Poisson step (TC_MIXED contexts; TC_ERR_ARG otherwise):
- * the pressure solve of every step (projection_fft.py:101-215) with an FP32
- * spectrum -- x transform, y transforms and the z tridiagonal solves of all
- * but the lowest wavenumbers in FP32, the (kx, ky) = (0,0) mode and the
+ * the pressure solve of every IMEX step (projection_fft.py:101-215) with an
+ * FP32 spectrum -- x transform, y transforms and the z tridiagonal solves of
+ * all but the lowest wavenumbers in FP32, the (kx, ky) = (0,0) mode and the
  * modes with kx < 3 and |ky| < 3 solved in FP64 -- for the increment of p
- * over the previous step's pressure: the right-hand side becomes
- * div(u**)/dt - L p_prev, so FP32 rounding scales with the change of p over
- * one step, not with p (whose FP32 rounding alone would leave a
- * post-projection divergence of about 1e-5 on stretched grids).  The first
- * `warm_steps` steps after tc_set_state (and every step until a previous
- * pressure exists) use the FP64 solve.  y transform, z solve and inverse y
- * transform run as one kernel per kx slab with the slab in shared memory:
- * TC_ERR_SIZE unless nx has a register transform, ny = 16 K (K <= 24) and
- * ny * nz * 8 bytes fit one CTA's shared memory (e.g. 192 x 128).  p from
- * tc_get_state is then FP32-rounded.  No reference counterpart (the
- * reference solves in its field precision, FP64). */
+ * over the previous step's pressure p_prev: the CN kernel takes
+ * dt grad p_prev out of the velocity before the divergence is formed, and
+ * the projection applies the increment's gradient (the same projected
+ * velocity, since the projection removes every discrete gradient).  FP32
+ * rounding then scales with the change of p over one step, not with p, whose
+ * FP32 rounding alone would leave a post-projection divergence of about 1e-5
+ * on stretched grids.  The first `warm_steps` steps after tc_set_state (and
+ * every step until a previous pressure exists, and AB2 / FE steps) use the
+ * FP64 solve.  y transform, z solve and inverse y transform run as one kernel
+ * per kx slab with the slab in shared memory: TC_ERR_SIZE unless nx has a
+ * register transform, ny = 16 K (K <= 24) and the slab (ny * nz * 8 bytes
+ * plus tables) fits one CTA's shared memory (e.g. 192 x 128).  p from
+ * tc_get_state is then FP32-rounded.  No reference counterpart (the reference
+ * solves in its field precision, FP64). */
 int tc_use_fp32_poisson(tc_ctx* ctx, int on, int warm_steps);
 
 /* Initial projection of a fresh field: div -> Poisson -> u -= grad p

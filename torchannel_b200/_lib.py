@@ -45,6 +45,7 @@ SIGNATURES = [
     ("tc_use_graphs", _I, [_V, _I]),
     ("tc_use_fused_poisson", _I, [_V, _I]),
     ("tc_use_fp32_poisson", _I, [_V, _I, _I]),
+    ("tc_use_tma_rhs", _I, [_V, _I]),
     ("tc_project_initial", _I, [_V, _V]),
     ("tc_scalars", _I, [_V, ctypes.POINTER(_V)]),
     ("tc_set_forcing", _I, [_V, _D, _V]),

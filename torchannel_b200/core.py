@@ -152,6 +152,11 @@ class Channel:
         kernels (off); raises when the grid's cluster shape does not fit."""
         L.check(self.lib.tc_use_fused_poisson(self.ctx, int(bool(on))))
 
+    def use_tma_rhs(self, on=True):
+        """Explicit-RHS tiles staged by tensor copies (on, the default where
+        the grid allows it) or by per-thread loads (off); bit-identical."""
+        L.check(self.lib.tc_use_tma_rhs(self.ctx, int(bool(on))))
+
     def use_fp32_poisson(self, on=True, warm_steps=10):
         """Single-precision Poisson step (mixed precision): FP32 spectrum,
         FP64 for the (0,0) and lowest modes, solving for the increment of p

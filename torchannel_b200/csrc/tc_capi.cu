@@ -18,6 +18,7 @@
 #include "tc_poisson32.cuh"
 #include "tc_stats.cuh"
 #include "tc_step.cuh"
+#include "tc_rhs_tma.cuh"
 #include "tc_adjoint.cuh"
 #include "tc_batch.cuh"
 
@@ -99,14 +100,17 @@ struct tc_ctx {
   // single-precision Poisson step (mixed contexts, tc_use_fp32_poisson): FP32
   // pressure pair (pf[pcur] = the last step's p, the base of the next solve;
   // the projection writes the new p into the other), FP32 factor tables and
-  // y twiddles, FP64 scratch of the low modes; the FP32 spectrum and the
-  // increment dp overlay X and p
+  // y twiddles; the FP32 spectrum and the increment dp overlay X and p
   float* pf[2];
   float* rden32; float* cp32;
   cpx<float>* twy32;
-  double* lowbuf;
+  double* cz_d;             // nz + 1: dt / dz_c of the CN tables' dt (PGrad)
+  // RHS with tensor-copy staging (k_rhs_tma): maps of the u, v, w buffers of
+  // both state parities, usable here, switched on, persistent CTAs
+  CUtensorMap tmap[2][3];
+  int rhs_tma_ok, rhs_tma_on, rhs_tma_grid;
   int pcur, p_hist, p_f32;  // pf[pcur] holds p; p of the last step is in pf (else in p)
-  int psp_on, psp_ok, psp_warm, nlow, since_set;
+  int psp_on, psp_ok, psp_warm, since_set;
   int yz32_thr;
   size_t yz32_smem;
   // adjoint: body force of the forward step (caller-owned, FP64 internal
@@ -151,10 +155,6 @@ template <class T> static Grid<T> make_grid(const tc_ctx* c, int which_unused = 
   g.ubase_d = mixed ? c->ubase_d : nullptr;
   return g;
 }
-
-// Lowest wavenumbers solved in FP64 by the single-precision Poisson step:
-// kx < PSP_NLOW and |ky| < PSP_NLOW (the (0,0) mode among them).
-#define PSP_NLOW 3
 
 static size_t carve(tc_ctx* c, char* base) {
   Carver cv; cv.base = base;
@@ -208,7 +208,7 @@ static size_t carve(tc_ctx* c, char* base) {
     c->rden32 = cv.take<float>(nspec * 4);
     c->cp32 = cv.take<float>(nspec * 4);
     c->twy32 = cv.take<cpx<float>>((size_t)c->ny * 8);
-    c->lowbuf = cv.take<double>(yz32_lowbuf_doubles(PSP_NLOW, c->nz) * 8);
+    c->cz_d = cv.take<double>((size_t)(c->nz + 1) * 8);
   }
   return cv.off + 256;
 }
@@ -499,6 +499,11 @@ template <class F> static void for_each_yz32(int n, F&& f) {
 }
 static bool yz32_len_ok(int ny) { return rowfft_supported(ny) && ny / 16 <= 24; }
 static bool psp_ready(const tc_ctx* c) { return c->psp_on && c->p_hist >= 1 && c->since_set >= c->psp_warm; }
+// dt / dz_c for the base-pressure gradient of the CN kernel.
+__global__ void k_cz_table(const double* __restrict__ dzc, double* __restrict__ cz, int n, double dt) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) cz[e] = dt / dzc[e];
+}
 
 template <class T> static void to_t(const std::vector<double>& src, std::vector<unsigned char>& dst) {
   dst.resize(src.size() * sizeof(T));
@@ -529,11 +534,89 @@ static std::vector<double> twiddles(int n) {
   return t;
 }
 
+// ---- RHS with tensor-copy staging ----------------------------------------
+typedef CUresult (*TensorMapEncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                           const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                           CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                           CUtensorMapFloatOOBfill);
+
+// Tensor maps of the six state buffers (3-D: x, y, planes; boxes of the
+// k_rhs_tma tile), kernel attributes and the persistent grid.  Leaves
+// rhs_tma_ok = 0 (the staged kernel k_rhs_update runs) where the grid does
+// not allow it: x rows must be a multiple of 16 bytes and the domain at least
+// two tiles wide.
+template <class T> static int rhs_tma_setup(tc_ctx* c) {
+  constexpr int KB = rhs_tma_kb<T>();
+  using S = RhsTma<T, KB>;
+  c->rhs_tma_ok = 0;
+  c->rhs_tma_on = 0;
+  if (((size_t)c->nx * sizeof(T)) % 16 != 0 || c->nx < 2 * RHS_TX || c->ny < 2 * S::TY) return TC_OK;
+  static TensorMapEncodeTiledFn enc = nullptr;
+  if (!enc) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f) {
+      cudaGetLastError();
+      return TC_OK;
+    }
+    enc = (TensorMapEncodeTiledFn)f;
+  }
+  const CUtensorMapDataType dty = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  for (int st = 0; st < 2; ++st)
+    for (int f = 0; f < 3; ++f) {
+      const cuuint64_t gdim[3] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)(f == 2 ? c->nz + 1 : c->nz)};
+      const cuuint64_t gstr[2] = {(cuuint64_t)c->nx * sizeof(T), (cuuint64_t)c->nx * c->ny * sizeof(T)};
+      const cuuint32_t box[3] = {(cuuint32_t)S::BX, (cuuint32_t)S::BY, (cuuint32_t)S::BZ};
+      const cuuint32_t est[3] = {1, 1, 1};
+      if (enc(&c->tmap[st][f], dty, 3, c->st[st][f], gdim, gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return TC_OK;
+    }
+  const int sm = (int)S::smem();
+  if (cudaFuncSetAttribute(k_rhs_tma<T, false, UPD_AB2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_rhs_tma<T, true, UPD_AB2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_rhs_tma<T, true, UPD_FE, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return TC_OK;
+  }
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rhs_tma<T, false, UPD_AB2, KB>, RHS_TX * S::TY, sm) !=
+          cudaSuccess ||
+      nb < 1) {
+    cudaGetLastError();
+    return TC_OK;
+  }
+  int ntx, nty, ntz;
+  rhs_tma_tiles(c->nx, c->ny, c->nz, KB, &ntx, &nty, &ntz);
+  c->rhs_tma_grid = std::min(ntx * nty * ntz, nb * c->nsm);
+  c->rhs_tma_ok = 1;
+  c->rhs_tma_on = 1;
+  return TC_OK;
+}
+
+template <class T, bool FULL, int UPD>
+static void launch_rhs_tma(const tc_ctx* c, const Grid<T>& g, T* const* A, T* const* B, T* const* R, double dt,
+                           int have_hist, cudaStream_t s) {
+  constexpr int KB = rhs_tma_kb<T>();
+  using S = RhsTma<T, KB>;
+  int ntx, nty, ntz;
+  rhs_tma_tiles(c->nx, c->ny, c->nz, KB, &ntx, &nty, &ntz);
+  const CUtensorMap* m = c->tmap[c->cur];
+  k_rhs_tma<T, FULL, UPD, KB><<<c->rhs_tma_grid, dim3(RHS_TX, S::TY), S::smem(), s>>>(
+      m[0], m[1], m[2], g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2], c->scal + SC_FORCING, (T)dt,
+      have_hist, ntx, nty, ntz, c->err);
+}
+
 // Whether the single-precision Poisson step can run on this grid (register x
 // transforms, a k_yz32 length, the kx slab within a CTA's shared memory),
 // and its tables and kernel attributes.
 static int psp_setup(tc_ctx* c, const std::vector<double>& twy) {
-  c->psp_ok = 0; c->psp_on = 0; c->psp_warm = 10; c->nlow = PSP_NLOW;
+  c->psp_ok = 0; c->psp_on = 0; c->psp_warm = 10;
   if (c->precision != TC_MIXED || !xreg_ok(c) || !yz32_len_ok(c->ny)) return TC_OK;
   int optin = 0;
   TC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
@@ -620,6 +703,8 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
   }
   if ((r2 = psp_setup(c, twy))) return bail(r2);
+  r2 = (c->tsz == 8) ? rhs_tma_setup<double>(c) : rhs_tma_setup<float>(c);
+  if (r2) return bail(r2);
   c->yz_ok = yz_probe(c);
   c->yzr_ok = c->yz_ok ? yzr_probe(c) : 0;
   c->yz_on = 0;  // the three-kernel path with register FFTs is faster
@@ -781,9 +866,10 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   return TC_OK;
 }
 
-// The single-precision Poisson solve of a step: L dp = div(u**)/dt - L pf[pcur]
-// with the FP32 spectrum (x transform with the base's Laplacian, the fused
-// y / z / inverse-y slab kernel, inverse x transform into dp = c->p as FP32).
+// The single-precision Poisson solve of a step: L dp = div(u**)/dt with the
+// FP32 spectrum (x transform, the fused y / z / inverse-y slab kernel,
+// inverse x transform into dp = c->p as FP32); u** already lacks the base
+// pressure's gradient (launch_cn with PGrad), so dp is the increment over it.
 template <class T> static int poisson32_impl(tc_ctx* c, const T* u, const T* v, const T* w, double dt,
                                              cudaStream_t s) {
   if constexpr (sizeof(T) != 4) {
@@ -793,20 +879,18 @@ template <class T> static int poisson32_impl(tc_ctx* c, const T* u, const T* v, 
     const int nx = c->nx, ny = c->ny, nz = c->nz;
     cpx<float>* Xf = reinterpret_cast<cpx<float>*>(c->X);
     float* dpf = reinterpret_cast<float*>(c->p);
-    const BaseLap bl{c->pf[c->pcur], 1.0 / (c->dx * c->dx), 1.0 / (c->dy * c->dy), c->cl, c->cr,
-                     1.0 / ((double)nx * (double)ny)};
     const double scale = 1.0 / (dt * (double)nx * (double)ny);
     mark(c, TC_PH_FFTX, s);
     for_each_n1(nx, [&](auto I) {
       constexpr int N1 = decltype(I)::value;
       k_div_fftx_reg32<float, N1, XROWS><<<dim3(ny / XROWS, nz), xreg_threads<N1>(), fftx_reg_smem<N1>(), s>>>(
-          g, u, v, w, Xf, c->twx_d, scale, bl);
+          g, u, v, w, Xf, c->twx_d, scale);
     });
     mark(c, TC_PH_FFTY, s);
     for_each_yz32(ny, [&](auto I) {
       constexpr int K = decltype(I)::value;
       k_yz32<K><<<c->nxh, c->yz32_thr, c->yz32_smem, s>>>(Xf, c->rden32, c->cp32, c->tri_rden, c->tri_cp, c->cl,
-                                                         c->twy32, nz, c->nlow, c->lowbuf, c->err);
+                                                         c->twy32, nz, c->err);
     });
     mark(c, TC_PH_TRI, s);
     mark(c, TC_PH_IFFTY, s);
@@ -832,24 +916,26 @@ template <class T> static size_t cn_smem(const tc_ctx* c) {
   const int vec = (cn_len(c) <= 16 && sizeof(T) == 4) ? 2 : 1;
   return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32 * vec) * 8;
 }
-template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s) {
+template <class T>
+static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const PGrad& pg = PGrad{}) {
   const int ncol = c->nx * c->ny;
   const dim3 blk(32, cn_chunks(c));
   const int Lr = cn_len(c);
   const size_t sm = cn_smem<T>(c);
+  const double* ub = ubase_of(c);
   if (Lr <= 16) {
     constexpr int V = sizeof(T) == 4 ? 2 : 1;
     const dim3 grid((ncol / V + 31) / 32, 1, 3);
     if (Lr == 16)
-      k_cn_solve<T, 16, V, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
+      k_cn_solve<T, 16, V, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
     else
-      k_cn_solve<T, 16, V, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
+      k_cn_solve<T, 16, V, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
   } else {
     const dim3 grid((ncol + 31) / 32, 1, 3);
     if (Lr == 32)
-      k_cn_solve<T, 32, 1, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
+      k_cn_solve<T, 32, 1, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
     else
-      k_cn_solve<T, 32, 1, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ubase_of(c), c->nx, c->ny, c->nz, Lr);
+      k_cn_solve<T, 32, 1, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
   }
 }
 
@@ -881,10 +967,23 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   if (scheme == TC_IMEX && c->tab_dt != dt) {
     k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c),
                                  ubase_of(c));
+    if (c->cz_d) k_cz_table<<<(c->nz + 1 + 127) / 128, 128, 0, s>>>(c->dzc_d, c->cz_d, c->nz + 1, dt);
     c->tab_dt = dt;
   }
+  // single-precision Poisson (IMEX): the increment over pf[pcur] once a base
+  // exists and the warm-up steps after set_state are done; the CN kernel then
+  // takes the base's gradient out of the velocity.  Before that, and for the
+  // explicit schemes, the FP64 solve, whose p (rounded) becomes the base.
+  const bool psp_now = psp_ready(c) && scheme == TC_IMEX;
   mark(c, TC_PH_RHS, s);
-  if (scheme == TC_IMEX)
+  if (c->rhs_tma_on) {
+    if (scheme == TC_IMEX)
+      launch_rhs_tma<T, false, UPD_AB2>(c, g, A, B, R, dt, c->have_hist, s);
+    else if (scheme == TC_AB2)
+      launch_rhs_tma<T, true, UPD_AB2>(c, g, A, B, R, dt, c->have_hist, s);
+    else
+      launch_rhs_tma<T, true, UPD_FE>(c, g, A, B, R, dt, 0, s);
+  } else if (scheme == TC_IMEX)
     RhsKernel<T, false, UPD_AB2>::fn<<<grd, blk, 0, s>>>(g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2],
                                                          c->scal + SC_FORCING, (T)dt, c->have_hist);
   else if (scheme == TC_AB2)
@@ -905,13 +1004,10 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   }
   mark(c, TC_PH_CN, s);
   if (scheme == TC_IMEX) {
-    launch_cn<T>(c, B[0], B[1], B[2], s);
+    const PGrad pg = psp_now ? PGrad{c->pf[c->pcur], dt / c->dx, dt / c->dy, c->cz_d} : PGrad{};
+    launch_cn<T>(c, B[0], B[1], B[2], s, pg);
     TC_LAUNCHED();
   }
-  // single-precision Poisson: the increment over pf[pcur] once a base exists
-  // and the warm-up steps after set_state are done; before that the FP64
-  // solve, whose p (rounded) becomes the base
-  const bool psp_now = psp_ready(c);
   int rc;
   if (psp_now)
     rc = poisson32_impl<T>(c, B[0], B[1], B[2], dt, s);
@@ -921,9 +1017,9 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   mark(c, TC_PH_PROJ, s);
   if constexpr (sizeof(T) == 4) {
     if (psp_now)
-      rc = project_impl_ps<T, PSrcInc>(c, B, PSrcInc{c->pf[c->pcur], reinterpret_cast<const float*>(c->p),
-                                                       c->pf[c->pcur ^ 1]},
-                                       dt, scheme != TC_FE, s);
+      rc = project_impl_ps<T, PSrcDelta>(c, B, PSrcDelta{reinterpret_cast<const float*>(c->p), c->pf[c->pcur],
+                                                           c->pf[c->pcur ^ 1]},
+                                         dt, scheme != TC_FE, s);
     else
       rc = project_impl_ps<T, PSrc64>(c, B, PSrc64{c->p, c->psp_on ? c->pf[c->pcur ^ 1] : nullptr}, dt,
                                       scheme != TC_FE, s);
@@ -1204,6 +1300,19 @@ extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
   if ((on ? 1 : 0) != c->yz_on) {
     c->yz_on = on ? 1 : 0;
     if (c->g_valid) {  // the captured steps hold the other path
+      cudaGraphExecDestroy(c->gexec);
+      c->g_valid = 0;
+    }
+  }
+  return TC_OK;
+}
+
+extern "C" int tc_use_tma_rhs(tc_ctx* c, int on) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (on && !c->rhs_tma_ok) return fail(TC_ERR_SIZE, "tensor-copy RHS not available for this grid");
+  if ((on ? 1 : 0) != c->rhs_tma_on) {
+    c->rhs_tma_on = on ? 1 : 0;
+    if (c->g_valid) {  // the captured steps hold the other kernel
       cudaGraphExecDestroy(c->gexec);
       c->g_valid = 0;
     }

@@ -174,42 +174,15 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
 // rows per block of the register x transforms (XR below)
 #define XROWS 16
 
-// Pressure base of the single-precision Poisson step: the right-hand side
-// becomes div(u**)/dt - L p_b (L the discrete operator the solve inverts:
-// 3-point periodic x/y differences and the z rows of projection_fft.py:44-82
-// with their Neumann closures), so that the solve returns the increment
-// p - p_b.  p == nullptr: no base.
-struct BaseLap {
-  const float* p;      // p_b, [nz][ny][nx]
-  double idx2, idy2;   // 1/dx^2, 1/dy^2
-  const double* cl;    // nz: 1/(dz_c[k] dz_f[k])
-  const double* cr;    // nz: 1/(dz_c[k+1] dz_f[k])
-  double scale;        // factor of L p_b in the transformed field (1/(nx ny))
-};
-
-// L p_b at (i, j, k) in FP64 from the FP32 values.
-__device__ __forceinline__ double base_lap(const BaseLap& bl, int i, int j, int k, int nx, int ny, int nz) {
-  const float* p = bl.p;
-  const double c = (double)p[pidx(k, j, i, ny, nx)];
-  const double xm = (double)p[pidx(k, j, i == 0 ? nx - 1 : i - 1, ny, nx)];
-  const double xp = (double)p[pidx(k, j, i == nx - 1 ? 0 : i + 1, ny, nx)];
-  const double ym = (double)p[pidx(k, j == 0 ? ny - 1 : j - 1, i, ny, nx)];
-  const double yp = (double)p[pidx(k, j == ny - 1 ? 0 : j + 1, i, ny, nx)];
-  double l = (xp - 2.0 * c + xm) * bl.idx2 + (yp - 2.0 * c + ym) * bl.idy2;
-  if (k < nz - 1) l += bl.cr[k] * ((double)p[pidx(k + 1, j, i, ny, nx)] - c);
-  if (k > 0) l -= bl.cl[k] * (c - (double)p[pidx(k - 1, j, i, ny, nx)]);
-  return l;
-}
-
 // Rows j0 = bx * XR .. of plane k; blockDim.x may exceed the warps the rows
 // need (ensemble kernel), the extra warps only take part in the barrier.
 // XT: element type of the written spectrum (double, or float for the
-// single-precision Poisson step, whose base pressure `bl` is subtracted).
+// single-precision Poisson step).
 template <class T, int N1, int XR, class XT = double>
 __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
                                           const T* __restrict__ w, const double* __restrict__ field,
                                           cpx<XT>* __restrict__ X, const cpx<double>* __restrict__ twx,
-                                          double scale, int bx, int k, const BaseLap& bl = BaseLap{}) {
+                                          double scale, int bx, int k) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int ZP = (RF::TILE + 7) / 8 * 8 + 1;          // row pitch of the spectra (16 B mod 128 B)
@@ -235,9 +208,7 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
     } else {
       val = field[pidx(k, j, i, ny, N)];
     }
-    val *= scale;
-    if (bl.p != nullptr) val -= base_lap(bl, i, j, k, N, ny, nz) * bl.scale;
-    return val;
+    return val * scale;
   };
   if (ok && l < RF::N2)
     rowfft_pass1<N1, false>([&](int i) { return cmake<double>(divv(ja, i), divv(jb, i)); }, l, tile, twx);
@@ -277,16 +248,16 @@ __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid
   fftx_tile<T, N1, XR>(g, u, v, w, field, X, twx, scale, blockIdx.x, blockIdx.y);
 }
 
-// The x transform of the single-precision Poisson step: divergence minus the
-// base pressure's Laplacian, FP64 arithmetic, FP32 spectrum out.
+// The x transform of the single-precision Poisson step: the divergence in
+// FP64 arithmetic, the spectrum written in FP32.
 template <class T, int N1, int XR>
 __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg32(Grid<T> g, const T* __restrict__ u,
                                                                              const T* __restrict__ v,
                                                                              const T* __restrict__ w,
                                                                              cpx<float>* __restrict__ X,
                                                                              const cpx<double>* __restrict__ twx,
-                                                                             double scale, BaseLap bl) {
-  fftx_tile<T, N1, XR, float>(g, u, v, w, nullptr, X, twx, scale, blockIdx.x, blockIdx.y, bl);
+                                                                             double scale) {
+  fftx_tile<T, N1, XR, float>(g, u, v, w, nullptr, X, twx, scale, blockIdx.x, blockIdx.y);
 }
 
 // Inverse real FFT along x of rows j0 .. j0+XR-1 of plane k with the

@@ -16,66 +16,26 @@
 // * z solve: one thread per (ky, real / imaginary part) sweeps the column in
 //   shared memory with the per-mode LU factors of k_tri_factors, rounded to
 //   FP32 once; the factor loads run two blocks of levels ahead of the
-//   recurrence.  The (0,0) mode and the lowest wavenumbers (kx < nlow and
-//   |ky| < nlow) are solved in FP64 with the FP64 factors (the (0,0) mode
+//   recurrence.  The (0,0) mode and the lowest wavenumbers (kx < 3 and
+//   |ky| < 3) are solved in FP64 with the FP64 factors (the (0,0) mode
 //   gauged as in k_tri_lu: x_{nz-1} = 0).
 //
 // The step that uses it solves for the increment of p over a base pressure
-// (fftx_tile's BaseLap), which keeps the FP32 rounding of the solve small in
+// (the previous step's p, whose gradient the CN kernel takes out of the
+// velocity first, PGrad), which keeps the FP32 rounding of the solve small in
 // absolute terms: FP32 rounding of p itself would reach the post-projection
 // divergence amplified by dt / (dz_c dz_f) next to the walls.
 #pragma once
+#include "tc_async.cuh"
 #include "tc_common.cuh"
 #include "tc_fft_reg.cuh"
 
 namespace tc {
 
-// ---- mbarrier and bulk-copy helpers (inline PTX, sm_90+) ------------------
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-// Make the initialised barriers visible to the bulk-copy (async) proxy.
-__device__ __forceinline__ void mbar_init_fence() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
-// 16-byte aligned), completing on `bar`.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Wait for phase `parity` of `bar`, giving up after `limit` polls (each poll
-// suspends the thread for at most the hardware's try-wait interval, then
-// sleeps 128 ns): false when the wait ran out.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned limit) {
-  for (unsigned it = 0; it < limit; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    __nanosleep(128);
-  }
-  return false;
-}
-
 #define YZ32_CHUNKS 8          // bulk copies (and barriers) per slab
 #define YZ32_WAIT_LIMIT (1u << 21)
 #define YZ32_B 16              // levels per factor-load block of the z sweeps
+#define YZ32_NLOW 3            // FP64 modes: kx < 3 and ky < 3 or ky > ny - 3
 
 // Threads of k_yz32 for ny = 16 K: one per (ky, part) of the z solve, at
 // least 8 warps.
@@ -83,10 +43,16 @@ template <int K> __host__ __device__ constexpr int yz32_threads() {
   return 2 * 16 * K < 256 ? 256 : (2 * 16 * K + 31) / 32 * 32;
 }
 
+// FP64 d' columns of the low modes of one kx slab: (2 YZ32_NLOW - 1) ky
+// values x 2 parts x nz levels.
+__host__ __device__ inline size_t yz32_low_doubles(int nz) { return (size_t)(2 * YZ32_NLOW - 1) * 2 * nz; }
+
 // Shared memory of k_yz32 for ny = N and nz levels: the slab, the FP32
-// twiddles, a_k in FP32 (even count) and the barriers.
+// twiddles, a_k in FP32 (even count), the barriers and the low modes' FP64
+// d' columns.
 __host__ __device__ inline size_t yz32_smem_bytes(int N, int nz) {
-  return (size_t)nz * N * 8 + (size_t)N * 8 + (size_t)((nz + 1) & ~1) * 4 + YZ32_CHUNKS * 8;
+  return (size_t)nz * N * 8 + (size_t)N * 8 + (size_t)((nz + 1) & ~1) * 4 + YZ32_CHUNKS * 8 +
+         yz32_low_doubles(nz) * 8;
 }
 
 // One row of N = N1 N2 FP32 complex values in shared memory, transformed in
@@ -193,12 +159,6 @@ __device__ __forceinline__ void yz32_sweep(float* col, int stride, R* dq, int dq
   }
 }
 
-// The FP64 modes of k_yz32: kx < nlow and ky < nlow or ky > ny - nlow.
-// Their d' columns live in `lowbuf`, [kx][2 nlow - 1][part][nz] doubles.
-__host__ __device__ inline size_t yz32_lowbuf_doubles(int nlow, int nz) {
-  return (size_t)nlow * (2 * nlow - 1) * 2 * nz;
-}
-
 // One CTA per kx slab (gridDim.x = nx/2+1), ny = RowFft<K>::N, blockDim.x a
 // multiple of 32 and >= 2 ny; `err` gets TCE_TIMEOUT if a bulk copy did not
 // complete within the wait limit (the CTA then waits, bounded, for its copies
@@ -207,8 +167,8 @@ template <int K>
 __global__ void __launch_bounds__(yz32_threads<K>()) k_yz32(cpx<float>* __restrict__ X, const float* __restrict__ rden32,
                                                const float* __restrict__ cp32, const double* __restrict__ rden64,
                                                const double* __restrict__ cp64, const double* __restrict__ cl,
-                                               const cpx<float>* __restrict__ tw32, int nz, int nlow,
-                                               double* __restrict__ lowbuf, int* __restrict__ err) {
+                                               const cpx<float>* __restrict__ tw32, int nz,
+                                               int* __restrict__ err) {
   using RF = RowFft<K>;
   constexpr int N = RF::N;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -216,6 +176,7 @@ __global__ void __launch_bounds__(yz32_threads<K>()) k_yz32(cpx<float>* __restri
   cpx<float>* stw = slab + (size_t)nz * N;                         // N twiddles
   float* scl = reinterpret_cast<float*>(stw + N);                  // a_k = cl[k] in FP32
   uint64_t* bar = reinterpret_cast<uint64_t*>(scl + ((nz + 1) & ~1));
+  double* dlow = reinterpret_cast<double*>(bar + YZ32_CHUNKS);     // low modes' d' columns
   const int kx = blockIdx.x;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int rc = (nz + YZ32_CHUNKS - 1) / YZ32_CHUNKS;            // rows per chunk
@@ -262,9 +223,10 @@ __global__ void __launch_bounds__(yz32_threads<K>()) k_yz32(cpx<float>* __restri
     float* col = reinterpret_cast<float*>(slab) + 2 * ky + part;
     const size_t tb = (size_t)kx * nz * N + ky;
     const bool gauge = kx == 0 && ky == 0;
+    constexpr int nlow = YZ32_NLOW;
     if (kx < nlow && (ky < nlow || ky > N - nlow)) {
       const int q = ky < nlow ? ky : ky - (N - 2 * nlow + 1);
-      double* dq = lowbuf + (((size_t)kx * (2 * nlow - 1) + q) * 2 + part) * nz;
+      double* dq = dlow + ((size_t)q * 2 + part) * nz;
       yz32_sweep<double>(col, 2 * N, dq, 1, rden64 + tb, cp64 + tb, cl, N, nz, gauge);
     } else {
       yz32_sweep<float>(col, 2 * N, col, 2 * N, rden32 + tb, cp32 + tb, scl, N, nz, gauge);

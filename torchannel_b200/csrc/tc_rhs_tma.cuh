@@ -1,0 +1,220 @@
+// Kernel (a) with its tiles staged by the tensor memory accelerator: the
+// stencils of rhs_point (advection + x/y or full diffusion + forcing + AB2,
+// operators.py:18-248, 474-548, 818-1225; solver.py:626-651) over tiles of
+// RHS_TX x 8 points and KB planes, in a persistent loop of CTAs that each
+// hold two stages in shared memory.  While a CTA evaluates one tile, one
+// thread has already issued the 3-D tensor copies (cp.async.bulk.tensor) of
+// the u, v and w boxes of its next tile into the other stage, so that the
+// staging costs no load or store instructions and its latency hides behind
+// the arithmetic.
+//
+// Box of a tile (i0, j0, kb): x from i0 - XA (XA = 16 bytes / sizeof(T), so
+// that the copy starts on a 16-byte boundary) over RHS_TX + 2 XA columns, y
+// from j0 - 1 over 10 rows, planes kb - 1 .. kb + KB.  What the box cannot
+// hold is patched after it lands:
+//  * periodic wraps (tiles at the x / y ends of the domain): the halo
+//    column / row from the other end, loaded from global memory;
+//  * u / v z ghosts (planes -1 and nz, which the box reads as zeros):
+//    -q[0] below, -q[nz-1] (no-slip) or +q[nz-1] (free-slip) above; w's
+//    plane -1 stays 0 and its plane nz is the stored wall;
+//  * mixed precision: u is stored as u - U0[k], and its planes get U0[k]
+//    added so that the stencils see the total velocity.
+// Each wait on a stage's barrier is bounded; if one runs out, the CTA sets
+// TCE_TIMEOUT in the error word and stops.
+#pragma once
+#include "tc_async.cuh"
+#include "tc_step.cuh"
+
+namespace tc {
+
+template <class T, int KB> struct RhsTma {
+  static constexpr int XA = 16 / (int)sizeof(T);  // x alignment of a box start (elements)
+  static constexpr int BX = RHS_TX + 2 * XA;      // box columns: x = i0 - XA ..
+  static constexpr int OX = XA;                   // box column of x = i0
+  static constexpr int TY = 8;                    // rows of a tile
+  static constexpr int BY = TY + 2;               // box rows: y = j0 - 1 ..
+  static constexpr int BZ = KB + 2;               // box planes: kb - 1 .. kb + KB
+  static constexpr int BOX = BX * BY * BZ;        // elements of one field's box
+  static constexpr int STAGE = 3 * BOX;           // u, v, w
+  static constexpr unsigned BOX_BYTES = (unsigned)(BOX * sizeof(T));
+  static_assert(BOX_BYTES % 128 == 0, "boxes must stay 128-byte aligned in shared memory");
+  static __host__ __device__ constexpr size_t smem() { return 2 * (size_t)STAGE * sizeof(T) + 2 * 8; }
+};
+// planes per tile: 8 in FP32 (48 KB a stage), 4 in FP64 (52 KB a stage);
+// two stages, two CTAs per SM
+template <class T> __host__ __device__ constexpr int rhs_tma_kb() { return sizeof(T) == 4 ? 8 : 4; }
+
+#define RHS_TMA_WAIT_LIMIT (1u << 21)
+
+template <class T, bool FULL, int UPD, int KB>
+__global__ void __launch_bounds__(RHS_TX * 8, 2)
+    k_rhs_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
+              const __grid_constant__ CUtensorMap mw, Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
+              const T* __restrict__ w, T* __restrict__ us, T* __restrict__ vs, T* __restrict__ ws,
+              T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw, const double* __restrict__ forcing_dev,
+              T dt, int have_hist, int ntx, int nty, int ntz, int* __restrict__ err) {
+  using S = RhsTma<T, KB>;
+  constexpr int BX = S::BX, BY = S::BY, BZ = S::BZ, OX = S::OX;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* buf = reinterpret_cast<T*>(smraw);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(buf + 2 * S::STAGE);
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t plane = (size_t)nx * ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx, nthr = RHS_TX * S::TY;
+  const int ntiles = ntx * nty * ntz;
+  const T top = g.top_neumann ? T(1) : T(-1);
+  const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
+  const T* __restrict__ base = g.ubase_t;
+  if (blockIdx.x >= ntiles) return;
+  if (smem_u32(buf) & 127u) {  // tensor copies need 128-byte aligned boxes
+    if (tid == 0) atomicOr(err, TCE_BOUNDS);
+    return;
+  }
+  if (tid == 0) {
+    tma_prefetch_desc(&mu);
+    tma_prefetch_desc(&mv);
+    tma_prefetch_desc(&mw);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  auto decode = [&](int t, int& bx, int& by, int& bz) {
+    bz = t % ntz;
+    const int r = t / ntz;
+    by = r % nty;
+    bx = r / nty;
+  };
+  auto issue = [&](int t, int st) {  // one thread
+    int bx, by, bz;
+    decode(t, bx, by, bz);
+    T* d = buf + (size_t)st * S::STAGE;
+    mbar_expect_tx(&bar[st], 3 * S::BOX_BYTES);
+    const int x = bx * RHS_TX - S::XA, y = by * S::TY - 1, z = bz * KB - 1;
+    tma_load_3d(d, &mu, x, y, z, &bar[st]);
+    tma_load_3d(d + S::BOX, &mv, x, y, z, &bar[st]);
+    tma_load_3d(d + 2 * S::BOX, &mw, x, y, z, &bar[st]);
+  };
+  if (tid == 0) issue(blockIdx.x, 0);
+  int it = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int st = it & 1;
+    // the other stage was released by the barrier that ended the last tile
+    if (tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, st ^ 1);
+    int bx, by, bz;
+    decode(t, bx, by, bz);
+    const int i0 = bx * RHS_TX, j0 = by * S::TY, kb = bz * KB;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = (i < nx) && (j < ny);
+    // AB2 history and stored u of this thread's points, in flight with the copy
+    T hru[KB], hrv[KB], hrw[KB], hu[KB];
+#pragma unroll
+    for (int q = 0; q < KB; ++q) {
+      const int k = kb + q;
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const bool cell = active && k < nz, face = active && k >= 1 && k <= nz - 1;
+      const bool hist = UPD == UPD_AB2 && have_hist;
+      hru[q] = (cell && hist) ? ru[o] : T(0);
+      hrv[q] = (cell && hist) ? rv[o] : T(0);
+      hrw[q] = (face && hist) ? rw[o] : T(0);
+      hu[q] = (cell && base && UPD != UPD_RHS_ONLY) ? ldg(u + o) : T(0);
+    }
+    const bool landed = mbar_wait_bounded(&bar[st], (unsigned)(it >> 1) & 1u, RHS_TMA_WAIT_LIMIT);
+    if (__syncthreads_or(!landed)) {
+      if (tid == 0) {
+        // let the copies in flight finish (bounded) before leaving
+        mbar_wait_bounded(&bar[st], (unsigned)(it >> 1) & 1u, RHS_TMA_WAIT_LIMIT);
+        if (t + (int)gridDim.x < ntiles)
+          mbar_wait_bounded(&bar[st ^ 1], (unsigned)((it + 1) >> 1) & 1u, RHS_TMA_WAIT_LIMIT);
+        atomicOr(err, TCE_TIMEOUT);
+      }
+      return;
+    }
+    T* su = buf + (size_t)st * S::STAGE;
+    T* sv = su + S::BOX;
+    T* sw = sv + S::BOX;
+    // (1) periodic wraps of the halo ring (raw stored values) on the planes
+    //     that exist, and U0 added to u's planes
+    const bool wrap_x = (i0 == 0) || (i0 + RHS_TX >= nx);
+    const bool wrap_y = (j0 == 0) || (j0 + S::TY >= ny);
+    if (wrap_x || wrap_y) {
+      // ring positions of a plane: 2 columns of BY rows, 2 rows of RHS_TX + 2
+      constexpr int RING = 2 * BY + 2 * (RHS_TX + 2);
+      for (int e = tid; e < RING * BZ; e += nthr) {
+        const int sl = e / RING, q = e - sl * RING;
+        const int p = kb - 1 + sl;
+        int hy, hx;  // box row, and box column relative to x = i0 - 1
+        if (q < 2 * BY) {
+          hy = q % BY;
+          hx = (q < BY) ? 0 : min(nx - i0, RHS_TX) + 1;
+        } else {
+          const int r = q - 2 * BY;
+          hx = r % (RHS_TX + 2);
+          hy = (r < RHS_TX + 2) ? 0 : min(ny - j0, S::TY) + 1;
+        }
+        const int xg = i0 - 1 + hx, yg = j0 - 1 + hy;
+        if (xg >= 0 && xg < nx && yg >= 0 && yg < ny) continue;  // inside the domain: the box holds it
+        const size_t off = (size_t)wrap(yg, ny) * nx + wrap(xg, nx);
+        const int sidx = (sl * BY + hy) * BX + OX - 1 + hx;
+        if (p >= 0 && p < nz) {
+          su[sidx] = ldg(u + (size_t)p * plane + off);
+          sv[sidx] = ldg(v + (size_t)p * plane + off);
+        }
+        if (p >= 0 && p <= nz) sw[sidx] = ldg(w + (size_t)p * plane + off);
+      }
+      __syncthreads();
+    }
+    if (base) {
+      for (int e = tid; e < BZ * BY * (RHS_TX + 2); e += nthr) {
+        const int sl = e / (BY * (RHS_TX + 2)), r = e - sl * (BY * (RHS_TX + 2));
+        const int hy = r / (RHS_TX + 2), hx = r - hy * (RHS_TX + 2);
+        const int p = kb - 1 + sl;
+        if (p >= 0 && p < nz) su[(sl * BY + hy) * BX + OX - 1 + hx] += ldg(base + p);
+      }
+      __syncthreads();
+    }
+    // (2) z ghosts of u and v: plane -1 (slot 0 of the first tile) and plane
+    //     nz (slot nz - kb + 1 when it is in the box)
+    const int sg_lo = (kb == 0) ? 0 : -1;
+    const int sg_hi = (nz - kb + 1 < BZ) ? nz - kb + 1 : -1;
+    if (sg_lo >= 0 || sg_hi >= 0) {
+      for (int e = tid; e < 2 * BY * (RHS_TX + 2); e += nthr) {
+        const int which = e / (BY * (RHS_TX + 2)), r = e - which * (BY * (RHS_TX + 2));
+        const int hy = r / (RHS_TX + 2), hx = r - hy * (RHS_TX + 2);
+        const int sl = which == 0 ? sg_lo : sg_hi;
+        if (sl < 0) continue;
+        const int from = which == 0 ? sl + 1 : sl - 1;
+        const T sgn = which == 0 ? T(-1) : top;
+        const int a = (sl * BY + hy) * BX + OX - 1 + hx, b = (from * BY + hy) * BX + OX - 1 + hx;
+        su[a] = sgn * su[b];
+        sv[a] = sgn * sv[b];
+      }
+      __syncthreads();
+    }
+    // (3) the stencils, plane by plane
+    constexpr int PY = BX, PS = BY * BX;
+#pragma unroll 1
+    for (int kk = 0; kk < KB; ++kk) {
+      const int k = kb + kk;
+      if (k >= nz) break;
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      rhs_point<T, FULL, UPD>(g, su, sv, sw, ((kk + 1) * BY + ty + 1) * BX + tx + OX, PY, PS, i, j, k, o,
+                              active, active && k >= 1, us, vs, ws, ru, rv, rw, forcing, dt, have_hist, hru[0],
+                              hrv[0], hrw[0], hu[0], base != nullptr);
+#pragma unroll
+      for (int q = 0; q + 1 < KB; ++q) {
+        hru[q] = hru[q + 1]; hrv[q] = hrv[q + 1]; hrw[q] = hrw[q + 1]; hu[q] = hu[q + 1];
+      }
+    }
+    __syncthreads();  // this stage is free for the copy issued two tiles on
+  }
+}
+
+// Tiles of k_rhs_tma: x tiles, y tiles, z tiles of KB planes (planes 0 .. nz-1).
+__host__ inline void rhs_tma_tiles(int nx, int ny, int nz, int kb, int* ntx, int* nty, int* ntz) {
+  *ntx = (nx + RHS_TX - 1) / RHS_TX;
+  *nty = (ny + 7) / 8;
+  *ntz = (nz + kb - 1) / kb;
+}
+
+}  // namespace tc
