@@ -476,6 +476,16 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  if constexpr (sizeof(T) == 4) {  // the variants that take a base pressure's gradient out
+    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 big));
+    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 big));
+    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 big));
+  }
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   (void)c;
@@ -916,8 +926,8 @@ template <class T> static size_t cn_smem(const tc_ctx* c) {
   const int vec = (cn_len(c) <= 16 && sizeof(T) == 4) ? 2 : 1;
   return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32 * vec) * 8;
 }
-template <class T>
-static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const PGrad& pg = PGrad{}) {
+template <class T, bool PG>
+static void launch_cn_t(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const PGrad& pg) {
   const int ncol = c->nx * c->ny;
   const dim3 blk(32, cn_chunks(c));
   const int Lr = cn_len(c);
@@ -927,16 +937,27 @@ static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const P
     constexpr int V = sizeof(T) == 4 ? 2 : 1;
     const dim3 grid((ncol / V + 31) / 32, 1, 3);
     if (Lr == 16)
-      k_cn_solve<T, 16, V, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 16, V, 512, true, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
     else
-      k_cn_solve<T, 16, V, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 16, V, 512, false, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
   } else {
     const dim3 grid((ncol + 31) / 32, 1, 3);
     if (Lr == 32)
-      k_cn_solve<T, 32, 1, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 32, 1, 512, true, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
     else
-      k_cn_solve<T, 32, 1, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 32, 1, 512, false, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
   }
+}
+// CN of u*, v*, w*; with a base pressure (pg.pb, mixed contexts) its gradient
+// is taken out of the result.
+template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const PGrad& pg = PGrad{}) {
+  if constexpr (sizeof(T) == 4) {
+    if (pg.pb) {
+      launch_cn_t<T, true>(c, u, v, w, s, pg);
+      return;
+    }
+  }
+  launch_cn_t<T, false>(c, u, v, w, s, pg);
 }
 
 static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, planes); }

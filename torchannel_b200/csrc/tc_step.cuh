@@ -482,7 +482,7 @@ struct PGrad {
 // rows (the tables' chunk length; L sizes the register windows; FIXED: Lr is
 // L, known at compile time); blockDim.y may exceed the chunks of this
 // system, the extra warps only take part in the barriers.
-template <class T, int L, int VEC, bool FIXED = false>
+template <class T, int L, int VEC, bool FIXED = false, bool PG = false>
 __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, const CnTab& t,
                                         const double* __restrict__ ubase, int nx, int ny, int nz, int bx, int comp,
                                         int Lr_arg, const PGrad& pg = PGrad{}) {
@@ -654,7 +654,7 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
         for (int c = 0; c < VEC; ++c) o[c] = F32 ? (y[tt][c] + h * Xin[c]) + bs : (y[tt][c] + h * Xin[c]) - bs;
         const int pl = comp < 2 ? m : m + 1;
-        if (pg.pb != nullptr) {
+        if constexpr (PG) {
           // q** - dt G p_b at this row's points (columns col .. col+VEC-1 of one x row)
           const float* pp = pg.pb + (size_t)pl * plane + col;
           double gr[VEC];
@@ -683,11 +683,11 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   }
 }
 
-template <class T, int L, int VEC, int MAXT, bool FIXED>
+template <class T, int L, int VEC, int MAXT, bool FIXED, bool PG = false>
 __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
                                                    CnTab t, const double* __restrict__ ubase, int nx, int ny,
                                                    int nz, int Lr, PGrad pg) {
-  cn_tile<T, L, VEC, FIXED>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr, pg);
+  cn_tile<T, L, VEC, FIXED, PG>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr, pg);
 }
 
 // Scalars slot layout (FP64, device).
