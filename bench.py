@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--batch-only", default=None, metavar="ROWS,CTAS",
                     help="--workload ensemble: only the ensemble launches, with this fixed shape (CN rows bound, "
                          "CTAs per SM) and graphs off, every launch visible to a profiler")
+    ap.add_argument("--no-tma-rhs", action="store_true",
+                    help="stage the explicit-RHS tiles with per-thread loads instead of tensor copies")
+    ap.add_argument("--tma-rhs-mode", type=int, default=0, help="shape of the tensor-copy RHS (1..4; 0: default)")
     ap.add_argument("--no-fp32-poisson", action="store_true",
                     help="skip the mixed step with the single-precision Poisson solve")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -175,6 +178,10 @@ def run_b200(a):
     grid, (u0, v0, w0) = initial_state(seed=rank)
     z_f, z_c, dz_f, dz_c = grid
     ch = Channel(NX, NY, NZ, LX, LY, LZ, 1.0 / RE, dz_f, dz_c, precision=a.precision)
+    if a.no_tma_rhs:
+        ch.use_tma_rhs(False)
+    elif a.tma_rhs_mode:
+        ch.use_tma_rhs(a.tma_rhs_mode)
     ch.set_state(u0, v0, w0)
     ub = ch.bulk_velocity()
     ch.set_state(u0 * (1.0 / ub), v0, w0)

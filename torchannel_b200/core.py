@@ -155,7 +155,7 @@ class Channel:
     def use_tma_rhs(self, on=True):
         """Explicit-RHS tiles staged by tensor copies (on, the default where
         the grid allows it) or by per-thread loads (off); bit-identical."""
-        L.check(self.lib.tc_use_tma_rhs(self.ctx, int(bool(on))))
+        L.check(self.lib.tc_use_tma_rhs(self.ctx, int(on)))
 
     def use_fp32_poisson(self, on=True, warm_steps=10):
         """Single-precision Poisson step (mixed precision): FP32 spectrum,

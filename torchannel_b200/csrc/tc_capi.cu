@@ -104,11 +104,10 @@ struct tc_ctx {
   float* pf[2];
   float* rden32; float* cp32;
   cpx<float>* twy32;
-  double* cz_d;             // nz + 1: dt / dz_c of the CN tables' dt (PGrad)
   // RHS with tensor-copy staging (k_rhs_tma): maps of the u, v, w buffers of
   // both state parities, usable here, switched on, persistent CTAs
   CUtensorMap tmap[2][3];
-  int rhs_tma_ok, rhs_tma_on, rhs_tma_grid;
+  int rhs_tma_ok, rhs_tma_on, rhs_tma_grid, rhs_tma_mode;
   int pcur, p_hist, p_f32;  // pf[pcur] holds p; p of the last step is in pf (else in p)
   int psp_on, psp_ok, psp_warm, since_set;
   int yz32_thr;
@@ -208,7 +207,6 @@ static size_t carve(tc_ctx* c, char* base) {
     c->rden32 = cv.take<float>(nspec * 4);
     c->cp32 = cv.take<float>(nspec * 4);
     c->twy32 = cv.take<cpx<float>>((size_t)c->ny * 8);
-    c->cz_d = cv.take<double>((size_t)(c->nz + 1) * 8);
   }
   return cv.off + 256;
 }
@@ -476,16 +474,6 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  if constexpr (sizeof(T) == 4) {  // the variants that take a base pressure's gradient out
-    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 big));
-    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, false, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 big));
-    TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 big));
-  }
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_rows_d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   (void)c;
@@ -509,11 +497,6 @@ template <class F> static void for_each_yz32(int n, F&& f) {
 }
 static bool yz32_len_ok(int ny) { return rowfft_supported(ny) && ny / 16 <= 24; }
 static bool psp_ready(const tc_ctx* c) { return c->psp_on && c->p_hist >= 1 && c->since_set >= c->psp_warm; }
-// dt / dz_c for the base-pressure gradient of the CN kernel.
-__global__ void k_cz_table(const double* __restrict__ dzc, double* __restrict__ cz, int n, double dt) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) cz[e] = dt / dzc[e];
-}
 
 template <class T> static void to_t(const std::vector<double>& src, std::vector<unsigned char>& dst) {
   dst.resize(src.size() * sizeof(T));
@@ -550,17 +533,38 @@ typedef CUresult (*TensorMapEncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cu
                                            CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
                                            CUtensorMapFloatOOBfill);
 
+// Shapes of the tensor-copy RHS: planes per tile, stages, resident CTAs per
+// SM the registers are bounded for.
+template <class T, int KB, int NST, int MINB> struct RhsV {
+  using S = RhsTma<T, KB, NST>;
+  static constexpr int kb = KB, nst = NST;
+  template <bool FULL, int UPD> static constexpr auto fn() { return k_rhs_tma<T, FULL, UPD, KB, NST, MINB>; }
+};
+// mode 1: 8 planes, two stages, 2 CTAs per SM; 2: 4 planes, two stages, 3;
+// 3: 4 planes, one stage (a tile per CTA), 4; 4: 8 planes, one stage, 3.
+// FP64 storage: 4 planes, two stages, 2 CTAs per SM.
+template <class T, class F> static void rhs_variant(int mode, F&& f) {
+  if constexpr (sizeof(T) == 8) {
+    f(RhsV<double, 4, 2, 2>{});
+  } else {
+    switch (mode) {
+      case 2: f(RhsV<float, 4, 2, 3>{}); break;
+      case 3: f(RhsV<float, 4, 1, 4>{}); break;
+      case 4: f(RhsV<float, 8, 1, 3>{}); break;
+      default: f(RhsV<float, 8, 2, 2>{}); break;
+    }
+  }
+}
+
 // Tensor maps of the six state buffers (3-D: x, y, planes; boxes of the
-// k_rhs_tma tile), kernel attributes and the persistent grid.  Leaves
+// k_rhs_tma tile of shape `mode`), kernel attributes and the grid.  Leaves
 // rhs_tma_ok = 0 (the staged kernel k_rhs_update runs) where the grid does
 // not allow it: x rows must be a multiple of 16 bytes and the domain at least
 // two tiles wide.
-template <class T> static int rhs_tma_setup(tc_ctx* c) {
-  constexpr int KB = rhs_tma_kb<T>();
-  using S = RhsTma<T, KB>;
+template <class T> static int rhs_tma_setup(tc_ctx* c, int mode) {
   c->rhs_tma_ok = 0;
   c->rhs_tma_on = 0;
-  if (((size_t)c->nx * sizeof(T)) % 16 != 0 || c->nx < 2 * RHS_TX || c->ny < 2 * S::TY) return TC_OK;
+  if (((size_t)c->nx * sizeof(T)) % 16 != 0 || c->nx < 2 * RHS_TX || c->ny < 16) return TC_OK;
   static TensorMapEncodeTiledFn enc = nullptr;
   if (!enc) {
     void* f = nullptr;
@@ -572,38 +576,44 @@ template <class T> static int rhs_tma_setup(tc_ctx* c) {
     }
     enc = (TensorMapEncodeTiledFn)f;
   }
-  const CUtensorMapDataType dty = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-  for (int st = 0; st < 2; ++st)
-    for (int f = 0; f < 3; ++f) {
-      const cuuint64_t gdim[3] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)(f == 2 ? c->nz + 1 : c->nz)};
-      const cuuint64_t gstr[2] = {(cuuint64_t)c->nx * sizeof(T), (cuuint64_t)c->nx * c->ny * sizeof(T)};
-      const cuuint32_t box[3] = {(cuuint32_t)S::BX, (cuuint32_t)S::BY, (cuuint32_t)S::BZ};
-      const cuuint32_t est[3] = {1, 1, 1};
-      if (enc(&c->tmap[st][f], dty, 3, c->st[st][f], gdim, gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return TC_OK;
-    }
-  const int sm = (int)S::smem();
-  if (cudaFuncSetAttribute(k_rhs_tma<T, false, UPD_AB2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_rhs_tma<T, true, UPD_AB2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_rhs_tma<T, true, UPD_FE, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) !=
-          cudaSuccess) {
+  bool ok = true;
+  rhs_variant<T>(mode, [&](auto V) {
+    using VV = decltype(V);
+    using S = typename VV::S;
+    const CUtensorMapDataType dty = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    for (int st = 0; st < 2 && ok; ++st)
+      for (int f = 0; f < 3 && ok; ++f) {
+        const cuuint64_t gdim[3] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny,
+                                    (cuuint64_t)(f == 2 ? c->nz + 1 : c->nz)};
+        const cuuint64_t gstr[2] = {(cuuint64_t)c->nx * sizeof(T), (cuuint64_t)c->nx * c->ny * sizeof(T)};
+        const cuuint32_t box[3] = {(cuuint32_t)S::BX, (cuuint32_t)S::BY, (cuuint32_t)S::BZ};
+        const cuuint32_t est[3] = {1, 1, 1};
+        ok = enc(&c->tmap[st][f], dty, 3, c->st[st][f], gdim, gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+      }
+    const int sm = (int)S::smem();
+    int nb = 0;
+    ok = ok &&
+         cudaFuncSetAttribute(VV::template fn<false, UPD_AB2>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+             cudaSuccess &&
+         cudaFuncSetAttribute(VV::template fn<true, UPD_AB2>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+             cudaSuccess &&
+         cudaFuncSetAttribute(VV::template fn<true, UPD_FE>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+             cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, VV::template fn<false, UPD_AB2>(), RHS_TX * S::TY, sm) ==
+             cudaSuccess &&
+         nb >= 1;
+    if (!ok) return;
+    int ntx, nty, ntz;
+    rhs_tma_tiles(c->nx, c->ny, c->nz, VV::kb, &ntx, &nty, &ntz);
+    c->rhs_tma_grid = VV::nst == 2 ? std::min(ntx * nty * ntz, nb * c->nsm) : ntx * nty * ntz;
+  });
+  if (!ok) {
     cudaGetLastError();
     return TC_OK;
   }
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rhs_tma<T, false, UPD_AB2, KB>, RHS_TX * S::TY, sm) !=
-          cudaSuccess ||
-      nb < 1) {
-    cudaGetLastError();
-    return TC_OK;
-  }
-  int ntx, nty, ntz;
-  rhs_tma_tiles(c->nx, c->ny, c->nz, KB, &ntx, &nty, &ntz);
-  c->rhs_tma_grid = std::min(ntx * nty * ntz, nb * c->nsm);
+  c->rhs_tma_mode = mode;
   c->rhs_tma_ok = 1;
   c->rhs_tma_on = 1;
   return TC_OK;
@@ -612,14 +622,16 @@ template <class T> static int rhs_tma_setup(tc_ctx* c) {
 template <class T, bool FULL, int UPD>
 static void launch_rhs_tma(const tc_ctx* c, const Grid<T>& g, T* const* A, T* const* B, T* const* R, double dt,
                            int have_hist, cudaStream_t s) {
-  constexpr int KB = rhs_tma_kb<T>();
-  using S = RhsTma<T, KB>;
-  int ntx, nty, ntz;
-  rhs_tma_tiles(c->nx, c->ny, c->nz, KB, &ntx, &nty, &ntz);
-  const CUtensorMap* m = c->tmap[c->cur];
-  k_rhs_tma<T, FULL, UPD, KB><<<c->rhs_tma_grid, dim3(RHS_TX, S::TY), S::smem(), s>>>(
-      m[0], m[1], m[2], g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2], c->scal + SC_FORCING, (T)dt,
-      have_hist, ntx, nty, ntz, c->err);
+  rhs_variant<T>(c->rhs_tma_mode, [&](auto V) {
+    using VV = decltype(V);
+    using S = typename VV::S;
+    int ntx, nty, ntz;
+    rhs_tma_tiles(c->nx, c->ny, c->nz, VV::kb, &ntx, &nty, &ntz);
+    const CUtensorMap* m = c->tmap[c->cur];
+    VV::template fn<FULL, UPD>()<<<c->rhs_tma_grid, dim3(RHS_TX, S::TY), S::smem(), s>>>(
+        m[0], m[1], m[2], g, A[0], A[1], A[2], B[0], B[1], B[2], R[0], R[1], R[2], c->scal + SC_FORCING, (T)dt,
+        have_hist, ntx, nty, ntz, c->err);
+  });
 }
 
 // Whether the single-precision Poisson step can run on this grid (register x
@@ -713,7 +725,7 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
     if (cudaGetLastError() != cudaSuccess) return bail(fail(TC_ERR_CUDA, "tri factors launch"));
   }
   if ((r2 = psp_setup(c, twy))) return bail(r2);
-  r2 = (c->tsz == 8) ? rhs_tma_setup<double>(c) : rhs_tma_setup<float>(c);
+  r2 = (c->tsz == 8) ? rhs_tma_setup<double>(c, 1) : rhs_tma_setup<float>(c, 1);
   if (r2) return bail(r2);
   c->yz_ok = yz_probe(c);
   c->yzr_ok = c->yz_ok ? yzr_probe(c) : 0;
@@ -876,10 +888,10 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
   return TC_OK;
 }
 
-// The single-precision Poisson solve of a step: L dp = div(u**)/dt with the
-// FP32 spectrum (x transform, the fused y / z / inverse-y slab kernel,
-// inverse x transform into dp = c->p as FP32); u** already lacks the base
-// pressure's gradient (launch_cn with PGrad), so dp is the increment over it.
+// The single-precision Poisson solve of a step: L dp = div(u**)/dt - L p_b,
+// p_b = pf[pcur] the previous step's pressure, with the FP32 spectrum
+// (L p_b into the dp buffer, x transform of the difference, the fused y / z /
+// inverse-y slab kernel, inverse x transform into dp = c->p as FP32).
 template <class T> static int poisson32_impl(tc_ctx* c, const T* u, const T* v, const T* w, double dt,
                                              cudaStream_t s) {
   if constexpr (sizeof(T) != 4) {
@@ -891,10 +903,12 @@ template <class T> static int poisson32_impl(tc_ctx* c, const T* u, const T* v, 
     float* dpf = reinterpret_cast<float*>(c->p);
     const double scale = 1.0 / (dt * (double)nx * (double)ny);
     mark(c, TC_PH_FFTX, s);
+    k_base_lap<<<dim3((nx + 31) / 32, (ny + 7) / 8, nz), dim3(32, 8), 0, s>>>(
+        c->pf[c->pcur], dpf, nx, ny, nz, 1.0 / (c->dx * c->dx), 1.0 / (c->dy * c->dy), c->cl, c->cr);
     for_each_n1(nx, [&](auto I) {
       constexpr int N1 = decltype(I)::value;
       k_div_fftx_reg32<float, N1, XROWS><<<dim3(ny / XROWS, nz), xreg_threads<N1>(), fftx_reg_smem<N1>(), s>>>(
-          g, u, v, w, Xf, c->twx_d, scale);
+          g, u, v, w, Xf, c->twx_d, scale, dpf, 1.0 / ((double)nx * (double)ny));
     });
     mark(c, TC_PH_FFTY, s);
     for_each_yz32(ny, [&](auto I) {
@@ -926,8 +940,7 @@ template <class T> static size_t cn_smem(const tc_ctx* c) {
   const int vec = (cn_len(c) <= 16 && sizeof(T) == 4) ? 2 : 1;
   return (size_t)(9 * c->nz + 2 * cn_chunks(c) * 32 * vec) * 8;
 }
-template <class T, bool PG>
-static void launch_cn_t(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const PGrad& pg) {
+template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s) {
   const int ncol = c->nx * c->ny;
   const dim3 blk(32, cn_chunks(c));
   const int Lr = cn_len(c);
@@ -937,27 +950,16 @@ static void launch_cn_t(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const
     constexpr int V = sizeof(T) == 4 ? 2 : 1;
     const dim3 grid((ncol / V + 31) / 32, 1, 3);
     if (Lr == 16)
-      k_cn_solve<T, 16, V, 512, true, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 16, V, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
     else
-      k_cn_solve<T, 16, V, 512, false, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 16, V, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
   } else {
     const dim3 grid((ncol + 31) / 32, 1, 3);
     if (Lr == 32)
-      k_cn_solve<T, 32, 1, 512, true, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 32, 1, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
     else
-      k_cn_solve<T, 32, 1, 512, false, PG><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr, pg);
+      k_cn_solve<T, 32, 1, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
   }
-}
-// CN of u*, v*, w*; with a base pressure (pg.pb, mixed contexts) its gradient
-// is taken out of the result.
-template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cudaStream_t s, const PGrad& pg = PGrad{}) {
-  if constexpr (sizeof(T) == 4) {
-    if (pg.pb) {
-      launch_cn_t<T, true>(c, u, v, w, s, pg);
-      return;
-    }
-  }
-  launch_cn_t<T, false>(c, u, v, w, s, pg);
 }
 
 static dim3 grid3(const tc_ctx* c, int planes) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, planes); }
@@ -988,13 +990,12 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   if (scheme == TC_IMEX && c->tab_dt != dt) {
     k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c),
                                  ubase_of(c));
-    if (c->cz_d) k_cz_table<<<(c->nz + 1 + 127) / 128, 128, 0, s>>>(c->dzc_d, c->cz_d, c->nz + 1, dt);
     c->tab_dt = dt;
   }
   // single-precision Poisson (IMEX): the increment over pf[pcur] once a base
-  // exists and the warm-up steps after set_state are done; the CN kernel then
-  // takes the base's gradient out of the velocity.  Before that, and for the
-  // explicit schemes, the FP64 solve, whose p (rounded) becomes the base.
+  // exists and the warm-up steps after set_state are done.  Before that, and
+  // for the explicit schemes, the FP64 solve, whose p (rounded) becomes the
+  // base.
   const bool psp_now = psp_ready(c) && scheme == TC_IMEX;
   mark(c, TC_PH_RHS, s);
   if (c->rhs_tma_on) {
@@ -1025,8 +1026,7 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   }
   mark(c, TC_PH_CN, s);
   if (scheme == TC_IMEX) {
-    const PGrad pg = psp_now ? PGrad{c->pf[c->pcur], dt / c->dx, dt / c->dy, c->cz_d} : PGrad{};
-    launch_cn<T>(c, B[0], B[1], B[2], s, pg);
+    launch_cn<T>(c, B[0], B[1], B[2], s);
     TC_LAUNCHED();
   }
   int rc;
@@ -1038,9 +1038,9 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   mark(c, TC_PH_PROJ, s);
   if constexpr (sizeof(T) == 4) {
     if (psp_now)
-      rc = project_impl_ps<T, PSrcDelta>(c, B, PSrcDelta{reinterpret_cast<const float*>(c->p), c->pf[c->pcur],
-                                                           c->pf[c->pcur ^ 1]},
-                                         dt, scheme != TC_FE, s);
+      rc = project_impl_ps<T, PSrcInc>(c, B, PSrcInc{c->pf[c->pcur], reinterpret_cast<const float*>(c->p),
+                                                       c->pf[c->pcur ^ 1]},
+                                       dt, scheme != TC_FE, s);
     else
       rc = project_impl_ps<T, PSrc64>(c, B, PSrc64{c->p, c->psp_on ? c->pf[c->pcur ^ 1] : nullptr}, dt,
                                       scheme != TC_FE, s);
@@ -1330,13 +1330,16 @@ extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
 
 extern "C" int tc_use_tma_rhs(tc_ctx* c, int on) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (on < 0 || on > 4) return fail(TC_ERR_ARG, "mode 0 .. 4");
+  if (on && on != c->rhs_tma_mode) {
+    const int rc = (c->tsz == 8) ? rhs_tma_setup<double>(c, on) : rhs_tma_setup<float>(c, on);
+    if (rc) return rc;
+  }
   if (on && !c->rhs_tma_ok) return fail(TC_ERR_SIZE, "tensor-copy RHS not available for this grid");
-  if ((on ? 1 : 0) != c->rhs_tma_on) {
-    c->rhs_tma_on = on ? 1 : 0;
-    if (c->g_valid) {  // the captured steps hold the other kernel
-      cudaGraphExecDestroy(c->gexec);
-      c->g_valid = 0;
-    }
+  c->rhs_tma_on = on ? 1 : 0;
+  if (c->g_valid) {  // the captured steps may hold the other kernel
+    cudaGraphExecDestroy(c->gexec);
+    c->g_valid = 0;
   }
   return TC_OK;
 }

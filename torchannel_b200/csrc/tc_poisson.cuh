@@ -177,12 +177,14 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
 // Rows j0 = bx * XR .. of plane k; blockDim.x may exceed the warps the rows
 // need (ensemble kernel), the extra warps only take part in the barrier.
 // XT: element type of the written spectrum (double, or float for the
-// single-precision Poisson step).
+// single-precision Poisson step, which also subtracts lsub * lsub_scale: the
+// base pressure's Laplacian).
 template <class T, int N1, int XR, class XT = double>
 __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
                                           const T* __restrict__ w, const double* __restrict__ field,
                                           cpx<XT>* __restrict__ X, const cpx<double>* __restrict__ twx,
-                                          double scale, int bx, int k) {
+                                          double scale, int bx, int k, const float* __restrict__ lsub = nullptr,
+                                          double lsub_scale = 0.0) {
   using RF = RowFft<N1>;
   constexpr int N = RF::N, NH = N / 2 + 1;
   constexpr int ZP = (RF::TILE + 7) / 8 * 8 + 1;          // row pitch of the spectra (16 B mod 128 B)
@@ -208,6 +210,7 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
     } else {
       val = field[pidx(k, j, i, ny, N)];
     }
+    if constexpr (sizeof(XT) == 4) return val * scale - (double)lsub[pidx(k, j, i, ny, N)] * lsub_scale;
     return val * scale;
   };
   if (ok && l < RF::N2)
@@ -248,16 +251,19 @@ __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg(Grid
   fftx_tile<T, N1, XR>(g, u, v, w, field, X, twx, scale, blockIdx.x, blockIdx.y);
 }
 
-// The x transform of the single-precision Poisson step: the divergence in
-// FP64 arithmetic, the spectrum written in FP32.
+// The x transform of the single-precision Poisson step: div(u**)/dt minus
+// the base pressure's Laplacian lp (k_base_lap), in FP64 arithmetic, the
+// spectrum written in FP32.
 template <class T, int N1, int XR>
 __global__ void __launch_bounds__(16 * XR / RowFft<N1>::RPW) k_div_fftx_reg32(Grid<T> g, const T* __restrict__ u,
                                                                              const T* __restrict__ v,
                                                                              const T* __restrict__ w,
                                                                              cpx<float>* __restrict__ X,
                                                                              const cpx<double>* __restrict__ twx,
-                                                                             double scale) {
-  fftx_tile<T, N1, XR, float>(g, u, v, w, nullptr, X, twx, scale, blockIdx.x, blockIdx.y);
+                                                                             double scale,
+                                                                             const float* __restrict__ lp,
+                                                                             double lp_scale) {
+  fftx_tile<T, N1, XR, float>(g, u, v, w, nullptr, X, twx, scale, blockIdx.x, blockIdx.y, lp, lp_scale);
 }
 
 // Inverse real FFT along x of rows j0 .. j0+XR-1 of plane k with the

@@ -21,10 +21,11 @@
 //   gauged as in k_tri_lu: x_{nz-1} = 0).
 //
 // The step that uses it solves for the increment of p over a base pressure
-// (the previous step's p, whose gradient the CN kernel takes out of the
-// velocity first, PGrad), which keeps the FP32 rounding of the solve small in
-// absolute terms: FP32 rounding of p itself would reach the post-projection
-// divergence amplified by dt / (dz_c dz_f) next to the walls.
+// p_b (the previous step's p): right-hand side div(u**)/dt - L p_b
+// (k_base_lap), projection with the gradient of p_b + dp summed in FP64.  FP32
+// rounding then scales with the change of p over a step, not with p, whose
+// own FP32 rounding would reach the post-projection divergence amplified by
+// dt / (dz_c dz_f) next to the walls.
 #pragma once
 #include "tc_async.cuh"
 #include "tc_common.cuh"
@@ -34,7 +35,8 @@ namespace tc {
 
 #define YZ32_CHUNKS 8          // bulk copies (and barriers) per slab
 #define YZ32_WAIT_LIMIT (1u << 21)
-#define YZ32_B 16              // levels per factor-load block of the z sweeps
+#define YZ32_B 32              // levels per factor-load block of the FP32 z sweeps
+#define YZ32_B64 16            // ... of the FP64 (low-mode) sweeps
 #define YZ32_NLOW 3            // FP64 modes: kx < 3 and ky < 3 or ky > ny - 3
 
 // Threads of k_yz32 for ny = 16 K: one per (ky, part) of the z solve, at
@@ -105,21 +107,21 @@ __device__ __forceinline__ void row32_fft(cpx<float>* row, int l, bool ok, const
 // scratch column for the FP64 modes), backward x_k = d'_k - c'_k x_{k+1}
 // (x_{nz-1} = d'_{nz-1}, or 0 when gauged) into `col`.  R: arithmetic type
 // of the recurrences, the factor tables ([k] at stride `ts`) and a_k.
-template <class R>
+template <class R, int B>
 __device__ __forceinline__ void yz32_sweep(float* col, int stride, R* dq, int dqs, const R* __restrict__ rd,
                                            const R* __restrict__ cpt, const R* a_tab, int ts, int nz, bool gauge) {
-  R fa[YZ32_B], fb[YZ32_B];
-  auto load = [&](R (&f)[YZ32_B], const R* __restrict__ tab, int k0, int dir) {
+  R fa[B], fb[B];
+  auto load = [&](R (&f)[B], const R* __restrict__ tab, int k0, int dir) {
 #pragma unroll
-    for (int b = 0; b < YZ32_B; ++b) {
+    for (int b = 0; b < B; ++b) {
       const int k = k0 + dir * b;
       f[b] = (k >= 0 && k < nz) ? ldg(tab + (size_t)k * ts) : (R)0;
     }
   };
   R dp = (R)0;
-  auto up = [&](const R (&f)[YZ32_B], int k0) {
+  auto up = [&](const R (&f)[B], int k0) {
 #pragma unroll
-    for (int b = 0; b < YZ32_B; ++b) {
+    for (int b = 0; b < B; ++b) {
       const int k = k0 + b;
       if (k < nz) {
         const R a = (k == 0) ? (R)0 : a_tab[k];
@@ -130,19 +132,19 @@ __device__ __forceinline__ void yz32_sweep(float* col, int stride, R* dq, int dq
     }
   };
   load(fa, rd, 0, 1);
-  for (int k0 = 0; k0 < nz; k0 += 2 * YZ32_B) {
-    load(fb, rd, k0 + YZ32_B, 1);
+  for (int k0 = 0; k0 < nz; k0 += 2 * B) {
+    load(fb, rd, k0 + B, 1);
     up(fa, k0);
-    load(fa, rd, k0 + 2 * YZ32_B, 1);
-    up(fb, k0 + YZ32_B);
+    load(fa, rd, k0 + 2 * B, 1);
+    up(fb, k0 + B);
   }
   // the backward sweep starts from x_{nz-1} = d'_{nz-1} (the singular (0,0)
   // mode: 0)
   R x = gauge ? (R)0 : dp;
   col[(size_t)(nz - 1) * stride] = (float)x;
-  auto dn = [&](const R (&f)[YZ32_B], int k1) {
+  auto dn = [&](const R (&f)[B], int k1) {
 #pragma unroll
-    for (int b = 0; b < YZ32_B; ++b) {
+    for (int b = 0; b < B; ++b) {
       const int k = k1 - b;
       if (k >= 0) {
         x = dq[(size_t)k * dqs] - f[b] * x;
@@ -151,11 +153,11 @@ __device__ __forceinline__ void yz32_sweep(float* col, int stride, R* dq, int dq
     }
   };
   load(fa, cpt, nz - 2, -1);
-  for (int k1 = nz - 2; k1 >= 0; k1 -= 2 * YZ32_B) {
-    load(fb, cpt, k1 - YZ32_B, -1);
+  for (int k1 = nz - 2; k1 >= 0; k1 -= 2 * B) {
+    load(fb, cpt, k1 - B, -1);
     dn(fa, k1);
-    load(fa, cpt, k1 - 2 * YZ32_B, -1);
-    dn(fb, k1 - YZ32_B);
+    load(fa, cpt, k1 - 2 * B, -1);
+    dn(fb, k1 - B);
   }
 }
 
@@ -227,9 +229,9 @@ __global__ void __launch_bounds__(yz32_threads<K>()) k_yz32(cpx<float>* __restri
     if (kx < nlow && (ky < nlow || ky > N - nlow)) {
       const int q = ky < nlow ? ky : ky - (N - 2 * nlow + 1);
       double* dq = dlow + ((size_t)q * 2 + part) * nz;
-      yz32_sweep<double>(col, 2 * N, dq, 1, rden64 + tb, cp64 + tb, cl, N, nz, gauge);
+      yz32_sweep<double, YZ32_B64>(col, 2 * N, dq, 1, rden64 + tb, cp64 + tb, cl, N, nz, gauge);
     } else {
-      yz32_sweep<float>(col, 2 * N, col, 2 * N, rden32 + tb, cp32 + tb, scl, N, nz, gauge);
+      yz32_sweep<float, YZ32_B>(col, 2 * N, col, 2 * N, rden32 + tb, cp32 + tb, scl, N, nz, gauge);
     }
   }
   __syncthreads();
@@ -241,6 +243,26 @@ __global__ void __launch_bounds__(yz32_threads<K>()) k_yz32(cpx<float>* __restri
     cpx<float>* grow = gslab + (size_t)(ok ? r : 0) * N;
     row32_fft<K, true>(row, l, ok, stw, [&](int e, cpx<float> val) { grow[e] = val; });
   }
+}
+
+// L p_b of the base pressure (FP32 in, FP64 arithmetic, FP32 out): 3-point
+// periodic differences in x and y and the z rows of projection_fft.py:44-82
+// with their Neumann closures, the operator the solve inverts.
+__global__ void __launch_bounds__(256) k_base_lap(const float* __restrict__ p, float* __restrict__ lp, int nx, int ny,
+                                                  int nz, double idx2, double idy2, const double* __restrict__ cl,
+                                                  const double* __restrict__ cr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  if (i >= nx || j >= ny) return;
+  const size_t o = pidx(k, j, i, ny, nx);
+  const double c = (double)p[o];
+  const double xm = (double)p[pidx(k, j, i == 0 ? nx - 1 : i - 1, ny, nx)];
+  const double xp = (double)p[pidx(k, j, i == nx - 1 ? 0 : i + 1, ny, nx)];
+  const double ym = (double)p[pidx(k, j == 0 ? ny - 1 : j - 1, i, ny, nx)];
+  const double yp = (double)p[pidx(k, j == ny - 1 ? 0 : j + 1, i, ny, nx)];
+  double l = (xp - 2.0 * c + xm) * idx2 + (yp - 2.0 * c + ym) * idy2;
+  if (k < nz - 1) l += cr[k] * ((double)p[o + (size_t)nx * ny] - c);
+  if (k > 0) l -= cl[k] * (c - (double)p[o - (size_t)nx * ny]);
+  lp[o] = (float)l;
 }
 
 // FP32 copies of the per-mode factor tables (k_tri_factors) for the

@@ -27,7 +27,7 @@
 
 namespace tc {
 
-template <class T, int KB> struct RhsTma {
+template <class T, int KB, int NST = 2> struct RhsTma {
   static constexpr int XA = 16 / (int)sizeof(T);  // x alignment of a box start (elements)
   static constexpr int BX = RHS_TX + 2 * XA;      // box columns: x = i0 - XA ..
   static constexpr int OX = XA;                   // box column of x = i0
@@ -38,26 +38,26 @@ template <class T, int KB> struct RhsTma {
   static constexpr int STAGE = 3 * BOX;           // u, v, w
   static constexpr unsigned BOX_BYTES = (unsigned)(BOX * sizeof(T));
   static_assert(BOX_BYTES % 128 == 0, "boxes must stay 128-byte aligned in shared memory");
-  static __host__ __device__ constexpr size_t smem() { return 2 * (size_t)STAGE * sizeof(T) + 2 * 8; }
+  static __host__ __device__ constexpr size_t smem() { return NST * (size_t)STAGE * sizeof(T) + 2 * 8; }
 };
-// planes per tile: 8 in FP32 (48 KB a stage), 4 in FP64 (52 KB a stage);
-// two stages, two CTAs per SM
-template <class T> __host__ __device__ constexpr int rhs_tma_kb() { return sizeof(T) == 4 ? 8 : 4; }
 
 #define RHS_TMA_WAIT_LIMIT (1u << 21)
 
-template <class T, bool FULL, int UPD, int KB>
-__global__ void __launch_bounds__(RHS_TX * 8, 2)
+// NST stages: 2 = a persistent pipeline (the next tile's copy in flight
+// while this one is evaluated), 1 = one tile per CTA (latency hidden by the
+// other resident CTAs); MINB = resident CTAs per SM the registers allow.
+template <class T, bool FULL, int UPD, int KB, int NST, int MINB>
+__global__ void __launch_bounds__(RHS_TX * 8, MINB)
     k_rhs_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
               const __grid_constant__ CUtensorMap mw, Grid<T> g, const T* __restrict__ u, const T* __restrict__ v,
               const T* __restrict__ w, T* __restrict__ us, T* __restrict__ vs, T* __restrict__ ws,
               T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw, const double* __restrict__ forcing_dev,
               T dt, int have_hist, int ntx, int nty, int ntz, int* __restrict__ err) {
-  using S = RhsTma<T, KB>;
+  using S = RhsTma<T, KB, NST>;
   constexpr int BX = S::BX, BY = S::BY, BZ = S::BZ, OX = S::OX;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* buf = reinterpret_cast<T*>(smraw);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(buf + 2 * S::STAGE);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(buf + NST * S::STAGE);
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx, nthr = RHS_TX * S::TY;
@@ -74,8 +74,7 @@ __global__ void __launch_bounds__(RHS_TX * 8, 2)
     tma_prefetch_desc(&mu);
     tma_prefetch_desc(&mv);
     tma_prefetch_desc(&mw);
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int q = 0; q < NST; ++q) mbar_init(&bar[q], 1);
     mbar_init_fence();
   }
   __syncthreads();
@@ -98,9 +97,11 @@ __global__ void __launch_bounds__(RHS_TX * 8, 2)
   if (tid == 0) issue(blockIdx.x, 0);
   int it = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-    const int st = it & 1;
-    // the other stage was released by the barrier that ended the last tile
-    if (tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, st ^ 1);
+    const int st = NST == 2 ? (it & 1) : 0;
+    const unsigned par = NST == 2 ? (unsigned)(it >> 1) & 1u : (unsigned)it & 1u;
+    // the other stage was released by the barrier that ended the last tile;
+    // with one stage the next copy waits for this tile's end
+    if (NST == 2 && tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, st ^ 1);
     int bx, by, bz;
     decode(t, bx, by, bz);
     const int i0 = bx * RHS_TX, j0 = by * S::TY, kb = bz * KB;
@@ -119,12 +120,12 @@ __global__ void __launch_bounds__(RHS_TX * 8, 2)
       hrw[q] = (face && hist) ? rw[o] : T(0);
       hu[q] = (cell && base && UPD != UPD_RHS_ONLY) ? ldg(u + o) : T(0);
     }
-    const bool landed = mbar_wait_bounded(&bar[st], (unsigned)(it >> 1) & 1u, RHS_TMA_WAIT_LIMIT);
+    const bool landed = mbar_wait_bounded(&bar[st], par, RHS_TMA_WAIT_LIMIT);
     if (__syncthreads_or(!landed)) {
       if (tid == 0) {
         // let the copies in flight finish (bounded) before leaving
-        mbar_wait_bounded(&bar[st], (unsigned)(it >> 1) & 1u, RHS_TMA_WAIT_LIMIT);
-        if (t + (int)gridDim.x < ntiles)
+        mbar_wait_bounded(&bar[st], par, RHS_TMA_WAIT_LIMIT);
+        if (NST == 2 && t + (int)gridDim.x < ntiles)
           mbar_wait_bounded(&bar[st ^ 1], (unsigned)((it + 1) >> 1) & 1u, RHS_TMA_WAIT_LIMIT);
         atomicOr(err, TCE_TIMEOUT);
       }
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(RHS_TX * 8, 2)
       }
     }
     __syncthreads();  // this stage is free for the copy issued two tiles on
+    if (NST == 1 && tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, 0);
   }
 }
 

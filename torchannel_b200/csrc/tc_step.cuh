@@ -465,27 +465,14 @@ template <> struct CnVec<float, 2> {
 template <class T> struct CnArith { using type = double; };
 template <> struct CnArith<float> { using type = float; };
 
-// Gradient of a base pressure taken out of the CN solution before it is
-// stored, q** - dt G p_b (the single-precision Poisson step then solves for
-// the increment p - p_b, and the projection applies only that increment's
-// gradient; mathematically the same projected velocity, since the
-// projection removes every discrete gradient).  pb == nullptr: nothing.
-// Differences as in project_tile: x and y periodic, w faces 1 .. nz-1 from
-// the cells on either side.
-struct PGrad {
-  const float* pb;     // p_b, [nz][ny][nx] FP32
-  double cx, cy;       // dt / dx, dt / dy
-  const double* cz;    // nz + 1: dt / dz_c[f]
-};
-
 // Column block bx of component comp (the block grid above), chunks of Lr <= L
 // rows (the tables' chunk length; L sizes the register windows; FIXED: Lr is
 // L, known at compile time); blockDim.y may exceed the chunks of this
 // system, the extra warps only take part in the barriers.
-template <class T, int L, int VEC, bool FIXED = false, bool PG = false>
+template <class T, int L, int VEC, bool FIXED = false>
 __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w, const CnTab& t,
                                         const double* __restrict__ ubase, int nx, int ny, int nz, int bx, int comp,
-                                        int Lr_arg, const PGrad& pg = PGrad{}) {
+                                        int Lr_arg) {
   using A = typename CnArith<T>::type;
   constexpr bool F32 = sizeof(A) == 4;
   const int Lr = FIXED ? L : Lr_arg;
@@ -654,28 +641,6 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
         for (int c = 0; c < VEC; ++c) o[c] = F32 ? (y[tt][c] + h * Xin[c]) + bs : (y[tt][c] + h * Xin[c]) - bs;
         const int pl = comp < 2 ? m : m + 1;
-        if constexpr (PG) {
-          // q** - dt G p_b at this row's points (columns col .. col+VEC-1 of one x row)
-          const float* pp = pg.pb + (size_t)pl * plane + col;
-          double gr[VEC];
-          if (comp == 0) {
-            const int ix = col % nx;
-#pragma unroll
-            for (int c = 0; c < VEC; ++c) {
-              const int nxt = (ix + c + 1 == nx) ? 1 - nx : 1;  // periodic in x
-              gr[c] = pg.cx * ((double)pp[c + nxt] - (double)pp[c]);
-            }
-          } else if (comp == 1) {
-            const int dn = (col + nx >= ncols) ? nx - ncols : nx;  // periodic in y
-#pragma unroll
-            for (int c = 0; c < VEC; ++c) gr[c] = pg.cy * ((double)pp[c + dn] - (double)pp[c]);
-          } else {
-#pragma unroll
-            for (int c = 0; c < VEC; ++c) gr[c] = pg.cz[pl] * ((double)pp[c] - (double)pp[(long)c - (long)ncols]);
-          }
-#pragma unroll
-          for (int c = 0; c < VEC; ++c) o[c] = (A)((double)o[c] - gr[c]);
-        }
         CnVec<T, VEC>::st(LEAN ? q + os : q + (size_t)pl * plane, o);
       }
       os += ucols;
@@ -683,11 +648,11 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   }
 }
 
-template <class T, int L, int VEC, int MAXT, bool FIXED, bool PG = false>
+template <class T, int L, int VEC, int MAXT, bool FIXED>
 __global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
                                                    CnTab t, const double* __restrict__ ubase, int nx, int ny,
-                                                   int nz, int Lr, PGrad pg) {
-  cn_tile<T, L, VEC, FIXED, PG>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr, pg);
+                                                   int nz, int Lr) {
+  cn_tile<T, L, VEC, FIXED>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr);
 }
 
 // Scalars slot layout (FP64, device).
@@ -759,20 +724,21 @@ struct PSrc64 {
   }
 };
 
-// PSrcDelta: only the increment dp is applied (the base's gradient was taken
-// out by the CN kernel, PGrad); out receives p_b + dp rounded to FP32.
-struct PSrcDelta {
-  const float* dp;
+// PSrcInc: the single-precision Poisson step's base p_b plus its increment
+// dp, both FP32 and summed in FP64 (the gradient of p_b + dp is exact to FP64
+// rounding, whatever the FP32 rounding of p_b); out receives p_b + dp
+// rounded to FP32, the next step's base.
+struct PSrcInc {
   const float* pb;
+  const float* dp;
   float* out;
   __device__ __forceinline__ double2 pair(size_t o) const {
-    const float2 b = *reinterpret_cast<const float2*>(dp + o);
-    return make_double2((double)b.x, (double)b.y);
+    const float2 a = *reinterpret_cast<const float2*>(pb + o), b = *reinterpret_cast<const float2*>(dp + o);
+    return make_double2((double)a.x + (double)b.x, (double)a.y + (double)b.y);
   }
-  __device__ __forceinline__ double one(size_t o) const { return (double)ldg(dp + o); }
+  __device__ __forceinline__ double one(size_t o) const { return (double)ldg(pb + o) + (double)ldg(dp + o); }
   __device__ __forceinline__ void keep(size_t o, double2 P) const {
-    const float2 a = *reinterpret_cast<const float2*>(pb + o);
-    *reinterpret_cast<float2*>(out + o) = make_float2((float)((double)a.x + P.x), (float)((double)a.y + P.y));
+    *reinterpret_cast<float2*>(out + o) = make_float2((float)P.x, (float)P.y);
   }
 };
 
