@@ -35,7 +35,7 @@ namespace tc {
 
 #define YZ32_CHUNKS 8          // bulk copies (and barriers) per slab
 #define YZ32_WAIT_LIMIT (1u << 21)
-#define YZ32_B 32              // levels per factor-load block of the FP32 z sweeps
+#define YZ32_B 16              // levels per factor-load block of the FP32 z sweeps
 #define YZ32_B64 16            // ... of the FP64 (low-mode) sweeps
 #define YZ32_NLOW 3            // FP64 modes: kx < 3 and ky < 3 or ky > ny - 3
 

@@ -192,16 +192,111 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       }
       __syncthreads();
     }
-    // (3) the stencils, plane by plane
-    constexpr int PY = BX, PS = BY * BX;
+    // (3) the stencils, plane by plane (the arithmetic of rhs_tile)
+    T(*su3)[BY][BX] = reinterpret_cast<T(*)[BY][BX]>(su);
+    T(*sv3)[BY][BX] = reinterpret_cast<T(*)[BY][BX]>(sv);
+    T(*sw3)[BY][BX] = reinterpret_cast<T(*)[BY][BX]>(sw);
+    const int cx = tx + OX, cy = ty + 1;
+    // Every advective flux is a product of two interpolations 0.5(a + b); the
+    // sums are multiplied unscaled and the two factors 0.5 are folded into the
+    // difference quotient as 0.25 / delta.  Scaling by powers of two is exact,
+    // so the fluxes are the same numbers as with the interpolations formed.
+    const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
 #pragma unroll 1
     for (int kk = 0; kk < KB; ++kk) {
       const int k = kb + kk;
-      if (k >= nz) break;
-      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-      rhs_point<T, FULL, UPD>(g, su, sv, sw, ((kk + 1) * BY + ty + 1) * BX + tx + OX, PY, PS, i, j, k, o,
-                              active, active && k >= 1, us, vs, ws, ru, rv, rw, forcing, dt, have_hist, hru[0],
-                              hrv[0], hrw[0], hu[0], base != nullptr);
+      if (k > nz) break;
+      const int sm = kk, s0 = kk + 1, sp = kk + 2;
+      if (active && k < nz) {
+        const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+        const T idzf = g.idzf[k];
+        const T qzf = T(0.25) * idzf;
+        // ---------------- u at cell k ----------------
+        {
+          const T U0 = su3[s0][cy][cx], Uxm = su3[s0][cy][cx - 1], Uxp = su3[s0][cy][cx + 1];
+          const T Uym = su3[s0][cy - 1][cx], Uyp = su3[s0][cy + 1][cx];
+          const T Uzm = su3[sm][cy][cx], Uzp = su3[sp][cy][cx];
+          const bool edge = (i == nx - 1);
+          T r = T(0);
+          if (!(edge && g.rhs_fused)) {
+            r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
+            if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
+          }
+          if (!edge) {
+            const T duudx = (sq(U0 + Uxp) - sq(Uxm + U0)) * qx;
+            const T vu_t = (sv3[s0][cy][cx] + sv3[s0][cy][cx + 1]) * (U0 + Uyp);
+            const T vu_b = (sv3[s0][cy - 1][cx] + sv3[s0][cy - 1][cx + 1]) * (Uym + U0);
+            const T wu_t = (sw3[sp][cy][cx] + sw3[sp][cy][cx + 1]) * (U0 + Uzp);
+            const T wu_b = (sw3[s0][cy][cx] + sw3[s0][cy][cx + 1]) * (Uzm + U0);
+            r -= duudx + (vu_t - vu_b) * qy + (wu_t - wu_b) * qzf;
+          }
+          if (UPD == UPD_RHS_ONLY) {
+            ru[o] = r;
+          } else {
+            const T Uraw = base ? hu[0] : U0;  // stored value (u - U0[k] in mixed precision)
+            if (UPD == UPD_FE) {
+              T q = Uraw + dt * r;
+              us[o] = q + dt * T(1);
+            } else {
+              r += forcing;
+              us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * hru[0]) : Uraw + dt * r;
+              ru[o] = r;
+            }
+          }
+        }
+        // ---------------- v at cell k ----------------
+        {
+          const T V0 = sv3[s0][cy][cx], Vxm = sv3[s0][cy][cx - 1], Vxp = sv3[s0][cy][cx + 1];
+          const T Vym = sv3[s0][cy - 1][cx], Vyp = sv3[s0][cy + 1][cx];
+          const T Vzm = sv3[sm][cy][cx], Vzp = sv3[sp][cy][cx];
+          const bool edge = (j == ny - 1);
+          T r = T(0);
+          if (!(edge && g.rhs_fused)) {
+            r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
+            if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
+          }
+          if (!edge) {
+            const T uv_r = (su3[s0][cy][cx] + su3[s0][cy + 1][cx]) * (V0 + Vxp);
+            const T uv_l = (su3[s0][cy][cx - 1] + su3[s0][cy + 1][cx - 1]) * (Vxm + V0);
+            const T dvvdy = (sq(V0 + Vyp) - sq(Vym + V0)) * qy;
+            const T wv_t = (sw3[sp][cy][cx] + sw3[sp][cy + 1][cx]) * (V0 + Vzp);
+            const T wv_b = (sw3[s0][cy][cx] + sw3[s0][cy + 1][cx]) * (Vzm + V0);
+            r -= (uv_r - uv_l) * qx + dvvdy + (wv_t - wv_b) * qzf;
+          }
+          if (UPD == UPD_RHS_ONLY) {
+            rv[o] = r;
+          } else if (UPD == UPD_FE) {
+            vs[o] = V0 + dt * r;
+          } else {
+            vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * hrv[0]) : V0 + dt * r;
+            rv[o] = r;
+          }
+        }
+      }
+      // ---------------- w at face k ----------------
+      if (active && k >= 1 && k <= nz - 1) {
+        const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+        const T W0 = sw3[s0][cy][cx], Wxm = sw3[s0][cy][cx - 1], Wxp = sw3[s0][cy][cx + 1];
+        const T Wym = sw3[s0][cy - 1][cx], Wyp = sw3[s0][cy + 1][cx];
+        const T Wzm = sw3[sm][cy][cx], Wzp = sw3[sp][cy][cx];
+        T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
+        // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+        if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
+        const T uw_r = (su3[sm][cy][cx] + su3[s0][cy][cx]) * (W0 + Wxp);
+        const T uw_l = (su3[sm][cy][cx - 1] + su3[s0][cy][cx - 1]) * (Wxm + W0);
+        const T vw_t = (sv3[sm][cy][cx] + sv3[s0][cy][cx]) * (W0 + Wyp);
+        const T vw_b = (sv3[sm][cy - 1][cx] + sv3[s0][cy - 1][cx]) * (Wym + W0);
+        const T dwwdz = (sq(W0 + Wzp) - sq(Wzm + W0)) * (T(0.25) * g.idzc[k]);
+        r -= (uw_r - uw_l) * qx + (vw_t - vw_b) * qy + dwwdz;
+        if (UPD == UPD_RHS_ONLY) {
+          rw[o] = r;
+        } else if (UPD == UPD_FE) {
+          ws[o] = W0 + dt * r;
+        } else {
+          ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * hrw[0]) : W0 + dt * r;
+          rw[o] = r;
+        }
+      }
 #pragma unroll
       for (int q = 0; q + 1 < KB; ++q) {
         hru[q] = hru[q + 1]; hrv[q] = hrv[q + 1]; hrw[q] = hrw[q + 1]; hu[q] = hu[q + 1];

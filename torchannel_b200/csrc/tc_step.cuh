@@ -59,115 +59,6 @@ template <class T> __host__ __device__ constexpr int rhs_ty() { return 8; }
 template <class T> __host__ __device__ constexpr int rhs_kb() { return sizeof(T) == 8 ? 3 : 4; }
 #define RHS_HX (RHS_TX + 2)
 
-// The stencils of one point (i, j) of plane k from staged values: su, sv,
-// sw hold u (with its base profile), v and w of planes k-1, k, k+1 (cells
-// for u / v, faces for w), `c` indexes (plane k, row j, column i), a row is
-// PY entries and a plane PS.  Writes u*, v* at cell k (cell: k < nz) and w*
-// at face k (face: 1 <= k <= nz-1) and the history / rhs as UPD says;
-// hru .. hu: this point's AB2 history and stored u (u - U0 in mixed
-// precision).
-template <class T, bool FULL, int UPD>
-__device__ __forceinline__ void rhs_point(const Grid<T>& g, const T* su, const T* sv, const T* sw, int c, int PY,
-                                          int PS, int i, int j, int k, size_t o, bool cell, bool face,
-                                          T* __restrict__ us, T* __restrict__ vs, T* __restrict__ ws,
-                                          T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw, T forcing,
-                                          T dt, int have_hist, T hru, T hrv, T hrw, T hu, bool based) {
-  const int nx = g.nx, ny = g.ny;
-  // Every advective flux is a product of two interpolations 0.5(a + b); the
-  // sums are multiplied unscaled and the two factors 0.5 are folded into the
-  // difference quotient as 0.25 / delta.  Scaling by powers of two is exact,
-  // so the fluxes are the same numbers as with the interpolations formed.
-  const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
-  if (cell) {
-    const T idzf = g.idzf[k];
-    const T qzf = T(0.25) * idzf;
-    // ---------------- u at cell k ----------------
-    {
-      const T U0 = su[c], Uxm = su[c - 1], Uxp = su[c + 1];
-      const T Uym = su[c - PY], Uyp = su[c + PY];
-      const T Uzm = su[c - PS], Uzp = su[c + PS];
-      const bool edge = (i == nx - 1);
-      T r = T(0);
-      if (!(edge && g.rhs_fused)) {
-        r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
-        if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
-      }
-      if (!edge) {
-        const T duudx = (sq(U0 + Uxp) - sq(Uxm + U0)) * qx;
-        const T vu_t = (sv[c] + sv[c + 1]) * (U0 + Uyp);
-        const T vu_b = (sv[c - PY] + sv[c - PY + 1]) * (Uym + U0);
-        const T wu_t = (sw[c + PS] + sw[c + PS + 1]) * (U0 + Uzp);
-        const T wu_b = (sw[c] + sw[c + 1]) * (Uzm + U0);
-        r -= duudx + (vu_t - vu_b) * qy + (wu_t - wu_b) * qzf;
-      }
-      if (UPD == UPD_RHS_ONLY) {
-        ru[o] = r;
-      } else {
-        const T Uraw = based ? hu : U0;  // stored value (u - U0[k] in mixed precision)
-        if (UPD == UPD_FE) {
-          T q = Uraw + dt * r;
-          us[o] = q + dt * T(1);
-        } else {
-          r += forcing;
-          us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * hru) : Uraw + dt * r;
-          ru[o] = r;
-        }
-      }
-    }
-    // ---------------- v at cell k ----------------
-    {
-      const T V0 = sv[c], Vxm = sv[c - 1], Vxp = sv[c + 1];
-      const T Vym = sv[c - PY], Vyp = sv[c + PY];
-      const T Vzm = sv[c - PS], Vzp = sv[c + PS];
-      const bool edge = (j == ny - 1);
-      T r = T(0);
-      if (!(edge && g.rhs_fused)) {
-        r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
-        if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
-      }
-      if (!edge) {
-        const T uv_r = (su[c] + su[c + PY]) * (V0 + Vxp);
-        const T uv_l = (su[c - 1] + su[c + PY - 1]) * (Vxm + V0);
-        const T dvvdy = (sq(V0 + Vyp) - sq(Vym + V0)) * qy;
-        const T wv_t = (sw[c + PS] + sw[c + PS + PY]) * (V0 + Vzp);
-        const T wv_b = (sw[c] + sw[c + PY]) * (Vzm + V0);
-        r -= (uv_r - uv_l) * qx + dvvdy + (wv_t - wv_b) * qzf;
-      }
-      if (UPD == UPD_RHS_ONLY) {
-        rv[o] = r;
-      } else if (UPD == UPD_FE) {
-        vs[o] = V0 + dt * r;
-      } else {
-        vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * hrv) : V0 + dt * r;
-        rv[o] = r;
-      }
-    }
-  }
-  // ---------------- w at face k ----------------
-  if (face) {
-    const T W0 = sw[c], Wxm = sw[c - 1], Wxp = sw[c + 1];
-    const T Wym = sw[c - PY], Wyp = sw[c + PY];
-    const T Wzm = sw[c - PS], Wzp = sw[c + PS];
-    T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
-    // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
-    if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
-    const T uw_r = (su[c - PS] + su[c]) * (W0 + Wxp);
-    const T uw_l = (su[c - PS - 1] + su[c - 1]) * (Wxm + W0);
-    const T vw_t = (sv[c - PS] + sv[c]) * (W0 + Wyp);
-    const T vw_b = (sv[c - PS - PY] + sv[c - PY]) * (Wym + W0);
-    const T dwwdz = (sq(W0 + Wzp) - sq(Wzm + W0)) * (T(0.25) * g.idzc[k]);
-    r -= (uw_r - uw_l) * qx + (vw_t - vw_b) * qy + dwwdz;
-    if (UPD == UPD_RHS_ONLY) {
-      rw[o] = r;
-    } else if (UPD == UPD_FE) {
-      ws[o] = W0 + dt * r;
-    } else {
-      ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * hrw) : W0 + dt * r;
-      rw[o] = r;
-    }
-  }
-}
-
 // The tile (bx, by, bz) of the block grid above; k_rhs_update runs one tile
 // per block, the ensemble kernel of tc_batch.cuh loops over the tiles of all
 // members (the shared tile is reused: callers separate tiles by a barrier).
@@ -250,18 +141,107 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
     }
   }
   __syncthreads();
-  constexpr int PY = RHS_HX, PS = RHS_HY * RHS_HX;
-  const T* fu = &su[0][0][0];
-  const T* fv = &sv[0][0][0];
-  const T* fw = &sw[0][0][0];
+  const int cx = tx + 1, cy = ty + 1;
+  // Every advective flux is a product of two interpolations 0.5(a + b); the
+  // sums are multiplied unscaled and the two factors 0.5 are folded into the
+  // difference quotient as 0.25 / delta.  Scaling by powers of two is exact,
+  // so the fluxes are the same numbers as with the interpolations formed.
+  const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
 #pragma unroll 1
   for (int kk = 0; kk < RHS_KB; ++kk) {
     const int k = kb + kk;
     if (k > nz) break;
-    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-    rhs_point<T, FULL, UPD>(g, fu, fv, fw, ((kk + 1) * RHS_HY + ty + 1) * RHS_HX + tx + 1, PY, PS, i, j, k, o,
-                            active && k < nz, active && k >= 1 && k <= nz - 1, us, vs, ws, ru, rv, rw, forcing, dt,
-                            have_hist, pf_ru[0], pf_rv[0], pf_rw[0], pf_u[0], base != nullptr);
+    const int sm = kk, s0 = kk + 1, sp = kk + 2;
+    if (active && k < nz) {
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const T idzf = g.idzf[k];
+      const T qzf = T(0.25) * idzf;
+      // ---------------- u at cell k ----------------
+      {
+        const T U0 = su[s0][cy][cx], Uxm = su[s0][cy][cx - 1], Uxp = su[s0][cy][cx + 1];
+        const T Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
+        const T Uzm = su[sm][cy][cx], Uzp = su[sp][cy][cx];
+        const bool edge = (i == nx - 1);
+        T r = T(0);
+        if (!(edge && g.rhs_fused)) {
+          r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
+          if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
+        }
+        if (!edge) {
+          const T duudx = (sq(U0 + Uxp) - sq(Uxm + U0)) * qx;
+          const T vu_t = (sv[s0][cy][cx] + sv[s0][cy][cx + 1]) * (U0 + Uyp);
+          const T vu_b = (sv[s0][cy - 1][cx] + sv[s0][cy - 1][cx + 1]) * (Uym + U0);
+          const T wu_t = (sw[sp][cy][cx] + sw[sp][cy][cx + 1]) * (U0 + Uzp);
+          const T wu_b = (sw[s0][cy][cx] + sw[s0][cy][cx + 1]) * (Uzm + U0);
+          r -= duudx + (vu_t - vu_b) * qy + (wu_t - wu_b) * qzf;
+        }
+        if (UPD == UPD_RHS_ONLY) {
+          ru[o] = r;
+        } else {
+          const T Uraw = base ? pf_u[0] : U0;  // stored value (u - U0[k] in mixed precision)
+          if (UPD == UPD_FE) {
+            T q = Uraw + dt * r;
+            us[o] = q + dt * T(1);
+          } else {
+            r += forcing;
+            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * pf_ru[0]) : Uraw + dt * r;
+            ru[o] = r;
+          }
+        }
+      }
+      // ---------------- v at cell k ----------------
+      {
+        const T V0 = sv[s0][cy][cx], Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1];
+        const T Vym = sv[s0][cy - 1][cx], Vyp = sv[s0][cy + 1][cx];
+        const T Vzm = sv[sm][cy][cx], Vzp = sv[sp][cy][cx];
+        const bool edge = (j == ny - 1);
+        T r = T(0);
+        if (!(edge && g.rhs_fused)) {
+          r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
+          if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
+        }
+        if (!edge) {
+          const T uv_r = (su[s0][cy][cx] + su[s0][cy + 1][cx]) * (V0 + Vxp);
+          const T uv_l = (su[s0][cy][cx - 1] + su[s0][cy + 1][cx - 1]) * (Vxm + V0);
+          const T dvvdy = (sq(V0 + Vyp) - sq(Vym + V0)) * qy;
+          const T wv_t = (sw[sp][cy][cx] + sw[sp][cy + 1][cx]) * (V0 + Vzp);
+          const T wv_b = (sw[s0][cy][cx] + sw[s0][cy + 1][cx]) * (Vzm + V0);
+          r -= (uv_r - uv_l) * qx + dvvdy + (wv_t - wv_b) * qzf;
+        }
+        if (UPD == UPD_RHS_ONLY) {
+          rv[o] = r;
+        } else if (UPD == UPD_FE) {
+          vs[o] = V0 + dt * r;
+        } else {
+          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * pf_rv[0]) : V0 + dt * r;
+          rv[o] = r;
+        }
+      }
+    }
+    // ---------------- w at face k ----------------
+    if (active && k >= 1 && k <= nz - 1) {
+      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const T W0 = sw[s0][cy][cx], Wxm = sw[s0][cy][cx - 1], Wxp = sw[s0][cy][cx + 1];
+      const T Wym = sw[s0][cy - 1][cx], Wyp = sw[s0][cy + 1][cx];
+      const T Wzm = sw[sm][cy][cx], Wzp = sw[sp][cy][cx];
+      T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
+      // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+      if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
+      const T uw_r = (su[sm][cy][cx] + su[s0][cy][cx]) * (W0 + Wxp);
+      const T uw_l = (su[sm][cy][cx - 1] + su[s0][cy][cx - 1]) * (Wxm + W0);
+      const T vw_t = (sv[sm][cy][cx] + sv[s0][cy][cx]) * (W0 + Wyp);
+      const T vw_b = (sv[sm][cy - 1][cx] + sv[s0][cy - 1][cx]) * (Wym + W0);
+      const T dwwdz = (sq(W0 + Wzp) - sq(Wzm + W0)) * (T(0.25) * g.idzc[k]);
+      r -= (uw_r - uw_l) * qx + (vw_t - vw_b) * qy + dwwdz;
+      if (UPD == UPD_RHS_ONLY) {
+        rw[o] = r;
+      } else if (UPD == UPD_FE) {
+        ws[o] = W0 + dt * r;
+      } else {
+        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * pf_rw[0]) : W0 + dt * r;
+        rw[o] = r;
+      }
+    }
 #pragma unroll
     for (int q = 0; q + 1 < RHS_KB; ++q) {
       pf_ru[q] = pf_ru[q + 1]; pf_rv[q] = pf_rv[q + 1]; pf_rw[q] = pf_rw[q + 1]; pf_u[q] = pf_u[q + 1];
