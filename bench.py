@@ -69,7 +69,8 @@ def parse():
                          "CTAs per SM) and graphs off, every launch visible to a profiler")
     ap.add_argument("--no-tma-rhs", action="store_true",
                     help="stage the explicit-RHS tiles with per-thread loads instead of tensor copies")
-    ap.add_argument("--tma-rhs-mode", type=int, default=0, help="shape of the tensor-copy RHS (1..4; 0: default)")
+    ap.add_argument("--tma-rhs-mode", type=int, default=0,
+                    help="tile shape of the tensor-copy RHS (1..4, tc_use_tma_rhs; 0: the default shape)")
     ap.add_argument("--no-fp32-poisson", action="store_true",
                     help="skip the mixed step with the single-precision Poisson solve")
     ap.add_argument("--no-adjoint", action="store_true",

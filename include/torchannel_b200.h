@@ -118,12 +118,14 @@ int tc_use_graphs(tc_ctx* ctx, int on);
  * counterpart. */
 int tc_use_fused_poisson(tc_ctx* ctx, int on);
 
-/* Staging of the explicit-RHS kernel: on (the default where the grid allows
- * it: x rows a multiple of 16 bytes, nx >= 64, ny >= 16), its u, v, w tiles
- * reach shared memory by 3-D tensor copies of the tensor memory accelerator
- * in a persistent two-stage pipeline; off, by per-thread loads.  Same
- * arithmetic, bit-identical results.  TC_ERR_SIZE when `on` is asked where it
- * is not available.  No reference counterpart. */
+/* Staging of the explicit-RHS kernel: mode 1 .. 4 (1 is the default where
+ * the grid allows it: x rows a multiple of 16 bytes, nx >= 64, ny >= 16), its
+ * u, v, w tiles reach shared memory by 3-D tensor copies of the tensor memory
+ * accelerator, in the tile shape the mode names (planes per tile, one stage
+ * per CTA or a persistent two-stage pipeline; tc_capi.cu lists them with
+ * their measured times); 0: by per-thread loads.  Same arithmetic,
+ * bit-identical results.  TC_ERR_SIZE when a mode is asked where tensor
+ * copies are not available.  No reference counterpart. */
 int tc_use_tma_rhs(tc_ctx* ctx, int on);
 
 /* Single-precision Poisson step (TC_MIXED contexts; TC_ERR_ARG otherwise):

@@ -371,7 +371,7 @@ def test_tma_rhs_is_bitwise_identical(torch_cuda, precision, scheme, nx, ny, nz,
     b.set_state(oc.u, oc.v, oc.w)
     b.step(scheme, dt, 7)
     ref = [np_(x) for x in b.get_state()[:3]]
-    for mode in range(1, 7):
+    for mode in range(1, 5):
         a = make_gpu(oc, precision)
         a.use_tma_rhs(mode)
         a.set_state(oc.u, oc.v, oc.w)

@@ -153,8 +153,9 @@ class Channel:
         L.check(self.lib.tc_use_fused_poisson(self.ctx, int(bool(on))))
 
     def use_tma_rhs(self, on=True):
-        """Explicit-RHS tiles staged by tensor copies (on, the default where
-        the grid allows it) or by per-thread loads (off); bit-identical."""
+        """Explicit-RHS tiles staged by tensor copies (True or a tile-shape
+        mode 1..4; mode 1 is the default where the grid allows it) or by
+        per-thread loads (False); bit-identical."""
         L.check(self.lib.tc_use_tma_rhs(self.ctx, int(on)))
 
     def use_fp32_poisson(self, on=True, warm_steps=10):

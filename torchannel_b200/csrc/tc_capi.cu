@@ -540,25 +540,27 @@ template <class T, int KB, int NST, int MINB> struct RhsV {
   static constexpr int kb = KB, nst = NST;
   template <bool FULL, int UPD> static constexpr auto fn() { return k_rhs_tma<T, FULL, UPD, KB, NST, MINB>; }
 };
-// Shapes (planes per tile, stages, CTAs per SM) by mode.  FP32 storage:
-// 1: 8, 2, 2; 2: 4, 2, 3; 3: 4, 1, 4; 4: 8, 1, 3; 5: 4, 1, 5; 6: 8, 1, 4.
-// FP64 storage: 1: 4, 2, 2; 2: 2, 1, 4; 3: 4, 1, 3; 4: 2, 1, 5; 5, 6: as 1.
+// Shapes (planes per tile, stages, resident CTAs per SM) by mode, FP32 /
+// FP64 storage: 1: 4, 1, 5 / 2, 1, 5 (the default); 2: 2, 1, 6 / 2, 1, 4;
+// 3: 2, 1, 5 / 4, 1, 3; 4: 8, 2, 2 / 4, 2, 2 (the persistent two-stage
+// pipeline).  Measured at 192 x 192 x 128 (ms of the kernel, FP32 / FP64):
+// per-thread staging 79.0 / 117.7; 4 planes, one stage, 5 CTAs 79.4; 2 planes,
+// one stage, 5 CTAs - / 111.7; 8 planes, two stages, 2 CTAs 91.0 / -;
+// 4 planes, two stages, 2 CTAs - / 121.5.
 template <class T, class F> static void rhs_variant(int mode, F&& f) {
   if constexpr (sizeof(T) == 8) {
     switch (mode) {
       case 2: f(RhsV<double, 2, 1, 4>{}); break;
       case 3: f(RhsV<double, 4, 1, 3>{}); break;
-      case 4: f(RhsV<double, 2, 1, 5>{}); break;
-      default: f(RhsV<double, 4, 2, 2>{}); break;
+      case 4: f(RhsV<double, 4, 2, 2>{}); break;
+      default: f(RhsV<double, 2, 1, 5>{}); break;
     }
   } else {
     switch (mode) {
-      case 2: f(RhsV<float, 4, 2, 3>{}); break;
-      case 3: f(RhsV<float, 4, 1, 4>{}); break;
-      case 4: f(RhsV<float, 8, 1, 3>{}); break;
-      case 5: f(RhsV<float, 4, 1, 5>{}); break;
-      case 6: f(RhsV<float, 8, 1, 4>{}); break;
-      default: f(RhsV<float, 8, 2, 2>{}); break;
+      case 2: f(RhsV<float, 2, 1, 6>{}); break;
+      case 3: f(RhsV<float, 2, 1, 5>{}); break;
+      case 4: f(RhsV<float, 8, 2, 2>{}); break;
+      default: f(RhsV<float, 4, 1, 5>{}); break;
     }
   }
 }
@@ -1337,7 +1339,7 @@ extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
 
 extern "C" int tc_use_tma_rhs(tc_ctx* c, int on) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
-  if (on < 0 || on > 6) return fail(TC_ERR_ARG, "mode 0 .. 6");
+  if (on < 0 || on > 4) return fail(TC_ERR_ARG, "mode 0 .. 4");
   if (on && on != c->rhs_tma_mode) {
     const int rc = (c->tsz == 8) ? rhs_tma_setup<double>(c, on) : rhs_tma_setup<float>(c, on);
     if (rc) return rc;
