@@ -37,7 +37,10 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 #define TC_BATCH_FFT_MINB 4
 #endif
 #ifndef TC_BATCH_RHS_MINB
-#define TC_BATCH_RHS_MINB 6
+#define TC_BATCH_RHS_MINB 6      // FP64 storage (the per-plane stencils)
+#endif
+#ifndef TC_BATCH_RHS_MINB32
+#define TC_BATCH_RHS_MINB32 3    // FP32 storage (the column march carries plane values: 80 registers)
 #endif
 #ifndef TC_BATCH_TRI_MINB
 #define TC_BATCH_TRI_MINB 6
@@ -99,7 +102,7 @@ __device__ __forceinline__ int batch_member(const int* st, int nm, int w) {
 }
 
 template <class T, bool FULL, int UPD>
-__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>(), TC_BATCH_RHS_MINB) kb_rhs(const BMember<T>* __restrict__ M, int nm, int total) {
+__global__ void __launch_bounds__(RHS_TX * rhs_ty<T>(), sizeof(T) == 4 ? TC_BATCH_RHS_MINB32 : TC_BATCH_RHS_MINB) kb_rhs(const BMember<T>* __restrict__ M, int nm, int total) {
   __shared__ int st[TC_BATCH_MAX + 1];
   batch_starts(M, nm, BK_RHS, total, st);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {

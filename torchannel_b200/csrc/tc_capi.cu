@@ -541,12 +541,12 @@ template <class T, int KB, int NST, int MINB> struct RhsV {
   template <bool FULL, int UPD> static constexpr auto fn() { return k_rhs_tma<T, FULL, UPD, KB, NST, MINB>; }
 };
 // Shapes (planes per tile, stages, resident CTAs per SM) by mode, FP32 /
-// FP64 storage: 1: 4, 1, 5 / 2, 1, 5 (the default); 2: 2, 1, 6 / 2, 1, 4;
-// 3: 2, 1, 5 / 4, 1, 3; 4: 8, 2, 2 / 4, 2, 2 (the persistent two-stage
-// pipeline).  Measured at 192 x 192 x 128 (ms of the kernel, FP32 / FP64):
-// per-thread staging 79.0 / 117.7; 4 planes, one stage, 5 CTAs 79.4; 2 planes,
-// one stage, 5 CTAs - / 111.7; 8 planes, two stages, 2 CTAs 91.0 / -;
-// 4 planes, two stages, 2 CTAs - / 121.5.
+// FP64 storage: 1: 8, 1, 3 / 2, 1, 5 (the default); 2: 4, 1, 4 / 2, 1, 4;
+// 3: 8, 1, 4 / 4, 1, 3; 4: 16, 1, 2 / 4, 2, 2 (the persistent two-stage
+// pipeline).  Measured at 192 x 192 x 128 (us of the kernel, FP32 column
+// march / FP64 per-plane stencils): mode 1 64.7 / 111.3, mode 2 66.7, mode 3
+// 70.0 (64 registers, spills), mode 4 67.9 / 121.5; per-thread staging
+// (k_rhs_update) 91.5 / 117.7.
 template <class T, class F> static void rhs_variant(int mode, F&& f) {
   if constexpr (sizeof(T) == 8) {
     switch (mode) {
@@ -557,10 +557,10 @@ template <class T, class F> static void rhs_variant(int mode, F&& f) {
     }
   } else {
     switch (mode) {
-      case 2: f(RhsV<float, 2, 1, 6>{}); break;
-      case 3: f(RhsV<float, 2, 1, 5>{}); break;
-      case 4: f(RhsV<float, 8, 2, 2>{}); break;
-      default: f(RhsV<float, 4, 1, 5>{}); break;
+      case 2: f(RhsV<float, 4, 1, 4>{}); break;
+      case 3: f(RhsV<float, 8, 1, 4>{}); break;
+      case 4: f(RhsV<float, 16, 1, 2>{}); break;
+      default: f(RhsV<float, 8, 1, 3>{}); break;
     }
   }
 }

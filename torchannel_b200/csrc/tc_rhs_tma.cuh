@@ -1,5 +1,5 @@
 // Kernel (a) with its tiles staged by the tensor memory accelerator: the
-// stencils of rhs_point (advection + x/y or full diffusion + forcing + AB2,
+// stencils of rhs_stencils (advection + x/y or full diffusion + forcing + AB2,
 // operators.py:18-248, 474-548, 818-1225; solver.py:626-651) over tiles of
 // RHS_TX x 8 points and KB planes, in a persistent loop of CTAs that each
 // hold two stages in shared memory.  While a CTA evaluates one tile, one
@@ -17,8 +17,8 @@
 //  * u / v z ghosts (planes -1 and nz, which the box reads as zeros):
 //    -q[0] below, -q[nz-1] (no-slip) or +q[nz-1] (free-slip) above; w's
 //    plane -1 stays 0 and its plane nz is the stored wall;
-//  * mixed precision: u is stored as u - U0[k], and its planes get U0[k]
-//    added so that the stencils see the total velocity.
+//  * mixed precision: u is stored as u - U0[k]; the stencils add U0[k] to
+//    their sums of u (rhs_march).
 // Each wait on a stage's barrier is bounded; if one runs out, the CTA sets
 // TCE_TIMEOUT in the error word and stops.
 #pragma once
@@ -64,7 +64,6 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
   const int ntiles = ntx * nty * ntz;
   const T top = g.top_neumann ? T(1) : T(-1);
   const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
-  const T* __restrict__ base = g.ubase_t;
   if (blockIdx.x >= ntiles) return;
   if (smem_u32(buf) & 127u) {  // tensor copies need 128-byte aligned boxes
     if (tid == 0) atomicOr(err, TCE_BOUNDS);
@@ -107,8 +106,8 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
     const int i0 = bx * RHS_TX, j0 = by * S::TY, kb = bz * KB;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = (i < nx) && (j < ny);
-    // AB2 history and stored u of this thread's points, in flight with the copy
-    T hru[KB], hrv[KB], hrw[KB], hu[KB];
+    // AB2 history of this thread's points, in flight with the copy
+    T hru[KB], hrv[KB], hrw[KB];
 #pragma unroll
     for (int q = 0; q < KB; ++q) {
       const int k = kb + q;
@@ -118,7 +117,6 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       hru[q] = (cell && hist) ? ru[o] : T(0);
       hrv[q] = (cell && hist) ? rv[o] : T(0);
       hrw[q] = (face && hist) ? rw[o] : T(0);
-      hu[q] = (cell && base && UPD != UPD_RHS_ONLY) ? ldg(u + o) : T(0);
     }
     const bool landed = mbar_wait_bounded(&bar[st], par, RHS_TMA_WAIT_LIMIT);
     if (__syncthreads_or(!landed)) {
@@ -134,8 +132,8 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
     T* su = buf + (size_t)st * S::STAGE;
     T* sv = su + S::BOX;
     T* sw = sv + S::BOX;
-    // (1) periodic wraps of the halo ring (raw stored values) on the planes
-    //     that exist, and U0 added to u's planes
+    // (1) periodic wraps of the halo ring (stored values) on the planes that
+    //     exist
     const bool wrap_x = (i0 == 0) || (i0 + RHS_TX >= nx);
     const bool wrap_y = (j0 == 0) || (j0 + S::TY >= ny);
     if (wrap_x || wrap_y) {
@@ -165,15 +163,6 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       }
       __syncthreads();
     }
-    if (base) {
-      for (int e = tid; e < BZ * BY * (RHS_TX + 2); e += nthr) {
-        const int sl = e / (BY * (RHS_TX + 2)), r = e - sl * (BY * (RHS_TX + 2));
-        const int hy = r / (RHS_TX + 2), hx = r - hy * (RHS_TX + 2);
-        const int p = kb - 1 + sl;
-        if (p >= 0 && p < nz) su[(sl * BY + hy) * BX + OX - 1 + hx] += ldg(base + p);
-      }
-      __syncthreads();
-    }
     // (2) z ghosts of u and v: plane -1 (slot 0 of the first tile) and plane
     //     nz (slot nz - kb + 1 when it is in the box)
     const int sg_lo = (kb == 0) ? 0 : -1;
@@ -192,116 +181,11 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       }
       __syncthreads();
     }
-    // (3) the stencils, plane by plane (the arithmetic of rhs_tile)
-    T(*su3)[BY][BX] = reinterpret_cast<T(*)[BY][BX]>(su);
-    T(*sv3)[BY][BX] = reinterpret_cast<T(*)[BY][BX]>(sv);
-    T(*sw3)[BY][BX] = reinterpret_cast<T(*)[BY][BX]>(sw);
-    const int cx = tx + OX, cy = ty + 1;
-    // Every advective flux is a product of two interpolations 0.5(a + b); the
-    // sums are multiplied unscaled and the two factors 0.5 are folded into the
-    // difference quotient as 0.25 / delta.  Scaling by powers of two is exact,
-    // so the fluxes are the same numbers as with the interpolations formed.
-    const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
-#pragma unroll 1
-    for (int kk = 0; kk < KB; ++kk) {
-      const int k = kb + kk;
-      if (k > nz) break;
-      const int sm = kk, s0 = kk + 1, sp = kk + 2;
-      if (active && k < nz) {
-        const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-        const T idzf = g.idzf[k];
-        const T qzf = T(0.25) * idzf;
-        // ---------------- u at cell k ----------------
-        {
-          const T U0 = su3[s0][cy][cx], Uxm = su3[s0][cy][cx - 1], Uxp = su3[s0][cy][cx + 1];
-          const T Uym = su3[s0][cy - 1][cx], Uyp = su3[s0][cy + 1][cx];
-          const T Uzm = su3[sm][cy][cx], Uzp = su3[sp][cy][cx];
-          const bool edge = (i == nx - 1);
-          T r = T(0);
-          if (!(edge && g.rhs_fused)) {
-            r = g.nu_idx2 * (Uxp - T(2) * U0 + Uxm) + g.nu_idy2 * (Uyp - T(2) * U0 + Uym);
-            if (FULL) r += g.nu * ((Uzp - U0) * g.idzc[k + 1] - (U0 - Uzm) * g.idzc[k]) * idzf;
-          }
-          if (!edge) {
-            const T duudx = (sq(U0 + Uxp) - sq(Uxm + U0)) * qx;
-            const T vu_t = (sv3[s0][cy][cx] + sv3[s0][cy][cx + 1]) * (U0 + Uyp);
-            const T vu_b = (sv3[s0][cy - 1][cx] + sv3[s0][cy - 1][cx + 1]) * (Uym + U0);
-            const T wu_t = (sw3[sp][cy][cx] + sw3[sp][cy][cx + 1]) * (U0 + Uzp);
-            const T wu_b = (sw3[s0][cy][cx] + sw3[s0][cy][cx + 1]) * (Uzm + U0);
-            r -= duudx + (vu_t - vu_b) * qy + (wu_t - wu_b) * qzf;
-          }
-          if (UPD == UPD_RHS_ONLY) {
-            ru[o] = r;
-          } else {
-            const T Uraw = base ? hu[0] : U0;  // stored value (u - U0[k] in mixed precision)
-            if (UPD == UPD_FE) {
-              T q = Uraw + dt * r;
-              us[o] = q + dt * T(1);
-            } else {
-              r += forcing;
-              us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * hru[0]) : Uraw + dt * r;
-              ru[o] = r;
-            }
-          }
-        }
-        // ---------------- v at cell k ----------------
-        {
-          const T V0 = sv3[s0][cy][cx], Vxm = sv3[s0][cy][cx - 1], Vxp = sv3[s0][cy][cx + 1];
-          const T Vym = sv3[s0][cy - 1][cx], Vyp = sv3[s0][cy + 1][cx];
-          const T Vzm = sv3[sm][cy][cx], Vzp = sv3[sp][cy][cx];
-          const bool edge = (j == ny - 1);
-          T r = T(0);
-          if (!(edge && g.rhs_fused)) {
-            r = g.nu_idx2 * (Vxp - T(2) * V0 + Vxm) + g.nu_idy2 * (Vyp - T(2) * V0 + Vym);
-            if (FULL) r += g.nu * ((Vzp - V0) * g.idzc[k + 1] - (V0 - Vzm) * g.idzc[k]) * idzf;
-          }
-          if (!edge) {
-            const T uv_r = (su3[s0][cy][cx] + su3[s0][cy + 1][cx]) * (V0 + Vxp);
-            const T uv_l = (su3[s0][cy][cx - 1] + su3[s0][cy + 1][cx - 1]) * (Vxm + V0);
-            const T dvvdy = (sq(V0 + Vyp) - sq(Vym + V0)) * qy;
-            const T wv_t = (sw3[sp][cy][cx] + sw3[sp][cy + 1][cx]) * (V0 + Vzp);
-            const T wv_b = (sw3[s0][cy][cx] + sw3[s0][cy + 1][cx]) * (Vzm + V0);
-            r -= (uv_r - uv_l) * qx + dvvdy + (wv_t - wv_b) * qzf;
-          }
-          if (UPD == UPD_RHS_ONLY) {
-            rv[o] = r;
-          } else if (UPD == UPD_FE) {
-            vs[o] = V0 + dt * r;
-          } else {
-            vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * hrv[0]) : V0 + dt * r;
-            rv[o] = r;
-          }
-        }
-      }
-      // ---------------- w at face k ----------------
-      if (active && k >= 1 && k <= nz - 1) {
-        const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-        const T W0 = sw3[s0][cy][cx], Wxm = sw3[s0][cy][cx - 1], Wxp = sw3[s0][cy][cx + 1];
-        const T Wym = sw3[s0][cy - 1][cx], Wyp = sw3[s0][cy + 1][cx];
-        const T Wzm = sw3[sm][cy][cx], Wzp = sw3[sp][cy][cx];
-        T r = g.nu_idx2 * (Wxp - T(2) * W0 + Wxm) + g.nu_idy2 * (Wyp - T(2) * W0 + Wym);
-        // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
-        if (FULL) r += g.nu * ((Wzp - W0) * g.idzf[k] - (W0 - Wzm) * g.idzf[k - 1]) * g.idzc[k - 1];
-        const T uw_r = (su3[sm][cy][cx] + su3[s0][cy][cx]) * (W0 + Wxp);
-        const T uw_l = (su3[sm][cy][cx - 1] + su3[s0][cy][cx - 1]) * (Wxm + W0);
-        const T vw_t = (sv3[sm][cy][cx] + sv3[s0][cy][cx]) * (W0 + Wyp);
-        const T vw_b = (sv3[sm][cy - 1][cx] + sv3[s0][cy - 1][cx]) * (Wym + W0);
-        const T dwwdz = (sq(W0 + Wzp) - sq(Wzm + W0)) * (T(0.25) * g.idzc[k]);
-        r -= (uw_r - uw_l) * qx + (vw_t - vw_b) * qy + dwwdz;
-        if (UPD == UPD_RHS_ONLY) {
-          rw[o] = r;
-        } else if (UPD == UPD_FE) {
-          ws[o] = W0 + dt * r;
-        } else {
-          ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * hrw[0]) : W0 + dt * r;
-          rw[o] = r;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q + 1 < KB; ++q) {
-        hru[q] = hru[q + 1]; hrv[q] = hrv[q + 1]; hrw[q] = hrw[q + 1]; hu[q] = hu[q + 1];
-      }
-    }
+    // (3) the stencils, marching up the thread's column (as in rhs_tile)
+    rhs_stencils<T, FULL, UPD, KB, BY, BX>(g, reinterpret_cast<const T(*)[BY][BX]>(su),
+                                           reinterpret_cast<const T(*)[BY][BX]>(sv),
+                                           reinterpret_cast<const T(*)[BY][BX]>(sw), tx + OX, ty + 1, i, j, active,
+                                           kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw, forcing, dt, have_hist);
     __syncthreads();  // this stage is free for the copy issued two tiles on
     if (NST == 1 && tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, 0);
   }

@@ -45,10 +45,9 @@ enum : int {
 // A block owns a RHS_TX x RHS_TY (rhs_ty<T>()) tile and RHS_KB (rhs_kb<T>()) consecutive
 // planes k = kb..kb+RHS_KB-1 (u, v at cell k, w at face k).  It first stages the u,
 // v, w planes kb-1 .. kb+RHS_KB with a one-cell periodic halo (z ghosts
-// applied, u with its base profile added) in shared memory -- every load of
-// the block is independent and issued up front; halo offsets are computed
-// once per thread -- then evaluates the stencils of each plane from shared
-// memory.  Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
+// applied) in shared memory -- every load of the block is independent and
+// issued up front; halo offsets are computed once per thread -- then marches
+// the stencils up its column from shared memory (rhs_march).  Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
 // v[:, ny]; both reference paths omit advection there, the separate-op path
 // keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
 // ---------------------------------------------------------------------------
@@ -59,96 +58,218 @@ template <class T> __host__ __device__ constexpr int rhs_ty() { return 8; }
 template <class T> __host__ __device__ constexpr int rhs_kb() { return sizeof(T) == 8 ? 3 : 4; }
 #define RHS_HX (RHS_TX + 2)
 
-// The tile (bx, by, bz) of the block grid above; k_rhs_update runs one tile
-// per block, the ensemble kernel of tc_batch.cuh loops over the tiles of all
-// members (the shared tile is reused: callers separate tiles by a barrier).
-template <class T, bool FULL, int UPD>
-__device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
-                                         const T* __restrict__ w, T* __restrict__ us, T* __restrict__ vs,
-                                         T* __restrict__ ws, T* __restrict__ ru, T* __restrict__ rv,
-                                         T* __restrict__ rw, const double* __restrict__ forcing_dev, T dt,
-                                         int have_hist, int bx, int by, int bz) {
-  constexpr int RHS_TY = rhs_ty<T>(), RHS_HY = RHS_TY + 2, RHS_NH = RHS_HX * RHS_HY;
-  constexpr int RHS_KB = rhs_kb<T>();
-  constexpr int RHS_NS = RHS_KB + 2;
-  static_assert(RHS_NH <= 2 * RHS_TX * RHS_TY, "two halo elements per thread at most");
-  __shared__ T su[RHS_NS][RHS_HY][RHS_HX];
-  __shared__ T sv[RHS_NS][RHS_HY][RHS_HX];
-  __shared__ T sw[RHS_NS][RHS_HY][RHS_HX];
+// Arithmetic with explicit rounding for the stencils below: every kernel
+// that evaluates them (one tile per block, tensor-copy staging, the ensemble
+// loops) produces the same bits, whatever the compiler would contract.
+template <class T> struct Rn;
+template <> struct Rn<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+};
+template <> struct Rn<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+};
+
+// The stencils of one thread's column of KB planes k = kb .. kb+KB-1 (u, v at
+// cell k, w at face k), marching up in z over a staged tile: slot s of the
+// shared arrays holds plane kb-1+s (slots 0 .. KB+1), (cy, cx) is the thread's
+// point.  The tile holds the stored values (u - U0[k] in mixed precision; z
+// ghosts with their sign rule applied); U0 enters the sums of u analytically.
+//
+// Each flux of the staggered advection is formed once per point and plane:
+//  * uu at i +- 1/2 and vv at j +- 1/2 (cell centres),
+//  * uv at the corners (i+1/2, j+1/2) (for u and v), (i+1/2, j-1/2) (u),
+//    (i-1/2, j+1/2) (v),
+//  * uw at (i +- 1/2, face k+1), vw at (j +- 1/2, face k+1) and ww at cell k:
+//    formed with plane k+1 and carried to the next plane, where the face is
+//    face k (u's and v's lower flux, w's four side fluxes, ww below).
+// With the plane values that the next plane needs also carried in registers,
+// a plane costs 17 shared loads (6 of u, 6 of v, 5 of w).  A flux is the
+// product of two unscaled sums; the factors 0.5 of both interpolations are
+// folded into the difference quotient as 0.25 / delta (exact: powers of two).
+// The fluxes of face kb are formed before the first plane by the same
+// expressions, so the results do not depend on KB or on the tile shape.
+template <class T, bool FULL, int UPD, int KB, int HY, int HX>
+__device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict__ su)[HY][HX],
+                                          const T (*__restrict__ sv)[HY][HX], const T (*__restrict__ sw)[HY][HX],
+                                          int cx, int cy, int i, int j, bool active, int kb, T* __restrict__ us,
+                                          T* __restrict__ vs, T* __restrict__ ws, T* __restrict__ ru,
+                                          T* __restrict__ rv, T* __restrict__ rw, T (&hru)[KB], T (&hrv)[KB],
+                                          T (&hrw)[KB], T forcing, T dt, int have_hist) {
+  using R = Rn<T>;
+  constexpr bool HB = sizeof(T) == 4;  // mixed precision: u stored as u - U0[k]
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx;
-  const int i0 = bx * RHS_TX, j0 = by * RHS_TY;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool active = (i < nx) && (j < ny);
-  const int kb = bz * RHS_KB;  // planes kb .. kb+RHS_KB-1 (<= nz)
   const T top = g.top_neumann ? T(1) : T(-1);
-  const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
-  const T* __restrict__ base = g.ubase_t;
-  // halo elements of this thread: e0 = tid, e1 = tid + block size (if < RHS_NH)
-  const int e1 = tid + RHS_TX * RHS_TY;
-  const bool has1 = e1 < RHS_NH;
-  size_t off[2];
-  int hyx[2][2];
+  // U0 of slot s (plane kb-1+s) with the z-ghost rule's sign
+  T bs[KB + 2];
+#pragma unroll
+  for (int s = 0; s < KB + 2; ++s) {
+    const int p = kb - 1 + s;
+    T b = T(0);
+    if (HB && g.ubase_t) {
+      const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
+      const T sgn = p < 0 ? T(-1) : (p >= nz ? top : T(1));
+      b = sgn * ldg(g.ubase_t + pc);
+    }
+    bs[s] = b;
+  }
+  const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
+  const bool edge_u = (i == nx - 1), edge_v = (j == ny - 1);
+  // plane kb-1 (slot 0) and plane kb (slot 1)
+  T pU0 = su[0][cy][cx], pV0 = sv[0][cy][cx], pW0 = sw[0][cy][cx];
+  T cU0 = su[1][cy][cx], cUxm = su[1][cy][cx - 1], cV0 = sv[1][cy][cx], cVym = sv[1][cy - 1][cx];
+  T cW0 = sw[1][cy][cx], cWxm = sw[1][cy][cx - 1], cWxp = sw[1][cy][cx + 1];
+  T cWym = sw[1][cy - 1][cx], cWyp = sw[1][cy + 1][cx];
+  // fluxes of face kb
+  T Fuw_p, Fuw_m, Fvw_p, Fvw_m, Fww;
   {
-    const int es[2] = {tid, e1};
+    const T bz = HB ? R::add(bs[0], bs[1]) : T(0);
+    T su_p = R::add(pU0, cU0), su_m = R::add(su[0][cy][cx - 1], cUxm);
+    if (HB) { su_p = R::add(su_p, bz); su_m = R::add(su_m, bz); }
+    Fuw_p = R::mul(R::add(cW0, cWxp), su_p);
+    Fuw_m = R::mul(R::add(cWxm, cW0), su_m);
+    Fvw_p = R::mul(R::add(cW0, cWyp), R::add(pV0, cV0));
+    Fvw_m = R::mul(R::add(cWym, cW0), R::add(sv[0][cy - 1][cx], cVym));
+    const T sww = R::add(pW0, cW0);
+    Fww = R::mul(sww, sww);
+  }
+  size_t o = (size_t)kb * plane + (size_t)j * nx + i;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int hy = es[q] / RHS_HX, hx = es[q] - (es[q] / RHS_HX) * RHS_HX;
-      int jj = j0 - 1 + hy, ii = i0 - 1 + hx;
-      while (jj < 0) jj += ny;
-      while (jj >= ny) jj -= ny;
-      while (ii < 0) ii += nx;
-      while (ii >= nx) ii -= nx;
-      off[q] = (size_t)jj * nx + ii;
-      hyx[q][0] = hy; hyx[q][1] = hx;
+  for (int kk = 0; kk < KB; ++kk, o += plane) {
+    const int k = kb + kk;
+    if (k >= nz) break;
+    const int s0 = kk + 1, sp = kk + 2;
+    // plane k: the in-plane neighbours not carried
+    const T Uxp = su[s0][cy][cx + 1], Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
+    const T Uypm = su[s0][cy + 1][cx - 1];
+    const T Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1], Vyp = sv[s0][cy + 1][cx];
+    const T Vymp = sv[s0][cy - 1][cx + 1];
+    // plane k+1
+    const T nU0 = su[sp][cy][cx], nUxm = su[sp][cy][cx - 1], nV0 = sv[sp][cy][cx], nVym = sv[sp][cy - 1][cx];
+    const T nW0 = sw[sp][cy][cx], nWxm = sw[sp][cy][cx - 1], nWxp = sw[sp][cy][cx + 1];
+    const T nWym = sw[sp][cy - 1][cx], nWyp = sw[sp][cy + 1][cx];
+    const T b2 = HB ? R::add(bs[s0], bs[s0]) : T(0);
+    const T bz = HB ? R::add(bs[s0], bs[sp]) : T(0);
+    auto ub = [&](T s, T b) { return HB ? R::add(s, b) : s; };
+    // fluxes of plane k
+    const T Sa = ub(R::add(cU0, Uxp), b2), Sb = ub(R::add(cUxm, cU0), b2);
+    const T Fuu = R::fma(Sa, Sa, -R::mul(Sb, Sb));
+    const T Sc = R::add(cV0, Vyp), Sd = R::add(cVym, cV0);
+    const T Fvv = R::fma(Sc, Sc, -R::mul(Sd, Sd));
+    const T Fuv_pp = R::mul(R::add(cV0, Vxp), ub(R::add(cU0, Uyp), b2));
+    const T Fuv_pm = R::mul(R::add(cVym, Vymp), ub(R::add(Uym, cU0), b2));
+    const T Fuv_mp = R::mul(ub(R::add(cUxm, Uypm), b2), R::add(Vxm, cV0));
+    // fluxes of face k+1 (carried)
+    const T Fuw_p1 = R::mul(R::add(nW0, nWxp), ub(R::add(cU0, nU0), bz));
+    const T Fuw_m1 = R::mul(R::add(nWxm, nW0), ub(R::add(cUxm, nUxm), bz));
+    const T Fvw_p1 = R::mul(R::add(nW0, nWyp), R::add(cV0, nV0));
+    const T Fvw_m1 = R::mul(R::add(nWym, nW0), R::add(cVym, nVym));
+    const T sww = R::add(cW0, nW0);
+    const T Fww1 = R::mul(sww, sww);
+    if (active) {
+      const T idzf = g.idzf[k];
+      const T qzf = T(0.25) * idzf;
+      // ---------------- u at cell k ----------------
+      {
+        T r = T(0);
+        if (!(edge_u && g.rhs_fused)) {
+          const T lx = R::add(R::fma(T(-2), cU0, Uxp), cUxm), ly = R::add(R::fma(T(-2), cU0, Uyp), Uym);
+          r = R::fma(g.nu_idx2, lx, R::mul(g.nu_idy2, ly));
+          if (FULL) {
+            T dp = R::sub(nU0, cU0), dm = R::sub(cU0, pU0);
+            if (HB) { dp = R::add(dp, R::sub(bs[sp], bs[s0])); dm = R::add(dm, R::sub(bs[s0], bs[kk])); }
+            const T t = R::sub(R::mul(dp, g.idzc[k + 1]), R::mul(dm, g.idzc[k]));
+            r = R::fma(R::mul(g.nu, idzf), t, r);
+          }
+        }
+        if (!edge_u) r = R::sub(r, R::fma(R::sub(Fuw_p1, Fuw_p), qzf, R::fma(R::sub(Fuv_pp, Fuv_pm), qy, R::mul(Fuu, qx))));
+        if (UPD == UPD_RHS_ONLY) {
+          ru[o] = r;
+        } else if (UPD == UPD_FE) {
+          us[o] = R::add(R::fma(dt, r, cU0), dt);
+        } else {
+          r = R::add(r, forcing);
+          const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hru[kk])) : r;
+          us[o] = R::fma(dt, a, cU0);
+          ru[o] = r;
+        }
+      }
+      // ---------------- v at cell k ----------------
+      {
+        T r = T(0);
+        if (!(edge_v && g.rhs_fused)) {
+          const T lx = R::add(R::fma(T(-2), cV0, Vxp), Vxm), ly = R::add(R::fma(T(-2), cV0, Vyp), cVym);
+          r = R::fma(g.nu_idx2, lx, R::mul(g.nu_idy2, ly));
+          if (FULL) {
+            const T t = R::sub(R::mul(R::sub(nV0, cV0), g.idzc[k + 1]), R::mul(R::sub(cV0, pV0), g.idzc[k]));
+            r = R::fma(R::mul(g.nu, idzf), t, r);
+          }
+        }
+        if (!edge_v) r = R::sub(r, R::fma(R::sub(Fvw_p1, Fvw_p), qzf, R::fma(R::sub(Fuv_pp, Fuv_mp), qx, R::mul(Fvv, qy))));
+        if (UPD == UPD_RHS_ONLY) {
+          rv[o] = r;
+        } else if (UPD == UPD_FE) {
+          vs[o] = R::fma(dt, r, cV0);
+        } else {
+          const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hrv[kk])) : r;
+          vs[o] = R::fma(dt, a, cV0);
+          rv[o] = r;
+        }
+      }
+      // ---------------- w at face k ----------------
+      if (k >= 1) {
+        const T lx = R::add(R::fma(T(-2), cW0, cWxp), cWxm), ly = R::add(R::fma(T(-2), cW0, cWyp), cWym);
+        T r = R::fma(g.nu_idx2, lx, R::mul(g.nu_idy2, ly));
+        // z term of diffusion_w divides by dz_c[K-1] (operators.py:120,1025)
+        if (FULL) {
+          const T t = R::sub(R::mul(R::sub(nW0, cW0), g.idzf[k]), R::mul(R::sub(cW0, pW0), g.idzf[k - 1]));
+          r = R::fma(R::mul(g.nu, g.idzc[k - 1]), t, r);
+        }
+        const T dww = R::mul(R::sub(Fww1, Fww), T(0.25) * g.idzc[k]);
+        r = R::sub(r, R::fma(R::sub(Fuw_p, Fuw_m), qx, R::fma(R::sub(Fvw_p, Fvw_m), qy, dww)));
+        if (UPD == UPD_RHS_ONLY) {
+          rw[o] = r;
+        } else if (UPD == UPD_FE) {
+          ws[o] = R::fma(dt, r, cW0);
+        } else {
+          const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hrw[kk])) : r;
+          ws[o] = R::fma(dt, a, cW0);
+          rw[o] = r;
+        }
+      }
     }
+    // carry plane k+1 and the fluxes of face k+1
+    pU0 = cU0; pV0 = cV0; pW0 = cW0;
+    cU0 = nU0; cUxm = nUxm; cV0 = nV0; cVym = nVym;
+    cW0 = nW0; cWxm = nWxm; cWxp = nWxp; cWym = nWym; cWyp = nWyp;
+    Fuw_p = Fuw_p1; Fuw_m = Fuw_m1; Fvw_p = Fvw_p1; Fvw_m = Fvw_m1; Fww = Fww1;
   }
-  // AB2 history and the stored u of this thread's points, loaded with the
-  // staging so that their latency overlaps it; one plane consumed per
-  // iteration (shifted down)
-  T pf_ru[RHS_KB], pf_rv[RHS_KB], pf_rw[RHS_KB], pf_u[RHS_KB];
-#pragma unroll
-  for (int q = 0; q < RHS_KB; ++q) {
-    const int k = kb + q;
-    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
-    const bool cell = active && k < nz, face = active && k >= 1 && k <= nz - 1;
-    const bool hist = UPD == UPD_AB2 && have_hist;
-    pf_ru[q] = (cell && hist) ? ru[o] : T(0);
-    pf_rv[q] = (cell && hist) ? rv[o] : T(0);
-    pf_rw[q] = (face && hist) ? rw[o] : T(0);
-    pf_u[q] = (cell && base && UPD != UPD_RHS_ONLY) ? ldg(u + o) : T(0);
-  }
-  // stage planes p = kb-1 .. kb+RHS_KB into slots 0 .. RHS_NS-1
-#pragma unroll
-  for (int sl = 0; sl < RHS_NS; ++sl) {
-    const int p = kb - 1 + sl;
-    // cell plane read for u/v with its z-ghost rule: sign * (q[pc] + base[pc])
-    const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
-    const T sgn = p < 0 ? T(-1) : (p >= nz ? top : T(1));
-    const T bb = base ? ldg(base + pc) : T(0);
-    const bool wok = (p >= 0) && (p <= nz);
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      if (q == 1 && !has1) break;
-      const size_t oc = (size_t)pc * plane + off[q];
-      const T uu = sgn * (ldg(u + oc) + bb);
-      const T vv = sgn * ldg(v + oc);
-      const T ww = wok ? ldg(w + (size_t)p * plane + off[q]) : T(0);
-      su[sl][hyx[q][0]][hyx[q][1]] = uu;
-      sv[sl][hyx[q][0]][hyx[q][1]] = vv;
-      sw[sl][hyx[q][0]][hyx[q][1]] = ww;
-    }
-  }
-  __syncthreads();
-  const int cx = tx + 1, cy = ty + 1;
-  // Every advective flux is a product of two interpolations 0.5(a + b); the
-  // sums are multiplied unscaled and the two factors 0.5 are folded into the
-  // difference quotient as 0.25 / delta.  Scaling by powers of two is exact,
-  // so the fluxes are the same numbers as with the interpolations formed.
+}
+
+// FP64 storage: the stencils plane by plane, every flux formed where it is
+// used (the registers that carrying values up the column would take cost
+// the double-precision kernels more than the loads they save).  Same slot
+// layout as rhs_march; no base profile (FP64 fields hold the total velocity).
+template <bool FULL, int UPD, int KB, int HY, int HX>
+__device__ __forceinline__ void rhs_planes(const Grid<double>& g, const double (*__restrict__ su)[HY][HX],
+                                           const double (*__restrict__ sv)[HY][HX],
+                                           const double (*__restrict__ sw)[HY][HX], int cx, int cy, int i, int j,
+                                           bool active, int kb, double* __restrict__ us, double* __restrict__ vs,
+                                           double* __restrict__ ws, double* __restrict__ ru, double* __restrict__ rv,
+                                           double* __restrict__ rw, double (&hru)[KB], double (&hrv)[KB],
+                                           double (&hrw)[KB], double forcing, double dt, int have_hist) {
+  using T = double;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t plane = (size_t)nx * ny;
   const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
 #pragma unroll 1
-  for (int kk = 0; kk < RHS_KB; ++kk) {
+  for (int kk = 0; kk < KB; ++kk) {
     const int k = kb + kk;
     if (k > nz) break;
     const int sm = kk, s0 = kk + 1, sp = kk + 2;
@@ -177,16 +298,13 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
         }
         if (UPD == UPD_RHS_ONLY) {
           ru[o] = r;
+        } else if (UPD == UPD_FE) {
+          T q = U0 + dt * r;
+          us[o] = q + dt * T(1);
         } else {
-          const T Uraw = base ? pf_u[0] : U0;  // stored value (u - U0[k] in mixed precision)
-          if (UPD == UPD_FE) {
-            T q = Uraw + dt * r;
-            us[o] = q + dt * T(1);
-          } else {
-            r += forcing;
-            us[o] = have_hist ? Uraw + dt * (T(1.5) * r - T(0.5) * pf_ru[0]) : Uraw + dt * r;
-            ru[o] = r;
-          }
+          r += forcing;
+          us[o] = have_hist ? U0 + dt * (T(1.5) * r - T(0.5) * hru[0]) : U0 + dt * r;
+          ru[o] = r;
         }
       }
       // ---------------- v at cell k ----------------
@@ -213,7 +331,7 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
         } else if (UPD == UPD_FE) {
           vs[o] = V0 + dt * r;
         } else {
-          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * pf_rv[0]) : V0 + dt * r;
+          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * hrv[0]) : V0 + dt * r;
           rv[o] = r;
         }
       }
@@ -238,15 +356,111 @@ __device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__
       } else if (UPD == UPD_FE) {
         ws[o] = W0 + dt * r;
       } else {
-        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * pf_rw[0]) : W0 + dt * r;
+        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * hrw[0]) : W0 + dt * r;
         rw[o] = r;
       }
     }
 #pragma unroll
-    for (int q = 0; q + 1 < RHS_KB; ++q) {
-      pf_ru[q] = pf_ru[q + 1]; pf_rv[q] = pf_rv[q + 1]; pf_rw[q] = pf_rw[q + 1]; pf_u[q] = pf_u[q + 1];
+    for (int q = 0; q + 1 < KB; ++q) {
+      hru[q] = hru[q + 1]; hrv[q] = hrv[q + 1]; hrw[q] = hrw[q + 1];
     }
   }
+}
+
+// The stencils of a staged tile: rhs_march (FP32 storage) or rhs_planes (FP64).
+template <class T, bool FULL, int UPD, int KB, int HY, int HX>
+__device__ __forceinline__ void rhs_stencils(const Grid<T>& g, const T (*su)[HY][HX], const T (*sv)[HY][HX],
+                                             const T (*sw)[HY][HX], int cx, int cy, int i, int j, bool active,
+                                             int kb, T* us, T* vs, T* ws, T* ru, T* rv, T* rw, T (&hru)[KB],
+                                             T (&hrv)[KB], T (&hrw)[KB], T forcing, T dt, int have_hist) {
+  if constexpr (sizeof(T) == 8)
+    rhs_planes<FULL, UPD, KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw,
+                                      forcing, dt, have_hist);
+  else
+    rhs_march<T, FULL, UPD, KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv,
+                                        hrw, forcing, dt, have_hist);
+}
+
+// The tile (bx, by, bz) of the block grid above; k_rhs_update runs one tile
+// per block, the ensemble kernel of tc_batch.cuh loops over the tiles of all
+// members (the shared tile is reused: callers separate tiles by a barrier).
+template <class T, bool FULL, int UPD>
+__device__ __forceinline__ void rhs_tile(const Grid<T>& g, const T* __restrict__ u, const T* __restrict__ v,
+                                         const T* __restrict__ w, T* __restrict__ us, T* __restrict__ vs,
+                                         T* __restrict__ ws, T* __restrict__ ru, T* __restrict__ rv,
+                                         T* __restrict__ rw, const double* __restrict__ forcing_dev, T dt,
+                                         int have_hist, int bx, int by, int bz) {
+  constexpr int RHS_TY = rhs_ty<T>(), RHS_HY = RHS_TY + 2, RHS_NH = RHS_HX * RHS_HY;
+  constexpr int RHS_KB = rhs_kb<T>();
+  constexpr int RHS_NS = RHS_KB + 2;
+  static_assert(RHS_NH <= 2 * RHS_TX * RHS_TY, "two halo elements per thread at most");
+  __shared__ T su[RHS_NS][RHS_HY][RHS_HX];
+  __shared__ T sv[RHS_NS][RHS_HY][RHS_HX];
+  __shared__ T sw[RHS_NS][RHS_HY][RHS_HX];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t plane = (size_t)nx * ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx;
+  const int i0 = bx * RHS_TX, j0 = by * RHS_TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = (i < nx) && (j < ny);
+  const int kb = bz * RHS_KB;  // planes kb .. kb+RHS_KB-1 (<= nz)
+  const T top = g.top_neumann ? T(1) : T(-1);
+  const T forcing = (UPD == UPD_AB2) ? (T)(*forcing_dev) : T(0);
+  // halo elements of this thread: e0 = tid, e1 = tid + block size (if < RHS_NH)
+  const int e1 = tid + RHS_TX * RHS_TY;
+  const bool has1 = e1 < RHS_NH;
+  size_t off[2];
+  int hyx[2][2];
+  {
+    const int es[2] = {tid, e1};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int hy = es[q] / RHS_HX, hx = es[q] - (es[q] / RHS_HX) * RHS_HX;
+      int jj = j0 - 1 + hy, ii = i0 - 1 + hx;
+      while (jj < 0) jj += ny;
+      while (jj >= ny) jj -= ny;
+      while (ii < 0) ii += nx;
+      while (ii >= nx) ii -= nx;
+      off[q] = (size_t)jj * nx + ii;
+      hyx[q][0] = hy; hyx[q][1] = hx;
+    }
+  }
+  // AB2 history of this thread's points, loaded with the staging so that
+  // their latency overlaps it
+  T pf_ru[RHS_KB], pf_rv[RHS_KB], pf_rw[RHS_KB];
+#pragma unroll
+  for (int q = 0; q < RHS_KB; ++q) {
+    const int k = kb + q;
+    const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+    const bool cell = active && k < nz, face = active && k >= 1 && k <= nz - 1;
+    const bool hist = UPD == UPD_AB2 && have_hist;
+    pf_ru[q] = (cell && hist) ? ru[o] : T(0);
+    pf_rv[q] = (cell && hist) ? rv[o] : T(0);
+    pf_rw[q] = (face && hist) ? rw[o] : T(0);
+  }
+  // stage planes p = kb-1 .. kb+RHS_KB into slots 0 .. RHS_NS-1 (stored
+  // values; u / v z ghosts: sign * q[pc])
+#pragma unroll
+  for (int sl = 0; sl < RHS_NS; ++sl) {
+    const int p = kb - 1 + sl;
+    const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
+    const T sgn = p < 0 ? T(-1) : (p >= nz ? top : T(1));
+    const bool wok = (p >= 0) && (p <= nz);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if (q == 1 && !has1) break;
+      const size_t oc = (size_t)pc * plane + off[q];
+      const T uu = sgn * ldg(u + oc);
+      const T vv = sgn * ldg(v + oc);
+      const T ww = wok ? ldg(w + (size_t)p * plane + off[q]) : T(0);
+      su[sl][hyx[q][0]][hyx[q][1]] = uu;
+      sv[sl][hyx[q][0]][hyx[q][1]] = vv;
+      sw[sl][hyx[q][0]][hyx[q][1]] = ww;
+    }
+  }
+  __syncthreads();
+  rhs_stencils<T, FULL, UPD, RHS_KB, RHS_HY, RHS_HX>(g, su, sv, sw, tx + 1, ty + 1, i, j, active, kb, us, vs, ws, ru,
+                                                     rv, rw, pf_ru, pf_rv, pf_rw, forcing, dt, have_hist);
 }
 
 // FP32 storage: the compiler's own register choice (48 in the IMEX form, 5
