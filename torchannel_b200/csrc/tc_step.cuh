@@ -42,14 +42,16 @@ enum : int {
 // (:1037-1225) and _v2 (:818-1034), AB2 combine solver.py:626-651.
 // FULL=false: IMEX (x/y diffusion only); FULL=true: full Laplacian (AB2/FE).
 //
-// A block owns a RHS_TX x RHS_TY (rhs_ty<T>()) tile and RHS_KB (rhs_kb<T>()) consecutive
-// planes k = kb..kb+RHS_KB-1 (u, v at cell k, w at face k).  It first stages the u,
-// v, w planes kb-1 .. kb+RHS_KB with a one-cell periodic halo (z ghosts
-// applied) in shared memory -- every load of the block is independent and
-// issued up front; halo offsets are computed once per thread -- then marches
-// the stencils up its column from shared memory (rhs_march).  Edge planes: internal i = nx-1 is reference u[nx] and j = ny-1 is
-// v[:, ny]; both reference paths omit advection there, the separate-op path
-// keeps the diffusion, the fused path writes 0 (operators.py:1122,1173).
+// A block owns a RHS_TX x RHS_TY (rhs_ty<T>()) tile and RHS_KB (rhs_kb<T>())
+// consecutive planes k = kb..kb+RHS_KB-1 (u, v at cell k, w at face k).  It
+// first stages the u, v, w planes kb-1 .. kb+RHS_KB with a one-cell periodic
+// halo (z ghosts applied) in shared memory -- every load of the block is
+// independent and issued up front; halo offsets are computed once per thread
+// -- then evaluates the stencils up its columns from shared memory
+// (rhs_stencils).  Edge planes: internal i = nx-1 is reference u[nx] and
+// j = ny-1 is v[:, ny]; both reference paths omit advection there, the
+// separate-op path keeps the diffusion, the fused path writes 0
+// (operators.py:1122,1173).
 // ---------------------------------------------------------------------------
 #define RHS_TX 32
 // tile rows and planes per block: 8 x 4 in FP32, 8 x 3 in FP64 (static
