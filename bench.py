@@ -70,7 +70,10 @@ def parse():
     ap.add_argument("--no-tma-rhs", action="store_true",
                     help="stage the explicit-RHS tiles with per-thread loads instead of tensor copies")
     ap.add_argument("--tma-rhs-mode", type=int, default=0,
-                    help="tile shape of the tensor-copy RHS (1..4, tc_use_tma_rhs; 0: the default shape)")
+                    help="tile shape of the tensor-copy RHS (1..6, tc_use_tma_rhs; 0: the default shape)")
+    ap.add_argument("--poisson-middle", type=int, default=None, choices=[0, 1, 2],
+                    help="form of the Poisson middle (tc_use_fused_poisson: 0 three kernels, 1 cluster kernel, "
+                         "2 two streaming passes; default: the library's choice)")
     ap.add_argument("--no-fp32-poisson", action="store_true",
                     help="skip the mixed step with the single-precision Poisson solve")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -183,6 +186,8 @@ def run_b200(a):
         ch.use_tma_rhs(False)
     elif a.tma_rhs_mode:
         ch.use_tma_rhs(a.tma_rhs_mode)
+    if a.poisson_middle is not None:
+        ch.use_fused_poisson(a.poisson_middle)
     ch.set_state(u0, v0, w0)
     ub = ch.bulk_velocity()
     ch.set_state(u0 * (1.0 / ub), v0, w0)

@@ -109,13 +109,15 @@ int tc_step(tc_ctx* ctx, int scheme, double dt, int n_steps, void* stream);
  * reference captures only its Poisson solve, solver.py:389-414). */
 int tc_use_graphs(tc_ctx* ctx, int on);
 
-/* Poisson path: on, the y transform, the z tridiagonal solve and the
- * inverse y transform of projection_fft.py:117-139 run as one kernel per kx
- * slab on a thread-block cluster; off (the default), as three kernels with
- * register-resident transforms, which measure faster on B200.  Same
- * arithmetic up to rounding of the chunked sweeps.  TC_ERR_SIZE when `on` is
- * asked for a grid whose cluster shape does not fit.  No reference
- * counterpart. */
+/* Form of the Poisson middle, the y transform, the z tridiagonal solve and
+ * the inverse y transform of projection_fft.py:117-139.  on = 0 (the
+ * default): three kernels with register-resident transforms; 1: one kernel
+ * per kx slab on a thread-block cluster (same arithmetic up to rounding of
+ * the chunked sweeps); 2: two streaming passes over each kx slab, the y
+ * transform with the forward elimination and the back substitution with the
+ * inverse y transform (bitwise the same results as 0; register y lengths of
+ * at most 256 points).  TC_ERR_SIZE when a form is asked for a grid it does
+ * not support, TC_ERR_ARG for another value.  No reference counterpart. */
 int tc_use_fused_poisson(tc_ctx* ctx, int on);
 
 /* Staging of the explicit-RHS kernel: mode 1 .. 4 (1 is the default where

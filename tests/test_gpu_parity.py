@@ -71,17 +71,23 @@ def test_implicit_diffusion(torch_cuda, nx, ny, nz, top):
         assert rel(dof(name, np_(g), nx, ny, nz), dof(name, r, nx, ny, nz)) < TOL, name
 
 
+REG_Y = (64, 96, 128, 144, 192, 256)   # y lengths of the streamed y / z passes
+
+
 def _fused(ch, fused, nz):
-    """Select the Poisson path; the fused cluster kernel must be available for
+    """Select the Poisson middle (0 three kernels, 1 fused cluster kernel, 2
+    streamed y / z passes); the fused cluster kernel must be available for
     portable cluster sizes (nz <= 128: at most 8 CTAs of 16 planes) and y
     rows of at most 384 points (it holds whole rows of its planes in shared
-    memory)."""
+    memory), the streamed passes for register y lengths up to 256."""
     try:
         ch.use_fused_poisson(fused)
     except Exception:
-        if nz <= 128 and ch.ny <= 384:
+        if fused == 1 and nz <= 128 and ch.ny <= 384:
             raise
-        pytest.skip("fused y/z kernel not schedulable for this shape")
+        if fused == 2 and ch.ny in REG_Y:
+            raise
+        pytest.skip("Poisson middle not available for this shape")
 
 
 # (32,24,128): 8 CTAs of 16 planes; (16,12,100): 8 CTAs, ragged last chunk;
@@ -92,7 +98,7 @@ POISSON_SIZES = SIZES + [(64, 64, 48), (96, 48, 32), (32, 24, 128), (16, 12, 100
 
 
 @pytest.mark.parametrize("nx,ny,nz", POISSON_SIZES)
-@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("fused", [0, 1, 2])
 def test_poisson(torch_cuda, nx, ny, nz, fused):
     oc = make_oracle(nx, ny, nz)
     rng = np.random.default_rng(1)
@@ -319,7 +325,7 @@ def test_graph_replay_is_bitwise_identical(torch_cuda, precision):
 
 
 @pytest.mark.parametrize("nx,ny,nz", [(192, 192, 128), (384, 384, 256)])
-@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("fused", [0, 1, 2])
 def test_poisson_full_size_residual(torch_cuda, nx, ny, nz, fused):
     """Full-size Poisson microbench grids: the discrete residual of the
     returned p (size-independent property; FP64 roundoff scale)."""
@@ -356,6 +362,27 @@ def test_fused_poisson_steps_match_three_kernel_path(torch_cuda, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nx,ny,nz,top", [(48, 64, 48, "dirichlet"), (32, 96, 13, "neumann"), (64, 128, 40, "dirichlet"),
+                                          (16, 144, 17, "neumann"), (192, 192, 128, "dirichlet"),
+                                          (32, 256, 33, "neumann")])
+def test_streamed_poisson_passes_are_bitwise_identical(torch_cuda, precision, nx, ny, nz, top):
+    """IMEX steps with the Poisson middle as two streaming passes (y transform
+    + forward elimination, back substitution + inverse y transform; whole
+    and partial groups of levels, the gauged (0,0) mode) and with the three
+    kernels: the same arithmetic, identical states and scalars."""
+    oc = make_oracle(nx, ny, nz, seed=33, top=top)
+    a, b = make_gpu(oc, precision), make_gpu(oc, precision)
+    a.use_fused_poisson(2)
+    b.use_fused_poisson(0)
+    for ch in (a, b):
+        ch.set_state(oc.u, oc.v, oc.w)
+        ch.step("IMEX", 0.003, 6)
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(np_(x), np_(y))
+    assert np.array_equal(np_(a.scalars)[:2], np_(b.scalars)[:2])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("scheme", ["IMEX", "AB2", "FE"])
 @pytest.mark.parametrize("nx,ny,nz,top", [(64, 64, 48, "dirichlet"), (144, 36, 13, "neumann"), (96, 16, 4, "dirichlet"),
                                           (192, 24, 9, "neumann")])
@@ -371,7 +398,7 @@ def test_tma_rhs_is_bitwise_identical(torch_cuda, precision, scheme, nx, ny, nz,
     b.set_state(oc.u, oc.v, oc.w)
     b.step(scheme, dt, 7)
     ref = [np_(x) for x in b.get_state()[:3]]
-    for mode in range(1, 5):
+    for mode in range(1, 7):
         a = make_gpu(oc, precision)
         a.use_tma_rhs(mode)
         a.set_state(oc.u, oc.v, oc.w)

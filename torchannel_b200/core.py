@@ -148,9 +148,12 @@ class Channel:
         L.check(self.lib.tc_set_cn_chunk(self.ctx, int(rows)))
 
     def use_fused_poisson(self, on=True):
-        """One cluster kernel for the y transforms and the z solve (on) or three
-        kernels (off); raises when the grid's cluster shape does not fit."""
-        L.check(self.lib.tc_use_fused_poisson(self.ctx, int(bool(on))))
+        """Form of the Poisson middle (y transforms and z solve): False / 0 three
+        kernels, True / 1 one cluster kernel, 2 two streaming passes (the
+        y transform fused with the forward elimination, the back substitution
+        with the inverse y transform; the default where the grid allows it).
+        Raises when the grid does not allow the form asked for."""
+        L.check(self.lib.tc_use_fused_poisson(self.ctx, int(on)))
 
     def use_tma_rhs(self, on=True):
         """Explicit-RHS tiles staged by tensor copies (True or a tile-shape

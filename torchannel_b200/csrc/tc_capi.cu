@@ -90,6 +90,9 @@ struct tc_ctx {
   // FFT batch rows, threads, shared memory; yz_ok = launchable here
   int yz_CS, yz_P, yz_FB, yz_thr, yz_ok, yz_on;
   int yzr_thr, yzr_ok;  // register-FFT form of the fused kernel (k_yz_solve_reg)
+  // the Poisson middle as two streaming passes (k_ffty_fwd, k_bwd_iffty):
+  // ys_ok = available for this grid, ys_on = used
+  int ys_ok, ys_on;
   size_t yzr_smem;
   int nsm, yreg_blocks;  // SM count; resident-block cap of the y register FFT
   int tri16_blocks;      // resident blocks of k_tri_lu2<16> on the device
@@ -269,6 +272,7 @@ static void fill_basic(tc_ctx* c, const tc_grid_desc* g) {
   if (c->yz_thr < 256) c->yz_thr = 256;
   c->yz_smem = yz_bytes(FB);
   c->yz_ok = 0; c->yz_on = 0;
+  c->ys_ok = 0; c->ys_on = 0;
 }
 
 extern "C" const char* tc_version(void) { return "torchannel_b200 0.1 (sm_100a)"; }
@@ -316,6 +320,10 @@ template <int N1> static size_t ffty_reg_smem() {
 static bool xreg_ok(const tc_ctx* c) { return rowfft_supported(c->nx) && c->ny % XROWS == 0; }
 static bool yreg_ok(const tc_ctx* c) { return rowfft_supported(c->ny); }
 
+// The streamed y / z passes (k_ffty_fwd, k_bwd_iffty): register y transforms
+// of at most 256 points (one sweep column per thread).
+static bool ys_supported(const tc_ctx* c) { return yreg_ok(c) && c->ny <= 256; }
+
 // Shared-memory opt-in and the resident-block count of the y kernel.
 template <class T> static int reg_fft_setup(tc_ctx* c) {
   int rc = TC_OK;
@@ -351,7 +359,34 @@ template <class T> static int reg_fft_setup(tc_ctx* c) {
       rc = fail(TC_ERR_CUDA, "z solve occupancy");
     c->tri16_blocks = nb * c->nsm;
   }
+  c->ys_ok = 0;
+  if (ys_supported(c)) {
+    for_each_n1(c->ny, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      if constexpr (YzPass<N1>::CPT == 1) {
+        const int sm = (int)YzPass<N1>::smem();
+        if (cudaFuncSetAttribute(k_ffty_fwd<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
+            cudaFuncSetAttribute(k_bwd_iffty<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
+          rc = fail(TC_ERR_CUDA, "streamed y / z pass attributes");
+        else
+          c->ys_ok = 1;
+      }
+    });
+  }
   return rc;
+}
+
+
+template <bool BWD> static void ys_pass(const tc_ctx* c, cpx<double>* X, cudaStream_t s) {
+  for_each_n1(c->ny, [&](auto I) {
+    constexpr int N1 = decltype(I)::value;
+    if constexpr (YzPass<N1>::CPT == 1) {
+      if (BWD)
+        k_bwd_iffty<N1><<<c->nxh, YzPass<N1>::NT, YzPass<N1>::smem(), s>>>(X, c->tri_cp, c->twy_d, c->nz);
+      else
+        k_ffty_fwd<N1><<<c->nxh, YzPass<N1>::NT, YzPass<N1>::smem(), s>>>(X, c->tri_rden, c->cl, c->twy_d, c->nz);
+    }
+  });
 }
 
 template <bool INV> static void ffty_reg(const tc_ctx* c, cpx<double>* X, int nrows, cudaStream_t s) {
@@ -543,10 +578,12 @@ template <class T, int KB, int NST, int MINB> struct RhsV {
 // Shapes (planes per tile, stages, resident CTAs per SM) by mode, FP32 /
 // FP64 storage: 1: 8, 1, 3 / 2, 1, 5 (the default); 2: 4, 1, 4 / 2, 1, 4;
 // 3: 8, 1, 4 / 4, 1, 3; 4: 16, 1, 2 / 4, 2, 2 (the persistent two-stage
-// pipeline).  Measured at 192 x 192 x 128 (us of the kernel, FP32 column
-// march / FP64 per-plane stencils): mode 1 64.7 / 111.3, mode 2 66.7, mode 3
-// 70.0 (64 registers, spills), mode 4 67.9 / 121.5; per-thread staging
-// (k_rhs_update) 91.5 / 117.7.
+// pipeline); 5: 8, 2, 2 and 6: 4, 2, 4 (FP32 only; two-stage pipelines).
+// Measured at 192 x 192 x 128 (us of the kernel, FP32 column march / FP64
+// per-plane stencils): mode 1 63.5 / 111.3 (64.7 before the march's per-tile
+// constants were staged in shared memory), mode 2 66.8, mode 3 70.0 (64
+// registers, spills), mode 4 67.9 / 121.5, mode 5 70.5 (108 registers),
+// mode 6 71.4; per-thread staging (k_rhs_update) 91.5 / 117.7.
 template <class T, class F> static void rhs_variant(int mode, F&& f) {
   if constexpr (sizeof(T) == 8) {
     switch (mode) {
@@ -560,6 +597,8 @@ template <class T, class F> static void rhs_variant(int mode, F&& f) {
       case 2: f(RhsV<float, 4, 1, 4>{}); break;
       case 3: f(RhsV<float, 8, 1, 4>{}); break;
       case 4: f(RhsV<float, 16, 1, 2>{}); break;
+      case 5: f(RhsV<float, 8, 2, 2>{}); break;
+      case 6: f(RhsV<float, 4, 2, 4>{}); break;
       default: f(RhsV<float, 8, 1, 3>{}); break;
     }
   }
@@ -739,6 +778,7 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
   c->yz_ok = yz_probe(c);
   c->yzr_ok = c->yz_ok ? yzr_probe(c) : 0;
   c->yz_on = 0;  // the three-kernel path with register FFTs is faster
+  c->ys_on = 0;  // so far also than the two streaming passes
   if (c->yz_ok) {
     PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
     const int nmodes = c->nxh * c->ny;
@@ -859,6 +899,20 @@ template <class T> static int poisson_impl(tc_ctx* c, const T* u, const T* v, co
                                  (const cpx<double>*)c->twy_d, ny, nz, c->yz_P, c->yz_FB));
     mark(c, TC_PH_TRI, s);
     mark(c, TC_PH_IFFTY, s);
+    mark(c, TC_PH_IFFTX, s);
+    if (xreg)
+      ifftx_reg(c, X, p, s);
+    else
+      k_ifftx<<<dim3(ny / c->JT, nz), 256, smx, s>>>(X, p, nx, ny, nz, c->planx, c->twx_d, c->JT);
+    TC_LAUNCHED();
+    return TC_OK;
+  }
+  if (c->ys_on && c->tri_rden) {
+    // two streaming passes: the tri phase is the forward pass's sweep
+    ys_pass<false>(c, X, s);
+    mark(c, TC_PH_TRI, s);
+    mark(c, TC_PH_IFFTY, s);
+    ys_pass<true>(c, X, s);
     mark(c, TC_PH_IFFTX, s);
     if (xreg)
       ifftx_reg(c, X, p, s);
@@ -1326,9 +1380,13 @@ extern "C" int tc_use_graphs(tc_ctx* c, int on) {
 
 extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
-  if (on && !c->yz_ok) return fail(TC_ERR_SIZE, "fused y/z Poisson kernel not launchable for this grid");
-  if ((on ? 1 : 0) != c->yz_on) {
-    c->yz_on = on ? 1 : 0;
+  if (on < 0 || on > 2) return fail(TC_ERR_ARG, "mode 0 .. 2");
+  if (on == 1 && !c->yz_ok) return fail(TC_ERR_SIZE, "fused y/z Poisson kernel not launchable for this grid");
+  if (on == 2 && !c->ys_ok) return fail(TC_ERR_SIZE, "streamed y/z Poisson passes not available for this grid");
+  const int yz = on == 1, ys = on == 2;
+  if (yz != c->yz_on || ys != c->ys_on) {
+    c->yz_on = yz;
+    c->ys_on = ys;
     if (c->g_valid) {  // the captured steps hold the other path
       cudaGraphExecDestroy(c->gexec);
       c->g_valid = 0;
@@ -1339,7 +1397,7 @@ extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
 
 extern "C" int tc_use_tma_rhs(tc_ctx* c, int on) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
-  if (on < 0 || on > 4) return fail(TC_ERR_ARG, "mode 0 .. 4");
+  if (on < 0 || on > 6) return fail(TC_ERR_ARG, "mode 0 .. 6");
   if (on && on != c->rhs_tma_mode) {
     const int rc = (c->tsz == 8) ? rhs_tma_setup<double>(c, on) : rhs_tma_setup<float>(c, on);
     if (rc) return rc;

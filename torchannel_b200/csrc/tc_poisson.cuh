@@ -852,6 +852,185 @@ __global__ void __launch_bounds__(64) k_tri_lu2(double* __restrict__ Xd, const d
   tri_lu2_thread<LEAN_B>(Xd, rden_t, cp_t, tb, nxh, ny, nz, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// The Poisson middle in two streaming passes over the spectrum instead of
+// three (register row transforms, tabulated LU factors):
+//   k_ffty_fwd:  FFT along y of the rows X[kx][k][:] of one kx slab, then the
+//                forward elimination d'_k = (d_k - a_k d'_{k-1}) rden_k of its
+//                modes' z systems, d' written over X;
+//   k_bwd_iffty: back substitution x_k = d'_k - c'_k x_{k+1} from the top
+//                level down (x_{nz-1} = d'_{nz-1}; the gauged (0,0) mode has
+//                d'_{nz-1} = 0 stored), then the inverse FFT along y.
+// One CTA per kx slab walks it in groups of R = 8 RowFft::RPW rows: the 8
+// warps transform R rows through shared-memory slots (a slot is a row's
+// transpose tile, then the row in natural order), and thread t sweeps the
+// columns ky = t, t + 256, .. of the group's levels (real and imaginary part
+// together: the factors are real).  The next group's rows and factors are in
+// flight while this group is transformed and swept.  Same arithmetic as
+// k_ffty_reg + k_tri_lu2 + k_ffty_reg<inv>, so the results are bitwise the
+// same; the spectrum crosses HBM twice less.
+template <int N1> struct YzPass {
+  using RF = RowFft<N1>;
+  static constexpr int N = RF::N;
+  static constexpr int NT = 256;                              // threads
+  static constexpr int R = (NT / 32) * RF::RPW;               // rows per group
+  static constexpr int SP = RF::TILE;                         // slot pitch (complex), >= N
+  static constexpr int CPT = (N + NT - 1) / NT;               // sweep columns per thread
+  static __host__ __device__ constexpr size_t smem() { return (size_t)R * SP * sizeof(cpx<double>); }
+};
+
+template <int N1>
+__global__ void __launch_bounds__(256, 1) k_ffty_fwd(cpx<double>* __restrict__ X, const double* __restrict__ rden_t,
+                                                     const double* __restrict__ cl,
+                                                     const cpx<double>* __restrict__ twy, int nz) {
+  using P = YzPass<N1>;
+  using RF = typename P::RF;
+  constexpr int N = P::N, R = P::R, SP = P::SP, CPT = P::CPT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cpx<double>* slots = reinterpret_cast<cpx<double>*>(smraw);
+  const int kx = blockIdx.x, tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
+  const int wr = warp * RF::RPW + sub;                        // the lane's row of a group
+  const bool rl = sub < RF::RPW;
+  cpx<double>* slab = X + (size_t)kx * nz * N;
+  const double* rd = rden_t + (size_t)kx * nz * N;
+  cpx<double>* tile = slots + (size_t)(rl ? wr : 0) * SP;
+  cpx<double> v[RF::N1];
+  auto ldrow = [&](int k0, cpx<double> (&o)[RF::N1]) {
+    const int k = k0 + wr;
+    if (rl && l < RF::N2 && k < nz) {
+      const cpx<double>* x = slab + (size_t)k * N;
+#pragma unroll
+      for (int n1 = 0; n1 < RF::N1; ++n1) o[n1] = x[RF::N2 * n1 + l];
+    }
+  };
+  double dr[CPT], di[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) { dr[c] = 0.0; di[c] = 0.0; }
+  const bool gauge_thread = kx == 0 && tid == 0;  // column ky = 0 of slab 0: the (0,0) mode
+  ldrow(0, v);
+  for (int k0 = 0; k0 < nz; k0 += R) {
+    // this group's factors (used after the transform)
+    double f[CPT][R];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int ky = tid + c * P::NT;
+#pragma unroll
+      for (int b = 0; b < R; ++b) f[c][b] = (ky < N && k0 + b < nz) ? ldg(rd + (size_t)(k0 + b) * N + ky) : 0.0;
+    }
+    cpx<double> vn[RF::N1];
+    ldrow(k0 + R, vn);
+    const bool rowok = rl && k0 + wr < nz;
+    if (rowok && l < RF::N2) rowfft_pass1_regs<N1, false>(v, l, tile, twy);
+    __syncwarp();
+    cpx<double> bq[RF::N2];
+    if (rowok && l < RF::N1) {
+#pragma unroll
+      for (int n2 = 0; n2 < RF::N2; ++n2) bq[n2] = tile[l * RF::TP + n2];
+    }
+    __syncwarp();
+    if (rowok && l < RF::N1) {
+      Dft<RF::N2, false>::run(bq);
+#pragma unroll
+      for (int k2 = 0; k2 < RF::N2; ++k2) tile[l + RF::N1 * k2] = bq[k2];  // the row in natural order
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int ky = tid + c * P::NT;
+      if (ky < N) {
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+          const int k = k0 + b;
+          if (k < nz) {
+            const double a = (k == 0) ? 0.0 : ldg(cl + k);
+            const cpx<double> d = slots[b * SP + ky];
+            dr[c] = fma(-(a * f[c][b]), dr[c], d.x * f[c][b]);
+            di[c] = fma(-(a * f[c][b]), di[c], d.y * f[c][b]);
+            const bool g0 = gauge_thread && c == 0 && k == nz - 1;
+            slab[(size_t)k * N + ky] = g0 ? cmake<double>(0.0, 0.0) : cmake<double>(dr[c], di[c]);
+          }
+        }
+      }
+    }
+    __syncthreads();  // the slots are free for the next group
+#pragma unroll
+    for (int n1 = 0; n1 < RF::N1; ++n1) v[n1] = vn[n1];
+  }
+}
+
+template <int N1>
+__global__ void __launch_bounds__(256, 1) k_bwd_iffty(cpx<double>* __restrict__ X, const double* __restrict__ cp_t,
+                                                      const cpx<double>* __restrict__ twy, int nz) {
+  using P = YzPass<N1>;
+  using RF = typename P::RF;
+  constexpr int N = P::N, R = P::R, SP = P::SP, CPT = P::CPT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cpx<double>* slots = reinterpret_cast<cpx<double>*>(smraw);
+  const int kx = blockIdx.x, tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;
+  const int wr = warp * RF::RPW + sub;
+  const bool rl = sub < RF::RPW;
+  cpx<double>* slab = X + (size_t)kx * nz * N;
+  const double* cpt = cp_t + (size_t)kx * nz * N;
+  cpx<double>* tile = slots + (size_t)(rl ? wr : 0) * SP;
+  // a group is the levels k1, k1-1, .. k1-R+1 (slot b holds level k1 - b)
+  cpx<double> d[CPT][R];
+  double f[CPT][R];
+  auto ldgrp = [&](int k1, cpx<double> (&dd)[CPT][R], double (&ff)[CPT][R]) {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int ky = tid + c * P::NT;
+#pragma unroll
+      for (int b = 0; b < R; ++b) {
+        const int k = k1 - b;
+        const bool ok = ky < N && k >= 0;
+        dd[c][b] = ok ? slab[(size_t)k * N + ky] : cmake<double>(0.0, 0.0);
+        ff[c][b] = ok ? ldg(cpt + (size_t)k * N + ky) : 0.0;
+      }
+    }
+  };
+  double xr[CPT], xi[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) { xr[c] = 0.0; xi[c] = 0.0; }
+  ldgrp(nz - 1, d, f);
+  for (int k1 = nz - 1; k1 >= 0; k1 -= R) {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int ky = tid + c * P::NT;
+      if (ky < N) {
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+          const int k = k1 - b;
+          if (k >= 0) {
+            // level nz-1 is d' itself: its factor c_{nz-1} rden_{nz-1} is 0,
+            // or not finite for the singular (0,0) mode
+            if (k == nz - 1) { xr[c] = d[c][b].x; xi[c] = d[c][b].y; }
+            else { xr[c] = d[c][b].x - f[c][b] * xr[c]; xi[c] = d[c][b].y - f[c][b] * xi[c]; }
+            slots[b * SP + ky] = cmake<double>(xr[c], xi[c]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (k1 - R >= 0) ldgrp(k1 - R, d, f);  // the next group's d' and factors, in flight during the transform
+    const int k = k1 - wr;
+    const bool rowok = rl && k >= 0;
+    cpx<double> vr[RF::N1];
+    if (rowok && l < RF::N2) {
+#pragma unroll
+      for (int n1 = 0; n1 < RF::N1; ++n1) vr[n1] = tile[RF::N2 * n1 + l];
+    }
+    __syncwarp();
+    if (rowok && l < RF::N2) rowfft_pass1_regs<N1, true>(vr, l, tile, twy);
+    __syncwarp();
+    cpx<double>* x = slab + (size_t)(rowok ? k : 0) * N;
+    if (rowok && l < RF::N1) rowfft_pass2<N1, true>([&](int e, cpx<double> val) { x[e] = val; }, l, tile);
+    __syncthreads();  // the slots are free for the next group's sweep
+  }
+}
+
 // k_yz_solve with the register-resident row transforms (ny = N1 * 16): the
 // CTA's rows sit unpadded in shared memory, each warp transforms RowFft::RPW
 // rows at a time through its own transpose tile (twiddles from the global

@@ -38,7 +38,9 @@ template <class T, int KB, int NST = 2> struct RhsTma {
   static constexpr int STAGE = 3 * BOX;           // u, v, w
   static constexpr unsigned BOX_BYTES = (unsigned)(BOX * sizeof(T));
   static_assert(BOX_BYTES % 128 == 0, "boxes must stay 128-byte aligned in shared memory");
-  static __host__ __device__ constexpr size_t smem() { return NST * (size_t)STAGE * sizeof(T) + 2 * 8; }
+  // stages, two mbarriers, the march's per-tile constants (rhs_pre_value)
+  static constexpr int PRE = rhs_pre_count<T, KB>();
+  static __host__ __device__ constexpr size_t smem() { return NST * (size_t)STAGE * sizeof(T) + 2 * 8 + PRE * sizeof(T); }
 };
 
 #define RHS_TMA_WAIT_LIMIT (1u << 21)
@@ -58,6 +60,7 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
   extern __shared__ __align__(16) unsigned char smraw[];
   T* buf = reinterpret_cast<T*>(smraw);
   uint64_t* bar = reinterpret_cast<uint64_t*>(buf + NST * S::STAGE);
+  T* pre = reinterpret_cast<T*>(bar + 2);
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx, nthr = RHS_TX * S::TY;
@@ -118,6 +121,9 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       hrv[q] = (cell && hist) ? rv[o] : T(0);
       hrw[q] = (face && hist) ? rw[o] : T(0);
     }
+    // the march's per-tile constants (the last tile's were read before the
+    // barrier that ended it)
+    if (sizeof(T) == 4 && tid < S::PRE) pre[tid] = rhs_pre_value<T, KB>(g, kb, tid);
     const bool landed = mbar_wait_bounded(&bar[st], par, RHS_TMA_WAIT_LIMIT);
     if (__syncthreads_or(!landed)) {
       if (tid == 0) {
@@ -185,7 +191,8 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
     rhs_stencils<T, FULL, UPD, KB, BY, BX>(g, reinterpret_cast<const T(*)[BY][BX]>(su),
                                            reinterpret_cast<const T(*)[BY][BX]>(sv),
                                            reinterpret_cast<const T(*)[BY][BX]>(sw), tx + OX, ty + 1, i, j, active,
-                                           kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw, forcing, dt, have_hist);
+                                           kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw, forcing, dt, have_hist,
+                                           sizeof(T) == 4 ? pre : nullptr);
     __syncthreads();  // this stage is free for the copy issued two tiles on
     if (NST == 1 && tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x, 0);
   }

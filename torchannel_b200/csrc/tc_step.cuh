@@ -96,31 +96,45 @@ template <> struct Rn<double> {
 // folded into the difference quotient as 0.25 / delta (exact: powers of two).
 // The fluxes of face kb are formed before the first plane by the same
 // expressions, so the results do not depend on KB or on the tile shape.
+// Per-tile constants of the march (FP32 storage): U0 of slot s with the
+// z-ghost rule's sign (KB + 2 values), then 1/dz_f[k] and 1/dz_c[k] of the
+// tile's planes k = kb .. kb+KB-1 (KB each; 0 beyond the grid).  Entry e of
+// the table, so that a kernel can stage it in shared memory before its tile
+// lands and the march reads it there instead of waiting on global loads.
+template <class T, int KB> __host__ __device__ constexpr int rhs_pre_count() { return 3 * KB + 2; }
+template <class T, int KB>
+__device__ __forceinline__ T rhs_pre_value(const Grid<T>& g, int kb, int e) {
+  const int nz = g.nz;
+  if (e < KB + 2) {
+    const int p = kb - 1 + e;
+    if (sizeof(T) != 4 || !g.ubase_t) return T(0);
+    const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
+    const T sgn = p < 0 ? T(-1) : (p >= nz ? (g.top_neumann ? T(1) : T(-1)) : T(1));
+    return sgn * ldg(g.ubase_t + pc);
+  }
+  const int k = kb + (e < 2 * KB + 2 ? e - (KB + 2) : e - (2 * KB + 2));
+  if (k >= nz) return T(0);
+  return e < 2 * KB + 2 ? ldg(g.idzf + k) : ldg(g.idzc + k);
+}
+
+// pre: the table of rhs_pre_value in shared memory, or nullptr (the march
+// loads the constants itself).
 template <class T, bool FULL, int UPD, int KB, int HY, int HX>
 __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict__ su)[HY][HX],
                                           const T (*__restrict__ sv)[HY][HX], const T (*__restrict__ sw)[HY][HX],
                                           int cx, int cy, int i, int j, bool active, int kb, T* __restrict__ us,
                                           T* __restrict__ vs, T* __restrict__ ws, T* __restrict__ ru,
                                           T* __restrict__ rv, T* __restrict__ rw, T (&hru)[KB], T (&hrv)[KB],
-                                          T (&hrw)[KB], T forcing, T dt, int have_hist) {
+                                          T (&hrw)[KB], T forcing, T dt, int have_hist,
+                                          const T* __restrict__ pre = nullptr) {
   using R = Rn<T>;
   constexpr bool HB = sizeof(T) == 4;  // mixed precision: u stored as u - U0[k]
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
-  const T top = g.top_neumann ? T(1) : T(-1);
   // U0 of slot s (plane kb-1+s) with the z-ghost rule's sign
   T bs[KB + 2];
 #pragma unroll
-  for (int s = 0; s < KB + 2; ++s) {
-    const int p = kb - 1 + s;
-    T b = T(0);
-    if (HB && g.ubase_t) {
-      const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
-      const T sgn = p < 0 ? T(-1) : (p >= nz ? top : T(1));
-      b = sgn * ldg(g.ubase_t + pc);
-    }
-    bs[s] = b;
-  }
+  for (int s = 0; s < KB + 2; ++s) bs[s] = pre ? pre[s] : rhs_pre_value<T, KB>(g, kb, s);
   const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
   const bool edge_u = (i == nx - 1), edge_v = (j == ny - 1);
   // plane kb-1 (slot 0) and plane kb (slot 1)
@@ -175,7 +189,7 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
     const T sww = R::add(cW0, nW0);
     const T Fww1 = R::mul(sww, sww);
     if (active) {
-      const T idzf = g.idzf[k];
+      const T idzf = pre ? pre[KB + 2 + kk] : g.idzf[k];
       const T qzf = T(0.25) * idzf;
       // ---------------- u at cell k ----------------
       {
@@ -233,7 +247,7 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
           const T t = R::sub(R::mul(R::sub(nW0, cW0), g.idzf[k]), R::mul(R::sub(cW0, pW0), g.idzf[k - 1]));
           r = R::fma(R::mul(g.nu, g.idzc[k - 1]), t, r);
         }
-        const T dww = R::mul(R::sub(Fww1, Fww), T(0.25) * g.idzc[k]);
+        const T dww = R::mul(R::sub(Fww1, Fww), T(0.25) * (pre ? pre[2 * KB + 2 + kk] : g.idzc[k]));
         r = R::sub(r, R::fma(R::sub(Fuw_p, Fuw_m), qx, R::fma(R::sub(Fvw_p, Fvw_m), qy, dww)));
         if (UPD == UPD_RHS_ONLY) {
           rw[o] = r;
@@ -374,13 +388,14 @@ template <class T, bool FULL, int UPD, int KB, int HY, int HX>
 __device__ __forceinline__ void rhs_stencils(const Grid<T>& g, const T (*su)[HY][HX], const T (*sv)[HY][HX],
                                              const T (*sw)[HY][HX], int cx, int cy, int i, int j, bool active,
                                              int kb, T* us, T* vs, T* ws, T* ru, T* rv, T* rw, T (&hru)[KB],
-                                             T (&hrv)[KB], T (&hrw)[KB], T forcing, T dt, int have_hist) {
+                                             T (&hrv)[KB], T (&hrw)[KB], T forcing, T dt, int have_hist,
+                                             const T* pre = nullptr) {
   if constexpr (sizeof(T) == 8)
     rhs_planes<FULL, UPD, KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw,
                                       forcing, dt, have_hist);
   else
     rhs_march<T, FULL, UPD, KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv,
-                                        hrw, forcing, dt, have_hist);
+                                        hrw, forcing, dt, have_hist, pre);
 }
 
 // The tile (bx, by, bz) of the block grid above; k_rhs_update runs one tile
