@@ -124,6 +124,54 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
     // the march's per-tile constants (the last tile's were read before the
     // barrier that ended it)
     if (sizeof(T) == 4 && tid < S::PRE) pre[tid] = rhs_pre_value<T, KB>(g, kb, tid);
+    // periodic wraps of the halo ring (tiles at the x / y ends of the domain):
+    // ring positions of a plane are 2 columns of BY rows and 2 rows of
+    // RHS_TX + 2; entry e of the box's ring gives its box index and, when it
+    // lies outside the domain, the wrapped offset in the plane.  The loads
+    // of the thread's first WR entries are in flight with the copy.
+    constexpr int RING = 2 * BY + 2 * (RHS_TX + 2), NRING = RING * BZ, WR = 4;
+    const bool wrap_x = (i0 == 0) || (i0 + RHS_TX >= nx);
+    const bool wrap_y = (j0 == 0) || (j0 + S::TY >= ny);
+    const bool wrap_tile = wrap_x || wrap_y;
+    auto ring_entry = [&](int e, int& sidx, size_t& off) -> bool {
+      const int sl = e / RING, q = e - sl * RING;
+      int hy, hx;  // box row, and box column relative to x = i0 - 1
+      if (q < 2 * BY) {
+        hy = q % BY;
+        hx = (q < BY) ? 0 : min(nx - i0, RHS_TX) + 1;
+      } else {
+        const int r = q - 2 * BY;
+        hx = r % (RHS_TX + 2);
+        hy = (r < RHS_TX + 2) ? 0 : min(ny - j0, S::TY) + 1;
+      }
+      const int xg = i0 - 1 + hx, yg = j0 - 1 + hy;
+      if (xg >= 0 && xg < nx && yg >= 0 && yg < ny) return false;  // inside the domain: the box holds it
+      off = (size_t)(kb - 1 + sl) * plane + (size_t)wrap(yg, ny) * nx + wrap(xg, nx);
+      sidx = (sl * BY + hy) * BX + OX - 1 + hx;
+      return true;
+    };
+    // plane of a ring entry's box index: slot sl = sidx / (BY BX) is plane kb-1+sl
+    auto ring_plane = [&](int sidx) { return kb - 1 + sidx / (BY * BX); };
+    T wu[WR], wv[WR], ww[WR];
+    int wsi[WR];
+#pragma unroll
+    for (int r = 0; r < WR; ++r) {
+      const int e = tid + r * nthr;
+      int sidx = -1;
+      size_t off = 0;
+      wu[r] = wv[r] = ww[r] = T(0);
+      if (wrap_tile && e < NRING && ring_entry(e, sidx, off)) {
+        const int p = ring_plane(sidx);
+        if (p >= 0 && p < nz) {
+          wu[r] = ldg(u + off);
+          wv[r] = ldg(v + off);
+        }
+        if (p >= 0 && p <= nz) ww[r] = ldg(w + off);
+      } else {
+        sidx = -1;
+      }
+      wsi[r] = sidx;
+    }
     const bool landed = mbar_wait_bounded(&bar[st], par, RHS_TMA_WAIT_LIMIT);
     if (__syncthreads_or(!landed)) {
       if (tid == 0) {
@@ -139,33 +187,29 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
     T* sv = su + S::BOX;
     T* sw = sv + S::BOX;
     // (1) periodic wraps of the halo ring (stored values) on the planes that
-    //     exist
-    const bool wrap_x = (i0 == 0) || (i0 + RHS_TX >= nx);
-    const bool wrap_y = (j0 == 0) || (j0 + S::TY >= ny);
-    if (wrap_x || wrap_y) {
-      // ring positions of a plane: 2 columns of BY rows, 2 rows of RHS_TX + 2
-      constexpr int RING = 2 * BY + 2 * (RHS_TX + 2);
-      for (int e = tid; e < RING * BZ; e += nthr) {
-        const int sl = e / RING, q = e - sl * RING;
-        const int p = kb - 1 + sl;
-        int hy, hx;  // box row, and box column relative to x = i0 - 1
-        if (q < 2 * BY) {
-          hy = q % BY;
-          hx = (q < BY) ? 0 : min(nx - i0, RHS_TX) + 1;
-        } else {
-          const int r = q - 2 * BY;
-          hx = r % (RHS_TX + 2);
-          hy = (r < RHS_TX + 2) ? 0 : min(ny - j0, S::TY) + 1;
-        }
-        const int xg = i0 - 1 + hx, yg = j0 - 1 + hy;
-        if (xg >= 0 && xg < nx && yg >= 0 && yg < ny) continue;  // inside the domain: the box holds it
-        const size_t off = (size_t)wrap(yg, ny) * nx + wrap(xg, nx);
-        const int sidx = (sl * BY + hy) * BX + OX - 1 + hx;
+    //     exist: the entries loaded before the copy landed, then the rest
+    if (wrap_tile) {
+#pragma unroll
+      for (int r = 0; r < WR; ++r) {
+        const int sidx = wsi[r];
+        if (sidx < 0) continue;
+        const int p = ring_plane(sidx);
         if (p >= 0 && p < nz) {
-          su[sidx] = ldg(u + (size_t)p * plane + off);
-          sv[sidx] = ldg(v + (size_t)p * plane + off);
+          su[sidx] = wu[r];
+          sv[sidx] = wv[r];
         }
-        if (p >= 0 && p <= nz) sw[sidx] = ldg(w + (size_t)p * plane + off);
+        if (p >= 0 && p <= nz) sw[sidx] = ww[r];
+      }
+      for (int e = tid + WR * nthr; e < NRING; e += nthr) {
+        int sidx;
+        size_t off;
+        if (!ring_entry(e, sidx, off)) continue;
+        const int p = ring_plane(sidx);
+        if (p >= 0 && p < nz) {
+          su[sidx] = ldg(u + off);
+          sv[sidx] = ldg(v + off);
+        }
+        if (p >= 0 && p <= nz) sw[sidx] = ldg(w + off);
       }
       __syncthreads();
     }
