@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--poisson-middle", type=int, default=None, choices=[0, 1, 2],
                     help="form of the Poisson middle (tc_use_fused_poisson: 0 three kernels, 1 cluster kernel, "
                          "2 two streaming passes; default: the library's choice)")
+    ap.add_argument("--bulk-ffty", action="store_true",
+                    help="y transforms staged by bulk copies (tc_use_bulk_ffty) instead of per-lane loads")
     ap.add_argument("--no-fp32-poisson", action="store_true",
                     help="skip the mixed step with the single-precision Poisson solve")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -188,6 +190,8 @@ def run_b200(a):
         ch.use_tma_rhs(a.tma_rhs_mode)
     if a.poisson_middle is not None:
         ch.use_fused_poisson(a.poisson_middle)
+    if a.bulk_ffty:
+        ch.use_bulk_ffty(True)
     ch.set_state(u0, v0, w0)
     ub = ch.bulk_velocity()
     ch.set_state(u0 * (1.0 / ub), v0, w0)

@@ -130,6 +130,13 @@ int tc_use_fused_poisson(tc_ctx* ctx, int on);
  * copies are not available.  No reference counterpart. */
 int tc_use_tma_rhs(tc_ctx* ctx, int on);
 
+/* y transforms of the Poisson solve (projection_fft.py:117-139 along y):
+ * on (register y lengths), the rows of X reach shared memory and return by
+ * bulk copies of the tensor memory accelerator; off (the default, which
+ * measures faster on B200), by per-lane loads and stores.  Same arithmetic, bit-identical results.
+ * TC_ERR_SIZE when asked where not available.  No reference counterpart. */
+int tc_use_bulk_ffty(tc_ctx* ctx, int on);
+
 /* Single-precision Poisson step (TC_MIXED contexts; TC_ERR_ARG otherwise):
  * the pressure solve of every IMEX step (projection_fft.py:101-215) with an
  * FP32 spectrum -- x transform, y transforms and the z tridiagonal solves of
@@ -250,6 +257,14 @@ int tc_timing_read(tc_ctx* ctx, double* ms_host, int* n_steps);
 
 /* Read and clear the device error word (syncs). */
 int tc_error(tc_ctx* ctx, int* code_host);
+
+/* Bounds-checked builds (the library compiled with -DTC_BOUNDS_CHECK,
+ * torchannel_b200.build.build_checked): *flag = 1 when a checked access of a
+ * step kernel fell outside its buffer since the last call (the access was
+ * skipped), with *where = file id * 100000 + source line of the first one;
+ * 0 otherwise.  Both are cleared.  In the normal build *flag = -1 (no checks
+ * compiled in).  Syncs the device.  No reference counterpart. */
+int tc_bounds_error(int* flag, int* where);
 
 /* ---- Adjoint of the IMEX step (FP64 contexts; TC_ERR_ARG otherwise) ------
  * No counterpart in the reference, which has no adjoint.  Reverse-mode

@@ -7,7 +7,10 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_tc_b200.so")
+# TORCHANNEL_B200_LIB selects another build of the library (the
+# bounds-checked _tc_b200_check.so); default: the in-tree _tc_b200.so
+LIB_PATH = os.environ.get("TORCHANNEL_B200_LIB") or os.path.join(HERE, "_tc_b200.so")
+CHECKED_LIB_PATH = os.path.join(HERE, "_tc_b200_check.so")
 
 TC_OK, TC_ERR_ARG, TC_ERR_SIZE, TC_ERR_CUDA, TC_ERR_WORKSPACE, TC_ERR_STATE, TC_ERR_NONFINITE = range(7)
 TC_FP64, TC_MIXED = 0, 1
@@ -46,6 +49,8 @@ SIGNATURES = [
     ("tc_use_fused_poisson", _I, [_V, _I]),
     ("tc_use_fp32_poisson", _I, [_V, _I, _I]),
     ("tc_use_tma_rhs", _I, [_V, _I]),
+    ("tc_use_bulk_ffty", _I, [_V, _I]),
+    ("tc_bounds_error", _I, [ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     ("tc_project_initial", _I, [_V, _V]),
     ("tc_scalars", _I, [_V, ctypes.POINTER(_V)]),
     ("tc_set_forcing", _I, [_V, _D, _V]),

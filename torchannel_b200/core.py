@@ -155,6 +155,11 @@ class Channel:
         Raises when the grid does not allow the form asked for."""
         L.check(self.lib.tc_use_fused_poisson(self.ctx, int(on)))
 
+    def use_bulk_ffty(self, on=True):
+        """y transforms of the Poisson solve staged by bulk copies (on) or by
+        per-lane loads (off, the default); same results."""
+        L.check(self.lib.tc_use_bulk_ffty(self.ctx, int(bool(on))))
+
     def use_tma_rhs(self, on=True):
         """Explicit-RHS tiles staged by tensor copies (True or a tile-shape
         mode 1..4; mode 1 is the default where the grid allows it) or by

@@ -32,6 +32,22 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// Shared -> global bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned) in the thread's current bulk group.  The shared-memory
+// writes it reads must be made visible to the async proxy first
+// (bulk_store_fence by every writing thread, then a barrier).
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Wait until the committed bulk stores have read their shared memory (the
+// source may be overwritten), or have completed (wait_all).
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   unsigned ok;
   asm volatile(

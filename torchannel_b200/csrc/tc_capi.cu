@@ -19,6 +19,7 @@
 #include "tc_stats.cuh"
 #include "tc_step.cuh"
 #include "tc_rhs_tma.cuh"
+#include "tc_ffty_bulk.cuh"
 #include "tc_adjoint.cuh"
 #include "tc_batch.cuh"
 
@@ -95,6 +96,8 @@ struct tc_ctx {
   int ys_ok, ys_on;
   size_t yzr_smem;
   int nsm, yreg_blocks;  // SM count; resident-block cap of the y register FFT
+  // y transforms with bulk-copy staging (k_ffty_bulk): available, used, grid
+  int ybulk_ok, ybulk_on, ybulk_grid;
   int tri16_blocks;      // resident blocks of k_tri_lu2<16> on the device
   int cn_L_force;        // CN chunk length chosen by tc_set_cn_chunk (0: by nz)
   size_t yz_smem;
@@ -273,6 +276,7 @@ static void fill_basic(tc_ctx* c, const tc_grid_desc* g) {
   c->yz_smem = yz_bytes(FB);
   c->yz_ok = 0; c->yz_on = 0;
   c->ys_ok = 0; c->ys_on = 0;
+  c->ybulk_ok = 0; c->ybulk_on = 0; c->ybulk_grid = 1;
 }
 
 extern "C" const char* tc_version(void) { return "torchannel_b200 0.1 (sm_100a)"; }
@@ -353,6 +357,24 @@ template <class T> static int reg_fft_setup(tc_ctx* c) {
     });
   }
   if (c->yreg_blocks < 1) c->yreg_blocks = 1;
+  c->ybulk_ok = 0;
+  if (yreg_ok(c)) {
+    for_each_n1(c->ny, [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      const int sm = (int)YBulk<N1>::smem();
+      int nb = 0;
+      if (cudaFuncSetAttribute(k_ffty_bulk<N1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+              cudaSuccess &&
+          cudaFuncSetAttribute(k_ffty_bulk<N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+              cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ffty_bulk<N1, false>, 128, sm) == cudaSuccess &&
+          nb >= 1) {
+        c->ybulk_ok = 1;
+        c->ybulk_grid = nb * c->nsm;
+      }
+    });
+    cudaGetLastError();
+  }
   {
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tri_lu2<16>, 64, 0) != cudaSuccess)
@@ -392,6 +414,12 @@ template <bool BWD> static void ys_pass(const tc_ctx* c, cpx<double>* X, cudaStr
 template <bool INV> static void ffty_reg(const tc_ctx* c, cpx<double>* X, int nrows, cudaStream_t s) {
   for_each_n1(c->ny, [&](auto I) {
     constexpr int N1 = decltype(I)::value;
+    if (c->ybulk_on) {
+      const int ntiles = (nrows + YBulk<N1>::R - 1) / YBulk<N1>::R;
+      k_ffty_bulk<N1, INV><<<std::min(ntiles, c->ybulk_grid), 128, YBulk<N1>::smem(), s>>>(X, nrows, c->twy_d,
+                                                                                          c->err);
+      return;
+    }
     const int rpb = 4 * RowFft<N1>::RPW;
     int nblk = (nrows + rpb - 1) / rpb;
     if (nblk > c->yreg_blocks) nblk = c->yreg_blocks;
@@ -779,6 +807,7 @@ extern "C" int tc_create(const tc_grid_desc* g, void* workspace, size_t bytes, t
   c->yzr_ok = c->yz_ok ? yzr_probe(c) : 0;
   c->yz_on = 0;  // the three-kernel path with register FFTs is faster
   c->ys_on = 0;  // so far also than the two streaming passes
+  c->ybulk_on = 0;  // measured slower than the per-lane loads with register prefetch
   if (c->yz_ok) {
     PoissonTabs tb{c->k2x, c->k2y, c->cl, c->cr};
     const int nmodes = c->nxh * c->ny;
@@ -1395,6 +1424,19 @@ extern "C" int tc_use_fused_poisson(tc_ctx* c, int on) {
   return TC_OK;
 }
 
+extern "C" int tc_use_bulk_ffty(tc_ctx* c, int on) {
+  if (!c) return fail(TC_ERR_ARG, "null ctx");
+  if (on && !c->ybulk_ok) return fail(TC_ERR_SIZE, "bulk-staged y transforms not available for this grid");
+  if ((on ? 1 : 0) != c->ybulk_on) {
+    c->ybulk_on = on ? 1 : 0;
+    if (c->g_valid) {  // the captured steps hold the other kernel
+      cudaGraphExecDestroy(c->gexec);
+      c->g_valid = 0;
+    }
+  }
+  return TC_OK;
+}
+
 extern "C" int tc_use_tma_rhs(tc_ctx* c, int on) {
   if (!c) return fail(TC_ERR_ARG, "null ctx");
   if (on < 0 || on > 6) return fail(TC_ERR_ARG, "mode 0 .. 6");
@@ -1689,6 +1731,27 @@ extern "C" int tc_error(tc_ctx* c, int* code) {
   TC_CUDA(cudaDeviceSynchronize());
   TC_CUDA(cudaMemcpy(code, c->err, sizeof(int), cudaMemcpyDeviceToHost));
   TC_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+  return TC_OK;
+}
+
+extern "C" int tc_bounds_error(int* flag, int* where) {
+  if (!flag || !where) return fail(TC_ERR_ARG, "null argument");
+#ifdef TC_BOUNDS_CHECK
+  TC_CUDA(cudaDeviceSynchronize());
+  unsigned int w = 0;
+  int at = 0;
+  TC_CUDA(cudaMemcpyFromSymbol(&w, tc::tc_bounds_word, sizeof(w)));
+  TC_CUDA(cudaMemcpyFromSymbol(&at, tc::tc_bounds_where, sizeof(at)));
+  const unsigned int zw = 0;
+  const int za = 0;
+  TC_CUDA(cudaMemcpyToSymbol(tc::tc_bounds_word, &zw, sizeof(zw)));
+  TC_CUDA(cudaMemcpyToSymbol(tc::tc_bounds_where, &za, sizeof(za)));
+  *flag = w ? 1 : 0;
+  *where = at;
+#else
+  *flag = -1;
+  *where = 0;
+#endif
   return TC_OK;
 }
 

@@ -16,6 +16,28 @@
 
 namespace tc {
 
+// ---- bounds-checked builds -----------------------------------------------
+// Built with -DTC_BOUNDS_CHECK, every access of the step kernels written as
+// TC_IN(i, n, w) ? access : fallback first checks that the w elements from
+// index i lie inside the n elements of their buffer; an access out of range
+// is skipped (loads give 0) and sets tc_bounds_word, with the code
+// file id * 100000 + source line of the first such access in tc_bounds_where
+// (tc_bounds_error() reads and clears both).  Without the flag TC_IN is
+// `true` and the accesses compile as written.  File ids: TC_FILE_ID of each
+// source (1 tc_step.cuh, 2 tc_rhs_tma.cuh, 3 tc_poisson.cuh).
+#ifdef TC_BOUNDS_CHECK
+__device__ unsigned int tc_bounds_word;
+__device__ int tc_bounds_where;
+__device__ __noinline__ bool tc_bounds_fail(int where) {
+  if (atomicOr(&tc_bounds_word, 1u) == 0u) atomicExch(&tc_bounds_where, where);
+  return false;
+}
+#define TC_IN(i, n, w) \
+  (((size_t)(i) + (size_t)(w) <= (size_t)(n)) || ::tc::tc_bounds_fail(TC_FILE_ID * 100000 + __LINE__))
+#else
+#define TC_IN(i, n, w) true
+#endif
+
 template <class T> struct cpx { T x, y; };
 
 template <class T> __device__ __forceinline__ cpx<T> cmake(T a, T b) { cpx<T> r; r.x = a; r.y = b; return r; }

@@ -13,6 +13,8 @@
 #include "tc_common.cuh"
 #include "tc_fft.cuh"
 #include "tc_fft_reg.cuh"
+#undef TC_FILE_ID
+#define TC_FILE_ID 3
 
 namespace tc {
 
@@ -120,7 +122,7 @@ __device__ __forceinline__ void ffty_rows(cpx<double>* __restrict__ X, int nrows
   const int sub = lane / RF::LANES, l = lane - sub * RF::LANES;   // row of the warp, lane in the row
   cpx<double>* tile = tiles + (size_t)sub * RF::TILE;
   const int row = row0 + sub;
-  const bool ok = sub < RF::RPW && row < nrows;
+  const bool ok = sub < RF::RPW && row < nrows && TC_IN((size_t)row * RF::N, (size_t)nrows * RF::N, RF::N);
   cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
   if (ok && l < RF::N2) rowfft_pass1<N1, INV>([&](int e) { return x[e]; }, l, tile, twy);
   __syncwarp();
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
   cpx<double> v[RF::N1];
   auto ldrow = [&](int r0, cpx<double> (&o)[RF::N1]) {
     const int row = r0 + sub;
-    if (lane_ld && row < nrows) {
+    if (lane_ld && row < nrows && TC_IN((size_t)row * RF::N, (size_t)nrows * RF::N, RF::N)) {
       const cpx<double>* x = X + (size_t)row * RF::N;
 #pragma unroll
       for (int n1 = 0; n1 < RF::N1; ++n1) o[n1] = x[RF::N2 * n1 + l];
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(128) k_ffty_reg(cpx<double>* __restrict__ X, i
   ldrow(row0, v);
   for (; row0 < nrows; row0 += rstep) {
     const int row = row0 + sub;
-    const bool ok = sub < RF::RPW && row < nrows;
+    const bool ok = sub < RF::RPW && row < nrows && TC_IN((size_t)row * RF::N, (size_t)nrows * RF::N, RF::N);
     cpx<double>* x = X + (size_t)(ok ? row : 0) * RF::N;
     cpx<double> vn[RF::N1];
     ldrow(row0 + rstep, vn);
@@ -200,6 +202,27 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
   const double idx = (double)g.idx, idy = (double)g.idy;
   const double idzf = (u != nullptr) ? (double)g.idzf[k] : 0.0;
   const int ja = j0 + 2 * pr, jb = ja + 1;
+#ifdef TC_BOUNDS_CHECK
+  const size_t ncell = (size_t)N * ny * nz, nface = (size_t)N * ny * (nz + 1);  // field extents
+  auto divv = [&](int j, int i) -> double {
+    double val;
+    const size_t o = pidx(k, j, i, ny, N);
+    if (u != nullptr) {
+      const size_t oxm = pidx(k, j, i == 0 ? N - 1 : i - 1, ny, N), oym = pidx(k, j == 0 ? ny - 1 : j - 1, i, ny, N);
+      const size_t ozp = pidx(k + 1, j, i, ny, N);
+      if (!(TC_IN(o, ncell, 1) && TC_IN(oxm, ncell, 1) && TC_IN(oym, ncell, 1) && TC_IN(ozp, nface, 1))) return 0.0;
+      val = ((double)u[o] - (double)u[oxm]) * idx + ((double)v[o] - (double)v[oym]) * idy +
+            ((double)w[ozp] - (double)w[o]) * idzf;
+    } else {
+      if (!TC_IN(o, ncell, 1)) return 0.0;
+      val = field[o];
+    }
+    if constexpr (sizeof(XT) == 4) return val * scale - (double)lsub[o] * lsub_scale;
+    return val * scale;
+  };
+#else
+  // (the checked form above measured 50% slower here even with its checks
+  // compiled out, so the normal build keeps this form)
   auto divv = [&](int j, int i) -> double {
     double val;
     if (u != nullptr) {
@@ -213,6 +236,7 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
     if constexpr (sizeof(XT) == 4) return val * scale - (double)lsub[pidx(k, j, i, ny, N)] * lsub_scale;
     return val * scale;
   };
+#endif
   if (ok && l < RF::N2)
     rowfft_pass1<N1, false>([&](int i) { return cmake<double>(divv(ja, i), divv(jb, i)); }, l, tile, twx);
   __syncwarp();
@@ -239,7 +263,8 @@ __device__ __forceinline__ void fftx_tile(const Grid<T>& g, const T* __restrict_
       const cpx<double> d = csub(Zm, Zn);
       out = cmake<double>(0.5 * d.y, -0.5 * d.x);
     }
-    X[((size_t)m * nz + k) * ny + j0 + r] = cmake<XT>((XT)out.x, (XT)out.y);
+    const size_t xo = ((size_t)m * nz + k) * ny + j0 + r;
+    if (TC_IN(xo, (size_t)NH * nz * ny, 1)) X[xo] = cmake<XT>((XT)out.x, (XT)out.y);
   }
 }
 
@@ -291,7 +316,8 @@ __device__ __forceinline__ void ifftx_tile(const cpx<XT>* __restrict__ X, PT* __
   const int j0 = bx * XR;
   for (int e = threadIdx.x; e < NH * XR; e += blockDim.x) {
     const int m = e / XR, r = e % XR;
-    const cpx<XT> x = X[((size_t)m * nz + k) * ny + j0 + r];
+    const size_t xo = ((size_t)m * nz + k) * ny + j0 + r;
+    const cpx<XT> x = TC_IN(xo, (size_t)NH * nz * ny, 1) ? X[xo] : cpx<XT>{};
     cpx<double> val = cmake<double>((double)x.x, (double)x.y);
     if (m == 0 || 2 * m == N) val.y = 0.0;  // irfft ignores these imaginary parts
     S[r * SP + m] = val;
@@ -320,9 +346,14 @@ __device__ __forceinline__ void ifftx_tile(const cpx<XT>* __restrict__ X, PT* __
   __syncwarp();
   if (ok && l < RF::N2) rowfft_pass1_regs<N1, true>(vr, l, tile, twx);
   __syncwarp();
-  PT* pa = p + ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
+  const size_t po = ((size_t)k * ny + j0 + 2 * (ok ? pr : 0)) * N;
+  PT* pa = p + po;
+  const size_t pn = (size_t)N * ny * nz;  // extent of p (bounds-checked builds)
+  (void)pn;
   if (ok && l < RF::N1)
-    rowfft_pass2<N1, true>([&](int i, cpx<double> z) { pa[i] = (PT)z.x; pa[N + i] = (PT)z.y; }, l, tile);
+    rowfft_pass2<N1, true>([&](int i, cpx<double> z) {
+      if (TC_IN(po + i, pn, 1) && TC_IN(po + N + i, pn, 1)) { pa[i] = (PT)z.x; pa[N + i] = (PT)z.y; }
+    }, l, tile);
 }
 
 template <int N1, int XR>
@@ -704,7 +735,9 @@ __global__ void __launch_bounds__(512) k_yz_solve(cpx<double>* __restrict__ X, c
 template <int LB>
 __device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const double* __restrict__ rd,
                                              const double* __restrict__ cpt, const double* __restrict__ cl,
-                                             unsigned st, int nz, bool gauge) {
+                                             unsigned st, int nz, bool gauge, size_t lim, size_t tlim) {
+  // lim / tlim: elements of X from col and of a table from rd / cpt (bounds-checked builds)
+  (void)lim; (void)tlim;
   const unsigned st2 = 2u * st;
   double da[LB], fa[LB], db[LB], fb[LB];
   // levels k0 .. k0+LB-1 of d and of a factor table
@@ -712,8 +745,8 @@ __device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const dou
     unsigned o = (unsigned)k0 * st2, q = (unsigned)k0 * st;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      d[b] = col[o];
-      f[b] = ldg(tab + q);
+      d[b] = TC_IN(o, lim, 1) ? col[o] : 0.0;
+      f[b] = TC_IN(q, tlim, 1) ? ldg(tab + q) : 0.0;
       o += st2;
       q += st;
     }
@@ -723,8 +756,8 @@ __device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const dou
     unsigned o = (unsigned)k1 * st2, q = (unsigned)k1 * st;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      d[b] = col[o];
-      f[b] = ldg(tab + q);
+      d[b] = TC_IN(o, lim, 1) ? col[o] : 0.0;
+      f[b] = TC_IN(q, tlim, 1) ? ldg(tab + q) : 0.0;
       o -= st2;
       q -= st;
     }
@@ -735,9 +768,9 @@ __device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const dou
     const double* a = cl + k0;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const double ak = (b == 0 && k0 == 0) ? 0.0 : ldg(a + b);
+      const double ak = (b == 0 && k0 == 0) ? 0.0 : (TC_IN(k0 + b, nz, 1) ? ldg(a + b) : 0.0);
       dp = fma(-(ak * f[b]), dp, d[b] * f[b]);
-      col[o] = dp;
+      if (TC_IN(o, lim, 1)) col[o] = dp;
       o += st2;
     }
   };
@@ -748,7 +781,7 @@ __device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const dou
     if (k0 + 2 * LB < nz) load_up(da, fa, rd, k0 + 2 * LB);
     sweep_up(db, fb, k0 + LB);
   }
-  if (gauge) col[(unsigned)(nz - 1) * st2] = 0.0;
+  if (gauge && TC_IN((unsigned)(nz - 1) * st2, lim, 1)) col[(unsigned)(nz - 1) * st2] = 0.0;
   double x = 0.0;
   auto sweep_dn = [&](const double (&d)[LB], const double (&f)[LB], int k1) {
     unsigned o = (unsigned)k1 * st2;
@@ -757,7 +790,7 @@ __device__ __forceinline__ void tri_lu2_lean(double* __restrict__ col, const dou
       // level nz-1 is d' itself: its table entry c_{nz-1} rden_{nz-1} is 0,
       // or not finite for the singular (0,0) mode
       x = (b == 0 && k1 == nz - 1) ? d[b] : d[b] - f[b] * x;
-      col[o] = x;
+      if (TC_IN(o, lim, 1)) col[o] = x;
       o -= st2;
     }
   };
@@ -783,9 +816,11 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
   double* col = Xd + 2 * base + part;
   const double* rd = rden_t + base;
   const double* cpt = cp_t + base;
+  const size_t tlim = (size_t)nxh * nz * ny - base, lim = 2 * tlim - part;  // extents (bounds-checked builds)
+  (void)tlim; (void)lim;
   if constexpr (LEAN_B > 0) {
     if (nz % (2 * LEAN_B) == 0) {
-      tri_lu2_lean<LEAN_B>(col, rd, cpt, tb.cl, (unsigned)ny, nz, kx == 0 && ky == 0);
+      tri_lu2_lean<LEAN_B>(col, rd, cpt, tb.cl, (unsigned)ny, nz, kx == 0 && ky == 0, lim, tlim);
       return;
     }
   }
@@ -793,14 +828,20 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
   double dc[TRIP_B], dn[TRIP_B], fc[TRIP_B], fn[TRIP_B];
 #pragma unroll
   for (int b = 0; b < TRIP_B; ++b) {
-    if (b < nz) { dc[b] = col[(size_t)b * st2]; fc[b] = ldg(rd + (size_t)b * st); }
+    if (b < nz && TC_IN((size_t)b * st2, lim, 1) && TC_IN((size_t)b * st, tlim, 1)) {
+      dc[b] = col[(size_t)b * st2];
+      fc[b] = ldg(rd + (size_t)b * st);
+    }
   }
   double dp = 0.0;
   for (int k0 = 0; k0 < nz; k0 += TRIP_B) {
 #pragma unroll
     for (int b = 0; b < TRIP_B; ++b) {
       const int kk = k0 + TRIP_B + b;
-      if (kk < nz) { dn[b] = col[(size_t)kk * st2]; fn[b] = ldg(rd + (size_t)kk * st); }
+      if (kk < nz && TC_IN((size_t)kk * st2, lim, 1) && TC_IN((size_t)kk * st, tlim, 1)) {
+        dn[b] = col[(size_t)kk * st2];
+        fn[b] = ldg(rd + (size_t)kk * st);
+      }
     }
 #pragma unroll
     for (int b = 0; b < TRIP_B; ++b) {
@@ -810,7 +851,7 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
         // recurrence: one dependent FMA per level
         const double a = (k == 0) ? 0.0 : tb.cl[k];
         dp = fma(-(a * fc[b]), dp, dc[b] * fc[b]);
-        col[(size_t)k * st2] = dp;
+        if (TC_IN((size_t)k * st2, lim, 1)) col[(size_t)k * st2] = dp;
       }
     }
 #pragma unroll
@@ -818,24 +859,30 @@ __device__ __forceinline__ void tri_lu2_thread(double* __restrict__ Xd, const do
   }
   double x = dp;
   if (kx == 0 && ky == 0) x = 0.0;
-  col[(size_t)(nz - 1) * st2] = x;
+  if (TC_IN((size_t)(nz - 1) * st2, lim, 1)) col[(size_t)(nz - 1) * st2] = x;
 #pragma unroll
   for (int b = 0; b < TRIP_B; ++b) {
     const int k = nz - 2 - b;
-    if (k >= 0) { dc[b] = col[(size_t)k * st2]; fc[b] = ldg(cpt + (size_t)k * st); }
+    if (k >= 0 && TC_IN((size_t)k * st2, lim, 1) && TC_IN((size_t)k * st, tlim, 1)) {
+      dc[b] = col[(size_t)k * st2];
+      fc[b] = ldg(cpt + (size_t)k * st);
+    }
   }
   for (int k1 = nz - 2; k1 >= 0; k1 -= TRIP_B) {
 #pragma unroll
     for (int b = 0; b < TRIP_B; ++b) {
       const int k = k1 - TRIP_B - b;
-      if (k >= 0) { dn[b] = col[(size_t)k * st2]; fn[b] = ldg(cpt + (size_t)k * st); }
+      if (k >= 0 && TC_IN((size_t)k * st2, lim, 1) && TC_IN((size_t)k * st, tlim, 1)) {
+        dn[b] = col[(size_t)k * st2];
+        fn[b] = ldg(cpt + (size_t)k * st);
+      }
     }
 #pragma unroll
     for (int b = 0; b < TRIP_B; ++b) {
       const int k = k1 - b;
       if (k >= 0) {
         x = dc[b] - fc[b] * x;
-        col[(size_t)k * st2] = x;
+        if (TC_IN((size_t)k * st2, lim, 1)) col[(size_t)k * st2] = x;
       }
     }
 #pragma unroll
@@ -898,7 +945,7 @@ __global__ void __launch_bounds__(256, 1) k_ffty_fwd(cpx<double>* __restrict__ X
   cpx<double> v[RF::N1];
   auto ldrow = [&](int k0, cpx<double> (&o)[RF::N1]) {
     const int k = k0 + wr;
-    if (rl && l < RF::N2 && k < nz) {
+    if (rl && l < RF::N2 && k < nz && TC_IN((size_t)k * N, (size_t)nz * N, N)) {
       const cpx<double>* x = slab + (size_t)k * N;
 #pragma unroll
       for (int n1 = 0; n1 < RF::N1; ++n1) o[n1] = x[RF::N2 * n1 + l];
@@ -916,7 +963,10 @@ __global__ void __launch_bounds__(256, 1) k_ffty_fwd(cpx<double>* __restrict__ X
     for (int c = 0; c < CPT; ++c) {
       const int ky = tid + c * P::NT;
 #pragma unroll
-      for (int b = 0; b < R; ++b) f[c][b] = (ky < N && k0 + b < nz) ? ldg(rd + (size_t)(k0 + b) * N + ky) : 0.0;
+      for (int b = 0; b < R; ++b)
+        f[c][b] = (ky < N && k0 + b < nz && TC_IN((size_t)(k0 + b) * N + ky, (size_t)nz * N, 1))
+                      ? ldg(rd + (size_t)(k0 + b) * N + ky)
+                      : 0.0;
     }
     cpx<double> vn[RF::N1];
     ldrow(k0 + R, vn);
@@ -943,12 +993,13 @@ __global__ void __launch_bounds__(256, 1) k_ffty_fwd(cpx<double>* __restrict__ X
         for (int b = 0; b < R; ++b) {
           const int k = k0 + b;
           if (k < nz) {
-            const double a = (k == 0) ? 0.0 : ldg(cl + k);
+            const double a = (k == 0) ? 0.0 : (TC_IN(k, nz, 1) ? ldg(cl + k) : 0.0);
             const cpx<double> d = slots[b * SP + ky];
             dr[c] = fma(-(a * f[c][b]), dr[c], d.x * f[c][b]);
             di[c] = fma(-(a * f[c][b]), di[c], d.y * f[c][b]);
             const bool g0 = gauge_thread && c == 0 && k == nz - 1;
-            slab[(size_t)k * N + ky] = g0 ? cmake<double>(0.0, 0.0) : cmake<double>(dr[c], di[c]);
+            if (TC_IN((size_t)k * N + ky, (size_t)nz * N, 1))
+              slab[(size_t)k * N + ky] = g0 ? cmake<double>(0.0, 0.0) : cmake<double>(dr[c], di[c]);
           }
         }
       }
@@ -985,7 +1036,7 @@ __global__ void __launch_bounds__(256, 1) k_bwd_iffty(cpx<double>* __restrict__ 
 #pragma unroll
       for (int b = 0; b < R; ++b) {
         const int k = k1 - b;
-        const bool ok = ky < N && k >= 0;
+        const bool ok = ky < N && k >= 0 && TC_IN((size_t)k * N + ky, (size_t)nz * N, 1);
         dd[c][b] = ok ? slab[(size_t)k * N + ky] : cmake<double>(0.0, 0.0);
         ff[c][b] = ok ? ldg(cpt + (size_t)k * N + ky) : 0.0;
       }
@@ -1016,7 +1067,7 @@ __global__ void __launch_bounds__(256, 1) k_bwd_iffty(cpx<double>* __restrict__ 
     __syncthreads();
     if (k1 - R >= 0) ldgrp(k1 - R, d, f);  // the next group's d' and factors, in flight during the transform
     const int k = k1 - wr;
-    const bool rowok = rl && k >= 0;
+    const bool rowok = rl && k >= 0 && TC_IN((size_t)k * N, (size_t)nz * N, N);
     cpx<double> vr[RF::N1];
     if (rowok && l < RF::N2) {
 #pragma unroll

@@ -24,6 +24,8 @@
 #pragma once
 #include "tc_async.cuh"
 #include "tc_step.cuh"
+#undef TC_FILE_ID
+#define TC_FILE_ID 2
 
 namespace tc {
 
@@ -63,6 +65,8 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
   T* pre = reinterpret_cast<T*>(bar + 2);
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
+  const size_t ncell = plane * nz, nface = plane * (nz + 1);  // field extents (bounds-checked builds)
+  (void)ncell; (void)nface;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RHS_TX + tx, nthr = RHS_TX * S::TY;
   const int ntiles = ntx * nty * ntz;
   const T top = g.top_neumann ? T(1) : T(-1);
@@ -117,9 +121,9 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       const size_t o = (size_t)k * plane + (size_t)j * nx + i;
       const bool cell = active && k < nz, face = active && k >= 1 && k <= nz - 1;
       const bool hist = UPD == UPD_AB2 && have_hist;
-      hru[q] = (cell && hist) ? ru[o] : T(0);
-      hrv[q] = (cell && hist) ? rv[o] : T(0);
-      hrw[q] = (face && hist) ? rw[o] : T(0);
+      hru[q] = (cell && hist && TC_IN(o, ncell, 1)) ? ru[o] : T(0);
+      hrv[q] = (cell && hist && TC_IN(o, ncell, 1)) ? rv[o] : T(0);
+      hrw[q] = (face && hist && TC_IN(o, nface, 1)) ? rw[o] : T(0);
     }
     // the march's per-tile constants (the last tile's were read before the
     // barrier that ended it)
@@ -162,11 +166,11 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
       wu[r] = wv[r] = ww[r] = T(0);
       if (wrap_tile && e < NRING && ring_entry(e, sidx, off)) {
         const int p = ring_plane(sidx);
-        if (p >= 0 && p < nz) {
+        if (p >= 0 && p < nz && TC_IN(off, ncell, 1)) {
           wu[r] = ldg(u + off);
           wv[r] = ldg(v + off);
         }
-        if (p >= 0 && p <= nz) ww[r] = ldg(w + off);
+        if (p >= 0 && p <= nz && TC_IN(off, nface, 1)) ww[r] = ldg(w + off);
       } else {
         sidx = -1;
       }
@@ -205,11 +209,11 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
         size_t off;
         if (!ring_entry(e, sidx, off)) continue;
         const int p = ring_plane(sidx);
-        if (p >= 0 && p < nz) {
+        if (p >= 0 && p < nz && TC_IN(off, ncell, 1)) {
           su[sidx] = ldg(u + off);
           sv[sidx] = ldg(v + off);
         }
-        if (p >= 0 && p <= nz) sw[sidx] = ldg(w + off);
+        if (p >= 0 && p <= nz && TC_IN(off, nface, 1)) sw[sidx] = ldg(w + off);
       }
       __syncthreads();
     }

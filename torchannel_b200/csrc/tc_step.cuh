@@ -3,6 +3,8 @@
 // and diagnostics reductions, and reference-layout conversions.
 #pragma once
 #include "tc_common.cuh"
+#undef TC_FILE_ID
+#define TC_FILE_ID 1
 
 namespace tc {
 
@@ -110,11 +112,11 @@ __device__ __forceinline__ T rhs_pre_value(const Grid<T>& g, int kb, int e) {
     if (sizeof(T) != 4 || !g.ubase_t) return T(0);
     const int pc = p < 0 ? 0 : (p >= nz ? nz - 1 : p);
     const T sgn = p < 0 ? T(-1) : (p >= nz ? (g.top_neumann ? T(1) : T(-1)) : T(1));
-    return sgn * ldg(g.ubase_t + pc);
+    return TC_IN(pc, nz, 1) ? sgn * ldg(g.ubase_t + pc) : T(0);
   }
   const int k = kb + (e < 2 * KB + 2 ? e - (KB + 2) : e - (2 * KB + 2));
   if (k >= nz) return T(0);
-  return e < 2 * KB + 2 ? ldg(g.idzf + k) : ldg(g.idzc + k);
+  return e < 2 * KB + 2 ? (TC_IN(k, nz, 1) ? ldg(g.idzf + k) : T(0)) : (TC_IN(k, nz + 1, 1) ? ldg(g.idzc + k) : T(0));
 }
 
 // pre: the table of rhs_pre_value in shared memory, or nullptr (the march
@@ -131,6 +133,8 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
   constexpr bool HB = sizeof(T) == 4;  // mixed precision: u stored as u - U0[k]
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
+  const size_t ncell = plane * nz, nface = plane * (nz + 1);  // field extents (bounds-checked builds)
+  (void)ncell; (void)nface;
   // U0 of slot s (plane kb-1+s) with the z-ghost rule's sign
   T bs[KB + 2];
 #pragma unroll
@@ -206,14 +210,14 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
         }
         if (!edge_u) r = R::sub(r, R::fma(R::sub(Fuw_p1, Fuw_p), qzf, R::fma(R::sub(Fuv_pp, Fuv_pm), qy, R::mul(Fuu, qx))));
         if (UPD == UPD_RHS_ONLY) {
-          ru[o] = r;
+          if (TC_IN(o, ncell, 1)) ru[o] = r;
         } else if (UPD == UPD_FE) {
-          us[o] = R::add(R::fma(dt, r, cU0), dt);
+          if (TC_IN(o, ncell, 1)) us[o] = R::add(R::fma(dt, r, cU0), dt);
         } else {
           r = R::add(r, forcing);
           const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hru[kk])) : r;
-          us[o] = R::fma(dt, a, cU0);
-          ru[o] = r;
+          if (TC_IN(o, ncell, 1)) us[o] = R::fma(dt, a, cU0);
+          if (TC_IN(o, ncell, 1)) ru[o] = r;
         }
       }
       // ---------------- v at cell k ----------------
@@ -229,13 +233,13 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
         }
         if (!edge_v) r = R::sub(r, R::fma(R::sub(Fvw_p1, Fvw_p), qzf, R::fma(R::sub(Fuv_pp, Fuv_mp), qx, R::mul(Fvv, qy))));
         if (UPD == UPD_RHS_ONLY) {
-          rv[o] = r;
+          if (TC_IN(o, ncell, 1)) rv[o] = r;
         } else if (UPD == UPD_FE) {
-          vs[o] = R::fma(dt, r, cV0);
+          if (TC_IN(o, ncell, 1)) vs[o] = R::fma(dt, r, cV0);
         } else {
           const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hrv[kk])) : r;
-          vs[o] = R::fma(dt, a, cV0);
-          rv[o] = r;
+          if (TC_IN(o, ncell, 1)) vs[o] = R::fma(dt, a, cV0);
+          if (TC_IN(o, ncell, 1)) rv[o] = r;
         }
       }
       // ---------------- w at face k ----------------
@@ -250,13 +254,13 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
         const T dww = R::mul(R::sub(Fww1, Fww), T(0.25) * (pre ? pre[2 * KB + 2 + kk] : g.idzc[k]));
         r = R::sub(r, R::fma(R::sub(Fuw_p, Fuw_m), qx, R::fma(R::sub(Fvw_p, Fvw_m), qy, dww)));
         if (UPD == UPD_RHS_ONLY) {
-          rw[o] = r;
+          if (TC_IN(o, nface, 1)) rw[o] = r;
         } else if (UPD == UPD_FE) {
-          ws[o] = R::fma(dt, r, cW0);
+          if (TC_IN(o, nface, 1)) ws[o] = R::fma(dt, r, cW0);
         } else {
           const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hrw[kk])) : r;
-          ws[o] = R::fma(dt, a, cW0);
-          rw[o] = r;
+          if (TC_IN(o, nface, 1)) ws[o] = R::fma(dt, a, cW0);
+          if (TC_IN(o, nface, 1)) rw[o] = r;
         }
       }
     }
@@ -283,6 +287,8 @@ __device__ __forceinline__ void rhs_planes(const Grid<double>& g, const double (
   using T = double;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
+  const size_t ncell = plane * nz, nface = plane * (nz + 1);  // field extents (bounds-checked builds)
+  (void)ncell; (void)nface;
   const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
 #pragma unroll 1
   for (int kk = 0; kk < KB; ++kk) {
@@ -313,14 +319,14 @@ __device__ __forceinline__ void rhs_planes(const Grid<double>& g, const double (
           r -= duudx + (vu_t - vu_b) * qy + (wu_t - wu_b) * qzf;
         }
         if (UPD == UPD_RHS_ONLY) {
-          ru[o] = r;
+          if (TC_IN(o, ncell, 1)) ru[o] = r;
         } else if (UPD == UPD_FE) {
           T q = U0 + dt * r;
-          us[o] = q + dt * T(1);
+          if (TC_IN(o, ncell, 1)) us[o] = q + dt * T(1);
         } else {
           r += forcing;
-          us[o] = have_hist ? U0 + dt * (T(1.5) * r - T(0.5) * hru[0]) : U0 + dt * r;
-          ru[o] = r;
+          if (TC_IN(o, ncell, 1)) us[o] = have_hist ? U0 + dt * (T(1.5) * r - T(0.5) * hru[0]) : U0 + dt * r;
+          if (TC_IN(o, ncell, 1)) ru[o] = r;
         }
       }
       // ---------------- v at cell k ----------------
@@ -343,12 +349,12 @@ __device__ __forceinline__ void rhs_planes(const Grid<double>& g, const double (
           r -= (uv_r - uv_l) * qx + dvvdy + (wv_t - wv_b) * qzf;
         }
         if (UPD == UPD_RHS_ONLY) {
-          rv[o] = r;
+          if (TC_IN(o, ncell, 1)) rv[o] = r;
         } else if (UPD == UPD_FE) {
-          vs[o] = V0 + dt * r;
+          if (TC_IN(o, ncell, 1)) vs[o] = V0 + dt * r;
         } else {
-          vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * hrv[0]) : V0 + dt * r;
-          rv[o] = r;
+          if (TC_IN(o, ncell, 1)) vs[o] = have_hist ? V0 + dt * (T(1.5) * r - T(0.5) * hrv[0]) : V0 + dt * r;
+          if (TC_IN(o, ncell, 1)) rv[o] = r;
         }
       }
     }
@@ -368,12 +374,12 @@ __device__ __forceinline__ void rhs_planes(const Grid<double>& g, const double (
       const T dwwdz = (sq(W0 + Wzp) - sq(Wzm + W0)) * (T(0.25) * g.idzc[k]);
       r -= (uw_r - uw_l) * qx + (vw_t - vw_b) * qy + dwwdz;
       if (UPD == UPD_RHS_ONLY) {
-        rw[o] = r;
+        if (TC_IN(o, nface, 1)) rw[o] = r;
       } else if (UPD == UPD_FE) {
-        ws[o] = W0 + dt * r;
+        if (TC_IN(o, nface, 1)) ws[o] = W0 + dt * r;
       } else {
-        ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * hrw[0]) : W0 + dt * r;
-        rw[o] = r;
+        if (TC_IN(o, nface, 1)) ws[o] = have_hist ? W0 + dt * (T(1.5) * r - T(0.5) * hrw[0]) : W0 + dt * r;
+        if (TC_IN(o, nface, 1)) rw[o] = r;
       }
     }
 #pragma unroll
@@ -702,6 +708,9 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   const int ncols = nx * ny;
   const bool colok = col < ncols;
   T* q = (comp == 0 ? u : (comp == 1 ? v : w)) + (colok ? col : 0);
+  // extent of the field from q (bounds-checked builds)
+  const size_t qn = (size_t)ncols * (comp < 2 ? nz : nz + 1) - (colok ? col : 0);
+  (void)qn;
   const int n = comp < 2 ? nz : nz - 1;
   const int s0 = chunk * Lr, e0 = min(s0 + Lr, n);          // rows [s0, e0)
   const bool act = s0 < n;
@@ -730,7 +739,11 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
     for (int tt = 0; tt < L + 2; ++tt) {
       const bool ok = tt >= wlo && tt < whi;
       T x[VEC];
-      CnVec<T, VEC>::ld(q + (ok ? ow : 0u), x);
+      if (TC_IN(ok ? ow : 0u, qn, VEC)) CnVec<T, VEC>::ld(q + (ok ? ow : 0u), x);
+      else {
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) x[c] = T(0);
+      }
 #pragma unroll
       for (int c = 0; c < VEC; ++c) wv[tt][c] = ok ? x[c] : T(0);
       ow += ucols;
@@ -739,7 +752,7 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
     for (int tt = 0; tt < L + 2; ++tt) {
       const int pl = s0 - 1 + tt;
-      if (act && colok && pl >= 0 && pl <= plmax && tt < Lr + 2) {
+      if (act && colok && pl >= 0 && pl <= plmax && tt < Lr + 2 && TC_IN((size_t)pl * plane, qn, VEC)) {
         CnVec<T, VEC>::ld(q + (size_t)pl * plane, wv[tt]);
       } else {
 #pragma unroll
@@ -852,7 +865,8 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
 #pragma unroll
         for (int c = 0; c < VEC; ++c) o[c] = F32 ? (y[tt][c] + h * Xin[c]) + bs : (y[tt][c] + h * Xin[c]) - bs;
         const int pl = comp < 2 ? m : m + 1;
-        CnVec<T, VEC>::st(LEAN ? q + os : q + (size_t)pl * plane, o);
+        if (TC_IN(LEAN ? (size_t)os : (size_t)pl * plane, qn, VEC))
+          CnVec<T, VEC>::st(LEAN ? q + os : q + (size_t)pl * plane, o);
       }
       os += ucols;
     }
@@ -966,6 +980,13 @@ __device__ __forceinline__ void project_tile_ps(const Grid<T>& g, T* __restrict_
   const int i = 2 * (bx * 32 + threadIdx.x);
   const int j = by * 8 + threadIdx.y;
   const int k0 = bz * PROJ_PK;  // planes k0 .. k0+PROJ_PK-1
+  const size_t ncell = (size_t)nx * ny * nz, nface = (size_t)nx * ny * (nz + 1);  // extents (bounds-checked builds)
+  (void)ncell; (void)nface;
+  // the accesses of plane k (pairs at o and at the y neighbour, the x neighbour of the pair)
+  auto plane_in = [&](int k, int jp, int ipp) {
+    return TC_IN(pidx(k, j, i, ny, nx), ncell, 2) && TC_IN(pidx(k, jp, i, ny, nx), ncell, 2) &&
+           TC_IN(pidx(k, j, ipp, ny, nx), ncell, 1);
+  };
   double acc = 0.0;
   if (i < nx && j < ny) {
     const int jp = wrap(j + 1, ny), ipp = wrap(i + 2, nx);
@@ -980,6 +1001,10 @@ __device__ __forceinline__ void project_tile_ps(const Grid<T>& g, T* __restrict_
       auto load = [&](int k) {
         Ld l;
         const size_t o = pidx(k, j, i, ny, nx);
+        if (!plane_in(k, jp, ipp)) {
+          l = Ld{};
+          return l;
+        }
         l.P = ps.pair(o);
         l.P2 = ps.one(pidx(k, j, ipp, ny, nx));
         l.Py = ps.pair(pidx(k, jp, i, ny, nx));
@@ -1003,15 +1028,17 @@ __device__ __forceinline__ void project_tile_ps(const Grid<T>& g, T* __restrict_
           uu.y = (T)((double)uu.y - cx * (P2 - P.y));
           vv.x = (T)((double)vv.x - cy * (Py.x - P.x));
           vv.y = (T)((double)vv.y - cy * (Py.y - P.y));
-          *reinterpret_cast<V2*>(u + o) = uu;
-          *reinterpret_cast<V2*>(v + o) = vv;
+          if (TC_IN(o, ncell, 2)) {
+            *reinterpret_cast<V2*>(u + o) = uu;
+            *reinterpret_cast<V2*>(v + o) = vv;
+          }
           acc += ((double)uu.x + (double)uu.y + (g.ubase_d ? 2.0 * g.ubase_d[k] : 0.0)) * dzf[k];
           if (k >= 1) {
             const double cz = dt * (double)g.idzc[k];
             V2 ww = cur.ww;
             ww.x = (T)((double)ww.x - cz * (P.x - Pm.x));
             ww.y = (T)((double)ww.y - cz * (P.y - Pm.y));
-            *reinterpret_cast<V2*>(w + o) = ww;
+            if (TC_IN(o, nface, 2)) *reinterpret_cast<V2*>(w + o) = ww;
           }
           ps.keep(o, P);
           Pm = P;
@@ -1022,7 +1049,7 @@ __device__ __forceinline__ void project_tile_ps(const Grid<T>& g, T* __restrict_
 #pragma unroll
       for (int kk = 0; kk < PROJ_PK; ++kk) {
         const int k = k0 + kk;
-        if (k < nz) {
+        if (k < nz && plane_in(k, jp, ipp)) {
           const size_t o = pidx(k, j, i, ny, nx);
           const double2 P = ps.pair(o);
           const double P2 = ps.one(pidx(k, j, ipp, ny, nx));
