@@ -120,7 +120,7 @@ int tc_use_graphs(tc_ctx* ctx, int on);
  * not support, TC_ERR_ARG for another value.  No reference counterpart. */
 int tc_use_fused_poisson(tc_ctx* ctx, int on);
 
-/* Staging of the explicit-RHS kernel: mode 1 .. 4 (1 is the default where
+/* Staging of the explicit-RHS kernel: mode 1 .. 6 (1 is the default where
  * the grid allows it: x rows a multiple of 16 bytes, nx >= 64, ny >= 16), its
  * u, v, w tiles reach shared memory by 3-D tensor copies of the tensor memory
  * accelerator, in the tile shape the mode names (planes per tile, one stage
@@ -350,17 +350,17 @@ int tc_set_cn_chunk(tc_ctx* ctx, int rows);
  * ensemble calls (the ensemble rebuilds its tables when it notices).
  * The caller owns the member-table memory (device, 16-byte aligned, size
  * from tc_batch_table_bytes); all calls on one stream.
- * tc_batch_set_shape: CN rows per chunk bound (16 or 32: the deepest
- *   member's chunk count fixes the CN block, every member's chunk length
- *   becomes ceil(nz / chunks) and its tables follow) and persistent CTAs per
- *   SM (0 = occupancy limit, -1 = one CTA per work unit), the ensemble
- *   autotuner's knobs.
+ * tc_batch_set_shape: CN rows per chunk (16 or 32: every member's CN
+ *   chunks take that many rows and its tables follow; the deepest member's
+ *   chunk count fixes the CN block, whose warps beyond a shallower member's
+ *   last chunk idle) and persistent CTAs per SM (0 = occupancy limit,
+ *   -1 = one CTA per work unit), the ensemble autotuner's knobs.
  * tc_batch_step: dts = host array of one dt per member; members without AB2
  *   history start with a forward step as tc_step does.  Members may carry no
  *   adjoint hooks (TC_ERR_ARG).
- * tc_batch_info: shape = {cn rows (the shape's bound), ctas per SM (-1: one
- *   CTA per work unit), tables built, CN chunks per column}; every member
- *   then solves CN in chunks of ceil(nz / chunks) rows; units and
+ * tc_batch_info: shape = {cn rows, ctas per SM (-1: one CTA per work
+ *   unit), tables built, CN chunk warps per block (the deepest member's
+ *   chunks)}; units and
  *   grids = work units and CTAs of the seven launches (RHS, CN, x transform,
  *   y transform, z solve, inverse x transform, projection). */
 typedef struct tc_batch tc_batch;

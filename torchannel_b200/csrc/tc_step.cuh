@@ -692,6 +692,8 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
                                         int Lr_arg) {
   using A = typename CnArith<T>::type;
   constexpr bool F32 = sizeof(A) == 4;
+  // FP32 sweeps of two columns per thread: packed FP32x2 arithmetic
+  constexpr bool PK = F32 && VEC == 2;
   const int Lr = FIXED ? L : Lr_arg;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x, chunk = threadIdx.y, nchunk = blockDim.y;
@@ -789,13 +791,25 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
       if (LEAN ? tt < nrow : m < e0) {
         const A bp = wb(tt + 2);
         const A f = a[m], ea = cA[m], eb = cB[m], ec = cC[m];
+        if constexpr (PK) {
+          // both columns in one packed FP32 operation (the same roundings);
+          // FP32 sweeps carry no base (bm = bc = bp = 0)
+          const float2 E = __ffma2_rn(make_float2(ea, ea), make_float2(wv[tt][0], wv[tt][1]),
+                                      __ffma2_rn(make_float2(eb, eb), make_float2(wv[tt + 1][0], wv[tt + 1][1]),
+                                                 __fmul2_rn(make_float2(ec, ec),
+                                                            make_float2(wv[tt + 2][0], wv[tt + 2][1]))));
+          const float2 Y = __ffma2_rn(make_float2(f, f), make_float2(yp[0], yp[1]), E);
+          yp[0] = Y.x; yp[1] = Y.y;
+          y[tt][0] = Y.x; y[tt][1] = Y.y;
+        } else {
 #pragma unroll
-        for (int c = 0; c < VEC; ++c) {
-          const A sm = (A)wv[tt][c] + bm, sc = (A)wv[tt + 1][c] + bc, sp = (A)wv[tt + 2][c] + bp;
-          // the explicit part first: one dependent FMA per row on the recurrence
-          const A E = fma(ea, sm, fma(eb, sc, ec * sp));
-          yp[c] = fma(f, yp[c], E);
-          y[tt][c] = yp[c];
+          for (int c = 0; c < VEC; ++c) {
+            const A sm = (A)wv[tt][c] + bm, sc = (A)wv[tt + 1][c] + bc, sp = (A)wv[tt + 2][c] + bp;
+            // the explicit part first: one dependent FMA per row on the recurrence
+            const A E = fma(ea, sm, fma(eb, sc, ec * sp));
+            yp[c] = fma(f, yp[c], E);
+            y[tt][c] = yp[c];
+          }
         }
         bm = bc; bc = bp;
       }
@@ -828,10 +842,17 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
       const int m = s0 + tt;
       if (LEAN ? tt < nrow : m < e0) {
         const A g = G[m], cpm = cp[m];
+        if constexpr (PK) {
+          const float2 t = __ffma2_rn(make_float2(g, g), make_float2(Din[0], Din[1]), make_float2(y[tt][0], y[tt][1]));
+          const float2 z = __ffma2_rn(make_float2(-cpm, -cpm), make_float2(zn[0], zn[1]), t);
+          zn[0] = z.x; zn[1] = z.y;
+          y[tt][0] = z.x; y[tt][1] = z.y;
+        } else {
 #pragma unroll
-        for (int c = 0; c < VEC; ++c) {
-          zn[c] = (y[tt][c] + g * Din[c]) - cpm * zn[c];
-          y[tt][c] = zn[c];
+          for (int c = 0; c < VEC; ++c) {
+            zn[c] = (y[tt][c] + g * Din[c]) - cpm * zn[c];
+            y[tt][c] = zn[c];
+          }
         }
       }
     }
@@ -862,8 +883,15 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
         const A h = H[m];
         const A bs = comp < 2 ? shb[m] : A(0);
         A o[VEC];
+        if constexpr (PK) {
+          const float2 r = __fadd2_rn(
+              __ffma2_rn(make_float2(h, h), make_float2(Xin[0], Xin[1]), make_float2(y[tt][0], y[tt][1])),
+              make_float2(bs, bs));
+          o[0] = r.x; o[1] = r.y;
+        } else {
 #pragma unroll
-        for (int c = 0; c < VEC; ++c) o[c] = F32 ? (y[tt][c] + h * Xin[c]) + bs : (y[tt][c] + h * Xin[c]) - bs;
+          for (int c = 0; c < VEC; ++c) o[c] = F32 ? (y[tt][c] + h * Xin[c]) + bs : (y[tt][c] + h * Xin[c]) - bs;
+        }
         const int pl = comp < 2 ? m : m + 1;
         if (TC_IN(LEAN ? (size_t)os : (size_t)pl * plane, qn, VEC))
           CnVec<T, VEC>::st(LEAN ? q + os : q + (size_t)pl * plane, o);
@@ -873,8 +901,10 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   }
 }
 
+// FP32 storage, two columns a thread: registers bounded to 64 (the packed
+// sweeps would take 95 and half the resident blocks otherwise).
 template <class T, int L, int VEC, int MAXT, bool FIXED>
-__global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+__global__ void __launch_bounds__(MAXT, sizeof(T) == 4 && VEC == 2 ? 1024 / MAXT : 1) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
                                                    CnTab t, const double* __restrict__ ubase, int nx, int ny,
                                                    int nz, int Lr) {
   cn_tile<T, L, VEC, FIXED>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr);
