@@ -34,10 +34,10 @@ def _same(torch, ea, eb):
         assert torch.equal(ca.scalars[:2], cb.scalars[:2])
 
 
-def _rows(e, bound=16):
-    """Each member's CN chunk length under the ensemble shape bound."""
-    chunks = -(-max(c.nz for c in e.channels) // bound)
-    return [-(-c.nz // chunks) for c in e.channels]
+def _rows(e, rows=16):
+    """Each member's CN chunk length under the ensemble shape: the shape's
+    rows for every member."""
+    return [rows for _ in e.channels]
 
 
 def _step_members(torch, e, n, scheme="IMEX", bound=16):

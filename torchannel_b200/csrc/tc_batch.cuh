@@ -49,7 +49,8 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 #define TC_BATCH_XP 4
 #endif
 #ifndef TC_BATCH_CN_CAP
-#define TC_BATCH_CN_CAP 1  // CN: cap at 128 registers (two 256-thread blocks per SM)
+#define TC_BATCH_CN_CAP 1  // CN: cap at 128 registers (two 256-thread blocks per SM); FP32 two
+                           // columns a thread: three 256-thread blocks (fewer spill)
 #endif
 
 template <class T> struct BMember {
@@ -121,12 +122,14 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>(), sizeof(T) == 4 ? TC_BATC
 template <class T, int L, int VEC>
 __device__ TC_BATCH_CN_CALL void batch_cn_call(const BMember<T>* __restrict__ bp, int bx, int comp) {
   const BMember<T>& b = *bp;
-  cn_tile<T, L, VEC>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.g.nx, b.g.ny, b.g.nz, bx, comp, b.cn_lr);
+  // every member's chunks are L rows (its tables' length), so the chunk
+  // length is a compile-time constant here as in k_cn_solve
+  cn_tile<T, L, VEC, true>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.g.nx, b.g.ny, b.g.nz, bx, comp, L);
 }
 
 // blockDim = (32, chunks of the deepest member) <= MAXT threads
 template <class T, int L, int VEC, int MAXT>
-__global__ void __launch_bounds__(MAXT, TC_BATCH_CN_CAP ? 512 / MAXT : 1) kb_cn(const BMember<T>* __restrict__ M, int nm, int total) {
+__global__ void __launch_bounds__(MAXT, TC_BATCH_CN_CAP ? (sizeof(T) == 4 && VEC == 2 ? 768 : 512) / MAXT : 1) kb_cn(const BMember<T>* __restrict__ M, int nm, int total) {
   __shared__ int st[TC_BATCH_MAX + 1];
   batch_starts(M, nm, BK_CN, total, st);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {

@@ -2465,14 +2465,15 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   int run[BK_COUNT] = {0, 0, 0, 0, 0, 0, 0};
   int maxnz = 0;
   for (auto* c : b->m) maxnz = std::max(maxnz, c->nz);
-  // one CN block of cn_y chunk warps for every member: member chunks of
-  // ceil(nz / cn_y) <= L rows fill all of its warps
+  // one CN block of cn_y chunk warps (the deepest member's chunks of L rows)
+  // for every member; a member's chunks are L rows, like a single-channel
+  // step's, and the warps beyond its last chunk idle
   const int maxchunks = (maxnz + L - 1) / L;
   size_t fx = 0, ifx = 0;
   int fyt = 0;
   for (int i = 0; i < n; ++i) {
     tc_ctx* c = b->m[i];
-    const int Lr = (c->nz + maxchunks - 1) / maxchunks;
+    const int Lr = L;
     if (c->cn_L_force != Lr) {  // the member's CN tables follow its chunk length
       c->cn_L_force = Lr;
       c->tab_dt = -1.0;

@@ -89,11 +89,11 @@ class ChannelBatch:
             pass
 
     def member_cn_rows(self, cn_rows=None):
-        """CN rows per chunk each member uses under the shape bound cn_rows
-        (default: the current shape)."""
+        """CN rows per chunk each member uses under the shape's cn_rows
+        (default: the current shape): the same for every member, its chunks
+        fill the CN block's first warps."""
         L = cn_rows or self.info()["cn_rows"]
-        chunks = -(-max(c.nz for c in self.channels) // L)
-        return [-(-c.nz // chunks) for c in self.channels]
+        return [L for _ in self.channels]
 
     def set_shape(self, cn_rows=16, ctas_per_sm=0):
         self.L.check(self.lib.tc_batch_set_shape(self.b, int(cn_rows), int(ctas_per_sm)))
