@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(RHS_TX * 8, MINB)
 #pragma unroll
     for (int q = 0; q < KB; ++q) {
       const int k = kb + q;
-      const size_t o = (size_t)k * plane + (size_t)j * nx + i;
+      const unsigned o = (unsigned)k * (unsigned)plane + (unsigned)j * (unsigned)nx + (unsigned)i;  // < 2^32
       const bool cell = active && k < nz, face = active && k >= 1 && k <= nz - 1;
       const bool hist = UPD == UPD_AB2 && have_hist;
       hru[q] = (cell && hist && TC_IN(o, ncell, 1)) ? ru[o] : T(0);
