@@ -274,130 +274,6 @@ __device__ __forceinline__ void rhs_march(const Grid<T>& g, const T (*__restrict
   }
 }
 
-// rhs_march for FP32 storage, the IMEX right-hand side (x/y diffusion) and
-// the AB2 update, with the u and v equations -- stencils of the same shape --
-// as the two halves of packed FP32x2 operations (__fadd2_rn, __fmul2_rn,
-// __ffma2_rn; a difference is a sum with the negated operand).  Every half
-// rounds as the scalar operation of rhs_march it replaces, so the results
-// are the same numbers (a zero can differ in sign where a v sum gains the +0
-// that u's base term adds).  w stays scalar.
-__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 pkneg(float2 a) { return make_float2(-a.x, -a.y); }
-template <int KB, int HY, int HX>
-__device__ __forceinline__ void rhs_march_pk(const Grid<float>& g, const float (*__restrict__ su)[HY][HX],
-                                             const float (*__restrict__ sv)[HY][HX],
-                                             const float (*__restrict__ sw)[HY][HX], int cx, int cy, int i, int j,
-                                             bool active, int kb, float* __restrict__ us, float* __restrict__ vs,
-                                             float* __restrict__ ws, float* __restrict__ ru, float* __restrict__ rv,
-                                             float* __restrict__ rw, float (&hru)[KB], float (&hrv)[KB],
-                                             float (&hrw)[KB], float forcing, float dt, int have_hist,
-                                             const float* __restrict__ pre) {
-  using R = Rn<float>;
-  using T = float;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const size_t plane = (size_t)nx * ny;
-  const size_t ncell = plane * nz, nface = plane * (nz + 1);  // field extents (bounds-checked builds)
-  (void)ncell; (void)nface;
-  T bs[KB + 2];
-#pragma unroll
-  for (int s = 0; s < KB + 2; ++s) bs[s] = pre ? pre[s] : rhs_pre_value<T, KB>(g, kb, s);
-  const T qx = T(0.25) * g.idx, qy = T(0.25) * g.idy;
-  const bool edge_u = (i == nx - 1), edge_v = (j == ny - 1);
-  const bool dz_u = !(edge_u && g.rhs_fused), dz_v = !(edge_v && g.rhs_fused);  // diffusion kept
-  T pW0 = sw[0][cy][cx];
-  T cU0 = su[1][cy][cx], cUxm = su[1][cy][cx - 1], cV0 = sv[1][cy][cx], cVym = sv[1][cy - 1][cx];
-  T cW0 = sw[1][cy][cx], cWxm = sw[1][cy][cx - 1], cWxp = sw[1][cy][cx + 1];
-  T cWym = sw[1][cy - 1][cx], cWyp = sw[1][cy + 1][cx];
-  // fluxes of face kb: FwP = (uw at i+1/2, vw at j+1/2), FwM = (uw at i-1/2, vw at j-1/2)
-  float2 FwP, FwM;
-  T Fww;
-  {
-    const T pU0 = su[0][cy][cx], pV0 = sv[0][cy][cx];
-    const T bz = R::add(bs[0], bs[1]);
-    T su_p = R::add(pU0, cU0), su_m = R::add(su[0][cy][cx - 1], cUxm);
-    su_p = R::add(su_p, bz); su_m = R::add(su_m, bz);
-    FwP = pk(R::mul(R::add(cW0, cWxp), su_p), R::mul(R::add(cW0, cWyp), R::add(pV0, cV0)));
-    FwM = pk(R::mul(R::add(cWxm, cW0), su_m), R::mul(R::add(cWym, cW0), R::add(sv[0][cy - 1][cx], cVym)));
-    const T sww = R::add(pW0, cW0);
-    Fww = R::mul(sww, sww);
-  }
-  unsigned o = (unsigned)kb * (unsigned)plane + (unsigned)j * (unsigned)nx + (unsigned)i;  // < 2^32
-#pragma unroll
-  for (int kk = 0; kk < KB; ++kk, o += (unsigned)plane) {
-    const int k = kb + kk;
-    if (k >= nz) break;
-    const int s0 = kk + 1, sp = kk + 2;
-    const T Uxp = su[s0][cy][cx + 1], Uym = su[s0][cy - 1][cx], Uyp = su[s0][cy + 1][cx];
-    const T Uypm = su[s0][cy + 1][cx - 1];
-    const T Vxm = sv[s0][cy][cx - 1], Vxp = sv[s0][cy][cx + 1], Vyp = sv[s0][cy + 1][cx];
-    const T Vymp = sv[s0][cy - 1][cx + 1];
-    const T nU0 = su[sp][cy][cx], nUxm = su[sp][cy][cx - 1], nV0 = sv[sp][cy][cx], nVym = sv[sp][cy - 1][cx];
-    const T nW0 = sw[sp][cy][cx], nWxm = sw[sp][cy][cx - 1], nWxp = sw[sp][cy][cx + 1];
-    const T nWym = sw[sp][cy - 1][cx], nWyp = sw[sp][cy + 1][cx];
-    const T b2 = R::add(bs[s0], bs[s0]);
-    const T bz = R::add(bs[s0], bs[sp]);
-    const float2 cUV = pk(cU0, cV0);
-    // (uu at i+1/2 and i-1/2, vv at j+1/2 and j-1/2): (Fuu, Fvv)
-    const float2 SaSc = __fadd2_rn(__fadd2_rn(cUV, pk(Uxp, Vyp)), pk(b2, 0.f));
-    const float2 SbSd = __fadd2_rn(__fadd2_rn(pk(cUxm, cVym), cUV), pk(b2, 0.f));
-    const float2 FF = __ffma2_rn(SaSc, SaSc, __fmul2_rn(SbSd, pkneg(SbSd)));
-    // uv at (i+1/2, j+1/2) and (i+1/2, j-1/2): (Fuv_pp, Fuv_pm); uv at (i-1/2, j+1/2)
-    const float2 Fpp_pm = __fmul2_rn(__fadd2_rn(pk(cV0, cVym), pk(Vxp, Vymp)),
-                                     __fadd2_rn(__fadd2_rn(pk(cU0, Uym), pk(Uyp, cU0)), pk(b2, b2)));
-    const T Fuv_mp = R::mul(R::add(R::add(cUxm, Uypm), b2), R::add(Vxm, cV0));
-    // fluxes of face k+1 (carried)
-    const float2 P1 = __fmul2_rn(__fadd2_rn(pk(nW0, nW0), pk(nWxp, nWyp)),
-                                 __fadd2_rn(__fadd2_rn(cUV, pk(nU0, nV0)), pk(bz, 0.f)));
-    const float2 M1 = __fmul2_rn(__fadd2_rn(pk(nWxm, nWym), pk(nW0, nW0)),
-                                 __fadd2_rn(__fadd2_rn(pk(cUxm, cVym), pk(nUxm, nVym)), pk(bz, 0.f)));
-    const T sww = R::add(cW0, nW0);
-    const T Fww1 = R::mul(sww, sww);
-    if (active) {
-      const T idzf = pre ? pre[KB + 2 + kk] : g.idzf[k];
-      const T qzf = T(0.25) * idzf;
-      // u and v at cell k: x/y diffusion, then advection where not on the edge plane
-      const float2 LX = __fadd2_rn(__ffma2_rn(pk(-2.f, -2.f), cUV, pk(Uxp, Vxp)), pk(cUxm, Vxm));
-      const float2 LY = __fadd2_rn(__ffma2_rn(pk(-2.f, -2.f), cUV, pk(Uyp, Vyp)), pk(Uym, cVym));
-      const float2 RD = __ffma2_rn(pk(g.nu_idx2, g.nu_idx2), LX, __fmul2_rn(pk(g.nu_idy2, g.nu_idy2), LY));
-      const float2 rd = pk(dz_u ? RD.x : T(0), dz_v ? RD.y : T(0));
-      const float2 D1 = __fadd2_rn(P1, pkneg(FwP));                                   // (Fuw_p1 - Fuw_p, Fvw_p1 - Fvw_p)
-      const float2 DA = __fadd2_rn(pk(Fpp_pm.x, Fpp_pm.x), pkneg(pk(Fpp_pm.y, Fuv_mp)));  // (pp - pm, pp - mp)
-      const float2 IN = __ffma2_rn(DA, pk(qy, qx), __fmul2_rn(FF, pk(qx, qy)));
-      const float2 RR = __fadd2_rn(rd, pkneg(__ffma2_rn(D1, pk(qzf, qzf), IN)));
-      T r_u = edge_u ? rd.x : RR.x;
-      const T r_v = edge_v ? rd.y : RR.y;
-      r_u = R::add(r_u, forcing);
-      const float2 RUV = pk(r_u, r_v);
-      const float2 AUV =
-          have_hist ? __ffma2_rn(pk(1.5f, 1.5f), RUV, __fmul2_rn(pk(-0.5f, -0.5f), pk(hru[kk], hrv[kk]))) : RUV;
-      const float2 UV = __ffma2_rn(pk(dt, dt), AUV, cUV);
-      if (TC_IN(o, ncell, 1)) {
-        us[o] = UV.x;
-        vs[o] = UV.y;
-        ru[o] = r_u;
-        rv[o] = r_v;
-      }
-      // w at face k
-      if (k >= 1) {
-        const T lx = R::add(R::fma(T(-2), cW0, cWxp), cWxm), ly = R::add(R::fma(T(-2), cW0, cWyp), cWym);
-        T r = R::fma(g.nu_idx2, lx, R::mul(g.nu_idy2, ly));
-        const T dww = R::mul(R::sub(Fww1, Fww), T(0.25) * (pre ? pre[2 * KB + 2 + kk] : g.idzc[k]));
-        const float2 DW = __fadd2_rn(FwP, pkneg(FwM));  // (Fuw_p - Fuw_m, Fvw_p - Fvw_m)
-        r = R::sub(r, R::fma(DW.x, qx, R::fma(DW.y, qy, dww)));
-        const T a = have_hist ? R::fma(T(1.5), r, R::mul(T(-0.5), hrw[kk])) : r;
-        if (TC_IN(o, nface, 1)) {
-          ws[o] = R::fma(dt, a, cW0);
-          rw[o] = r;
-        }
-      }
-    }
-    // carry plane k+1 and the fluxes of face k+1
-    cU0 = nU0; cUxm = nUxm; cV0 = nV0; cVym = nVym;
-    cW0 = nW0; cWxm = nWxm; cWxp = nWxp; cWym = nWym; cWyp = nWyp;
-    FwP = P1; FwM = M1; Fww = Fww1;
-  }
-}
-
 // FP64 storage: the stencils plane by plane, every flux formed where it is
 // used (the registers that carrying values up the column would take cost
 // the double-precision kernels more than the loads they save).  Same slot
@@ -515,11 +391,7 @@ __device__ __forceinline__ void rhs_planes(const Grid<double>& g, const double (
   }
 }
 
-// The stencils of a staged tile: rhs_march (FP32 storage; its packed form for
-// the IMEX AB2 step unless TC_RHS_PACKED is 0) or rhs_planes (FP64).
-#ifndef TC_RHS_PACKED
-#define TC_RHS_PACKED 0
-#endif
+// The stencils of a staged tile: rhs_march (FP32 storage) or rhs_planes (FP64).
 template <class T, bool FULL, int UPD, int KB, int HY, int HX>
 __device__ __forceinline__ void rhs_stencils(const Grid<T>& g, const T (*su)[HY][HX], const T (*sv)[HY][HX],
                                              const T (*sw)[HY][HX], int cx, int cy, int i, int j, bool active,
@@ -529,9 +401,6 @@ __device__ __forceinline__ void rhs_stencils(const Grid<T>& g, const T (*su)[HY]
   if constexpr (sizeof(T) == 8)
     rhs_planes<FULL, UPD, KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw,
                                       forcing, dt, have_hist);
-  else if constexpr (!FULL && UPD == UPD_AB2 && TC_RHS_PACKED)
-    rhs_march_pk<KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv, hrw, forcing,
-                             dt, have_hist, pre);
   else
     rhs_march<T, FULL, UPD, KB, HY, HX>(g, su, sv, sw, cx, cy, i, j, active, kb, us, vs, ws, ru, rv, rw, hru, hrv,
                                         hrw, forcing, dt, have_hist, pre);
