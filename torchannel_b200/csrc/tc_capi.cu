@@ -1023,6 +1023,16 @@ template <class T> static int poisson32_impl(tc_ctx* c, const T* u, const T* v, 
 
 // Chunk length of the CN solve: 16 rows up to nz = 256 (at most 16 warps),
 // 32 rows for deeper channels (nz <= 512).  The G/H tables follow it.
+// CN tables of the context for time step dt and chunk length L: the build
+// stages its work in shared memory where 17 nz doubles fit in the default
+// 48 KB (nz <= 361), else it works in the tables themselves.
+static void launch_cn_tables(tc_ctx* c, double dt, int L, cudaStream_t s) {
+  const size_t sm = (size_t)17 * c->nz * sizeof(double);
+  const bool staged = sm <= 48 * 1024;
+  k_cn_tables<<<1, 32, staged ? sm : 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, L,
+                                             ubase_of(c), staged ? 1 : 0);
+}
+
 static int cn_len(const tc_ctx* c) {
   if (c->cn_L_force) return c->cn_L_force;
   return c->nz <= 256 ? 16 : 32;
@@ -1080,8 +1090,7 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   dim3 blk(RHS_TX, rhs_ty<T>());
   dim3 grd((c->nx + RHS_TX - 1) / RHS_TX, (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>(), (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>());
   if (scheme == TC_IMEX && c->tab_dt != dt) {
-    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c),
-                                 ubase_of(c));
+    launch_cn_tables(c, dt, cn_len(c), s);
     c->tab_dt = dt;
   }
   // single-precision Poisson (IMEX): the increment over pf[pcur] once a base
@@ -1577,8 +1586,7 @@ extern "C" int tc_explicit_rhs(tc_ctx* c, int full, double* ru, double* rv, doub
 template <class T> static int cn_hook_impl(tc_ctx* c, double dt, cudaStream_t s) {
   T** A = (T**)c->st[c->cur];
   if (c->tab_dt != dt) {
-    k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dt, c->top_neumann, cn_len(c),
-                                 ubase_of(c));
+    launch_cn_tables(c, dt, cn_len(c), s);
     c->tab_dt = dt;
   }
   launch_cn<T>(c, A[0], A[1], A[2], s);
@@ -2480,8 +2488,7 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
       drop_graph(c);
     }
     if (scheme == TC_IMEX && c->tab_dt != dts[i]) {
-      k_cn_tables<<<1, 32, 0, s>>>(c->tab, c->dzf_d, c->dzc_d, c->nz, c->nu, dts[i], c->top_neumann, Lr,
-                                   ubase_of(c));
+      launch_cn_tables(c, dts[i], Lr, s);
       TC_LAUNCHED();
       c->tab_dt = dts[i];
     }

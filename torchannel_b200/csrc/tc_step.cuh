@@ -572,13 +572,27 @@ __device__ __forceinline__ void cn_fold(double* a, const double* iv, double* cA,
   }
 }
 
+// staged != 0: the two sequential builds work in dynamic shared memory
+// (8 nz + 8 nz + nz doubles, zeroed first) and the block copies the tables
+// out at the end; each level's values are re-read by the next level, which
+// from global memory costs an L2 round trip per access.  Same arithmetic.
 __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const double* __restrict__ dzc, int nz,
-                            double nu, double dt, int top_neumann, int L, const double* __restrict__ ubase) {
+                            double nu, double dt, int top_neumann, int L, const double* __restrict__ ubase,
+                            int staged) {
   const double theta = 0.5;
   const double alpha = theta * dt * nu;
   const int sys = threadIdx.x;
+  extern __shared__ double cn_sm[];
+  CnTab g = t;  // where the builds write
+  if (staged) {
+    for (int e = threadIdx.x; e < 17 * nz; e += blockDim.x) cn_sm[e] = 0.0;
+    __syncthreads();
+    g.uv = cn_sm;
+    g.w = cn_sm + 8 * nz;
+    g.corr = cn_sm + 16 * nz;
+  }
   if (sys == 0) {
-    double* a = t.uv; double* iv = a + nz; double* cp = iv + nz;
+    double* a = g.uv; double* iv = a + nz; double* cp = iv + nz;
     double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
     double cprev = 0.0;
     for (int m = 0; m < nz; ++m) {
@@ -612,19 +626,19 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
       for (int m = 0; m < nz; ++m) {
         const double sm = m > 0 ? ubase[m - 1] : 0.0, sp = m + 1 < nz ? ubase[m + 1] : 0.0;
         dp = a[m] * dp + (cA[m] * sm + cB[m] * ubase[m] + cC[m] * sp);
-        t.corr[m] = dp;
+        g.corr[m] = dp;
       }
       double x = 0.0;
       for (int m = nz - 1; m >= 0; --m) {
-        x = t.corr[m] - cp[m] * x;
-        t.corr[m] = x - ubase[m];
+        x = g.corr[m] - cp[m] * x;
+        g.corr[m] = x - ubase[m];
       }
     } else {
-      for (int m = 0; m < nz; ++m) t.corr[m] = 0.0;
+      for (int m = 0; m < nz; ++m) g.corr[m] = 0.0;
     }
   } else if (sys == 1) {
     const int n = nz - 1;
-    double* a = t.w; double* iv = a + nz; double* cp = iv + nz;
+    double* a = g.w; double* iv = a + nz; double* cp = iv + nz;
     double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
     double cprev = 0.0;
     for (int m = 0; m < n; ++m) {
@@ -643,6 +657,14 @@ __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const doubl
     }
     cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n, L);
     cn_fold(a, iv, cA, cB, cC, n, (1.0 - theta) * dt * nu, true);
+  }
+  if (staged) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 8 * nz; e += blockDim.x) {
+      t.uv[e] = cn_sm[e];
+      t.w[e] = cn_sm[8 * nz + e];
+    }
+    for (int e = threadIdx.x; e < nz; e += blockDim.x) t.corr[e] = cn_sm[16 * nz + e];
   }
 }
 
