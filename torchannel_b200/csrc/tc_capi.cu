@@ -521,6 +521,15 @@ static int yz_probe(tc_ctx* c) {
   return ncl > 0;
 }
 
+// The CN kernel of 16-row chunks: the packed FP32 sweeps (two columns a
+// thread) for FP32 storage, one FP64 column a thread otherwise.
+template <class T, bool FIXED> static auto cn16_kernel() {
+  if constexpr (sizeof(T) == 4)
+    return k_cn_solve_pk<16, 512, FIXED>;
+  else
+    return k_cn_solve<double, 16, 1, 512, FIXED>;
+}
+
 template <class T> static int set_smem_attrs(const tc_ctx* c) {
   const int big = 200 * 1024;
   TC_CUDA(cudaFuncSetAttribute(k_div_fftx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -532,9 +541,8 @@ template <class T> static int set_smem_attrs(const tc_ctx* c) {
   TC_CUDA(cudaFuncSetAttribute(k_yz_solve<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   TC_CUDA(cudaFuncSetAttribute(k_yz_solve<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_yz_solve<32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  constexpr int V16 = sizeof(T) == 4 ? 2 : 1;
-  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 16, V16, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(cn16_kernel<T, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TC_CUDA(cudaFuncSetAttribute(cn16_kernel<T, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_cn_solve<T, 32, 1, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   TC_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -1052,9 +1060,9 @@ template <class T> static void launch_cn(const tc_ctx* c, T* u, T* v, T* w, cuda
     constexpr int V = sizeof(T) == 4 ? 2 : 1;
     const dim3 grid((ncol / V + 31) / 32, 1, 3);
     if (Lr == 16)
-      k_cn_solve<T, 16, V, 512, true><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
+      cn16_kernel<T, true>()<<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
     else
-      k_cn_solve<T, 16, V, 512, false><<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
+      cn16_kernel<T, false>()<<<grid, blk, sm, s>>>(u, v, w, c->tab, ub, c->nx, c->ny, c->nz, Lr);
   } else {
     const dim3 grid((ncol + 31) / 32, 1, 3);
     if (Lr == 32)

@@ -561,110 +561,186 @@ __device__ __forceinline__ void cn_chunk_products(double* a, double* iv, double*
 // coefficients, d'_m = eA s_{-1} + eB s_0 + eC s_{+1} + f d'_{m-1}, with
 // f = -a_m rden_m, eX = rden_m (beta cX_m + [X is the row's own point]); the
 // own point is s_0 for u/v and s_{+1} for w (stored over a, cA, cB, cC).
+__device__ __forceinline__ void cn_fold_row(double* a, const double* iv, double* cA, double* cB, double* cC, int m,
+                                            double beta, bool w_rows) {
+  const double r = iv[m];
+  a[m] = -a[m] * r;
+  cA[m] = r * (beta * cA[m]);
+  cB[m] = r * (beta * cB[m] + (w_rows ? 0.0 : 1.0));
+  cC[m] = r * (beta * cC[m] + (w_rows ? 1.0 : 0.0));
+}
 __device__ __forceinline__ void cn_fold(double* a, const double* iv, double* cA, double* cB, double* cC, int n,
                                         double beta, bool w_rows) {
-  for (int m = 0; m < n; ++m) {
-    const double r = iv[m];
-    a[m] = -a[m] * r;
-    cA[m] = r * (beta * cA[m]);
-    cB[m] = r * (beta * cB[m] + (w_rows ? 0.0 : 1.0));
-    cC[m] = r * (beta * cC[m] + (w_rows ? 1.0 : 0.0));
+  for (int m = 0; m < n; ++m) cn_fold_row(a, iv, cA, cB, cC, m, beta, w_rows);
+}
+
+// CN image of the base profile minus itself (zero without a base), from the
+// folded u / v rows: unchunked sweeps, FP64.
+__device__ __forceinline__ void cn_base_corr(const CnTab& t, int nz, const double* __restrict__ ubase) {
+  const double* a = t.uv; const double* cp = a + 2 * nz;
+  const double* cA = a + 3 * nz; const double* cB = cA + nz; const double* cC = cB + nz;
+  if (ubase) {
+    double dp = 0.0;
+    for (int m = 0; m < nz; ++m) {
+      const double sm = m > 0 ? ubase[m - 1] : 0.0, sp = m + 1 < nz ? ubase[m + 1] : 0.0;
+      dp = a[m] * dp + (cA[m] * sm + cB[m] * ubase[m] + cC[m] * sp);
+      t.corr[m] = dp;
+    }
+    double x = 0.0;
+    for (int m = nz - 1; m >= 0; --m) {
+      x = t.corr[m] - cp[m] * x;
+      t.corr[m] = x - ubase[m];
+    }
+  } else {
+    for (int m = 0; m < nz; ++m) t.corr[m] = 0.0;
   }
 }
 
-// staged != 0: the two sequential builds work in dynamic shared memory
-// (8 nz + 8 nz + nz doubles, zeroed first) and the block copies the tables
-// out at the end; each level's values are re-read by the next level, which
-// from global memory costs an L2 round trip per access.  Same arithmetic.
+// Rows of the CN systems at level m (operators.py:581-644 for u / v,
+// 753-803 for w): the implicit row (am, bm, cm) with the wall closures and
+// the explicit half's stencil (ea, eb, ec).
+struct CnRow { double am, bm, cm, ea, eb, ec; };
+__device__ __forceinline__ CnRow cn_row_uv(const double* __restrict__ dzf, const double* __restrict__ dzc, int m,
+                                           int nz, double alpha, int top_neumann) {
+  CnRow r;
+  double dl = dzc[m], dr = dzc[m + 1], dc = dzf[m];
+  double lo = -alpha / (dl * dc);
+  double ce = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dc;
+  double up = -alpha / (dr * dc);
+  r.am = lo; r.bm = ce; r.cm = up;
+  if (m == 0) { r.am = 0.0; r.bm = ce - lo; }
+  if (m == nz - 1) { r.bm = top_neumann ? ce + up : ce - up; r.cm = 0.0; }
+  // explicit half (operators.py:635-644)
+  r.ea = 1.0 / (dl * dc); r.eb = -(1.0 / dr + 1.0 / dl) / dc; r.ec = 1.0 / (dr * dc);
+  if (m == 0) { r.ea = 0.0; r.eb = (-1.0 / dr - 2.0 / dl) / dc; }
+  if (m == nz - 1) {
+    if (top_neumann) { r.eb = -1.0 / (dl * dc); }
+    else { r.eb = (-2.0 / dr - 1.0 / dl) / dc; }
+    r.ec = 0.0;
+  }
+  return r;
+}
+__device__ __forceinline__ CnRow cn_row_w(const double* __restrict__ dzf, const double* __restrict__ dzc, int m,
+                                          int n, double alpha) {
+  CnRow r;
+  double dl = dzf[m], dr = dzf[m + 1], dcv = dzc[m + 1];
+  double lo = -alpha / (dl * dcv);
+  double ce = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dcv;
+  double up = -alpha / (dr * dcv);
+  r.am = (m == 0) ? 0.0 : lo; r.bm = ce; r.cm = (m == n - 1) ? 0.0 : up;
+  r.ea = 1.0 / (dl * dcv); r.eb = -(1.0 / dr + 1.0 / dl) / dcv; r.ec = 1.0 / (dr * dcv);
+  if (m == 0) r.ea = 0.0;
+  if (m == n - 1) r.ec = 0.0;
+  return r;
+}
+
+// The CN tables of the u / v system (t.uv, and t.corr: the CN image of the
+// base profile minus itself) and of the w system (t.w), for time step dt and
+// chunk length L.  staged != 0: the block works in dynamic shared memory
+// (8 nz + 8 nz + nz doubles): every thread forms rows of both systems, one
+// thread per system runs the Thomas factor recurrence (its only sequential
+// part), the chunk products, the fold and the base profile's sweeps follow,
+// and the block copies the tables out.  staged == 0: one thread per system
+// does everything in the tables themselves.  The same operations on the same
+// values either way.
 __global__ void k_cn_tables(CnTab t, const double* __restrict__ dzf, const double* __restrict__ dzc, int nz,
                             double nu, double dt, int top_neumann, int L, const double* __restrict__ ubase,
                             int staged) {
   const double theta = 0.5;
   const double alpha = theta * dt * nu;
-  const int sys = threadIdx.x;
+  const double beta = (1.0 - theta) * dt * nu;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int n = nz - 1;  // rows of the w system
   extern __shared__ double cn_sm[];
   CnTab g = t;  // where the builds write
   if (staged) {
-    for (int e = threadIdx.x; e < 17 * nz; e += blockDim.x) cn_sm[e] = 0.0;
-    __syncthreads();
     g.uv = cn_sm;
     g.w = cn_sm + 8 * nz;
     g.corr = cn_sm + 16 * nz;
-  }
-  if (sys == 0) {
-    double* a = g.uv; double* iv = a + nz; double* cp = iv + nz;
-    double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
-    double cprev = 0.0;
-    for (int m = 0; m < nz; ++m) {
-      double dl = dzc[m], dr = dzc[m + 1], dc = dzf[m];
-      double lo = -alpha / (dl * dc);
-      double ce = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dc;
-      double up = -alpha / (dr * dc);
-      double am = lo, bm = ce, cm = up;
-      if (m == 0) { am = 0.0; bm = ce - lo; }
-      if (m == nz - 1) { bm = top_neumann ? ce + up : ce - up; cm = 0.0; }
-      double den = bm - am * cprev;
-      double rden = 1.0 / den;
-      a[m] = am; iv[m] = rden; cp[m] = cm * rden; cprev = cp[m];
-      // explicit half (operators.py:635-644)
-      double ea = 1.0 / (dl * dc), eb = -(1.0 / dr + 1.0 / dl) / dc, ec = 1.0 / (dr * dc);
-      if (m == 0) { ea = 0.0; eb = (-1.0 / dr - 2.0 / dl) / dc; }
-      if (m == nz - 1) {
-        if (top_neumann) { eb = -1.0 / (dl * dc); }
-        else { eb = (-2.0 / dr - 1.0 / dl) / dc; }
-        ec = 0.0;
-      }
-      cA[m] = ea; cB[m] = eb; cC[m] = ec;
-    }
-    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz, L);
-    *t.beta = (1.0 - theta) * dt * nu;
-    cn_fold(a, iv, cA, cB, cC, nz, (1.0 - theta) * dt * nu, false);
-    // CN image of the base profile minus itself (zero without a base):
-    // unchunked sweeps with the folded rows, FP64
-    if (ubase) {
-      double dp = 0.0;
-      for (int m = 0; m < nz; ++m) {
-        const double sm = m > 0 ? ubase[m - 1] : 0.0, sp = m + 1 < nz ? ubase[m + 1] : 0.0;
-        dp = a[m] * dp + (cA[m] * sm + cB[m] * ubase[m] + cC[m] * sp);
-        g.corr[m] = dp;
-      }
-      double x = 0.0;
-      for (int m = nz - 1; m >= 0; --m) {
-        x = g.corr[m] - cp[m] * x;
-        g.corr[m] = x - ubase[m];
-      }
-    } else {
-      for (int m = 0; m < nz; ++m) g.corr[m] = 0.0;
-    }
-  } else if (sys == 1) {
-    const int n = nz - 1;
-    double* a = g.w; double* iv = a + nz; double* cp = iv + nz;
-    double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
-    double cprev = 0.0;
-    for (int m = 0; m < n; ++m) {
-      double dl = dzf[m], dr = dzf[m + 1], dcv = dzc[m + 1];
-      double lo = -alpha / (dl * dcv);
-      double ce = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dcv;
-      double up = -alpha / (dr * dcv);
-      double am = (m == 0) ? 0.0 : lo, bm = ce, cm = (m == n - 1) ? 0.0 : up;
-      double den = bm - am * cprev;
-      double rden = 1.0 / den;
-      a[m] = am; iv[m] = rden; cp[m] = cm * rden; cprev = cp[m];
-      double ea = 1.0 / (dl * dcv), eb = -(1.0 / dr + 1.0 / dl) / dcv, ec = 1.0 / (dr * dcv);
-      if (m == 0) ea = 0.0;
-      if (m == n - 1) ec = 0.0;
-      cA[m] = ea; cB[m] = eb; cC[m] = ec;
-    }
-    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n, L);
-    cn_fold(a, iv, cA, cB, cC, n, (1.0 - theta) * dt * nu, true);
-  }
-  if (staged) {
+    for (int e = tid; e < 17 * nz; e += nthr) cn_sm[e] = 0.0;
     __syncthreads();
-    for (int e = threadIdx.x; e < 8 * nz; e += blockDim.x) {
+    // rows: a <- am, iv <- bm, cp <- cm until the recurrence replaces them
+    for (int m = tid; m < nz; m += nthr) {
+      const CnRow r = cn_row_uv(dzf, dzc, m, nz, alpha, top_neumann);
+      double* u = g.uv;
+      u[m] = r.am; u[nz + m] = r.bm; u[2 * nz + m] = r.cm;
+      u[3 * nz + m] = r.ea; u[4 * nz + m] = r.eb; u[5 * nz + m] = r.ec;
+      if (m < n) {
+        const CnRow q = cn_row_w(dzf, dzc, m, n, alpha);
+        double* w = g.w;
+        w[m] = q.am; w[nz + m] = q.bm; w[2 * nz + m] = q.cm;
+        w[3 * nz + m] = q.ea; w[4 * nz + m] = q.eb; w[5 * nz + m] = q.ec;
+      }
+    }
+    __syncthreads();
+    if (tid < 2) {
+      double* a = tid == 0 ? g.uv : g.w;
+      double* iv = a + nz; double* cp = iv + nz;
+      const int rows = tid == 0 ? nz : n;
+      double cprev = 0.0;
+      for (int m = 0; m < rows; ++m) {
+        const double den = iv[m] - a[m] * cprev;
+        const double rden = 1.0 / den;
+        iv[m] = rden; cp[m] = cp[m] * rden; cprev = cp[m];
+      }
+    }
+    __syncthreads();
+    if (tid < 2) {
+      double* a = tid == 0 ? g.uv : g.w;
+      double* iv = a + nz; double* cp = iv + nz;
+      double* cC = cp + 3 * nz;
+      cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, tid == 0 ? nz : n, L);
+    }
+    __syncthreads();
+    for (int m = tid; m < nz; m += nthr) {
+      double* a = g.uv; double* iv = a + nz; double* cA = a + 3 * nz;
+      cn_fold_row(a, iv, cA, cA + nz, cA + 2 * nz, m, beta, false);
+      if (m < n) {
+        double* aw = g.w; double* ivw = aw + nz; double* cAw = aw + 3 * nz;
+        cn_fold_row(aw, ivw, cAw, cAw + nz, cAw + 2 * nz, m, beta, true);
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      *t.beta = beta;
+      cn_base_corr(g, nz, ubase);
+    }
+    __syncthreads();
+    for (int e = tid; e < 8 * nz; e += nthr) {
       t.uv[e] = cn_sm[e];
       t.w[e] = cn_sm[8 * nz + e];
     }
-    for (int e = threadIdx.x; e < nz; e += blockDim.x) t.corr[e] = cn_sm[16 * nz + e];
+    for (int e = tid; e < nz; e += nthr) t.corr[e] = cn_sm[16 * nz + e];
+    return;
+  }
+  if (tid == 0) {
+    double* a = t.uv; double* iv = a + nz; double* cp = iv + nz;
+    double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
+    double cprev = 0.0;
+    for (int m = 0; m < nz; ++m) {
+      const CnRow r = cn_row_uv(dzf, dzc, m, nz, alpha, top_neumann);
+      const double den = r.bm - r.am * cprev;
+      const double rden = 1.0 / den;
+      a[m] = r.am; iv[m] = rden; cp[m] = r.cm * rden; cprev = cp[m];
+      cA[m] = r.ea; cB[m] = r.eb; cC[m] = r.ec;
+    }
+    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, nz, L);
+    *t.beta = beta;
+    cn_fold(a, iv, cA, cB, cC, nz, beta, false);
+    cn_base_corr(t, nz, ubase);
+  } else if (tid == 1) {
+    double* a = t.w; double* iv = a + nz; double* cp = iv + nz;
+    double* cA = cp + nz; double* cB = cA + nz; double* cC = cB + nz;
+    double cprev = 0.0;
+    for (int m = 0; m < n; ++m) {
+      const CnRow r = cn_row_w(dzf, dzc, m, n, alpha);
+      const double den = r.bm - r.am * cprev;
+      const double rden = 1.0 / den;
+      a[m] = r.am; iv[m] = rden; cp[m] = r.cm * rden; cprev = cp[m];
+      cA[m] = r.ea; cB[m] = r.eb; cC[m] = r.ec;
+    }
+    cn_chunk_products(a, iv, cp, cC + nz, cC + 2 * nz, n, L);
+    cn_fold(a, iv, cA, cB, cC, n, beta, true);
   }
 }
 
@@ -925,13 +1001,22 @@ __device__ __forceinline__ void cn_tile(T* __restrict__ u, T* __restrict__ v, T*
   }
 }
 
-// FP32 storage, two columns a thread: registers bounded to 64 (the packed
-// sweeps would take 95 and half the resident blocks otherwise).
 template <class T, int L, int VEC, int MAXT, bool FIXED>
-__global__ void __launch_bounds__(MAXT, sizeof(T) == 4 && VEC == 2 ? 1024 / MAXT : 1) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+__global__ void __launch_bounds__(MAXT) k_cn_solve(T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
                                                    CnTab t, const double* __restrict__ ubase, int nx, int ny,
                                                    int nz, int Lr) {
   cn_tile<T, L, VEC, FIXED>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr);
+}
+
+// FP32 storage, two columns a thread (the packed sweeps): registers bounded
+// to 64, four 256-thread blocks per SM (left free the sweeps take 95
+// registers and half the resident blocks).
+template <int L, int MAXT, bool FIXED>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT) k_cn_solve_pk(float* __restrict__ u, float* __restrict__ v,
+                                                                 float* __restrict__ w, CnTab t,
+                                                                 const double* __restrict__ ubase, int nx, int ny,
+                                                                 int nz, int Lr) {
+  cn_tile<float, L, 2, FIXED>(u, v, w, t, ubase, nx, ny, nz, blockIdx.x, blockIdx.z, Lr);
 }
 
 // Scalars slot layout (FP64, device).
