@@ -432,54 +432,60 @@ __global__ void __launch_bounds__(256) k_ke_partials(const double* __restrict__ 
   if (threadIdx.x == 0 && threadIdx.y == 0)
     partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
 }
-// Variant inside a step: the weight comes from device memory (a zero weight
-// skips the loads), so a captured step needs no re-capture when it changes.
-__global__ void __launch_bounds__(256) k_ke_partials_w(const double* __restrict__ u, const double* __restrict__ v,
-                                                       const double* __restrict__ w, const double* __restrict__ dzf,
-                                                       const double* __restrict__ dzc, const double* wt,
-                                                       double* partials, int nx, int ny, int nz) {
+// The forward step's adjoint hooks in one pass over the new state:
+//  * (when `partials` is non-null) the block partials of the volume-weighted
+//    kinetic energy 0.5 sum W q^2 as k_ke_partials forms them, skipped when
+//    the weight in device memory is 0 (a captured step needs no re-capture
+//    when the weight changes);
+//  * (when `tape` is non-null) the copy of u, v, w into slot *ctr of the
+//    state tape when *ctr < nslots (slot stride 3 (nz+1) nx ny doubles; u, v
+//    with a zero top plane).
+__global__ void __launch_bounds__(256) k_step_hooks(const double* __restrict__ u, const double* __restrict__ v,
+                                                    const double* __restrict__ w, const double* __restrict__ dzf,
+                                                    const double* __restrict__ dzc, const double* wt,
+                                                    double* partials, double* tape, const int* ctr, int nslots,
+                                                    int nx, int ny, int nz) {
   __shared__ double sh[32];
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
-  double s = 0.0;
-  if (*wt != 0.0 && i < nx && j < ny) {
-    const size_t o = (size_t)k * nx * ny + (size_t)j * nx + i;
-    if (k < nz) s += (u[o] * u[o] + v[o] * v[o]) * dzf[k];
-    if (k >= 1 && k <= nz - 1) s += w[o] * w[o] * dzc[k];
-  }
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0)
-    partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
-}
-__global__ void __launch_bounds__(256) k_ke_finalize_w(const double* __restrict__ partials, int n, double* acc,
-                                                       const double* wt, double coef) {
-  __shared__ double sh[32];
-  const double wv = *wt;
-  if (wv == 0.0) return;
-  double s = 0.0;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) s += partials[e];
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) *acc += wv * coef * 0.5 * s;
-}
-
-// State tape: copy u, v, w of the new state into slot *ctr of `tape` (slot
-// stride 3 (nz+1) nx ny doubles; u, v with a zero top plane) when *ctr <
-// nslots; k_tape_advance then increments *ctr (saturating at nslots).
-__global__ void __launch_bounds__(256) k_tape_copy(const double* __restrict__ u, const double* __restrict__ v,
-                                                   const double* __restrict__ w, double* tape, const int* ctr,
-                                                   int nslots, int nx, int ny, int nz) {
-  const int slot = *ctr;
-  if (slot < 0 || slot >= nslots) return;
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
-  if (i >= nx || j >= ny) return;
-  const size_t pl = (size_t)nx * ny, f = (size_t)(nz + 1) * pl;
+  const bool in = i < nx && j < ny;
+  const size_t pl = (size_t)nx * ny;
   const size_t o = (size_t)k * pl + (size_t)j * nx + i;
-  double* t = tape + (size_t)slot * 3 * f;
-  t[o] = k < nz ? u[o] : 0.0;
-  t[f + o] = k < nz ? v[o] : 0.0;
-  t[2 * f + o] = (k >= 1 && k <= nz - 1) ? w[o] : 0.0;
+  if (partials) {
+    double s = 0.0;
+    if (*wt != 0.0 && in) {
+      if (k < nz) s += (u[o] * u[o] + v[o] * v[o]) * dzf[k];
+      if (k >= 1 && k <= nz - 1) s += w[o] * w[o] * dzc[k];
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+      partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+  }
+  if (tape) {
+    const int slot = *ctr;
+    if (slot < 0 || slot >= nslots || !in) return;
+    const size_t f = (size_t)(nz + 1) * pl;
+    double* t = tape + (size_t)slot * 3 * f;
+    t[o] = k < nz ? u[o] : 0.0;
+    t[f + o] = k < nz ? v[o] : 0.0;
+    t[2 * f + o] = (k >= 1 && k <= nz - 1) ? w[o] : 0.0;
+  }
 }
-__global__ void k_tape_advance(int* ctr, int nslots) {
-  if (threadIdx.x == 0 && *ctr < nslots) *ctr += 1;
+// After k_step_hooks: acc += weight coef 0.5 (sum of the partials) when
+// `partials` is non-null and the weight is not 0, and the tape counter's
+// advance (saturating at nslots) when `ctr` is non-null.
+__global__ void __launch_bounds__(256) k_step_hooks_finalize(const double* __restrict__ partials, int n, double* acc,
+                                                             const double* wt, double coef, int* ctr, int nslots) {
+  __shared__ double sh[32];
+  if (partials) {
+    const double wv = *wt;
+    if (wv != 0.0) {
+      double s = 0.0;
+      for (int e = threadIdx.x; e < n; e += blockDim.x) s += partials[e];
+      s = block_sum(s, sh);
+      if (threadIdx.x == 0) *acc += wv * coef * 0.5 * s;
+    }
+  }
+  if (ctr && threadIdx.x == 0 && *ctr < nslots) *ctr += 1;
 }
 
 __global__ void __launch_bounds__(256) k_ke_finalize(const double* __restrict__ partials, int n, double* acc,

@@ -1159,17 +1159,13 @@ template <class T> static int step_impl(tc_ctx* c, int scheme, double dt, cudaSt
   if (rc) return rc;
   if constexpr (sizeof(T) == 8) {
     const dim3 ag((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz + 1);
-    if (c->ke_acc) {
-      k_ke_partials_w<<<ag, dim3(32, 8), 0, s>>>(B[0], B[1], B[2], c->dzf_d, c->dzc_d, c->ke_w, c->ke_part, c->nx,
-                                                 c->ny, c->nz);
-      k_ke_finalize_w<<<1, 256, 0, s>>>(c->ke_part, (int)(ag.x * ag.y * ag.z), c->ke_acc, c->ke_w,
-                                        c->dx * c->dy / (c->Lx * c->Ly * c->Lz));
-      TC_LAUNCHED();
-    }
-    if (c->tape) {
-      k_tape_copy<<<ag, dim3(32, 8), 0, s>>>(B[0], B[1], B[2], c->tape, c->tape_ctr, c->tape_slots, c->nx, c->ny,
-                                             c->nz);
-      k_tape_advance<<<1, 32, 0, s>>>(c->tape_ctr, c->tape_slots);
+    if (c->ke_acc || c->tape) {  // the adjoint hooks: one pass over the new state, one finishing block
+      double* part = c->ke_acc ? c->ke_part : nullptr;
+      k_step_hooks<<<ag, dim3(32, 8), 0, s>>>(B[0], B[1], B[2], c->dzf_d, c->dzc_d, c->ke_w, part, c->tape,
+                                              c->tape_ctr, c->tape_slots, c->nx, c->ny, c->nz);
+      k_step_hooks_finalize<<<1, 256, 0, s>>>(part, (int)(ag.x * ag.y * ag.z), c->ke_acc, c->ke_w,
+                                              c->dx * c->dy / (c->Lx * c->Ly * c->Lz),
+                                              c->tape ? c->tape_ctr : nullptr, c->tape_slots);
       TC_LAUNCHED();
     }
   }
