@@ -357,7 +357,10 @@ int tc_set_cn_chunk(tc_ctx* ctx, int rows);
  *   -1 = one CTA per work unit), the ensemble autotuner's knobs.
  * tc_batch_step: dts = host array of one dt per member; members without AB2
  *   history start with a forward step as tc_step does.  Members may carry no
- *   adjoint hooks (TC_ERR_ARG).
+ *   adjoint hooks (TC_ERR_ARG).  The RHS launch stages its tiles by tensor
+ *   copies (one work unit per tile of the tensor-copy RHS) while every
+ *   member has tc_use_tma_rhs mode 1 on, and by per-thread loads otherwise;
+ *   switching a member rebuilds the tables at the next call.
  * tc_batch_info: shape = {cn rows, ctas per SM (-1: one CTA per work
  *   unit), tables built, CN chunk warps per block (the deepest member's
  *   chunks)}; units and

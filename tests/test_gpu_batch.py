@@ -184,3 +184,47 @@ def test_autotune_mode_restores_state(torch_cuda):
     for ch, b in zip(e.channels, before):
         for x, y in zip(ch.get_state()[:3], b):
             assert torch.equal(x, y)
+
+
+def test_batch_rhs_follows_member_rhs_form(torch_cuda):
+    """The ensemble's RHS stages its tiles by tensor copies (kb_rhs_tma, one
+    unit per k_rhs_tma tile) while every member has its tensor-copy RHS on in
+    the default shape, and runs the per-thread staged kernel otherwise; a
+    member switched between ensemble calls rebuilds the tables, and the
+    members stay bit-identical to their own steps through both forms."""
+    torch = torch_cuda
+    from torchannel_b200.ensemble import Ensemble
+    ms = _members(4, seed=3)
+    a, b = Ensemble(ms, precision="mixed"), Ensemble(ms, precision="mixed")
+    a.batch()
+    a.step_batch(5)
+    torch.cuda.synchronize()
+    tiles = sum(-(-c.nx // 32) * -(-c.ny // 8) * -(-c.nz // 8) for c in a.channels)
+    assert a.batched.info()["units"]["rhs"] == tiles
+    a.channels[2].use_tma_rhs(0)
+    b.channels[2].use_tma_rhs(0)
+    a.step_batch(4)
+    torch.cuda.synchronize()
+    assert a.batched.info()["units"]["rhs"] != tiles
+    a.channels[2].use_tma_rhs(1)
+    b.channels[2].use_tma_rhs(1)
+    a.batched.set_shape(16, -1)
+    a.step_batch(5)
+    torch.cuda.synchronize()
+    info = a.batched.info()
+    assert info["units"]["rhs"] == tiles and info["ctas"]["rhs"] == tiles
+    _step_members(torch, b, 14)
+    _same(torch, a, b)
+
+
+def test_batch_rhs_member_groups(torch_cuda):
+    """More members than one RHS launch parameter holds (32): the tensor-copy
+    RHS runs as one launch per group, bit-identical to the members' steps."""
+    torch = torch_cuda
+    from torchannel_b200.ensemble import make_members
+    a, b = _pair("mixed", make_members(34, seed=4, sizes_xy=(64,), sizes_z=(16, 24)))
+    a.batch()
+    a.step_batch(5)
+    torch.cuda.synchronize()
+    _step_members(torch, b, 5)
+    _same(torch, a, b)

@@ -70,6 +70,16 @@ for nx, ny, nz, prec, top, middle, bulk, tma in cases:
     assert lib.tc_bounds_error(ctypes.byref(flag), ctypes.byref(where)) == 0
     print(nx, ny, nz, prec, top, middle, bulk, tma, "flag", flag.value, "where", where.value, flush=True)
     assert flag.value == 0, (nx, ny, nz, prec, "out-of-range access at", where.value)
+# ensemble launches (the tensor-copy RHS of several members in one launch)
+from torchannel_b200.ensemble import Ensemble, make_members
+for prec in ("mixed", "fp64"):
+    e = Ensemble(make_members(3, seed=2, sizes_xy=(64, 96), sizes_z=(16, 24)), precision=prec)
+    e.batch()
+    e.step_batch(5)
+    torch.cuda.synchronize()
+    assert lib.tc_bounds_error(ctypes.byref(flag), ctypes.byref(where)) == 0
+    print("ensemble", prec, "flag", flag.value, "where", where.value, flush=True)
+    assert flag.value == 0, ("ensemble", prec, "out-of-range access at", where.value)
 print("bounds ok")
 """
 

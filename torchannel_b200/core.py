@@ -162,8 +162,9 @@ class Channel:
 
     def use_tma_rhs(self, on=True):
         """Explicit-RHS tiles staged by tensor copies (True or a tile-shape
-        mode 1..4; mode 1 is the default where the grid allows it) or by
-        per-thread loads (False); bit-identical."""
+        mode 1..6; mode 1 is the default where the grid allows it) or by
+        per-thread loads (False); bit-identical.  An ensemble's RHS stages
+        its tiles by tensor copies while all its members have mode 1 on."""
         L.check(self.lib.tc_use_tma_rhs(self.ctx, int(on)))
 
     def use_fp32_poisson(self, on=True, warm_steps=10):

@@ -14,6 +14,7 @@
 #pragma once
 #include "tc_common.cuh"
 #include "tc_poisson.cuh"
+#include "tc_rhs_tma.cuh"
 #include "tc_step.cuh"
 
 namespace tc {
@@ -75,6 +76,7 @@ template <class T> struct BMember {
   BulkArgs ba;
   int n1x, n1y, nxh, nrows;
   int rgx, rgy, rgz;       // block grid of k_rhs_update
+  int tnx, tny, tnz;       // tiles of the tensor-copy RHS (k_rhs_tma's default shape)
   int cgx;                 // column blocks per component of k_cn_solve
   int cn_lr;               // CN rows per chunk of this member (its tables' length)
   int xgx;                 // row blocks per plane of the x transforms
@@ -116,6 +118,102 @@ __global__ void __launch_bounds__(RHS_TX * rhs_ty<T>(), sizeof(T) == 4 ? TC_BATC
     rhs_tile<T, FULL, UPD>(b.g, b.A[0], b.A[1], b.A[2], b.B[0], b.B[1], b.B[2], b.R[0], b.R[1], b.R[2], b.forcing,
                            b.dt, UPD == UPD_FE ? 0 : b.have_hist, bx, by, bz);
     __syncthreads();
+  }
+}
+
+// The explicit RHS of the members with their tiles staged by tensor copies
+// (kb_rhs_tma).  Everything a tile reads of its member -- the tensor maps of
+// u, v, w for the step's parity, the grid, the buffers, dt -- travels in the
+// launch's __grid_constant__ parameter, as the single-channel kernel's does:
+// the CTA's member is uniform, so its fields are uniform parameter loads and
+// take no per-thread registers (read from a table in global memory they
+// would, and spill).  A parameter holds TC_BATCH_TMA_GROUP members (within
+// the 32,764-byte parameter limit); larger ensembles take one launch per
+// group.
+#define TC_BATCH_TMA_GROUP 32
+template <class T> struct BRhsRec {
+  Grid<T> g;
+  T* A[3];
+  T* B[3];
+  T* R[3];
+  const double* forcing;
+  int* err;
+  T dt;
+  int have_hist;
+  int tny, tnz;  // y and z tiles (z fastest)
+};
+template <class T> struct BatchRhsArgs {
+  CUtensorMap map[TC_BATCH_TMA_GROUP][3];
+  BRhsRec<T> r[TC_BATCH_TMA_GROUP];
+  int st[TC_BATCH_TMA_GROUP + 1];  // first unit of each member of the group (global unit index), then the end
+  int nm;
+};
+static_assert(sizeof(BatchRhsArgs<double>) + 64 <= 32764, "kernel parameter limit");
+
+// Unit w = tile (bx, by, bz) of k_rhs_tma's default shape of its member,
+// evaluated by the same tile code (rhs_tma_tile).  Persistent CTAs walk the
+// group's units with one stage: the next unit's copies are issued once the
+// barrier that ends a unit has released the stage (the other resident CTAs
+// hide their latency, as for k_rhs_tma's one-tile CTAs).  Dynamic shared
+// memory: the stage, its barrier and the march's constants.
+template <class T> struct BatchRhsTmaShape {
+  static constexpr int KB = sizeof(T) == 4 ? 8 : 2, MINB = sizeof(T) == 4 ? 3 : 5;
+  using S = RhsTma<T, KB, 1>;
+  static __host__ __device__ constexpr size_t smem() { return S::smem(); }
+};
+template <class T, bool FULL, int UPD>
+__global__ void __launch_bounds__(RHS_TX * 8, BatchRhsTmaShape<T>::MINB)
+    kb_rhs_tma(const __grid_constant__ BatchRhsArgs<T> a) {
+  using B = BatchRhsTmaShape<T>;
+  using S = typename B::S;
+  constexpr int KB = B::KB;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* buf = reinterpret_cast<T*>(smraw);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(buf + S::STAGE);
+  T* pre = reinterpret_cast<T*>(bar + 2);
+  const int tid = threadIdx.y * RHS_TX + threadIdx.x;
+  const int u0 = a.st[0], u1 = a.st[a.nm];
+  if (u0 + (int)blockIdx.x >= u1) return;
+  if (smem_u32(buf) & 127u) {  // tensor copies need 128-byte aligned boxes
+    if (tid == 0) atomicOr(a.r[0].err, TCE_BOUNDS);
+    return;
+  }
+  auto decode = [&](int w, int& m, int& bx, int& by, int& bz) {
+    int lo = 0, hi = a.nm - 1;  // the last member whose first unit is <= w
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.st[mid] <= w) lo = mid; else hi = mid - 1;
+    }
+    m = lo;
+    int l = w - a.st[m];
+    bz = l % a.r[m].tnz;
+    l /= a.r[m].tnz;
+    by = l % a.r[m].tny;
+    bx = l / a.r[m].tny;
+  };
+  auto issue = [&](int w) {  // one thread
+    int m, bx, by, bz;
+    decode(w, m, bx, by, bz);
+    rhs_tma_issue<T, KB, 1>(buf, &bar[0], &a.map[m][0], &a.map[m][1], &a.map[m][2], bx, by, bz);
+  };
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0) issue(u0 + blockIdx.x);
+  int it = 0;
+  for (int w = u0 + blockIdx.x; w < u1; w += gridDim.x, ++it) {
+    int m, bx, by, bz;
+    decode(w, m, bx, by, bz);
+    const BRhsRec<T>& b = a.r[m];
+    const T forcing = (UPD == UPD_AB2) ? (T)(*b.forcing) : T(0);
+    if (!rhs_tma_tile<T, FULL, UPD, KB, 1>(b.g, b.A[0], b.A[1], b.A[2], b.B[0], b.B[1], b.B[2], b.R[0], b.R[1],
+                                           b.R[2], forcing, b.dt, UPD == UPD_FE ? 0 : b.have_hist, bx, by, bz, buf,
+                                           &bar[0], (unsigned)it & 1u, pre, b.err, nullptr, 0u))
+      return;
+    __syncthreads();  // the stage and the constants are free for the next unit
+    if (tid == 0 && w + (int)gridDim.x < u1) issue(w + gridDim.x);
   }
 }
 

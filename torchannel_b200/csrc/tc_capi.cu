@@ -2284,6 +2284,9 @@ struct tc_batch {
   std::vector<int> cur0;
   int q;                     // steps since the tables were built, mod 2
   int total[BK_COUNT], grid[BK_COUNT];
+  int rhs_tma;               // the RHS stages its tiles by tensor copies (kb_rhs_tma)
+  std::vector<BatchRhsArgs<float>> rargs_f[3];   // kb_rhs_tma parameters of tables 0, 1, 2, one per member group
+  std::vector<BatchRhsArgs<double>> rargs_d[3];
   int cn_y, cn_maxt, nmax, fy_tile;
   size_t smem_cn, smem_fx, smem_ifx, smem_fy;
   int graphs_on;
@@ -2291,6 +2294,15 @@ struct tc_batch {
   cudaGraphExec_t gexec;
   int g_valid, g_scheme, g_q;
 };
+
+// Whether the ensemble's RHS stages its tiles by tensor copies (kb_rhs_tma):
+// every member has its tensor-copy RHS on in the default tile shape, the
+// shape of its tensor maps' boxes.  Otherwise kb_rhs runs.
+static bool batch_tma_ok(const tc_batch* b) {
+  for (const tc_ctx* c : b->m)
+    if (!c->rhs_tma_ok || !c->rhs_tma_on || c->rhs_tma_mode != 1) return false;
+  return true;
+}
 
 static bool batch_grid_ok(const tc_ctx* c) {
   return c->nx % 16 == 0 && c->ny % 16 == 0 && batch_n1_ok(c->nx / 16) && batch_n1_ok(c->ny / 16) &&
@@ -2400,6 +2412,7 @@ static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int sche
   r.rgx = (c->nx + RHS_TX - 1) / RHS_TX;
   r.rgy = (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>();
   r.rgz = (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>();
+  rhs_tma_tiles(c->nx, c->ny, c->nz, BatchRhsTmaShape<T>::KB, &r.tnx, &r.tny, &r.tnz);
   const int V = batch_cn_vec<T>(L);
   r.cgx = (c->nx * c->ny / V + 31) / 32;
   r.cn_lr = Lr;
@@ -2409,8 +2422,8 @@ static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int sche
   return r;
 }
 
-template <class T> static void batch_units(const BMember<T>& r, const tc_ctx* c, int cnt[BK_COUNT]) {
-  cnt[BK_RHS] = r.rgx * r.rgy * r.rgz;
+template <class T> static void batch_units(const BMember<T>& r, const tc_ctx* c, bool tma, int cnt[BK_COUNT]) {
+  cnt[BK_RHS] = tma ? r.tnx * r.tny * r.tnz : r.rgx * r.rgy * r.rgz;
   cnt[BK_CN] = 3 * r.cgx;
   cnt[BK_FX] = r.xgx * r.xpg;
   cnt[BK_FY] = (r.nrows + 1) / 2;
@@ -2458,8 +2471,21 @@ template <class T> static int batch_shapes(tc_batch* b, int scheme) {
   if (rc) return rc;
   rc = b->nmax == 8 ? batch_fft_shapes<T, 8>(b) : batch_fft_shapes<T, 16>(b);
   if (rc) return rc;
+  if (b->rhs_tma) {
+    using B = BatchRhsTmaShape<T>;
+    const int sm = (int)B::smem();
+    auto k0 = kb_rhs_tma<T, false, UPD_AB2>, k1 = kb_rhs_tma<T, true, UPD_AB2>, k2 = kb_rhs_tma<T, true, UPD_FE>;
+    TC_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    TC_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    TC_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    rc = batch_grid<T>(b, scheme == TC_IMEX ? k0 : scheme == TC_AB2 ? k1 : k2, RHS_TX * B::S::TY, sm,
+                       b->total[BK_RHS], &b->grid[BK_RHS]);
+    if (rc) return rc;
+  }
   const int rthr = RHS_TX * rhs_ty<T>();
-  if (scheme == TC_IMEX)
+  if (b->rhs_tma)
+    rc = TC_OK;
+  else if (scheme == TC_IMEX)
     rc = batch_grid<T>(b, kb_rhs<T, false, UPD_AB2>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
   else if (scheme == TC_AB2)
     rc = batch_grid<T>(b, kb_rhs<T, true, UPD_AB2>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
@@ -2468,6 +2494,45 @@ template <class T> static int batch_shapes(tc_batch* b, int scheme) {
   if (!rc) rc = batch_grid<T>(b, kb_tri<T>, 64, 0, b->total[BK_TRI], &b->grid[BK_TRI]);
   if (!rc) rc = batch_grid<T>(b, kb_proj<T>, 256, 0, b->total[BK_PROJ], &b->grid[BK_PROJ]);
   return rc;
+}
+
+template <class T> static std::vector<BatchRhsArgs<T>>* batch_rargs(tc_batch* b) {
+  if constexpr (sizeof(T) == 8)
+    return b->rargs_d;
+  else
+    return b->rargs_f;
+}
+
+// Parameters of kb_rhs_tma for the three tables (tab: 3 n member records
+// with their first units): per group of TC_BATCH_TMA_GROUP members, each
+// member's tensor maps of the parity its table reads (tables 0 and 2: the
+// current state, table 1: the other buffer set) and what its tiles read.
+template <class T> static void batch_rhs_args(tc_batch* b, const std::vector<BMember<T>>& tab) {
+  const int n = b->n, ng = (n + TC_BATCH_TMA_GROUP - 1) / TC_BATCH_TMA_GROUP;
+  std::vector<BatchRhsArgs<T>>* ra = batch_rargs<T>(b);
+  for (int t = 0; t < 3; ++t) {
+    ra[t].assign(ng, BatchRhsArgs<T>());
+    for (int i = 0; i < n; ++i) {
+      BatchRhsArgs<T>& a = ra[t][i / TC_BATCH_TMA_GROUP];
+      const int k = i % TC_BATCH_TMA_GROUP;
+      const BMember<T>& r = tab[(size_t)t * n + i];
+      const tc_ctx* c = b->m[i];
+      const int par = t == 1 ? c->cur ^ 1 : c->cur;
+      for (int f = 0; f < 3; ++f) a.map[k][f] = c->tmap[par][f];
+      BRhsRec<T>& q = a.r[k];
+      q.g = r.g;
+      for (int f = 0; f < 3; ++f) { q.A[f] = r.A[f]; q.B[f] = r.B[f]; q.R[f] = r.R[f]; }
+      q.forcing = r.forcing;
+      q.err = c->err;
+      q.dt = r.dt;
+      q.have_hist = r.have_hist;
+      q.tny = r.tny;
+      q.tnz = r.tnz;
+      a.st[k] = r.u0[BK_RHS];
+      a.st[k + 1] = r.u0[BK_RHS] + r.tnx * r.tny * r.tnz;
+      a.nm = k + 1;
+    }
+  }
 }
 
 template <class T> static int batch_build_impl(tc_batch* b, int scheme, const double* dts, cudaStream_t s) {
@@ -2481,6 +2546,7 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   // for every member; a member's chunks are L rows, like a single-channel
   // step's, and the warps beyond its last chunk idle
   const int maxchunks = (maxnz + L - 1) / L;
+  b->rhs_tma = batch_tma_ok(b) ? 1 : 0;
   size_t fx = 0, ifx = 0;
   int fyt = 0;
   for (int i = 0; i < n; ++i) {
@@ -2501,7 +2567,7 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
     tab[n + i] = batch_record<T>(c, c->cur ^ 1, dts[i], 1, scheme, L, Lr);
     tab[2 * n + i] = batch_record<T>(c, c->cur, dts[i], hist, scheme, L, Lr);
     int cnt[BK_COUNT];
-    batch_units<T>(tab[i], c, cnt);
+    batch_units<T>(tab[i], c, b->rhs_tma != 0, cnt);
     for (int k = 0; k < BK_COUNT; ++k) {
       tab[i].u0[k] = tab[n + i].u0[k] = tab[2 * n + i].u0[k] = run[k];
       run[k] += cnt[k];
@@ -2514,6 +2580,7 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
     for_each_n1(c->ny, [&](auto I) { fyt = std::max(fyt, RowFft<decltype(I)::value>::TILE); });
   }
   for (int k = 0; k < BK_COUNT; ++k) b->total[k] = run[k];
+  if (b->rhs_tma) batch_rhs_args<T>(b, tab);
   const int V = L == 16 ? VL16 : 1;
   b->cn_y = maxchunks;
   b->smem_cn = (size_t)(9 * maxnz + 2 * maxchunks * 32 * V) * 8;
@@ -2552,7 +2619,19 @@ template <class T> static int batch_step_impl(tc_batch* b, int scheme, int ti, c
   const BMember<T>* M = reinterpret_cast<const BMember<T>*>(b->table) + (size_t)ti * b->n;
   const int n = b->n;
   const dim3 rb(RHS_TX, rhs_ty<T>());
-  if (scheme == TC_IMEX)
+  if (b->rhs_tma) {
+    const dim3 tb(RHS_TX, BatchRhsTmaShape<T>::S::TY);
+    const size_t sm = BatchRhsTmaShape<T>::smem();
+    for (const BatchRhsArgs<T>& a : batch_rargs<T>(b)[ti]) {  // one launch per member group
+      const int gr = std::max(1, std::min(b->grid[BK_RHS], a.st[a.nm] - a.st[0]));
+      if (scheme == TC_IMEX)
+        kb_rhs_tma<T, false, UPD_AB2><<<gr, tb, sm, s>>>(a);
+      else if (scheme == TC_AB2)
+        kb_rhs_tma<T, true, UPD_AB2><<<gr, tb, sm, s>>>(a);
+      else
+        kb_rhs_tma<T, true, UPD_FE><<<gr, tb, sm, s>>>(a);
+    }
+  } else if (scheme == TC_IMEX)
     kb_rhs<T, false, UPD_AB2><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
   else if (scheme == TC_AB2)
     kb_rhs<T, true, UPD_AB2><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
@@ -2620,6 +2699,7 @@ extern "C" int tc_batch_step(tc_batch* b, int scheme, const double* dts, int n_s
     if (c->body[0] || c->ke_acc || c->tape) return fail(TC_ERR_ARG, "ensemble launches take no adjoint hooks");
     if (c->psp_on) return fail(TC_ERR_ARG, "ensemble launches take no single-precision Poisson members");
     if (b->valid && (b->dts[i] != dts[i] || c->cur != (b->cur0[i] ^ b->q))) rebuild = true;
+    if (b->valid && b->rhs_tma != (batch_tma_ok(b) ? 1 : 0)) rebuild = true;
     if (scheme == TC_IMEX && c->tab_dt != dts[i]) rebuild = true;
     lack = lack || (scheme != TC_FE && !c->have_hist);
   }

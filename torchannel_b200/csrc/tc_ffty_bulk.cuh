@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128, YBulk<N1>::MINB) k_ffty_bulk(cpx<double>*
   using B = YBulk<N1>;
   using RF = typename B::RF;
   constexpr int N = B::N, R = B::R, SP = B::SP;
-  extern __shared__ __align__(128) unsigned char smraw[];
+  extern __shared__ __align__(16) unsigned char smraw[];  // 128-byte alignment checked below
   cpx<double>* stages = reinterpret_cast<cpx<double>*>(smraw);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + B::NST * B::STAGE);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
