@@ -23,11 +23,15 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 #define TC_BATCH_MAX 64  // members per ensemble launch
 
 // Register allocation of the unit loops.  Inlining every transform length
-// into one switch makes the x transform spill heavily, so that tile is a
-// called function (TC_BATCH_FX_CALL) over TC_BATCH_XP planes per unit (the
-// call's register saves are paid once per group).  The other loops inline
-// their tiles under occupancy-driven register caps (minimum resident blocks
-// per SM below).
+// into one switch makes the forward x transform spill heavily, so that tile
+// is a called function (TC_BATCH_FX_CALL) over TC_BATCH_XP planes per unit
+// (the call's register saves are paid once per group; consecutive planes
+// reuse the w plane above in L1).  The inverse x transform runs one launch
+// per transform length (kb_ifftx_n: the registers of that length alone), one
+// CTA per unit (a row block of a plane), as the single-channel kernel: a
+// persistent unit loop around the same tile took 128-192 registers, and
+// capped at 96 it spilled.  The other loops inline their tiles under
+// occupancy-driven register caps (minimum resident blocks per SM below).
 #ifndef TC_BATCH_FX_CALL
 #define TC_BATCH_FX_CALL __noinline__
 #endif
@@ -240,8 +244,9 @@ __global__ void __launch_bounds__(MAXT, TC_BATCH_CN_CAP ? (sizeof(T) == 4 && VEC
 
 // Register-FFT lengths of the ensemble kernels: N = 16 N1, N1 in {4, 6, 8, 12, 16}
 // (64 .. 256 points), all with two rows per warp (128-thread x blocks).  The
-// FFT kernels come in two sets, NMAX = 8 (every member's N1 <= 8) and
-// NMAX = 16, since a kernel's registers are those of its longest transform.
+// forward x and the y transforms come in two sets, NMAX = 8 (every member's
+// N1 <= 8) and NMAX = 16, since a kernel's registers are those of its longest
+// transform; the inverse x transform takes one launch per length.
 __host__ __device__ constexpr bool batch_n1_ok(int n1) { return n1 == 4 || n1 == 6 || n1 == 8 || n1 == 12 || n1 == 16; }
 
 template <int NMAX, class F> __device__ __forceinline__ void batch_n1_switch(int n1, F&& f) {
@@ -271,15 +276,36 @@ __device__ TC_BATCH_FX_CALL void batch_fftx_call(const BMember<T>* __restrict__ 
     fftx_tile<T, N1, XROWS>(b.g, b.B[0], b.B[1], b.B[2], nullptr, b.X, b.twx, b.scale, bx, k);
   }
 }
-template <class T, int N1>
-__device__ __forceinline__ void batch_ifftx_call(const BMember<T>* __restrict__ bp, int bx, int k) {
-  const BMember<T>& b = *bp;
-  ifftx_tile<N1, XROWS>(b.X, b.p, b.g.ny, b.g.nz, b.twx, bx, k);
-}
 template <class T, int N1, bool INV>
 __device__ __forceinline__ void batch_ffty_call(const BMember<T>* __restrict__ bp, int row0, cpx<double>* tiles) {
   const BMember<T>& b = *bp;
   ffty_rows<N1, INV>(b.X, b.nrows, b.twy, row0, tiles);
+}
+
+// The inverse x transforms of the members whose nx is 16 N1, one launch per
+// N1.  What the transform reads of a member travels in the launch's
+// __grid_constant__ parameter (uniform loads, no per-thread registers).
+template <class T> struct BXRec {
+  Grid<T> g;
+  cpx<double>* X;
+  const cpx<double>* twx;
+  double* p;
+  int xgx;        // row blocks per plane
+};
+template <class T> struct BatchXArgs {
+  BXRec<T> r[TC_BATCH_MAX];
+  int st[TC_BATCH_MAX + 1];  // first unit (row block, plane) of each member of the class, then the end
+  int n;
+};
+static_assert(sizeof(BatchXArgs<double>) + 64 <= 32764, "kernel parameter limit");
+
+__device__ __forceinline__ int batch_class_member(const int* st, int n, int w) {
+  int lo = 0, hi = n - 1;  // the last member whose first unit is <= w
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (st[mid] <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
 }
 
 template <class T, int NMAX>
@@ -326,17 +352,14 @@ __global__ void __launch_bounds__(64, TC_BATCH_TRI_MINB) kb_tri(const BMember<T>
   }
 }
 
-template <class T, int NMAX>
-__global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_ifftx(const BMember<T>* __restrict__ M, int nm, int total) {
-  __shared__ int st[TC_BATCH_MAX + 1];
-  batch_starts(M, nm, BK_IFX, total, st);
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    const int m = batch_member(st, nm, w);
-    const BMember<T>& b = M[m];
-    const int l = w - st[m];
-    batch_n1_switch<NMAX>(b.n1x, [&](auto I) { batch_ifftx_call<T, decltype(I)::value>(&b, l % b.xgx, l / b.xgx); });
-    __syncthreads();
-  }
+template <class T, int N1>
+__global__ void __launch_bounds__(128) kb_ifftx_n(const __grid_constant__ BatchXArgs<T> a) {
+  const int w = blockIdx.x;
+  if (w >= a.st[a.n]) return;
+  const int m = batch_class_member(a.st, a.n, w);
+  const BXRec<T>& b = a.r[m];
+  const int l = w - a.st[m];
+  ifftx_tile<N1, XROWS>(b.X, b.p, b.g.ny, b.g.nz, b.twx, l % b.xgx, l / b.xgx);
 }
 
 // The member's last block (atomic ticket, per member) reduces its partials

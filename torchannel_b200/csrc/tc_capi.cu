@@ -2288,7 +2288,11 @@ struct tc_batch {
   std::vector<BatchRhsArgs<float>> rargs_f[3];   // kb_rhs_tma parameters of tables 0, 1, 2, one per member group
   std::vector<BatchRhsArgs<double>> rargs_d[3];
   int cn_y, cn_maxt, nmax, fy_tile;
-  size_t smem_cn, smem_fx, smem_ifx, smem_fy;
+  size_t smem_cn, smem_fx, smem_fy;
+  std::vector<int> xcls;     // x-transform lengths N1 of the members, one inverse launch each
+  std::vector<int> xgrid_i;  // CTAs of each class's inverse launch
+  std::vector<BatchXArgs<float>> xargs_f;   // kb_ifftx_n parameters per class
+  std::vector<BatchXArgs<double>> xargs_d;
   int graphs_on;
   cudaStream_t cap_stream;
   cudaGraphExec_t gexec;
@@ -2452,15 +2456,78 @@ template <class T, int L, int MAXT> static int batch_cn_shape(tc_batch* b) {
   TC_CUDA(cudaFuncSetAttribute(kb_cn<T, L, V, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_cn));
   return batch_grid<T>(b, kb_cn<T, L, V, MAXT>, 32 * b->cn_y, b->smem_cn, b->total[BK_CN], &b->grid[BK_CN]);
 }
+template <class F> static void batch_n1_host(int n1, F&& f) {
+  switch (n1) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 12: f(std::integral_constant<int, 12>{}); break;
+    default: f(std::integral_constant<int, 16>{}); break;
+  }
+}
+template <class T> static std::vector<BatchXArgs<T>>& batch_xargs(tc_batch* b) {
+  if constexpr (sizeof(T) == 8)
+    return b->xargs_d;
+  else
+    return b->xargs_f;
+}
 template <class T, int NMAX> static int batch_fft_shapes(tc_batch* b) {
   TC_CUDA(cudaFuncSetAttribute(kb_fftx<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fx));
-  TC_CUDA(cudaFuncSetAttribute(kb_ifftx<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_ifx));
   TC_CUDA(cudaFuncSetAttribute(kb_ffty<T, NMAX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fy));
   TC_CUDA(cudaFuncSetAttribute(kb_ffty<T, NMAX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fy));
   int rc = batch_grid<T>(b, kb_fftx<T, NMAX>, 128, b->smem_fx, b->total[BK_FX], &b->grid[BK_FX]);
   if (!rc) rc = batch_grid<T>(b, kb_ffty<T, NMAX, false>, 128, b->smem_fy, (b->total[BK_FY] + 3) / 4, &b->grid[BK_FY]);
-  if (!rc) rc = batch_grid<T>(b, kb_ifftx<T, NMAX>, 128, b->smem_ifx, b->total[BK_IFX], &b->grid[BK_IFX]);
+  // inverse x transform: one launch per length class, one CTA per unit (the
+  // grids add up in the info)
+  const std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b);
+  const int nc = (int)b->xcls.size();
+  b->xgrid_i.assign(nc, 1);
+  b->grid[BK_IFX] = 0;
+  for (int c = 0; c < nc && !rc; ++c)
+    batch_n1_host(b->xcls[c], [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      if (cudaFuncSetAttribute(kb_ifftx_n<T, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ifftx_reg_smem<N1>()) != cudaSuccess) {
+        rc = fail(TC_ERR_CUDA, "ensemble inverse x transform attributes");
+        return;
+      }
+      b->xgrid_i[c] = std::max(1, xa[c].st[xa[c].n]);
+      b->grid[BK_IFX] += b->xgrid_i[c];
+    });
   return rc;
+}
+
+// Parameters of the inverse x-transform class launches (the same for every
+// table: the transform reads the spectrum and writes the pressure): the
+// members of each length N1 (ascending) with their first units.
+template <class T> static void batch_x_args(tc_batch* b, const std::vector<BMember<T>>& tab) {
+  const int n = b->n;
+  b->xcls.clear();
+  for (int i = 0; i < n; ++i) {
+    const int n1 = b->m[i]->nx / 16;
+    if (std::find(b->xcls.begin(), b->xcls.end(), n1) == b->xcls.end()) b->xcls.push_back(n1);
+  }
+  std::sort(b->xcls.begin(), b->xcls.end());
+  std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b);
+  xa.assign(b->xcls.size(), BatchXArgs<T>());
+  for (size_t c = 0; c < b->xcls.size(); ++c) {
+    BatchXArgs<T>& a = xa[c];
+    a.n = 0;
+    a.st[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      const tc_ctx* ctx = b->m[i];
+      if (ctx->nx / 16 != b->xcls[c]) continue;
+      const BMember<T>& r = tab[i];
+      BXRec<T>& q = a.r[a.n];
+      q.g = r.g;
+      q.X = r.X;
+      q.twx = r.twx;
+      q.p = r.p;
+      q.xgx = r.xgx;
+      a.st[a.n + 1] = a.st[a.n] + r.xgx * ctx->nz;
+      ++a.n;
+    }
+  }
 }
 template <class T> static int batch_shapes(tc_batch* b, int scheme) {
   int rc;
@@ -2547,7 +2614,7 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   // step's, and the warps beyond its last chunk idle
   const int maxchunks = (maxnz + L - 1) / L;
   b->rhs_tma = batch_tma_ok(b) ? 1 : 0;
-  size_t fx = 0, ifx = 0;
+  size_t fx = 0;
   int fyt = 0;
   for (int i = 0; i < n; ++i) {
     tc_ctx* c = b->m[i];
@@ -2572,19 +2639,16 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
       tab[i].u0[k] = tab[n + i].u0[k] = tab[2 * n + i].u0[k] = run[k];
       run[k] += cnt[k];
     }
-    for_each_n1(c->nx, [&](auto I) {
-      constexpr int N1 = decltype(I)::value;
-      fx = std::max(fx, fftx_reg_smem<N1>());
-      ifx = std::max(ifx, ifftx_reg_smem<N1>());
-    });
+    for_each_n1(c->nx, [&](auto I) { fx = std::max(fx, fftx_reg_smem<decltype(I)::value>()); });
     for_each_n1(c->ny, [&](auto I) { fyt = std::max(fyt, RowFft<decltype(I)::value>::TILE); });
   }
   for (int k = 0; k < BK_COUNT; ++k) b->total[k] = run[k];
   if (b->rhs_tma) batch_rhs_args<T>(b, tab);
+  batch_x_args<T>(b, tab);
   const int V = L == 16 ? VL16 : 1;
   b->cn_y = maxchunks;
+  b->smem_fx = fx;
   b->smem_cn = (size_t)(9 * maxnz + 2 * maxchunks * 32 * V) * 8;
-  b->smem_fx = fx; b->smem_ifx = ifx;
   b->fy_tile = fyt;
   b->smem_fy = (size_t)4 * 2 * fyt * sizeof(cpx<double>);
   b->cn_maxt = 32 * b->cn_y <= 256 ? 256 : 512;
@@ -2605,13 +2669,19 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   return TC_OK;
 }
 
-template <class T, int NMAX> static void batch_poisson(const tc_batch* b, const BMember<T>* M, cudaStream_t s) {
+template <class T, int NMAX>
+static void batch_poisson(tc_batch* b, const BMember<T>* M, cudaStream_t s) {
   const int n = b->n;
   kb_fftx<T, NMAX><<<b->grid[BK_FX], 128, b->smem_fx, s>>>(M, n, b->total[BK_FX]);
   kb_ffty<T, NMAX, false><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
   kb_tri<T><<<b->grid[BK_TRI], 64, 0, s>>>(M, n, b->total[BK_TRI]);
   kb_ffty<T, NMAX, true><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
-  kb_ifftx<T, NMAX><<<b->grid[BK_IFX], 128, b->smem_ifx, s>>>(M, n, b->total[BK_IFX]);
+  const std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b);
+  for (size_t c = 0; c < xa.size(); ++c)
+    batch_n1_host(b->xcls[c], [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      kb_ifftx_n<T, N1><<<b->xgrid_i[c], 128, ifftx_reg_smem<N1>(), s>>>(xa[c]);
+    });
 }
 
 // One step of every member with table `ti` (0, 1: parity; 2: first step).
