@@ -25,13 +25,14 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 // Register allocation of the unit loops.  Inlining every transform length
 // into one switch makes the forward x transform spill heavily, so that tile
 // is a called function (TC_BATCH_FX_CALL) over TC_BATCH_XP planes per unit
-// (the call's register saves are paid once per group; consecutive planes
-// reuse the w plane above in L1).  The inverse x transform runs one launch
-// per transform length (kb_ifftx_n: the registers of that length alone), one
-// CTA per unit (a row block of a plane), as the single-channel kernel: a
-// persistent unit loop around the same tile took 128-192 registers, and
-// capped at 96 it spilled.  The other loops inline their tiles under
-// occupancy-driven register caps (minimum resident blocks per SM below).
+// (the call's register saves are paid once per group; split into one launch
+// per length with one plane a CTA it measured slower).  The inverse x
+// transform runs one launch per transform length (kb_ifftx_n: the registers
+// of that length alone), one CTA per unit (a row block of a plane), as the
+// single-channel kernel: a persistent unit loop around the same tile took
+// 128-192 registers, and capped at 96 it spilled.  The other loops inline
+// their tiles under occupancy-driven register caps (minimum resident blocks
+// per SM below).
 #ifndef TC_BATCH_FX_CALL
 #define TC_BATCH_FX_CALL __noinline__
 #endif
