@@ -36,9 +36,6 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 #ifndef TC_BATCH_FX_CALL
 #define TC_BATCH_FX_CALL __noinline__
 #endif
-#ifndef TC_BATCH_CN_CALL
-#define TC_BATCH_CN_CALL __forceinline__
-#endif
 #ifndef TC_BATCH_FFT_MINB
 #define TC_BATCH_FFT_MINB 4
 #endif
@@ -53,10 +50,6 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 #endif
 #ifndef TC_BATCH_XP
 #define TC_BATCH_XP 4
-#endif
-#ifndef TC_BATCH_CN_CAP
-#define TC_BATCH_CN_CAP 1  // CN: cap at 128 registers (two 256-thread blocks per SM); FP32 two
-                           // columns a thread: three 256-thread blocks (fewer spill)
 #endif
 
 template <class T> struct BMember {
@@ -89,6 +82,17 @@ template <class T> struct BMember {
   int pgx, pgy, pgz;       // block grid of k_project_bulk
   int u0[BK_COUNT];        // first unit of the member in each launch
 };
+
+// Member of a class launch owning unit w: the last k with st[k] <= w
+// (binary search over the launch parameter's first units).
+__device__ __forceinline__ int batch_class_member(const int* st, int n, int w) {
+  int lo = 0, hi = n - 1;  // the last member whose first unit is <= w
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (st[mid] <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
 
 // Stage the members' first units of launch K (and the total) in shared memory.
 template <class T>
@@ -222,25 +226,41 @@ __global__ void __launch_bounds__(RHS_TX * 8, BatchRhsTmaShape<T>::MINB)
   }
 }
 
-template <class T, int L, int VEC>
-__device__ TC_BATCH_CN_CALL void batch_cn_call(const BMember<T>* __restrict__ bp, int bx, int comp) {
-  const BMember<T>& b = *bp;
-  // every member's chunks are L rows (its tables' length), so the chunk
-  // length is a compile-time constant here as in k_cn_solve
-  cn_tile<T, L, VEC, true>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.g.nx, b.g.ny, b.g.nz, bx, comp, L);
-}
+// CN of the members whose chunk count (nz over L-row chunks) is the same, one
+// launch per chunk count: the block is (32, chunks) as in k_cn_solve, so no
+// warp idles for a shallower member, one CTA per unit (component, column
+// block), and what the tile reads of a member travels in the launch's
+// __grid_constant__ parameter.  Every member's chunks are L rows (its
+// tables' length), a compile-time constant as in k_cn_solve.
+template <class T> struct BCnRec {
+  T* B[3];  // u*, v*, w*, solved in place
+  CnTab tab;
+  const double* ubase;
+  int nx, ny, nz, cgx;  // cgx: column blocks per component
+};
+template <class T> struct BatchCnArgs {
+  BCnRec<T> r[TC_BATCH_MAX];
+  int st[TC_BATCH_MAX + 1];  // first unit of each member of the class, then the end
+  int n;
+};
+static_assert(sizeof(BatchCnArgs<double>) + 64 <= 32764, "kernel parameter limit");
 
-// blockDim = (32, chunks of the deepest member) <= MAXT threads
-template <class T, int L, int VEC, int MAXT>
-__global__ void __launch_bounds__(MAXT, TC_BATCH_CN_CAP ? (sizeof(T) == 4 && VEC == 2 ? 768 : 512) / MAXT : 1) kb_cn(const BMember<T>* __restrict__ M, int nm, int total) {
-  __shared__ int st[TC_BATCH_MAX + 1];
-  batch_starts(M, nm, BK_CN, total, st);
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    const int m = batch_member(st, nm, w);
-    const int l = w - st[m];
-    batch_cn_call<T, L, VEC>(M + m, l % M[m].cgx, l / M[m].cgx);
-    __syncthreads();
-  }
+template <class T, int L, int VEC> __device__ __forceinline__ void batch_cn_unit(const BatchCnArgs<T>& a) {
+  const int w = blockIdx.x;
+  if (w >= a.st[a.n]) return;
+  const int m = batch_class_member(a.st, a.n, w);
+  const BCnRec<T>& b = a.r[m];
+  const int l = w - a.st[m];
+  cn_tile<T, L, VEC, true>(b.B[0], b.B[1], b.B[2], b.tab, b.ubase, b.nx, b.ny, b.nz, l % b.cgx, l / b.cgx, L);
+}
+// FP32 storage, 16-row chunks: the packed sweeps under k_cn_solve_pk's bound
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT) kb_cn_pk(const __grid_constant__ BatchCnArgs<float> a) {
+  batch_cn_unit<float, 16, 2>(a);
+}
+template <class T, int L, int MAXT>
+__global__ void __launch_bounds__(MAXT) kb_cn_n(const __grid_constant__ BatchCnArgs<T> a) {
+  batch_cn_unit<T, L, 1>(a);
 }
 
 // Register-FFT lengths of the ensemble kernels: N = 16 N1, N1 in {4, 6, 8, 12, 16}
@@ -299,15 +319,6 @@ template <class T> struct BatchXArgs {
   int n;
 };
 static_assert(sizeof(BatchXArgs<double>) + 64 <= 32764, "kernel parameter limit");
-
-__device__ __forceinline__ int batch_class_member(const int* st, int n, int w) {
-  int lo = 0, hi = n - 1;  // the last member whose first unit is <= w
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (st[mid] <= w) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
 
 template <class T, int NMAX>
 __global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_fftx(const BMember<T>* __restrict__ M, int nm, int total) {

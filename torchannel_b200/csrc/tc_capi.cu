@@ -2287,8 +2287,12 @@ struct tc_batch {
   int rhs_tma;               // the RHS stages its tiles by tensor copies (kb_rhs_tma)
   std::vector<BatchRhsArgs<float>> rargs_f[3];   // kb_rhs_tma parameters of tables 0, 1, 2, one per member group
   std::vector<BatchRhsArgs<double>> rargs_d[3];
-  int cn_y, cn_maxt, nmax, fy_tile;
-  size_t smem_cn, smem_fx, smem_fy;
+  int cn_y, nmax, fy_tile;   // cn_y: CN chunks of the deepest member
+  size_t smem_fx, smem_fy;
+  std::vector<int> ccls;     // CN chunk counts of the members, one launch each
+  std::vector<int> cmaxnz, cgrid;    // deepest member and CTAs of each CN class
+  std::vector<BatchCnArgs<float>> cargs_f[3];   // kb_cn_pk / kb_cn_n parameters of tables 0, 1, 2 per class
+  std::vector<BatchCnArgs<double>> cargs_d[3];
   std::vector<int> xcls;     // x-transform lengths N1 of the members, one inverse launch each
   std::vector<int> xgrid_i;  // CTAs of each class's inverse launch
   std::vector<BatchXArgs<float>> xargs_f;   // kb_ifftx_n parameters per class
@@ -2451,10 +2455,86 @@ template <class T, class K> static int batch_grid(const tc_batch* b, K kernel, i
 }
 
 // Shared-memory opt-in and persistent grid of every ensemble kernel.
-template <class T, int L, int MAXT> static int batch_cn_shape(tc_batch* b) {
-  constexpr int V = batch_cn_vec<T>(L);
-  TC_CUDA(cudaFuncSetAttribute(kb_cn<T, L, V, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_cn));
-  return batch_grid<T>(b, kb_cn<T, L, V, MAXT>, 32 * b->cn_y, b->smem_cn, b->total[BK_CN], &b->grid[BK_CN]);
+template <class T> static std::vector<BatchCnArgs<T>>* batch_cargs(tc_batch* b) {
+  if constexpr (sizeof(T) == 8)
+    return b->cargs_d;
+  else
+    return b->cargs_f;
+}
+// The CN kernel of chunk length L for blocks of `threads` threads.
+template <class T, class F> static void batch_cn_kernel(int L, int threads, F&& f) {
+  if (L == 16) {
+    if constexpr (sizeof(T) == 4) {
+      if (threads <= 256) f(kb_cn_pk<256>); else f(kb_cn_pk<512>);
+    } else {
+      if (threads <= 256) f(kb_cn_n<T, 16, 256>); else f(kb_cn_n<T, 16, 512>);
+    }
+  } else {
+    if (threads <= 256) f(kb_cn_n<T, 32, 256>); else f(kb_cn_n<T, 32, 512>);
+  }
+}
+template <class T> static size_t batch_cn_smem(int L, int chunks, int maxnz) {
+  return (size_t)(9 * maxnz + 2 * chunks * 32 * batch_cn_vec<T>(L)) * 8;
+}
+// Shared-memory opt-in of each CN class's kernel; one CTA per unit.
+template <class T> static int batch_cn_shapes(tc_batch* b) {
+  const std::vector<BatchCnArgs<T>>& ca = batch_cargs<T>(b)[0];
+  const int nc = (int)b->ccls.size();
+  b->cgrid.assign(nc, 1);
+  b->grid[BK_CN] = 0;
+  int rc = TC_OK;
+  for (int c = 0; c < nc && !rc; ++c) {
+    const int ch = b->ccls[c];
+    const size_t sm = batch_cn_smem<T>(b->cn_L, ch, b->cmaxnz[c]);
+    batch_cn_kernel<T>(b->cn_L, 32 * ch, [&](auto k) {
+      int occ = 0;
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * ch, sm) != cudaSuccess || occ < 1)
+        rc = fail(TC_ERR_SIZE, "ensemble CN block does not fit on an SM");
+    });
+    b->cgrid[c] = std::max(1, ca[c].st[ca[c].n]);
+    b->grid[BK_CN] += b->cgrid[c];
+  }
+  return rc;
+}
+
+// Parameters of the CN class launches for the three tables: the members of
+// each chunk count (ascending) with their first units (component, column
+// block; column blocks fastest).
+template <class T> static void batch_cn_args(tc_batch* b, const std::vector<BMember<T>>& tab) {
+  const int n = b->n, L = b->cn_L;
+  b->ccls.clear();
+  for (int i = 0; i < n; ++i) {
+    const int ch = (b->m[i]->nz + L - 1) / L;
+    if (std::find(b->ccls.begin(), b->ccls.end(), ch) == b->ccls.end()) b->ccls.push_back(ch);
+  }
+  std::sort(b->ccls.begin(), b->ccls.end());
+  b->cmaxnz.assign(b->ccls.size(), 0);
+  std::vector<BatchCnArgs<T>>* ca = batch_cargs<T>(b);
+  for (int t = 0; t < 3; ++t) {
+    ca[t].assign(b->ccls.size(), BatchCnArgs<T>());
+    for (size_t c = 0; c < b->ccls.size(); ++c) {
+      BatchCnArgs<T>& a = ca[t][c];
+      a.n = 0;
+      a.st[0] = 0;
+      for (int i = 0; i < n; ++i) {
+        const tc_ctx* ctx = b->m[i];
+        if ((ctx->nz + L - 1) / L != b->ccls[c]) continue;
+        const BMember<T>& r = tab[(size_t)t * n + i];
+        BCnRec<T>& q = a.r[a.n];
+        for (int f = 0; f < 3; ++f) q.B[f] = r.B[f];
+        q.tab = r.tab;
+        q.ubase = r.ubase;
+        q.nx = ctx->nx;
+        q.ny = ctx->ny;
+        q.nz = ctx->nz;
+        q.cgx = r.cgx;
+        a.st[a.n + 1] = a.st[a.n] + 3 * r.cgx;
+        ++a.n;
+        b->cmaxnz[c] = std::max(b->cmaxnz[c], ctx->nz);
+      }
+    }
+  }
 }
 template <class F> static void batch_n1_host(int n1, F&& f) {
   switch (n1) {
@@ -2530,11 +2610,7 @@ template <class T> static void batch_x_args(tc_batch* b, const std::vector<BMemb
   }
 }
 template <class T> static int batch_shapes(tc_batch* b, int scheme) {
-  int rc;
-  if (b->cn_L == 16)
-    rc = b->cn_maxt == 256 ? batch_cn_shape<T, 16, 256>(b) : batch_cn_shape<T, 16, 512>(b);
-  else
-    rc = b->cn_maxt == 256 ? batch_cn_shape<T, 32, 256>(b) : batch_cn_shape<T, 32, 512>(b);
+  int rc = batch_cn_shapes<T>(b);
   if (rc) return rc;
   rc = b->nmax == 8 ? batch_fft_shapes<T, 8>(b) : batch_fft_shapes<T, 16>(b);
   if (rc) return rc;
@@ -2604,14 +2680,12 @@ template <class T> static void batch_rhs_args(tc_batch* b, const std::vector<BMe
 
 template <class T> static int batch_build_impl(tc_batch* b, int scheme, const double* dts, cudaStream_t s) {
   const int n = b->n, L = b->cn_L;
-  constexpr int VL16 = sizeof(T) == 4 ? 2 : 1;
   std::vector<BMember<T>> tab(3 * (size_t)n);
   int run[BK_COUNT] = {0, 0, 0, 0, 0, 0, 0};
   int maxnz = 0;
   for (auto* c : b->m) maxnz = std::max(maxnz, c->nz);
-  // one CN block of cn_y chunk warps (the deepest member's chunks of L rows)
-  // for every member; a member's chunks are L rows, like a single-channel
-  // step's, and the warps beyond its last chunk idle
+  // a member's CN chunks are L rows, like a single-channel step's; one CN
+  // launch per chunk count
   const int maxchunks = (maxnz + L - 1) / L;
   b->rhs_tma = batch_tma_ok(b) ? 1 : 0;
   size_t fx = 0;
@@ -2645,13 +2719,11 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   for (int k = 0; k < BK_COUNT; ++k) b->total[k] = run[k];
   if (b->rhs_tma) batch_rhs_args<T>(b, tab);
   batch_x_args<T>(b, tab);
-  const int V = L == 16 ? VL16 : 1;
+  batch_cn_args<T>(b, tab);
   b->cn_y = maxchunks;
   b->smem_fx = fx;
-  b->smem_cn = (size_t)(9 * maxnz + 2 * maxchunks * 32 * V) * 8;
   b->fy_tile = fyt;
   b->smem_fy = (size_t)4 * 2 * fyt * sizeof(cpx<double>);
-  b->cn_maxt = 32 * b->cn_y <= 256 ? 256 : 512;
   int n1max = 0;
   for (auto* c : b->m) n1max = std::max(n1max, std::max(c->nx, c->ny) / 16);
   b->nmax = n1max <= 8 ? 8 : 16;
@@ -2707,17 +2779,13 @@ template <class T> static int batch_step_impl(tc_batch* b, int scheme, int ti, c
     kb_rhs<T, true, UPD_AB2><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
   else
     kb_rhs<T, true, UPD_FE><<<b->grid[BK_RHS], rb, 0, s>>>(M, n, b->total[BK_RHS]);
-  if (scheme == TC_IMEX) {
-    const dim3 cb(32, b->cn_y);
-    constexpr int V16 = batch_cn_vec<T>(16);
-    if (b->cn_L == 16 && b->cn_maxt == 256)
-      kb_cn<T, 16, V16, 256><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
-    else if (b->cn_L == 16)
-      kb_cn<T, 16, V16, 512><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
-    else if (b->cn_maxt == 256)
-      kb_cn<T, 32, 1, 256><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
-    else
-      kb_cn<T, 32, 1, 512><<<b->grid[BK_CN], cb, b->smem_cn, s>>>(M, n, b->total[BK_CN]);
+  if (scheme == TC_IMEX) {  // one launch per chunk count, blocks of (32, chunks)
+    const std::vector<BatchCnArgs<T>>& ca = batch_cargs<T>(b)[ti];
+    for (size_t c = 0; c < ca.size(); ++c) {
+      const int ch = b->ccls[c];
+      const size_t sm = batch_cn_smem<T>(b->cn_L, ch, b->cmaxnz[c]);
+      batch_cn_kernel<T>(b->cn_L, 32 * ch, [&](auto k) { k<<<b->cgrid[c], dim3(32, ch), sm, s>>>(ca[c]); });
+    }
   }
   if (b->nmax == 8)
     batch_poisson<T, 8>(b, M, s);
