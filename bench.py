@@ -644,10 +644,11 @@ def run_ensemble(a):
                                               "note": "autotuned member shapes; 2 steps of all members per graph launch"},
                           "tuning": tuning,
                           "batched": {"value": value_batch, "ms_per_step": ms_batch / (2 * pairs),
-                                      "launches_per_step": 8, "shape": btun, "units": binfo["units"],
-                                      "ctas": binfo["ctas"],
-                                      "note": "one persistent launch per substep for all members, "
-                                              "two steps per graph launch (tc_batch_step)"},
+                                      "launches_per_step": ens.batched.launches_per_step(), "shape": btun,
+                                      "units": binfo["units"], "ctas": binfo["ctas"],
+                                      "note": "one launch per substep for all members (CN per chunk count, "
+                                              "inverse x transform per length), two steps per graph launch "
+                                              "(tc_batch_step)"},
                           "max_div_after": max(d["max_div"] for d in diag)}), flush=True)
 
 

@@ -94,6 +94,9 @@ def test_batch_shapes(torch_cuda, rows, ctas):
             assert g <= ctas * nsm
         if ctas < 0 and k != "ffty":
             assert g == info["units"][k]
+    # RHS, CN per chunk count, forward x, two y, z solve, inverse x per length, projection
+    assert a.batched.launches_per_step() == (1 + len({-(-c.nz // rows) for c in a.channels}) + 4
+                                             + len({c.nx for c in a.channels}) + 1)
 
 
 def test_batch_interleaved_with_member_steps(torch_cuda):

@@ -109,6 +109,20 @@ class ChannelBatch:
                                             d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(n_steps),
                                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
+    def launches_per_step(self, scheme="IMEX"):
+        """Kernel launches of one ensemble step: the RHS (one per 32 members
+        with the tensor-copy tiles), the CN (IMEX: one per chunk count), the
+        forward x, both y transforms and the z solve (one each), the inverse x
+        transform (one per transform length) and the projection."""
+        info = self.info()
+        L = info["cn_rows"]
+        chans = self.channels
+        kb = 8 if chans[0]._desc.precision == self.L.TC_MIXED else 2  # planes of a tensor-copy tile
+        tiles = sum(-(-c.nx // 32) * -(-c.ny // 8) * -(-c.nz // kb) for c in chans)
+        rhs = -(-len(chans) // 32) if info["units"]["rhs"] == tiles else 1
+        cn = len({-(-c.nz // L) for c in chans}) if scheme == "IMEX" else 0
+        return rhs + cn + 4 + len({c.nx for c in chans}) + 1
+
     def info(self):
         shape, units, grids = (ctypes.c_int * 4)(), (ctypes.c_int * 7)(), (ctypes.c_int * 7)()
         self.L.check(self.lib.tc_batch_info(self.b, shape, units, grids))
