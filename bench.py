@@ -647,7 +647,7 @@ def run_ensemble(a):
                                       "launches_per_step": ens.batched.launches_per_step(), "shape": btun,
                                       "units": binfo["units"], "ctas": binfo["ctas"],
                                       "note": "one launch per substep for all members (CN per chunk count, "
-                                              "inverse x transform per length), two steps per graph launch "
+                                              "x transforms per length), two steps per graph launch "
                                               "(tc_batch_step)"},
                           "max_div_after": max(d["max_div"] for d in diag)}), flush=True)
 

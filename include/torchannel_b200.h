@@ -342,9 +342,9 @@ int tc_set_cn_chunk(tc_ctx* ctx, int rows);
  * precision on one device whose nx and ny are 64, 96, 128, 192 or 256; each
  * substep (RHS, CN, x / y transforms, z solve, inverse transforms,
  * projection) of every member runs as ONE launch over the concatenated work
- * of all members (the CN: one launch per chunk count; the inverse x
- * transform: one per transform length; the tensor-copy RHS: one per 32
- * members), and tc_batch_step with n_steps >= 4 replays two such steps as
+ * of all members (the CN: one launch per chunk count; the x transforms:
+ * one per transform length each; the tensor-copy RHS: one per 32 members),
+ * and tc_batch_step with n_steps >= 4 replays two such steps as
  * one CUDA graph.  Each member advances exactly
  * as tc_step would advance it (same kernels' tile code; bit-identical with
  * the same CN chunk length), its scalars, statistics and state entries stay
@@ -356,8 +356,8 @@ int tc_set_cn_chunk(tc_ctx* ctx, int rows);
  *   chunks take that many rows and its tables follow; the deepest member's
  *   chunk count fixes the CN block, whose warps beyond a shallower member's
  *   last chunk idle) and persistent CTAs per SM (0 = occupancy limit,
- *   -1 = one CTA per work unit; the CN and inverse x launches always take
- *   one CTA per unit), the ensemble autotuner's knobs.
+ *   -1 = one CTA per work unit; the CN and x-transform launches always
+ *   take one CTA per unit), the ensemble autotuner's knobs.
  * tc_batch_step: dts = host array of one dt per member; members without AB2
  *   history start with a forward step as tc_step does.  Members may carry no
  *   adjoint hooks (TC_ERR_ARG).  The RHS launch stages its tiles by tensor

@@ -88,15 +88,15 @@ def test_batch_shapes(torch_cuda, rows, ctas):
     nsm = torch.cuda.get_device_properties(0).multi_processor_count
     for k, g in info["ctas"].items():
         assert 1 <= g <= info["units"][k]
-        if k in ("ifftx", "cn"):  # one launch per transform length / chunk count, one CTA per unit
+        if k in ("fftx", "ifftx", "cn"):  # one launch per transform length / chunk count, one CTA per unit
             assert g == info["units"][k]
         elif ctas > 0:
             assert g <= ctas * nsm
         if ctas < 0 and k != "ffty":
             assert g == info["units"][k]
-    # RHS, CN per chunk count, forward x, two y, z solve, inverse x per length, projection
-    assert a.batched.launches_per_step() == (1 + len({-(-c.nz // rows) for c in a.channels}) + 4
-                                             + len({c.nx for c in a.channels}) + 1)
+    # RHS, CN per chunk count, x per length, two y, z solve, inverse x per length, projection
+    assert a.batched.launches_per_step() == (1 + len({-(-c.nz // rows) for c in a.channels}) + 3
+                                             + 2 * len({c.nx for c in a.channels}) + 1)
 
 
 def test_batch_interleaved_with_member_steps(torch_cuda):

@@ -22,20 +22,15 @@ namespace tc {
 enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT };
 #define TC_BATCH_MAX 64  // members per ensemble launch
 
-// Register allocation of the unit loops.  Inlining every transform length
-// into one switch makes the forward x transform spill heavily, so that tile
-// is a called function (TC_BATCH_FX_CALL) over TC_BATCH_XP planes per unit
-// (the call's register saves are paid once per group; split into one launch
-// per length with one plane a CTA it measured slower).  The inverse x
-// transform runs one launch per transform length (kb_ifftx_n: the registers
-// of that length alone), one CTA per unit (a row block of a plane), as the
-// single-channel kernel: a persistent unit loop around the same tile took
-// 128-192 registers, and capped at 96 it spilled.  The other loops inline
-// their tiles under occupancy-driven register caps (minimum resident blocks
-// per SM below).
-#ifndef TC_BATCH_FX_CALL
-#define TC_BATCH_FX_CALL __noinline__
-#endif
+// Register allocation of the unit loops.  The x transforms run one launch
+// per transform length (kb_fftx_n, kb_ifftx_n: the registers of that length
+// alone, where one kernel over all lengths takes those of the longest and
+// spills), one CTA per unit: TC_BATCH_XP planes of a row block (forward) or
+// one plane (inverse).  A persistent unit loop around the same tiles took
+// 128-192 registers and, capped at 96, spilled; the forward transform with
+// one plane a CTA measured slower than with TC_BATCH_XP.  The other loops
+// inline their tiles under occupancy-driven register caps (minimum resident
+// blocks per SM below).
 #ifndef TC_BATCH_FFT_MINB
 #define TC_BATCH_FFT_MINB 4
 #endif
@@ -265,9 +260,9 @@ __global__ void __launch_bounds__(MAXT) kb_cn_n(const __grid_constant__ BatchCnA
 
 // Register-FFT lengths of the ensemble kernels: N = 16 N1, N1 in {4, 6, 8, 12, 16}
 // (64 .. 256 points), all with two rows per warp (128-thread x blocks).  The
-// forward x and the y transforms come in two sets, NMAX = 8 (every member's
-// N1 <= 8) and NMAX = 16, since a kernel's registers are those of its longest
-// transform; the inverse x transform takes one launch per length.
+// y transforms come in two sets, NMAX = 8 (every member's N1 <= 8) and
+// NMAX = 16, since a kernel's registers are those of its longest transform;
+// the x transforms take one launch per length.
 __host__ __device__ constexpr bool batch_n1_ok(int n1) { return n1 == 4 || n1 == 6 || n1 == 8 || n1 == 12 || n1 == 16; }
 
 template <int NMAX, class F> __device__ __forceinline__ void batch_n1_switch(int n1, F&& f) {
@@ -288,52 +283,31 @@ template <int NMAX, class F> __device__ __forceinline__ void batch_n1_switch(int
   }
 }
 
-template <class T, int N1>
-__device__ TC_BATCH_FX_CALL void batch_fftx_call(const BMember<T>* __restrict__ bp, int bx, int k0) {
-  const BMember<T>& b = *bp;
-  const int k1 = min(k0 + TC_BATCH_XP, b.g.nz);
-  for (int k = k0; k < k1; ++k) {
-    if (k > k0) __syncthreads();  // the previous plane's spectra are read
-    fftx_tile<T, N1, XROWS>(b.g, b.B[0], b.B[1], b.B[2], nullptr, b.X, b.twx, b.scale, bx, k);
-  }
-}
 template <class T, int N1, bool INV>
 __device__ __forceinline__ void batch_ffty_call(const BMember<T>* __restrict__ bp, int row0, cpx<double>* tiles) {
   const BMember<T>& b = *bp;
   ffty_rows<N1, INV>(b.X, b.nrows, b.twy, row0, tiles);
 }
 
-// The inverse x transforms of the members whose nx is 16 N1, one launch per
-// N1.  What the transform reads of a member travels in the launch's
+// The x transforms of the members whose nx is 16 N1, one launch per N1.
+// What the transforms read of a member travels in the launch's
 // __grid_constant__ parameter (uniform loads, no per-thread registers).
 template <class T> struct BXRec {
   Grid<T> g;
+  const T* B[3];  // u**, v**, w** (forward transform)
   cpx<double>* X;
   const cpx<double>* twx;
   double* p;
+  double scale;
   int xgx;        // row blocks per plane
 };
 template <class T> struct BatchXArgs {
   BXRec<T> r[TC_BATCH_MAX];
-  int st[TC_BATCH_MAX + 1];  // first unit (row block, plane) of each member of the class, then the end
+  int st[TC_BATCH_MAX + 1];   // first inverse unit (row block, plane) of each member of the class, then the end
+  int stf[TC_BATCH_MAX + 1];  // the same for the forward units (row block, group of TC_BATCH_XP planes)
   int n;
 };
 static_assert(sizeof(BatchXArgs<double>) + 64 <= 32764, "kernel parameter limit");
-
-template <class T, int NMAX>
-__global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_fftx(const BMember<T>* __restrict__ M, int nm, int total) {
-  __shared__ int st[TC_BATCH_MAX + 1];
-  batch_starts(M, nm, BK_FX, total, st);
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    const int m = batch_member(st, nm, w);
-    const BMember<T>& b = M[m];
-    const int l = w - st[m];
-    batch_n1_switch<NMAX>(b.n1x, [&](auto I) {
-      batch_fftx_call<T, decltype(I)::value>(&b, l % b.xgx, (l / b.xgx) * TC_BATCH_XP);
-    });
-    __syncthreads();
-  }
-}
 
 // Units are warp tasks of two rows; no block barrier.
 template <class T, int NMAX, bool INV>
@@ -361,6 +335,22 @@ __global__ void __launch_bounds__(64, TC_BATCH_TRI_MINB) kb_tri(const BMember<T>
     const BMember<T>& b = M[m];
     tri_lu2_thread<8>(reinterpret_cast<double*>(b.X), b.rden, b.cpt, b.tb, b.nxh, b.g.ny, b.g.nz,
                       (w - st[m]) * 64 + threadIdx.x);
+  }
+}
+
+// Forward x transform of the members of one length N1: one CTA per unit of
+// TC_BATCH_XP planes of a row block (units as kb_fftx's).
+template <class T, int N1>
+__global__ void __launch_bounds__(128) kb_fftx_n(const __grid_constant__ BatchXArgs<T> a) {
+  const int w = blockIdx.x;
+  if (w >= a.stf[a.n]) return;
+  const int m = batch_class_member(a.stf, a.n, w);
+  const BXRec<T>& b = a.r[m];
+  const int l = w - a.stf[m], bx = l % b.xgx, k0 = (l / b.xgx) * TC_BATCH_XP;
+  const int k1 = min(k0 + TC_BATCH_XP, b.g.nz);
+  for (int k = k0; k < k1; ++k) {
+    if (k > k0) __syncthreads();  // the previous plane's spectra are read
+    fftx_tile<T, N1, XROWS>(b.g, b.B[0], b.B[1], b.B[2], nullptr, b.X, b.twx, b.scale, bx, k);
   }
 }
 

@@ -2288,15 +2288,14 @@ struct tc_batch {
   std::vector<BatchRhsArgs<float>> rargs_f[3];   // kb_rhs_tma parameters of tables 0, 1, 2, one per member group
   std::vector<BatchRhsArgs<double>> rargs_d[3];
   int cn_y, nmax, fy_tile;   // cn_y: CN chunks of the deepest member
-  size_t smem_fx, smem_fy;
+  size_t smem_fy;
   std::vector<int> ccls;     // CN chunk counts of the members, one launch each
   std::vector<int> cmaxnz, cgrid;    // deepest member and CTAs of each CN class
   std::vector<BatchCnArgs<float>> cargs_f[3];   // kb_cn_pk / kb_cn_n parameters of tables 0, 1, 2 per class
   std::vector<BatchCnArgs<double>> cargs_d[3];
-  std::vector<int> xcls;     // x-transform lengths N1 of the members, one inverse launch each
-  std::vector<int> xgrid_i;  // CTAs of each class's inverse launch
-  std::vector<BatchXArgs<float>> xargs_f;   // kb_ifftx_n parameters per class
-  std::vector<BatchXArgs<double>> xargs_d;
+  std::vector<int> xcls;     // x-transform lengths N1 of the members, one launch each
+  std::vector<BatchXArgs<float>> xargs_f[3];   // kb_fftx_n / kb_ifftx_n parameters per table and class
+  std::vector<BatchXArgs<double>> xargs_d[3];
   int graphs_on;
   cudaStream_t cap_stream;
   cudaGraphExec_t gexec;
@@ -2545,41 +2544,41 @@ template <class F> static void batch_n1_host(int n1, F&& f) {
     default: f(std::integral_constant<int, 16>{}); break;
   }
 }
-template <class T> static std::vector<BatchXArgs<T>>& batch_xargs(tc_batch* b) {
+template <class T> static std::vector<BatchXArgs<T>>* batch_xargs(tc_batch* b) {
   if constexpr (sizeof(T) == 8)
     return b->xargs_d;
   else
     return b->xargs_f;
 }
 template <class T, int NMAX> static int batch_fft_shapes(tc_batch* b) {
-  TC_CUDA(cudaFuncSetAttribute(kb_fftx<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fx));
   TC_CUDA(cudaFuncSetAttribute(kb_ffty<T, NMAX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fy));
   TC_CUDA(cudaFuncSetAttribute(kb_ffty<T, NMAX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_fy));
-  int rc = batch_grid<T>(b, kb_fftx<T, NMAX>, 128, b->smem_fx, b->total[BK_FX], &b->grid[BK_FX]);
-  if (!rc) rc = batch_grid<T>(b, kb_ffty<T, NMAX, false>, 128, b->smem_fy, (b->total[BK_FY] + 3) / 4, &b->grid[BK_FY]);
-  // inverse x transform: one launch per length class, one CTA per unit (the
-  // grids add up in the info)
-  const std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b);
+  int rc = batch_grid<T>(b, kb_ffty<T, NMAX, false>, 128, b->smem_fy, (b->total[BK_FY] + 3) / 4, &b->grid[BK_FY]);
+  // x transforms: one launch per length class, one CTA per unit (the grids
+  // add up in the info)
+  const std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b)[0];
   const int nc = (int)b->xcls.size();
-  b->xgrid_i.assign(nc, 1);
   b->grid[BK_IFX] = 0;
+  b->grid[BK_FX] = 0;
   for (int c = 0; c < nc && !rc; ++c)
     batch_n1_host(b->xcls[c], [&](auto I) {
       constexpr int N1 = decltype(I)::value;
       if (cudaFuncSetAttribute(kb_ifftx_n<T, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)ifftx_reg_smem<N1>()) != cudaSuccess) {
-        rc = fail(TC_ERR_CUDA, "ensemble inverse x transform attributes");
+                               (int)ifftx_reg_smem<N1>()) != cudaSuccess ||
+          cudaFuncSetAttribute(kb_fftx_n<T, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)fftx_reg_smem<N1>()) != cudaSuccess) {
+        rc = fail(TC_ERR_CUDA, "ensemble x transform attributes");
         return;
       }
-      b->xgrid_i[c] = std::max(1, xa[c].st[xa[c].n]);
-      b->grid[BK_IFX] += b->xgrid_i[c];
+      b->grid[BK_IFX] += std::max(1, xa[c].st[xa[c].n]);
+      b->grid[BK_FX] += std::max(1, xa[c].stf[xa[c].n]);
     });
   return rc;
 }
 
-// Parameters of the inverse x-transform class launches (the same for every
-// table: the transform reads the spectrum and writes the pressure): the
-// members of each length N1 (ascending) with their first units.
+// Parameters of the x-transform class launches for the three tables: the
+// members of each length N1 (ascending) with their first forward and
+// inverse units.
 template <class T> static void batch_x_args(tc_batch* b, const std::vector<BMember<T>>& tab) {
   const int n = b->n;
   b->xcls.clear();
@@ -2588,24 +2587,29 @@ template <class T> static void batch_x_args(tc_batch* b, const std::vector<BMemb
     if (std::find(b->xcls.begin(), b->xcls.end(), n1) == b->xcls.end()) b->xcls.push_back(n1);
   }
   std::sort(b->xcls.begin(), b->xcls.end());
-  std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b);
-  xa.assign(b->xcls.size(), BatchXArgs<T>());
-  for (size_t c = 0; c < b->xcls.size(); ++c) {
-    BatchXArgs<T>& a = xa[c];
-    a.n = 0;
-    a.st[0] = 0;
-    for (int i = 0; i < n; ++i) {
-      const tc_ctx* ctx = b->m[i];
-      if (ctx->nx / 16 != b->xcls[c]) continue;
-      const BMember<T>& r = tab[i];
-      BXRec<T>& q = a.r[a.n];
-      q.g = r.g;
-      q.X = r.X;
-      q.twx = r.twx;
-      q.p = r.p;
-      q.xgx = r.xgx;
-      a.st[a.n + 1] = a.st[a.n] + r.xgx * ctx->nz;
-      ++a.n;
+  std::vector<BatchXArgs<T>>* xa = batch_xargs<T>(b);
+  for (int t = 0; t < 3; ++t) {
+    xa[t].assign(b->xcls.size(), BatchXArgs<T>());
+    for (size_t c = 0; c < b->xcls.size(); ++c) {
+      BatchXArgs<T>& a = xa[t][c];
+      a.n = 0;
+      a.st[0] = a.stf[0] = 0;
+      for (int i = 0; i < n; ++i) {
+        const tc_ctx* ctx = b->m[i];
+        if (ctx->nx / 16 != b->xcls[c]) continue;
+        const BMember<T>& r = tab[(size_t)t * n + i];
+        BXRec<T>& q = a.r[a.n];
+        q.g = r.g;
+        for (int f = 0; f < 3; ++f) q.B[f] = r.B[f];
+        q.X = r.X;
+        q.twx = r.twx;
+        q.p = r.p;
+        q.scale = r.scale;
+        q.xgx = r.xgx;
+        a.st[a.n + 1] = a.st[a.n] + r.xgx * ctx->nz;
+        a.stf[a.n + 1] = a.stf[a.n] + r.xgx * r.xpg;
+        ++a.n;
+      }
     }
   }
 }
@@ -2688,7 +2692,6 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   // launch per chunk count
   const int maxchunks = (maxnz + L - 1) / L;
   b->rhs_tma = batch_tma_ok(b) ? 1 : 0;
-  size_t fx = 0;
   int fyt = 0;
   for (int i = 0; i < n; ++i) {
     tc_ctx* c = b->m[i];
@@ -2713,7 +2716,6 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
       tab[i].u0[k] = tab[n + i].u0[k] = tab[2 * n + i].u0[k] = run[k];
       run[k] += cnt[k];
     }
-    for_each_n1(c->nx, [&](auto I) { fx = std::max(fx, fftx_reg_smem<decltype(I)::value>()); });
     for_each_n1(c->ny, [&](auto I) { fyt = std::max(fyt, RowFft<decltype(I)::value>::TILE); });
   }
   for (int k = 0; k < BK_COUNT; ++k) b->total[k] = run[k];
@@ -2721,7 +2723,6 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   batch_x_args<T>(b, tab);
   batch_cn_args<T>(b, tab);
   b->cn_y = maxchunks;
-  b->smem_fx = fx;
   b->fy_tile = fyt;
   b->smem_fy = (size_t)4 * 2 * fyt * sizeof(cpx<double>);
   int n1max = 0;
@@ -2742,17 +2743,21 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
 }
 
 template <class T, int NMAX>
-static void batch_poisson(tc_batch* b, const BMember<T>* M, cudaStream_t s) {
+static void batch_poisson(tc_batch* b, const BMember<T>* M, int ti, cudaStream_t s) {
   const int n = b->n;
-  kb_fftx<T, NMAX><<<b->grid[BK_FX], 128, b->smem_fx, s>>>(M, n, b->total[BK_FX]);
-  kb_ffty<T, NMAX, false><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
-  kb_tri<T><<<b->grid[BK_TRI], 64, 0, s>>>(M, n, b->total[BK_TRI]);
-  kb_ffty<T, NMAX, true><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
-  const std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b);
+  const std::vector<BatchXArgs<T>>& xa = batch_xargs<T>(b)[ti];
   for (size_t c = 0; c < xa.size(); ++c)
     batch_n1_host(b->xcls[c], [&](auto I) {
       constexpr int N1 = decltype(I)::value;
-      kb_ifftx_n<T, N1><<<b->xgrid_i[c], 128, ifftx_reg_smem<N1>(), s>>>(xa[c]);
+      kb_fftx_n<T, N1><<<std::max(1, xa[c].stf[xa[c].n]), 128, fftx_reg_smem<N1>(), s>>>(xa[c]);
+    });
+  kb_ffty<T, NMAX, false><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
+  kb_tri<T><<<b->grid[BK_TRI], 64, 0, s>>>(M, n, b->total[BK_TRI]);
+  kb_ffty<T, NMAX, true><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
+  for (size_t c = 0; c < xa.size(); ++c)
+    batch_n1_host(b->xcls[c], [&](auto I) {
+      constexpr int N1 = decltype(I)::value;
+      kb_ifftx_n<T, N1><<<std::max(1, xa[c].st[xa[c].n]), 128, ifftx_reg_smem<N1>(), s>>>(xa[c]);
     });
 }
 
@@ -2788,9 +2793,9 @@ template <class T> static int batch_step_impl(tc_batch* b, int scheme, int ti, c
     }
   }
   if (b->nmax == 8)
-    batch_poisson<T, 8>(b, M, s);
+    batch_poisson<T, 8>(b, M, ti, s);
   else
-    batch_poisson<T, 16>(b, M, s);
+    batch_poisson<T, 16>(b, M, ti, s);
   kb_proj<T><<<b->grid[BK_PROJ], dim3(32, 8), 0, s>>>(M, n, b->total[BK_PROJ]);
   TC_LAUNCHED();
   return TC_OK;

@@ -112,8 +112,8 @@ class ChannelBatch:
     def launches_per_step(self, scheme="IMEX"):
         """Kernel launches of one ensemble step: the RHS (one per 32 members
         with the tensor-copy tiles), the CN (IMEX: one per chunk count), the
-        forward x, both y transforms and the z solve (one each), the inverse x
-        transform (one per transform length) and the projection."""
+        forward and inverse x transforms (one per transform length each), both
+        y transforms and the z solve (one each) and the projection."""
         info = self.info()
         L = info["cn_rows"]
         chans = self.channels
@@ -121,7 +121,7 @@ class ChannelBatch:
         tiles = sum(-(-c.nx // 32) * -(-c.ny // 8) * -(-c.nz // kb) for c in chans)
         rhs = -(-len(chans) // 32) if info["units"]["rhs"] == tiles else 1
         cn = len({-(-c.nz // L) for c in chans}) if scheme == "IMEX" else 0
-        return rhs + cn + 4 + len({c.nx for c in chans}) + 1
+        return rhs + cn + 3 + 2 * len({c.nx for c in chans}) + 1
 
     def info(self):
         shape, units, grids = (ctypes.c_int * 4)(), (ctypes.c_int * 7)(), (ctypes.c_int * 7)()
