@@ -339,7 +339,8 @@ __global__ void __launch_bounds__(64, TC_BATCH_TRI_MINB) kb_tri(const BMember<T>
 }
 
 // Forward x transform of the members of one length N1: one CTA per unit of
-// TC_BATCH_XP planes of a row block (units as kb_fftx's).
+// TC_BATCH_XP planes of a row block (units in the order of the plane groups,
+// row blocks fastest).
 template <class T, int N1>
 __global__ void __launch_bounds__(128) kb_fftx_n(const __grid_constant__ BatchXArgs<T> a) {
   const int w = blockIdx.x;
