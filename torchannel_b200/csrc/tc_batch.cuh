@@ -40,9 +40,6 @@ enum : int { BK_RHS = 0, BK_CN, BK_FX, BK_FY, BK_TRI, BK_IFX, BK_PROJ, BK_COUNT 
 #ifndef TC_BATCH_RHS_MINB32
 #define TC_BATCH_RHS_MINB32 3    // FP32 storage (the column march carries plane values: 80 registers)
 #endif
-#ifndef TC_BATCH_TRI_MINB
-#define TC_BATCH_TRI_MINB 6
-#endif
 #ifndef TC_BATCH_XP
 #define TC_BATCH_XP 4
 #endif
@@ -325,17 +322,28 @@ __global__ void __launch_bounds__(128, TC_BATCH_FFT_MINB) kb_ffty(const BMember<
   }
 }
 
-// Units are 64-thread groups of the z sweeps.
-template <class T>
-__global__ void __launch_bounds__(64, TC_BATCH_TRI_MINB) kb_tri(const BMember<T>* __restrict__ M, int nm, int total) {
-  __shared__ int st[TC_BATCH_MAX + 1];
-  batch_starts(M, nm, BK_TRI, total, st);
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    const int m = batch_member(st, nm, w);
-    const BMember<T>& b = M[m];
-    tri_lu2_thread<8>(reinterpret_cast<double*>(b.X), b.rden, b.cpt, b.tb, b.nxh, b.g.ny, b.g.nz,
-                      (w - st[m]) * 64 + threadIdx.x);
-  }
+// The z sweeps of every member's modes, one CTA of 64 threads per unit (as
+// k_tri_lu2), what a sweep reads of its member in the launch's
+// __grid_constant__ parameter: a persistent unit loop reading the member
+// table from global memory spilled 428 bytes a thread at its register cap.
+struct BTriRec {
+  double* X;  // the spectrum, solved in place
+  const double* rden;
+  const double* cpt;
+  PoissonTabs tb;
+  int nxh, ny, nz;
+};
+struct BatchTriArgs {
+  BTriRec r[TC_BATCH_MAX];
+  int st[TC_BATCH_MAX + 1];  // first unit of each member, then the end
+  int n;
+};
+__global__ void __launch_bounds__(64) kb_tri_n(const __grid_constant__ BatchTriArgs a) {
+  const int w = blockIdx.x;
+  if (w >= a.st[a.n]) return;
+  const int m = batch_class_member(a.st, a.n, w);
+  const BTriRec& b = a.r[m];
+  tri_lu2_thread<8>(b.X, b.rden, b.cpt, b.tb, b.nxh, b.ny, b.nz, (w - a.st[m]) * 64 + threadIdx.x);
 }
 
 // Forward x transform of the members of one length N1: one CTA per unit of

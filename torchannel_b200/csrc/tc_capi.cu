@@ -2294,6 +2294,7 @@ struct tc_batch {
   std::vector<BatchCnArgs<float>> cargs_f[3];   // kb_cn_pk / kb_cn_n parameters of tables 0, 1, 2 per class
   std::vector<BatchCnArgs<double>> cargs_d[3];
   std::vector<int> xcls;     // x-transform lengths N1 of the members, one launch each
+  BatchTriArgs targs;        // kb_tri_n parameter
   std::vector<BatchXArgs<float>> xargs_f[3];   // kb_fftx_n / kb_ifftx_n parameters per table and class
   std::vector<BatchXArgs<double>> xargs_d[3];
   int graphs_on;
@@ -2638,7 +2639,7 @@ template <class T> static int batch_shapes(tc_batch* b, int scheme) {
     rc = batch_grid<T>(b, kb_rhs<T, true, UPD_AB2>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
   else
     rc = batch_grid<T>(b, kb_rhs<T, true, UPD_FE>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
-  if (!rc) rc = batch_grid<T>(b, kb_tri<T>, 64, 0, b->total[BK_TRI], &b->grid[BK_TRI]);
+  b->grid[BK_TRI] = std::max(1, b->total[BK_TRI]);  // one CTA per unit
   if (!rc) rc = batch_grid<T>(b, kb_proj<T>, 256, 0, b->total[BK_PROJ], &b->grid[BK_PROJ]);
   return rc;
 }
@@ -2722,6 +2723,20 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   if (b->rhs_tma) batch_rhs_args<T>(b, tab);
   batch_x_args<T>(b, tab);
   batch_cn_args<T>(b, tab);
+  b->targs = BatchTriArgs();
+  for (int i = 0; i < n; ++i) {  // the z sweeps read the spectrum: the same for every table
+    BTriRec& q = b->targs.r[i];
+    q.X = reinterpret_cast<double*>(tab[i].X);
+    q.rden = tab[i].rden;
+    q.cpt = tab[i].cpt;
+    q.tb = tab[i].tb;
+    q.nxh = tab[i].nxh;
+    q.ny = b->m[i]->ny;
+    q.nz = b->m[i]->nz;
+    b->targs.st[i] = tab[i].u0[BK_TRI];
+  }
+  b->targs.st[n] = b->total[BK_TRI];
+  b->targs.n = n;
   b->cn_y = maxchunks;
   b->fy_tile = fyt;
   b->smem_fy = (size_t)4 * 2 * fyt * sizeof(cpx<double>);
@@ -2752,7 +2767,7 @@ static void batch_poisson(tc_batch* b, const BMember<T>* M, int ti, cudaStream_t
       kb_fftx_n<T, N1><<<std::max(1, xa[c].stf[xa[c].n]), 128, fftx_reg_smem<N1>(), s>>>(xa[c]);
     });
   kb_ffty<T, NMAX, false><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
-  kb_tri<T><<<b->grid[BK_TRI], 64, 0, s>>>(M, n, b->total[BK_TRI]);
+  kb_tri_n<<<b->grid[BK_TRI], 64, 0, s>>>(b->targs);
   kb_ffty<T, NMAX, true><<<b->grid[BK_FY], 128, b->smem_fy, s>>>(M, n, b->total[BK_FY], b->fy_tile);
   for (size_t c = 0; c < xa.size(); ++c)
     batch_n1_host(b->xcls[c], [&](auto I) {
