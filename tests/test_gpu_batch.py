@@ -88,7 +88,7 @@ def test_batch_shapes(torch_cuda, rows, ctas):
     nsm = torch.cuda.get_device_properties(0).multi_processor_count
     for k, g in info["ctas"].items():
         assert 1 <= g <= info["units"][k]
-        if k in ("fftx", "ifftx", "cn", "tri"):  # one CTA per unit (CN, x transforms: a launch per class)
+        if k in ("fftx", "ifftx", "cn", "tri", "proj"):  # one CTA per unit (CN, x transforms: a launch per class)
             assert g == info["units"][k]
         elif ctas > 0:
             assert g <= ctas * nsm

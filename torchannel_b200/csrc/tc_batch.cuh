@@ -373,22 +373,37 @@ __global__ void __launch_bounds__(128) kb_ifftx_n(const __grid_constant__ BatchX
   ifftx_tile<N1, XROWS>(b.X, b.p, b.g.ny, b.g.nz, b.twx, l % b.xgx, l / b.xgx);
 }
 
-// The member's last block (atomic ticket, per member) reduces its partials
-// and updates its forcing, as in k_project_bulk.
+// The projection of every member, one CTA per unit (a k_project_bulk
+// block), what the tile reads of its member in the launch's
+// __grid_constant__ parameter.  The member's last block (atomic ticket, per
+// member) reduces its partials and updates its forcing, as in
+// k_project_bulk.
+template <class T> struct BProjRec {
+  Grid<T> g;
+  T* B[3];  // u**, v**, w**: corrected in place
+  double* p;
+  const double* dzf;
+  BulkArgs ba;
+  int pgx, pgy, pgz;  // block grid of k_project_bulk
+};
+template <class T> struct BatchProjArgs {
+  BProjRec<T> r[TC_BATCH_MAX];
+  int st[TC_BATCH_MAX + 1];  // first unit of each member, then the end
+  int n;
+};
+static_assert(sizeof(BatchProjArgs<double>) + 64 <= 32764, "kernel parameter limit");
+
 template <class T>
-__global__ void __launch_bounds__(256) kb_proj(const BMember<T>* __restrict__ M, int nm, int total) {
-  __shared__ int st[TC_BATCH_MAX + 1];
-  batch_starts(M, nm, BK_PROJ, total, st);
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    const int m = batch_member(st, nm, w);
-    const BMember<T>& b = M[m];
-    int l = w - st[m];
-    const int bx = l % b.pgx;
-    l /= b.pgx;
-    const int by = l % b.pgy, bz = l / b.pgy;
-    project_tile<T>(b.g, b.B[0], b.B[1], b.B[2], b.p, (double)b.ba.dt, b.dzf, b.ba, bx, by, bz, b.pgx, b.pgy, b.pgz);
-    __syncthreads();
-  }
+__global__ void __launch_bounds__(256) kb_proj_n(const __grid_constant__ BatchProjArgs<T> a) {
+  const int w = blockIdx.x;
+  if (w >= a.st[a.n]) return;
+  const int m = batch_class_member(a.st, a.n, w);
+  const BProjRec<T>& b = a.r[m];
+  int l = w - a.st[m];
+  const int bx = l % b.pgx;
+  l /= b.pgx;
+  const int by = l % b.pgy, bz = l / b.pgy;
+  project_tile<T>(b.g, b.B[0], b.B[1], b.B[2], b.p, (double)b.ba.dt, b.dzf, b.ba, bx, by, bz, b.pgx, b.pgy, b.pgz);
 }
 
 }  // namespace tc

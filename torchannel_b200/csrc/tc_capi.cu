@@ -2295,6 +2295,8 @@ struct tc_batch {
   std::vector<BatchCnArgs<double>> cargs_d[3];
   std::vector<int> xcls;     // x-transform lengths N1 of the members, one launch each
   BatchTriArgs targs;        // kb_tri_n parameter
+  BatchProjArgs<float> pargs_f[3];   // kb_proj_n parameters of tables 0, 1, 2
+  BatchProjArgs<double> pargs_d[3];
   std::vector<BatchXArgs<float>> xargs_f[3];   // kb_fftx_n / kb_ifftx_n parameters per table and class
   std::vector<BatchXArgs<double>> xargs_d[3];
   int graphs_on;
@@ -2455,6 +2457,12 @@ template <class T, class K> static int batch_grid(const tc_batch* b, K kernel, i
 }
 
 // Shared-memory opt-in and persistent grid of every ensemble kernel.
+template <class T> static BatchProjArgs<T>* batch_pargs(tc_batch* b) {
+  if constexpr (sizeof(T) == 8)
+    return b->pargs_d;
+  else
+    return b->pargs_f;
+}
 template <class T> static std::vector<BatchCnArgs<T>>* batch_cargs(tc_batch* b) {
   if constexpr (sizeof(T) == 8)
     return b->cargs_d;
@@ -2640,7 +2648,7 @@ template <class T> static int batch_shapes(tc_batch* b, int scheme) {
   else
     rc = batch_grid<T>(b, kb_rhs<T, true, UPD_FE>, rthr, 0, b->total[BK_RHS], &b->grid[BK_RHS]);
   b->grid[BK_TRI] = std::max(1, b->total[BK_TRI]);  // one CTA per unit
-  if (!rc) rc = batch_grid<T>(b, kb_proj<T>, 256, 0, b->total[BK_PROJ], &b->grid[BK_PROJ]);
+  b->grid[BK_PROJ] = std::max(1, b->total[BK_PROJ]);  // one CTA per unit
   return rc;
 }
 
@@ -2737,6 +2745,25 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
   }
   b->targs.st[n] = b->total[BK_TRI];
   b->targs.n = n;
+  for (int t = 0; t < 3; ++t) {
+    BatchProjArgs<T>& a = batch_pargs<T>(b)[t];
+    a = BatchProjArgs<T>();
+    for (int i = 0; i < n; ++i) {
+      const BMember<T>& r = tab[(size_t)t * n + i];
+      BProjRec<T>& q = a.r[i];
+      q.g = r.g;
+      for (int f = 0; f < 3; ++f) q.B[f] = r.B[f];
+      q.p = r.p;
+      q.dzf = r.dzf;
+      q.ba = r.ba;
+      q.pgx = r.pgx;
+      q.pgy = r.pgy;
+      q.pgz = r.pgz;
+      a.st[i] = r.u0[BK_PROJ];
+    }
+    a.st[n] = b->total[BK_PROJ];
+    a.n = n;
+  }
   b->cn_y = maxchunks;
   b->fy_tile = fyt;
   b->smem_fy = (size_t)4 * 2 * fyt * sizeof(cpx<double>);
@@ -2811,7 +2838,7 @@ template <class T> static int batch_step_impl(tc_batch* b, int scheme, int ti, c
     batch_poisson<T, 8>(b, M, ti, s);
   else
     batch_poisson<T, 16>(b, M, ti, s);
-  kb_proj<T><<<b->grid[BK_PROJ], dim3(32, 8), 0, s>>>(M, n, b->total[BK_PROJ]);
+  kb_proj_n<T><<<b->grid[BK_PROJ], dim3(32, 8), 0, s>>>(batch_pargs<T>(b)[ti]);
   TC_LAUNCHED();
   return TC_OK;
 }
