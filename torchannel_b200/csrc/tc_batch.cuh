@@ -64,11 +64,10 @@ template <class T> struct BMember {
   double* p;
   const double* dzf;
   BulkArgs ba;
-  int n1x, n1y, nxh, nrows;
+  int n1y, nxh, nrows;
   int rgx, rgy, rgz;       // block grid of k_rhs_update
   int tnx, tny, tnz;       // tiles of the tensor-copy RHS (k_rhs_tma's default shape)
   int cgx;                 // column blocks per component of k_cn_solve
-  int cn_lr;               // CN rows per chunk of this member (its tables' length)
   int xgx;                 // row blocks per plane of the x transforms
   int xpg;                 // plane groups of the forward x transform
   int pgx, pgy, pgz;       // block grid of k_project_bulk

@@ -2400,7 +2400,7 @@ extern "C" int tc_batch_use_graphs(tc_batch* b, int on) {
 template <class T> static constexpr int batch_cn_vec(int L) { return (L == 16 && sizeof(T) == 4) ? 2 : 1; }
 
 template <class T>
-static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int scheme, int L, int Lr) {
+static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int scheme, int L) {
   BMember<T> r;
   std::memset(&r, 0, sizeof(r));
   r.g = make_grid<T>(c);
@@ -2418,14 +2418,13 @@ static BMember<T> batch_record(tc_ctx* c, int cur, double dt, int hist, int sche
   r.tb = PoissonTabs{c->k2x, c->k2y, c->cl, c->cr};
   r.p = c->p; r.dzf = c->dzf_d;
   r.ba = BulkArgs{c->partials, c->ticket, c->scal, bulk_scale(c), c->U_bulk, dt, scheme != TC_FE};
-  r.n1x = c->nx / 16; r.n1y = c->ny / 16; r.nxh = c->nxh; r.nrows = c->nxh * c->nz;
+  r.n1y = c->ny / 16; r.nxh = c->nxh; r.nrows = c->nxh * c->nz;
   r.rgx = (c->nx + RHS_TX - 1) / RHS_TX;
   r.rgy = (c->ny + rhs_ty<T>() - 1) / rhs_ty<T>();
   r.rgz = (c->nz + 1 + rhs_kb<T>() - 1) / rhs_kb<T>();
   rhs_tma_tiles(c->nx, c->ny, c->nz, BatchRhsTmaShape<T>::KB, &r.tnx, &r.tny, &r.tnz);
   const int V = batch_cn_vec<T>(L);
   r.cgx = (c->nx * c->ny / V + 31) / 32;
-  r.cn_lr = Lr;
   r.xgx = c->ny / XROWS;
   r.xpg = (c->nz + TC_BATCH_XP - 1) / TC_BATCH_XP;
   r.pgx = (c->nx / 2 + 31) / 32; r.pgy = (c->ny + 7) / 8; r.pgz = (c->nz + PROJ_PK - 1) / PROJ_PK;
@@ -2716,9 +2715,9 @@ template <class T> static int batch_build_impl(tc_batch* b, int scheme, const do
       c->tab_dt = dts[i];
     }
     const int hist = scheme == TC_FE ? 0 : c->have_hist;
-    tab[i] = batch_record<T>(c, c->cur, dts[i], 1, scheme, L, Lr);
-    tab[n + i] = batch_record<T>(c, c->cur ^ 1, dts[i], 1, scheme, L, Lr);
-    tab[2 * n + i] = batch_record<T>(c, c->cur, dts[i], hist, scheme, L, Lr);
+    tab[i] = batch_record<T>(c, c->cur, dts[i], 1, scheme, L);
+    tab[n + i] = batch_record<T>(c, c->cur ^ 1, dts[i], 1, scheme, L);
+    tab[2 * n + i] = batch_record<T>(c, c->cur, dts[i], hist, scheme, L);
     int cnt[BK_COUNT];
     batch_units<T>(tab[i], c, b->rhs_tma != 0, cnt);
     for (int k = 0; k < BK_COUNT; ++k) {
